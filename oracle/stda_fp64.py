@@ -1,0 +1,441 @@
+"""FP64 CPU oracle of std2's sTDA / sTD-DFT path (TEST INFRASTRUCTURE ONLY).
+
+This module is the checker for the CUDA engine.  Only ``tests/``,
+``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline leg may import
+it; the engine itself never calls it.  It restates, in double precision and
+numpy, what ``SUBROUTINE stda`` (``stda.f:53-1606``) does between the AO
+integrals and ``tda.dat``, plus the sTD-DFT (``srpapack.f``) and the dynamic
+polarizability (``linear_response.f:23-192``) branches.  The reference keeps
+charges, gamma matrices and A in ``real*4``; this oracle keeps everything in
+``real*8`` so that it can serve as the FP64 yardstick.  It is pinned against
+the reference's golden files (``tests/expected_results/EXCI_TEST*.dat`` and the
+excitation energies of ``2PA_TEST*.txt``) by ``tests/test_oracle_golden.py``.
+
+Conscious deviations (also applied by the engine, so both agree bit-for-bit
+on the CSF set):
+
+* ``sort_vec`` (``sutda.f:1789``) is called on ``c`` rather than on the active
+  copy ``ca`` (``stda.f:333``); here the active MOs *and* their energies are
+  sorted together with a stable sort, which is identical for energy-ordered
+  input and consistent otherwise.
+* The primary-CSF selection sort (``stda.f:651-668``) is not stable for equal
+  diagonal energies; here ties are broken by CSF enumeration order (i, a).
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+import scipy.linalg as sla
+
+EH2EV_IN = 27.211385050      # stda.f:142 (input conversion)
+EH2EV_OUT = 27.21139         # stda.f:1455, print_tdadat
+ROT_FAC = -235.7220          # stda.f:1264
+NM_FAC = 45.56335            # linear_response.f:85
+
+# atomic chemical hardness eta (Eh), setrep (stda.f:2060-2167)
+ETA = np.array([
+    0.472592880, 0.922033910, 0.174528880, 0.257007330, 0.339490860,
+    0.421954120, 0.504381930, 0.586918630, 0.669313510, 0.751916070,
+    0.179641050, 0.221572760, 0.263485780, 0.305396450, 0.347340140,
+    0.389247250, 0.431156700, 0.473082690, 0.171054690, 0.202762440,
+    0.210073220, 0.217396470, 0.224710390, 0.232015010, 0.239339690,
+    0.246656380, 0.253982550, 0.261288630, 0.268594760, 0.275925650,
+    0.307629990, 0.339315800, 0.372359850, 0.402735490, 0.434457760,
+    0.466117080, 0.155850790, 0.186493240, 0.193562100, 0.200633110,
+    0.207705220, 0.214772540, 0.221846140, 0.228918720, 0.235986210,
+    0.243056120, 0.250130180, 0.257199370, 0.287847800, 0.318486730,
+    0.349124310, 0.379765930, 0.410408080, 0.441057770, 0.050193320,
+    0.067625700, 0.085044450, 0.102477360, 0.119911050, 0.137327720,
+    0.154762970, 0.172182650, 0.189612880, 0.207047600, 0.224467520,
+    0.241896450, 0.259325030, 0.276760940, 0.294182310, 0.311595870,
+    0.329022740, 0.345922980, 0.363880480, 0.381305860, 0.398774760,
+    0.416142980, 0.433645100, 0.451040140, 0.468489860, 0.485845500,
+    0.125267300, 0.142686770, 0.160116150, 0.177558890, 0.194975570,
+    0.212407780, 0.072635250, 0.094221580, 0.099202950, 0.104186210,
+    0.142356330, 0.163942940, 0.185519410, 0.223701390])
+
+# atomic masses (block.f:24-35) for the MMASS header; index = Z-1
+AMS = np.zeros(107)
+AMS[:56] = [1.00790, 4.00260, 6.94000, 9.01218, 10.81000, 12.01100, 14.00670,
+            15.99940, 18.99840, 20.17900, 22.98977, 24.30500, 26.98154,
+            28.08550, 30.97376, 32.06000, 35.45300, 39.94800, 39.09830,
+            40.08000, 44.95590, 47.90000, 50.94150, 51.99600, 54.93800,
+            55.84700, 58.93320, 58.71000, 63.54600, 65.38000, 69.73500,
+            72.59000, 74.92160, 78.96000, 79.90400, 83.80000, 85.46780,
+            87.62000, 88.90590, 91.22000, 92.90640, 95.94000, 98.90620,
+            101.0700, 102.9055, 106.4000, 107.8680, 112.4100, 114.8200,
+            118.6900, 121.7500, 127.6000, 126.9045, 131.3000, 132.9054,
+            137.3300]
+AMS[71:83] = [178.4900, 180.9479, 183.8500, 186.2070, 190.2000, 192.2200,
+              195.0900, 196.9665, 200.5900, 204.3700, 207.2000, 208.9804]
+AMS[101] = 1.0079
+
+
+@dataclass
+class Params:
+    """Keywords of the sTDA path (``main.f:84-131``, ``stda.f:53-54``)."""
+    ax: float = 0.5           # -ax
+    e_thr_ev: float = 7.0     # -e  (thre)
+    thrp: float = 1e-4        # -p x -> 10**-x
+    alpha_k: float = -100.0   # -al (-100: default 1.42+0.48 ax)
+    beta_j: float = -100.0    # -be (-100: default 0.20+1.83 ax)
+    fthr_ev: float = 1.7976931348623157e308   # -lpt
+    triplet: bool = False     # -t
+    rpa: bool = False         # -rpa
+    velcorr: bool = True      # default for sTDA
+    kshift: bool = False      # -xtb / -kshift
+    shftmax: float = 0.5
+    shftwidth: float = 0.1
+    shftsteep: float = 4.0
+
+
+@dataclass
+class Result:
+    no: int = 0
+    nv: int = 0
+    occ_idx: np.ndarray = None     # active occupied MO indices (0-based, sorted)
+    virt_idx: np.ndarray = None
+    eps_act: np.ndarray = None
+    nex: int = 0                  # primaries
+    nexpt: int = 0                # PT candidates
+    new: int = 0                  # PT-selected
+    iconf: np.ndarray = None      # (nci, 2) 0-based (i over active occ, a over active virt)
+    ed: np.ndarray = None         # (nci,) diagonal after PT lowering
+    pt2: np.ndarray = None
+    A: np.ndarray = None          # TDA: A ; RPA: (A+B, A-B)
+    Apb: np.ndarray = None
+    Amb: np.ndarray = None
+    omega: np.ndarray = None      # roots in Eh
+    X: np.ndarray = None          # (nci, nroot)  TDA X or X (RPA)
+    Y: np.ndarray = None
+    fL: np.ndarray = None
+    fV: np.ndarray = None
+    RL: np.ndarray = None
+    RV: np.ndarray = None
+    alpha0: np.ndarray = None     # packed xx xy yy xz yz zz  (stda.f:1247-1252, x2)
+    mu_ia: dict = field(default_factory=dict)
+    xmolw: float = 0.0
+    extras: dict = field(default_factory=dict)
+
+
+class OracleError(RuntimeError):
+    pass
+
+
+# ---------------------------------------------------------------- helpers ---
+
+def gamma_matrices(xyz4: np.ndarray, ax: float, alpha_k: float, beta_j: float):
+    """gamma^J and gamma^K, Mataga-Nishimoto-Ohno-Klopman form (stda.f:509-532)."""
+    Z = np.rint(xyz4[3]).astype(int)
+    eta = ETA[Z - 1]
+    xyz = xyz4[:3].T
+    r = np.sqrt(np.sum((xyz[:, None, :] - xyz[None, :, :]) ** 2, axis=-1))
+    etab = 0.5 * (eta[:, None] + eta[None, :])
+    xj = etab * ax
+    xk = etab
+    with np.errstate(divide="ignore"):
+        inv_xj = np.where(xj > 0, 1.0 / np.where(xj > 0, xj, 1.0) ** beta_j, np.inf)
+    gj = 1.0 / (r ** beta_j + inv_xj) ** (1.0 / beta_j)
+    gk = 1.0 / (r ** alpha_k + 1.0 / xk ** alpha_k) ** (1.0 / alpha_k)
+    return gj, gk
+
+
+def default_alpha_beta(p: Params):
+    """stda.f:490-500."""
+    beta = p.beta_j if p.beta_j >= -99.0 else 0.20 + 1.830 * p.ax
+    alpha = p.alpha_k if p.alpha_k >= -99.0 else 1.420 + 0.480 * p.ax
+    return alpha, beta
+
+
+def select_window(eps, occ, ax, thr_eh):
+    """Orbital window (stda.f:145-192): returns active occ / virt MO indices."""
+    deps = 2.0 * (1.0 + 0.8 * ax) * thr_eh
+    occm = occ > 1.990
+    virm = occ < 0.010
+    omax = eps[occm].max() if occm.any() else -1e42
+    vmin = eps[virm].min() if virm.any() else 1e42
+    othr = vmin - deps
+    vthr = deps + omax
+    oidx = np.nonzero(occm & (eps > othr))[0]
+    vidx = np.nonzero(virm & (eps < vthr))[0]
+    return oidx, vidx
+
+
+def lowdin_orthogonal_mos(S, Cact):
+    """makel (stda.f:1615-1691) + C_low = S^1/2 C (stda.f:436-452)."""
+    e, U = np.linalg.eigh(S)
+    if (e < 0).any():
+        raise OracleError("S^1/2: negative overlap eigenvalue")
+    X = (U * np.sqrt(e)) @ U.T
+    Clow = X @ Cact
+    nrm = np.sum(Clow ** 2, axis=0)
+    if (np.abs(nrm - 1.0) > 1e-2).any():
+        raise OracleError("internal MO norm error")
+    return Clow
+
+
+def charges(Clow, iaoat, ncent, p_idx, q_idx):
+    """lo12pop (stda.f:1727-1744) for MO pairs (p_idx[k], q_idx[k]) -> (ncent, npairs)."""
+    prod = Clow[:, p_idx] * Clow[:, q_idx]
+    out = np.zeros((ncent, prod.shape[1]))
+    np.add.at(out, iaoat, prod)
+    return out
+
+
+def mo_ov(mat_ao, C_occ, C_virt):
+    """ONETRI (onetri.f:20-55) restricted to the occ-virt block: C_i^T B C_a."""
+    return C_occ.T @ mat_ao @ C_virt
+
+
+# ------------------------------------------------------------- pipeline ---
+
+def stda(xyz4, C, eps, occ, iaoat, S, Lao, Vao, Mao, p: Params, want_A=True):
+    """Run the sTDA / sTD-DFT excitation path in FP64.
+
+    Inputs follow the boundary: ``xyz4`` (4, ncent) Bohr + Z, ``C`` (nao, nmo),
+    ``eps``/``occ`` (nmo), ``iaoat`` (nao) 0-based, dense AO matrices ``S``
+    (nao, nao) and ``Lao``/``Vao``/``Mao`` (3, nao, nao) with the conventions
+    of :mod:`stda_b200.integrals`.
+    """
+    res = Result()
+    ncent = xyz4.shape[1]
+    thr = p.e_thr_ev / EH2EV_IN
+    fthr = p.fthr_ev / EH2EV_IN if p.fthr_ev < 1.79e308 else np.inf
+    Z = np.rint(xyz4[3]).astype(int)
+    res.xmolw = float(np.sum(AMS[Z - 1]))
+
+    oidx, vidx = select_window(eps, occ, p.ax, thr)
+    no, nv = len(oidx), len(vidx)
+    if no == 0 or nv == 0:
+        raise OracleError("no CSF, increase energy threshold (-e option)")
+    # sort_vec (stda.f:333), stable, applied to active copies
+    oo = oidx[np.argsort(eps[oidx], kind="stable")]
+    vv = vidx[np.argsort(eps[vidx], kind="stable")]
+    res.no, res.nv, res.occ_idx, res.virt_idx = no, nv, oo, vv
+    epsi = np.concatenate([eps[oo], eps[vv]])
+    res.eps_act = epsi
+    Cact = C[:, np.concatenate([oo, vv])]
+    Co, Cv = Cact[:, :no], Cact[:, no:]
+
+    # property integrals, occ-virt block (stda.f:351-412)
+    mu = {}
+    for name, mat in (("L", Lao), ("V", Vao), ("M", Mao)):
+        mu[name] = np.stack([mo_ov(mat[d], Co, Cv) for d in range(3)])  # (3,no,nv)
+    res.mu_ia = mu
+
+    Clow = lowdin_orthogonal_mos(S, Cact)
+    ak = 0.0 if p.triplet else 2.0
+    alpha_k, beta_j = default_alpha_beta(p)
+    gj, gk = gamma_matrices(xyz4, p.ax, alpha_k, beta_j)
+
+    io_all, ia_all = np.meshgrid(np.arange(no), np.arange(nv), indexing="ij")
+    io_all, ia_all = io_all.ravel(), ia_all.ravel()          # k = i*nv + a
+    qii = charges(Clow, iaoat, ncent, np.arange(no), np.arange(no))
+    qaa = charges(Clow, iaoat, ncent, no + np.arange(nv), no + np.arange(nv))
+    uci = qaa.T @ (gj @ qii)                                  # (nv, no): (ii|aa)
+    qia = charges(Clow, iaoat, ncent, io_all, no + ia_all)    # (N, no*nv)
+    pia = gk @ qia
+    ek_all = np.einsum("Ak,Ak->k", pia, qia)                  # (ia|ia)
+    de_all = (epsi[no + ia_all] - epsi[io_all]) - uci[ia_all, io_all] + ak * ek_all
+    if p.kshift:
+        sau = p.shftmax * 0.036749320
+        wau = p.shftwidth * 0.036749320
+        de_all = de_all + sau / (1.0 + (ek_all / wau) ** p.shftsteep)
+    prim = de_all <= thr
+    cand = (de_all > thr) & (de_all < fthr)
+    pk = np.nonzero(prim)[0]
+    ck = np.nonzero(cand)[0]
+    res.nex, res.nexpt = len(pk), len(ck)
+    if len(pk) < 1:
+        raise OracleError("no CSF, increase energy threshold (-e option)")
+    # energy sort of primaries, ties by enumeration order (stda.f:651-668)
+    pk = pk[np.argsort(de_all[pk], kind="stable")]
+    ed = de_all[pk].copy()
+
+    # J-type charges for all occ pairs and virt pairs (stda.f:728-763)
+    ii, jj = np.meshgrid(np.arange(no), np.arange(no), indexing="ij")
+    qoo = charges(Clow, iaoat, ncent, ii.ravel(), jj.ravel()).reshape(ncent, no, no)
+    aa, bb = np.meshgrid(np.arange(nv), np.arange(nv), indexing="ij")
+    qvv = charges(Clow, iaoat, ncent, no + aa.ravel(), no + bb.ravel()).reshape(ncent, nv, nv)
+    poo = np.einsum("AB,Bij->Aij", gj, qoo)
+
+    def coupling(krow, kcol):
+        """ak*(ia|jb) - (ij|ab) for CSF index arrays (ravelled i*nv+a)."""
+        i1, a1 = io_all[krow], ia_all[krow]
+        i2, a2 = io_all[kcol], ia_all[kcol]
+        K = pia[:, krow].T @ qia[:, kcol]
+        # (ij|ab): gather over the occ/virt boxes actually touched
+        ou1, oinv1 = np.unique(i1, return_inverse=True)
+        ou2, oinv2 = np.unique(i2, return_inverse=True)
+        vu1, vinv1 = np.unique(a1, return_inverse=True)
+        vu2, vinv2 = np.unique(a2, return_inverse=True)
+        P = poo[:, ou1][:, :, ou2].reshape(ncent, -1)          # (N, o1*o2)
+        Q = qvv[:, vu1][:, :, vu2].reshape(ncent, -1)          # (N, v1*v2)
+        J4 = (P.T @ Q).reshape(len(ou1), len(ou2), len(vu1), len(vu2))
+        J = J4[oinv1[:, None], oinv2[None, :], vinv1[:, None], vinv2[None, :]]
+        return ak * K - J
+
+    # PT selection (stda.f:1773-1863)
+    pt2 = np.zeros(len(pk))
+    incl = np.zeros(len(ck), dtype=bool)
+    blk = max(1, int(4e6 // max(1, len(pk))))
+    for s0 in range(0, len(ck), blk):
+        kk = ck[s0:s0 + blk]
+        amat = coupling(kk, pk)                                  # (nk, nex)
+        pt = amat ** 2 / (de_all[kk][:, None] - ed[None, :] + 1e-10)
+        pert = pt.sum(axis=1)
+        sel = pert > p.thrp
+        incl[s0:s0 + blk] = sel
+        pt2 += pt[~sel].sum(axis=0)
+    newk = ck[incl]
+    res.new = len(newk)
+    res.pt2 = pt2
+    ed = np.concatenate([ed - pt2, de_all[newk]])
+    allk = np.concatenate([pk, newk])
+    nci = len(allk)
+    res.iconf = np.stack([io_all[allk], ia_all[allk]], axis=1)
+    res.ed = ed
+    res.extras.update(de_all=de_all, ek_all=ek_all, pk=pk, ck=ck, allk=allk)
+
+    mL = mu["L"][:, io_all[allk], ia_all[allk]]              # (3, nci)
+    mV = mu["V"][:, io_all[allk], ia_all[allk]]
+    mM = mu["M"][:, io_all[allk], ia_all[allk]]
+
+    if not want_A:
+        return res
+
+    # A matrix (rtdamat stda.f:2010-2056)
+    A = coupling(allk, allk)
+    np.fill_diagonal(A, ed)
+
+    if p.rpa:
+        # exchange-type (ib|ja) with gamma^K (rrpamat stda.f:1930-1963)
+        i1, a1 = io_all[allk], ia_all[allk]
+        kib = i1[:, None] * nv + a1[None, :]      # (ib): occ of row, virt of col
+        kja = i1[None, :] * nv + a1[:, None]      # (ja): occ of col, virt of row
+        Kx = np.einsum("Auv,Auv->uv", pia[:, kib], qia[:, kja])
+        Kd = ek_all[allk]
+        Kov = pia[:, allk].T @ qia[:, allk]
+        Apb = 2.0 * ak * Kov - p.ax * Kx - (ak * Kov - A)       # 2ak(ia|jb) - ax(ib|ja) - (ij|ab)
+        Amb = p.ax * Kx - (ak * Kov - A)                         # ax(ib|ja) - (ij|ab)
+        np.fill_diagonal(Apb, ed - p.ax * Kd + ak * Kd)
+        np.fill_diagonal(Amb, ed - ak * Kd + p.ax * Kd)
+        if abs(p.ax) < 1e-6:
+            Amb = np.diag(ed - ak * Kd)
+        res.Apb, res.Amb = Apb, Amb
+        # srpapack (srpapack.f:32-197): M = (A-B)^1/2 (A+B) (A-B)^1/2
+        e, U = np.linalg.eigh(Amb)
+        if e[0] < 0:
+            raise OracleError("matrix power impossible")
+        Ambh = (U * np.sqrt(e)) @ U.T
+        Mmat = Ambh @ Apb @ Ambh
+        w, Zv = sla.eigh(Mmat, subset_by_value=(0.0, thr * thr))
+        if len(w) < 1:
+            raise OracleError("RPA diag failed")
+        om = np.sqrt(w)
+        XpY = (Ambh @ Zv) / np.sqrt(om)
+        XmY = (Apb @ XpY) / om
+        X = 0.5 * (XpY + XmY)
+        Y = XpY - X
+        res.omega, res.X, res.Y = om, X, Y
+        uu, pp = XpY, XmY
+    else:
+        res.A = A
+        w, Xv = sla.eigh(A, subset_by_value=(0.0, thr))
+        if len(w) < 1:
+            raise OracleError("internal error in diag")
+        res.omega, res.X = w, Xv
+        uu = pp = Xv
+
+    # properties (stda.f:1207-1289)
+    sak = math.sqrt(ak)
+    om = res.omega
+    ef = 1.0 / (om + 1e-8)
+    tl = sak * (mL @ uu)          # (3, nroot)
+    tv = sak * (mV @ pp)
+    tm = sak * (mM @ pp)
+    res.fL = om * (2.0 / 3.0) * np.sum(tl * tl, axis=0)
+    res.fV = ef * (2.0 / 3.0) * np.sum(tv * tv, axis=0)
+    res.RL = ROT_FAC * np.sum(tl * tm, axis=0)
+    res.RV = ROT_FAC * np.sum(tv * tm, axis=0) * ef
+    a = np.array([np.sum(tl[0] * tl[0] * ef), np.sum(tl[0] * tl[1] * ef), np.sum(tl[1] * tl[1] * ef),
+                  np.sum(tl[0] * tl[2] * ef), np.sum(tl[1] * tl[2] * ef), np.sum(tl[2] * tl[2] * ef)])
+    res.alpha0 = 2.0 * a
+
+    if (not p.rpa) and p.velcorr:
+        # rtdacorr (apbtrafo.f:580-643) + apbtrafo (apbtrafo.f:23-300)
+        i1, a1 = io_all[allk], ia_all[allk]
+        kib = i1[:, None] * nv + a1[None, :]
+        kja = i1[None, :] * nv + a1[:, None]
+        Kx = np.einsum("Auv,Auv->uv", pia[:, kib], qia[:, kja])
+        Kov = pia[:, allk].T @ qia[:, allk]
+        Bh = 0.5 * ak * Kov - 0.5 * p.ax * Kx
+        np.fill_diagonal(Bh, 0.5 * (ak * np.diag(Kov) - p.ax * np.diag(Kov)))
+        Xn = (Bh @ res.X) * ef[None, :]
+        xl = mL @ res.X
+        xv = mV @ res.X
+        xm = mM @ res.X
+        xv2 = mV @ Xn
+        xm2 = mM @ Xn
+        hilf = 1.0 - np.exp(-150.0 * om * om)
+        efmod = 1.0 / (om ** hilf + 1e-8)
+        p23 = ak * 2.0 / 3.0
+        res.fL = np.sum(xl * xl, axis=0) * p23 * om
+        res.fV = p23 * ef * np.sum(xv * xv, axis=0)
+        res.RL = ROT_FAC * np.sum(xl * xm, axis=0) * ak
+        res.RV = ROT_FAC * np.sum(xv * xm + xv2 * xm + xv * xm2, axis=0) * ak * efmod
+        res.extras["Bhalf"] = Bh
+    return res
+
+
+def tda_dat_text(res: Result, p: Params) -> str:
+    """tda.dat as written by apbtrafo (velocity-corrected sTDA, apbtrafo.f:100-243)
+    or print_tdadat (stda.f:2235-2265) otherwise."""
+    velo = (not p.rpa) and p.velcorr
+    thr = p.e_thr_ev / EH2EV_IN
+    lines = [" NM", " VELO" if velo else " UV", " MMASS", f"   {res.xmolw:.15f}     ",
+             " LFAKTOR", "  0.5", " RFAKTOR", "  1.0", " WIDTH", "  0.20", " SHIFT", "  0.00", " DATXY"]
+    for i, om in enumerate(res.omega):
+        if (not velo) and om > thr:
+            continue
+        lines.append("%4d%10.4f%13.6f%13.6f%13.6f%13.6f" % (
+            i + 1, om * EH2EV_OUT, res.fL[i], res.fV[i], res.RL[i], res.RV[i]))
+    return "\n".join(lines) + "\n"
+
+
+def dynamic_polarizability(res: Result, omegas_eh) -> np.ndarray:
+    """lresp (linear_response.f:23-192): alpha(omega) for each omega (Eh).
+
+    Solves [(A+B) - w^2 (A-B)^-1] (X+Y) = -2 mu for the three Cartesian
+    right-hand sides and returns alpha[w, x, y] = -2 sum mu_x (X+Y)_y.
+    Requires a result computed with ``Params(rpa=True)``.
+    """
+    if res.Apb is None:
+        raise OracleError("dynamic polarizability needs the A+B / A-B matrices (rpa=True)")
+    nv = res.nv
+    allk = res.extras["allk"]
+    i1, a1 = allk // nv, allk % nv
+    mL = res.mu_ia["L"][:, i1, a1]                    # (3, nci)
+    rhs = -2.0 * mL.T
+    inv_amb = np.linalg.inv(res.Amb)
+    out = []
+    for w in omegas_eh:
+        Mw = res.Apb - (w * w) * inv_amb
+        XpY = np.linalg.solve(Mw, rhs)
+        out.append(-2.0 * mL @ XpY)
+    return np.array(out)
+
+
+def read_tda_dat(text: str):
+    """Parse the DATXY rows of a tda.dat text into an (n, 6) array."""
+    rows = []
+    on = False
+    for ln in text.splitlines():
+        if "DATXY" in ln:
+            on = True
+            continue
+        if on and ln.strip():
+            rows.append([float(t) for t in ln.split()])
+    return np.array(rows)

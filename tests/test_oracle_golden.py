@@ -1,0 +1,72 @@
+"""The FP64 oracle against the reference's own regression goldens.
+
+Cases and tolerances are those of the reference test driver
+(``tests/run_tests.sh``, ``tests/compare.py:163-215``): excitation energies
+(eV, 4 decimals) and f_L within 1e-3; for the 2PA cases only the sTD-DFT
+excitation energies are compared (the 2PA cross sections are out of scope).
+Unlike ``compare.py`` the number of roots is checked exactly.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from oracle.stda_fp64 import Params, read_tda_dat, stda, tda_dat_text
+from tests.conftest import GOLDEN
+
+EXPECTED = json.load(open(os.path.join(GOLDEN, "reference_expected.json")))
+
+
+def run(water, **kw):
+    mol, (S, L, V, M) = water
+    p = Params(**kw)
+    return p, stda(mol.xyz4(), mol.C, mol.eps, mol.occ, mol.iaoat(), S, L, V, M, p)
+
+
+@pytest.mark.parametrize("name", ["EXCI_TEST1", "EXCI_TEST2", "EXCI_TEST3"])
+def test_exci_golden(water, name):
+    case = EXPECTED[name]
+    p, res = run(water, **case["args"])
+    text = tda_dat_text(res, p)
+    got = read_tda_dat(text)
+    exp = np.array(case["rows"])
+    assert got.shape == exp.shape, (got.shape, exp.shape)
+    assert np.all(np.abs(got[:, 1] - exp[:, 1]) <= 1e-3)      # eV
+    assert np.all(np.abs(got[:, 2] - exp[:, 2]) <= 1e-3)      # f_L
+    assert np.all(np.abs(got[:, 3] - exp[:, 3]) <= 1e-3)      # f_V (not compared upstream)
+    # the header of the velocity-corrected tda.dat, including MMASS
+    hdr = [ln.strip() for ln in text.splitlines()[:13]]
+    assert hdr == case["header"]
+
+
+@pytest.mark.parametrize("name", ["2PA_TEST1", "2PA_TEST2", "2PA_TEST3"])
+def test_std_dft_energies_golden(water, name):
+    case = EXPECTED[name]
+    p, res = run(water, rpa=True, **case["args"])
+    exp = np.array(case["rows"])
+    ev = res.omega * 27.21139
+    assert len(ev) >= len(exp)
+    assert np.all(np.abs(ev[:len(exp)] - exp[:, 1]) <= 1e-3)
+
+
+def test_oracle_csf_counts(water):
+    # EXCI_TEST1: 4 primaries, 4 PT candidates all selected (small system)
+    p, res = run(water, ax=1.0, e_thr_ev=20.0)
+    assert (res.nex, res.nexpt, res.new) == (4, 4, 4)
+    assert res.iconf.shape == (8, 2)
+
+
+def test_oracle_polarizability_static_limit(water):
+    """alpha(0) from the response solve equals the sum over all sTD-DFT states."""
+    from oracle.stda_fp64 import dynamic_polarizability
+    p, res = run(water, rpa=True, ax=0.5, e_thr_ev=1e4)     # all roots
+    a0 = dynamic_polarizability(res, [0.0])[0]
+    assert np.allclose(a0, a0.T, atol=1e-10)
+    # sum over states: alpha_xy = 2 sum_n mu_x mu_y / w with mu = sqrt(2) mu_ia (X+Y)
+    nv = res.nv
+    k = res.extras["allk"]
+    mL = res.mu_ia["L"][:, k // nv, k % nv]
+    t = np.sqrt(2.0) * (mL @ (res.X + res.Y))
+    sos = 2.0 * (t / res.omega) @ t.T
+    assert np.allclose(a0, sos, rtol=1e-8, atol=1e-10)
