@@ -1,0 +1,166 @@
+/*
+ * std2g -- B200 (sm_100a) engine for the sTDA / sTD-DFT excited-state path of
+ * std2.  Plain C ABI: plain pointers and sizes, integer status codes, no
+ * C++ or framework types, so that the Fortran host can bind it with
+ * iso_c_binding and any other host through its FFI.
+ *
+ * The boundary replaces one Fortran call of the reference,
+ *
+ *   call stda(ncent,nmo,nao,xyz,cc,eps,occ,iaoat,thre,thrp,ax,alpha,beta,
+ *             ptlim,nvec,nprims)                      (main.f:928-929)
+ *   SUBROUTINE stda(...)                              (stda.f:53-54)
+ *
+ * together with the scratch files the reference passes between its phases
+ * (AO integrals sint/x?lint/x?vint/x?mint written at main.f:756-797 and read at
+ * stda.f:351-425; amb/apbmat/bmat, stda.f:1926-1995 and apbtrafo.f:603).  The
+ * split into create / load / solve keeps inputs resident on the device so that
+ * several solves (sTDA, sTD-DFT, alpha(omega)) reuse them.
+ *
+ * All arrays are caller-owned and follow the Fortran layout of the reference:
+ * column-major matrices, packed lower triangles enumerated row by row
+ * (k = i*(i-1)/2 + j for i >= j, 1-based as in lin(), stda.f:2174-2181).
+ *
+ * Error convention: every entry point returns 0 on success and a positive
+ * STD2G_E* code otherwise; it never calls exit() or stop.  The reference's
+ * equivalents are Fortran `stop` statements (e.g. stda.f:316-318, 644, 1150,
+ * 1658-1670; srpapack.f:92,229).
+ *
+ * Threading: one context is used by one host thread at a time.  Separate
+ * contexts may share a device; each owns a CUDA stream.
+ */
+#ifndef STD2G_H
+#define STD2G_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+enum {
+  STD2G_OK = 0,
+  STD2G_EINVAL = 1,        /* bad argument (null pointer, size <= 0, bad index) */
+  STD2G_ECUDA = 2,         /* CUDA runtime / driver error */
+  STD2G_ENOMEM = 3,        /* device allocation failed or budget exceeded */
+  STD2G_ENOCSF = 4,        /* 'no CSF, increase energy threshold' (stda.f:316-318,644) */
+  STD2G_ES_NOT_PD = 5,     /* negative overlap eigenvalue in S^1/2 (stda.f:1658-1670) */
+  STD2G_EMONORM = 6,       /* 'internal MO norm error' (stda.f:448-451) */
+  STD2G_ENOROOT = 7,       /* no root below E_thr ('internal error in diag', stda.f:1150) */
+  STD2G_ENOCONV = 8,       /* Davidson / iterative solve did not converge */
+  STD2G_EAMB_NOT_PD = 9,   /* A-B not positive definite ('matrix power impossible', srpapack.f:229) */
+  STD2G_ESTATE = 10,       /* call order (solve before load, response before sTD-DFT) */
+  STD2G_ECAP = 11,         /* caller buffer too small */
+  STD2G_ENODEV = 12,       /* no CUDA device / not an sm_100 device */
+  STD2G_ETIMEOUT = 13      /* a bounded device-side wait ran out */
+};
+
+/* ---- engine options (per context) -------------------------------------- */
+typedef struct {
+  int device;            /* CUDA device ordinal */
+  int precision;         /* 0: FP64 form (all contractions FP64)
+                            1: mixed form (BF16-split tensor-core contractions,
+                               FP32 A storage, FP64 screen / Rayleigh-Ritz) */
+  int verbose;           /* 0 silent; 1 per-phase timings to stderr */
+  int reserved;
+  int64_t max_device_bytes; /* 0 = no limit */
+} std2g_opts;
+
+/* ---- keywords of the sTDA path (main.f:84-131, stda.f:53-54) ------------ */
+typedef struct {
+  double ax;         /* -ax  Fock exchange mixing */
+  double e_thr_ev;   /* -e   energy threshold / spectral range (eV) */
+  double thrp;       /* -p   PT selection threshold (already 10**-x) */
+  double alpha_k;    /* -al  (-100: default 1.42+0.48 ax, stda.f:497-500) */
+  double beta_j;     /* -be  (-100: default 0.20+1.83 ax, stda.f:494-496) */
+  double fthr_ev;    /* -lpt PT limit (eV); >= 1.79e308 means off */
+  int triplet;       /* -t   */
+  int rpa;           /* -rpa sTD-DFT (A+B, A-B) instead of TDA */
+  int velcorr;       /* velocity correction of R_V (default on for sTDA) */
+  int kshift;        /* K(ia,ia)-dependent diagonal shift (-xtb / -kshift) */
+  double shftmax, shftwidth, shftsteep;   /* kshiftcommon, eV */
+  int nroots;        /* 0: every root in (0, E_thr] as ssyevr's window does;
+                        k > 0: the lowest k roots (Davidson) */
+  int solver;        /* 0 auto, 1 dense diagonalisation, 2 blocked Davidson */
+  double conv_tol;   /* Davidson residual norm tolerance (0: 1e-6) */
+} std2g_params;
+
+/* ---- results of one solve ---------------------------------------------- */
+typedef struct {
+  int cap;           /* capacity of the per-root arrays below (in) */
+  int nroot;         /* roots returned (out) */
+  int no, nv;        /* active occupied / virtual MOs */
+  int nex;           /* primary CSFs (diagonal <= E_thr) */
+  int nexpt;         /* CSFs considered in PT */
+  int new_pt;        /* CSFs added by PT selection */
+  int nci;           /* total CSFs */
+  double *omega;     /* [cap] excitation energies (Eh) */
+  double *fL, *fV;   /* [cap] oscillator strengths, length / velocity */
+  double *RL, *RV;   /* [cap] rotatory strengths (R_V velocity-corrected for sTDA) */
+  double *resid;     /* [cap] residual norm ||A x - w x|| per root (may be NULL) */
+  double alpha0[6];  /* alpha(0) sum over states, xx xy yy xz yz zz (stda.f:1247-1252) */
+  uint64_t csf_hash; /* FNV-1a hash of the selected CSF list (i,a) in order */
+  double ms_total;   /* device time of the solve (ms) */
+} std2g_result;
+
+/* Create a context on opts->device.  Replaces the allocation part of stda.f
+   (stda.f:195-206); no reference counterpart otherwise. */
+int std2g_create(void **ctx, const std2g_opts *opts);
+
+/* Copy one wavefunction and its AO integrals to the device.
+   Arguments mirror stda(ncent,nmo,nao,xyz,c,eps,occ,iaoat,...) (stda.f:53-66):
+     xyz    [4*ncent]        x,y,z (Bohr) and nuclear charge per atom (xyz(4,ncent))
+     C      [nao*nmo]        MO coefficients, column-major (c(nao*nmo))
+     eps    [nmo], occ [nmo] orbital energies (Eh) and occupations
+     iaoat  [nao]            AO -> atom, 1-based
+   plus the AO integrals the reference reads from scratch files
+   (stda.f:351-425), packed lower triangles of nao*(nao+1)/2 each:
+     S        overlap (sint)
+     mu_L     [3*npk] dipole length  -<a|r|b>   (xlint, ylint, zlint)
+     mu_V     [3*npk] velocity       -<a|d|b>, element (a>=b) (xvint ...)
+     mu_M     [3*npk] angular mom.  <a|r x d|b>, element (a>=b) (xmint ...) */
+int std2g_load(void *ctx, int ncent, int nmo, int nao,
+               const double *xyz, const double *C, const double *eps,
+               const double *occ, const int *iaoat, const double *S,
+               const double *mu_L, const double *mu_V, const double *mu_M);
+
+/* Run the excitation path: orbital window, S^1/2, Loewdin charges, gamma,
+   diagonal screen, PT selection, A (or A+B / A-B), eigen-solve, properties and
+   (sTDA) the velocity correction.  Replaces stda.f:142-1471 for the RKS
+   singlet/triplet sTDA branch and the sTD-DFT branch (srpapack.f:32-197). */
+int std2g_solve(void *ctx, const std2g_params *par, std2g_result *res);
+
+/* Dynamic polarizability alpha(omega) from the A+B / A-B matrices of the last
+   sTD-DFT build (params.rpa=1 path of std2g_solve, or built here if needed).
+   Replaces lresp (linear_response.f:23-192).  omega in Eh (the reference reads
+   wavelengths and converts with 45.56335/lambda, linear_response.f:85).
+   alpha: [nomega*9] row-major 3x3 tensors.  resid: [nomega] max relative
+   residual of the solves (may be NULL). */
+int std2g_polarizability(void *ctx, const std2g_params *par, const double *omega,
+                         int nomega, double *alpha, double *resid);
+
+/* Selected CSF list of the last solve: iconf [2*cap] as (i,a) pairs, 1-based
+   MO indices within the active window (occupied 1..no, virtual no+1..no+nv,
+   as iconf(:,1:2) in stda.f), and the diagonal ed [cap] after PT lowering. */
+int std2g_get_csf(void *ctx, int *iconf, double *ed, int cap, int *nci);
+
+/* Eigenvectors of the last solve: X [nci*cap] column-major (TDA X, or sTD-DFT
+   X with Y in the second array when non-NULL). */
+int std2g_get_vectors(void *ctx, double *X, double *Y, int cap, int *nroot, int *nci);
+
+/* Per-phase device timings of the last solve in ms (names via
+   std2g_phase_name); returns the number of phases. */
+int std2g_phase_times(void *ctx, double *ms, int cap);
+const char *std2g_phase_name(int phase);
+
+/* Number of kernels this library launched since the context was created. */
+int64_t std2g_kernel_launches(void *ctx);
+
+const char *std2g_error_string(int status);
+void std2g_destroy(void *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* STD2G_H */

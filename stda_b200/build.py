@@ -1,0 +1,45 @@
+"""Build ``libstd2g.so`` in-tree with nvcc for sm_100a (no JIT, no torch)."""
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+OUT = os.path.join(HERE, "libstd2g.so")
+SOURCES = ["engine.cu"]
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
+         "-Xcompiler", "-fPIC", "-shared", "-Xptxas", "-v"]
+LIBS = ["-lcublas", "-lcusolver"]
+
+
+def _stale():
+    if not os.path.exists(OUT):
+        return True
+    t = os.path.getmtime(OUT)
+    deps = [os.path.join(CSRC, f) for f in os.listdir(CSRC)]
+    deps.append(os.path.join(HERE, "..", "include", "std2g.h"))
+    return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
+
+
+def build(force: bool = False, verbose: bool = False) -> str:
+    if not force and not _stale():
+        return OUT
+    cmd = [NVCC, *FLAGS, *[os.path.join(CSRC, s) for s in SOURCES], "-o", OUT + ".tmp", *LIBS]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    log = os.path.join(CSRC, "ptxas.log")
+    with open(log, "w") as fh:
+        fh.write(r.stdout + r.stderr)
+    if r.returncode != 0:
+        sys.stderr.write(r.stderr[-4000:])
+        raise RuntimeError("nvcc failed building libstd2g.so")
+    os.replace(OUT + ".tmp", OUT)
+    if verbose:
+        print(r.stderr[-2000:])
+    return OUT
+
+
+if __name__ == "__main__":
+    print(build(force="--force" in sys.argv, verbose=True))

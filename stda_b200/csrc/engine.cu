@@ -1,0 +1,939 @@
+// std2g engine: context, inputs, and the sTDA / sTD-DFT solve.
+//
+// The solve follows SUBROUTINE stda (stda.f:53-1606) phase by phase; each
+// phase runs on the context's stream.  Dense FP64 contractions that are plain
+// library GEMMs (AO->MO transforms, gamma*Q) go to cuBLAS; the symmetric
+// eigen-decompositions of S and of the small dense CI matrices go to cuSOLVER;
+// the charge formation, the screen, the PT selection and the A build use the
+// kernels of this library (kernels_fp64.cuh, tc_gemm.cuh).
+#include <algorithm>
+#include <functional>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+#include <vector>
+
+#include <cub/cub.cuh>
+
+#include "common.cuh"
+#include "kernels_fp64.cuh"
+#include "mixed.cuh"
+
+namespace std2g {
+
+int64_t g_launches = 0;
+
+static const double kEta[94] = {
+    0.472592880, 0.922033910, 0.174528880, 0.257007330, 0.339490860, 0.421954120, 0.504381930,
+    0.586918630, 0.669313510, 0.751916070, 0.179641050, 0.221572760, 0.263485780, 0.305396450,
+    0.347340140, 0.389247250, 0.431156700, 0.473082690, 0.171054690, 0.202762440, 0.210073220,
+    0.217396470, 0.224710390, 0.232015010, 0.239339690, 0.246656380, 0.253982550, 0.261288630,
+    0.268594760, 0.275925650, 0.307629990, 0.339315800, 0.372359850, 0.402735490, 0.434457760,
+    0.466117080, 0.155850790, 0.186493240, 0.193562100, 0.200633110, 0.207705220, 0.214772540,
+    0.221846140, 0.228918720, 0.235986210, 0.243056120, 0.250130180, 0.257199370, 0.287847800,
+    0.318486730, 0.349124310, 0.379765930, 0.410408080, 0.441057770, 0.050193320, 0.067625700,
+    0.085044450, 0.102477360, 0.119911050, 0.137327720, 0.154762970, 0.172182650, 0.189612880,
+    0.207047600, 0.224467520, 0.241896450, 0.259325030, 0.276760940, 0.294182310, 0.311595870,
+    0.329022740, 0.345922980, 0.363880480, 0.381305860, 0.398774760, 0.416142980, 0.433645100,
+    0.451040140, 0.468489860, 0.485845500, 0.125267300, 0.142686770, 0.160116150, 0.177558890,
+    0.194975570, 0.212407780, 0.072635250, 0.094221580, 0.099202950, 0.104186210, 0.142356330,
+    0.163942940, 0.185519410, 0.223701390};   // setrep, stda.f:2060-2167
+
+enum Phase {
+  PH_SETUP = 0, PH_SQRTS, PH_MOINT, PH_CHARGES, PH_SCREEN, PH_PT, PH_BUILD, PH_EIGEN, PH_PROPS,
+  PH_RESPONSE, PH_COUNT
+};
+static const char *kPhaseNames[PH_COUNT] = {"setup", "sqrt_S", "mo_integrals", "charges",
+                                            "screen", "pt_select", "build", "eigen",
+                                            "properties", "response"};
+
+struct Ctx {
+  std2g_opts opts{};
+  cudaStream_t stream = nullptr;
+  cublasHandle_t blas = nullptr;
+  cusolverDnHandle_t solver = nullptr;
+  bool loaded = false;
+  int ncent = 0, nmo = 0, nao = 0;
+  std::vector<double> h_eps, h_occ, h_xyz;
+  // device inputs
+  DBuf<double> d_xyz, d_C, d_eps_act, d_eta, d_Sfull, d_sqrtS, d_ao9;
+  DBuf<int> d_ao_ptr, d_ao_list, d_iaoat;
+  bool sqrtS_ready = false;
+  // work buffers
+  DBuf<double> w_Cact, w_Clow, w_T, w_mu_ov, w_gj, w_gk, w_Qii, w_Qaa, w_Pii, w_uci;
+  DBuf<double> w_Qia, w_Pia, w_Qoo, w_Poo, w_Qvv, w_de, w_ek;
+  DBuf<int> w_flag, w_act_idx, w_pk, w_ck, w_tmpi, w_pj, w_pb, w_omap, w_vmap, w_OP, w_VP, w_ci,
+      w_ca, w_allk, w_status;
+  DBuf<double> w_ed, w_edsorted, w_Qp, w_QvvP, w_W, w_Pc, w_Kbuf, w_Jbuf, w_pert, w_colpart,
+      w_pt2, w_edp;
+  DBuf<unsigned char> w_sel;
+  DBuf<double> w_Qs, w_Ps, w_K, w_J, w_Kx, w_A, w_Apb, w_Amb, w_Bh, w_Ambh, w_M, w_eval, w_X,
+      w_Y, w_tmp, w_musel, w_TL, w_TVM, w_T2, w_props, w_work;
+  DBuf<float> m_A;   // mixed-form FP32 A storage
+  DBuf<int> w_info;
+  DBuf<char> w_cub;
+  MixedWork mixed;
+  // last results
+  int last_nci = 0, last_nroot = 0, last_no = 0, last_nv = 0;
+  bool last_rpa = false;
+  double ph_ms[PH_COUNT] = {0};
+  cudaEvent_t ev[PH_COUNT + 1];
+};
+
+// --------------------------------------------------------------------------
+static void gemm(Ctx &c, cublasOperation_t ta, cublasOperation_t tb, int m, int n, int k,
+                 double alpha, const double *A, int lda, const double *B, int ldb, double beta,
+                 double *C, int ldc) {
+  if (m == 0 || n == 0) return;
+  S2G_CUBLAS(cublasDgemm(c.blas, ta, tb, m, n, k, &alpha, A, lda, B, ldb, &beta, C, ldc));
+}
+
+static int grid_for(int64_t n, int block = 256) {
+  int64_t g = div_up(n, block);
+  return (int)std::max<int64_t>(1, std::min<int64_t>(g, 148 * 64));
+}
+
+static void record(Ctx &c, int ph) { S2G_CUDA(cudaEventRecord(c.ev[ph], c.stream)); }
+
+// Dense symmetric eigen-decomposition with an eigenvalue window (vl, vu]
+// (ssyevr 'V' range, stda.f:1143-1147) or the lowest k (range 'I').
+// A (n x n) is overwritten by the eigenvectors; returns the number found.
+static int dense_eig(Ctx &c, double *A, int n, double vl, double vu, int kmax, double *w) {
+  int meig = 0, lwork = 0;
+  cusolverEigRange_t range = kmax > 0 ? CUSOLVER_EIG_RANGE_I : CUSOLVER_EIG_RANGE_V;
+  int il = 1, iu = kmax > 0 ? std::min(kmax, n) : n;
+  S2G_CUSOLVER(cusolverDnDsyevdx_bufferSize(c.solver, CUSOLVER_EIG_MODE_VECTOR, range,
+                                            CUBLAS_FILL_MODE_LOWER, n, A, n, vl, vu, il, iu,
+                                            &meig, w, &lwork));
+  double *work = c.w_work.ensure((size_t)lwork + 1);
+  int *info = c.w_info.ensure(1);
+  S2G_CUSOLVER(cusolverDnDsyevdx(c.solver, CUSOLVER_EIG_MODE_VECTOR, range,
+                                 CUBLAS_FILL_MODE_LOWER, n, A, n, vl, vu, il, iu, &meig, w, work,
+                                 lwork, info));
+  int h_info = 0;
+  S2G_CUDA(cudaMemcpyAsync(&h_info, info, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+  S2G_CUDA(cudaStreamSynchronize(c.stream));
+  if (h_info != 0) throw Error{STD2G_ECUDA, "syevdx info " + std::to_string(h_info)};
+  return meig;
+}
+
+// Full symmetric eigen-decomposition (makel stda.f:1615-1691, smatpow srpapack.f:201-256)
+static void dense_eig_full(Ctx &c, double *A, int n, double *w) {
+  int lwork = 0;
+  S2G_CUSOLVER(cusolverDnDsyevd_bufferSize(c.solver, CUSOLVER_EIG_MODE_VECTOR,
+                                           CUBLAS_FILL_MODE_LOWER, n, A, n, w, &lwork));
+  double *work = c.w_work.ensure((size_t)lwork + 1);
+  int *info = c.w_info.ensure(1);
+  S2G_CUSOLVER(cusolverDnDsyevd(c.solver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, n, A,
+                                n, w, work, lwork, info));
+  int h_info = 0;
+  S2G_CUDA(cudaMemcpyAsync(&h_info, info, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+  S2G_CUDA(cudaStreamSynchronize(c.stream));
+  if (h_info != 0) throw Error{STD2G_ECUDA, "syevd info " + std::to_string(h_info)};
+}
+
+// X = U diag(sqrt(w)) U^T, U overwritten (tmp n*n)
+static void sym_sqrt(Ctx &c, double *U, const double *w, int n, double *out, double *tmp) {
+  S2G_CUDA(cudaMemcpyAsync(tmp, U, sizeof(double) * n * n, cudaMemcpyDeviceToDevice, c.stream));
+  S2G_LAUNCH(k_scale_cols_sqrt, grid_for((int64_t)n * n), 256, 0, c.stream, tmp, w, n);
+  gemm(c, CUBLAS_OP_N, CUBLAS_OP_T, n, n, n, 1.0, tmp, n, U, n, 0.0, out, n);
+}
+
+static uint64_t fnv1a(const std::vector<int> &a, const std::vector<int> &b) {
+  uint64_t h = 1469598103934665603ull;
+  for (size_t k = 0; k < a.size(); ++k) {
+    int v[2] = {a[k], b[k]};
+    const unsigned char *p = (const unsigned char *)v;
+    for (int q = 0; q < 8; ++q) {
+      h ^= p[q];
+      h *= 1099511628211ull;
+    }
+  }
+  return h;
+}
+
+// --------------------------------------------------------------------------
+static void load(Ctx &c, int ncent, int nmo, int nao, const double *xyz, const double *C,
+                 const double *eps, const double *occ, const int *iaoat, const double *S,
+                 const double *muL, const double *muV, const double *muM) {
+  if (ncent <= 0 || nmo <= 0 || nao <= 0 || !xyz || !C || !eps || !occ || !iaoat || !S || !muL ||
+      !muV || !muM)
+    throw Error{STD2G_EINVAL, "load: bad arguments"};
+  c.ncent = ncent;
+  c.nmo = nmo;
+  c.nao = nao;
+  c.h_eps.assign(eps, eps + nmo);
+  c.h_occ.assign(occ, occ + nmo);
+  c.h_xyz.assign(xyz, xyz + 4 * (size_t)ncent);
+  std::vector<double> eta(ncent);
+  for (int a = 0; a < ncent; ++a) {
+    int z = (int)std::lround(xyz[4 * a + 3]);
+    if (z < 1 || z > 94) throw Error{STD2G_EINVAL, "load: nuclear charge out of range"};
+    eta[a] = kEta[z - 1];
+  }
+  std::vector<int> cnt(ncent + 1, 0), ptr(ncent + 1, 0), list(nao);
+  for (int k = 0; k < nao; ++k) {
+    int a = iaoat[k] - 1;
+    if (a < 0 || a >= ncent) throw Error{STD2G_EINVAL, "load: iaoat out of range"};
+    cnt[a]++;
+  }
+  for (int a = 0; a < ncent; ++a) ptr[a + 1] = ptr[a] + cnt[a];
+  std::vector<int> fill(ptr.begin(), ptr.end() - 1);
+  for (int k = 0; k < nao; ++k) list[fill[iaoat[k] - 1]++] = k;
+  size_t npk = (size_t)nao * (nao + 1) / 2;
+  cudaStream_t s = c.stream;
+  S2G_CUDA(cudaMemcpyAsync(c.d_xyz.ensure(4 * ncent), xyz, sizeof(double) * 4 * ncent,
+                           cudaMemcpyHostToDevice, s));
+  S2G_CUDA(cudaMemcpyAsync(c.d_eta.ensure(ncent), eta.data(), sizeof(double) * ncent,
+                           cudaMemcpyHostToDevice, s));
+  S2G_CUDA(cudaMemcpyAsync(c.d_C.ensure((size_t)nao * nmo), C, sizeof(double) * nao * nmo,
+                           cudaMemcpyHostToDevice, s));
+  S2G_CUDA(cudaMemcpyAsync(c.d_ao_ptr.ensure(ncent + 1), ptr.data(), sizeof(int) * (ncent + 1),
+                           cudaMemcpyHostToDevice, s));
+  S2G_CUDA(cudaMemcpyAsync(c.d_ao_list.ensure(nao), list.data(), sizeof(int) * nao,
+                           cudaMemcpyHostToDevice, s));
+  // packed integrals -> full AO matrices (BLOWSY, onetri.f:62-80)
+  double *pk = c.w_work.ensure(npk * 10);
+  S2G_CUDA(cudaMemcpyAsync(pk, S, sizeof(double) * npk, cudaMemcpyHostToDevice, s));
+  S2G_CUDA(cudaMemcpyAsync(pk + npk, muL, sizeof(double) * npk * 3, cudaMemcpyHostToDevice, s));
+  S2G_CUDA(cudaMemcpyAsync(pk + 4 * npk, muV, sizeof(double) * npk * 3, cudaMemcpyHostToDevice, s));
+  S2G_CUDA(cudaMemcpyAsync(pk + 7 * npk, muM, sizeof(double) * npk * 3, cudaMemcpyHostToDevice, s));
+  size_t nn = (size_t)nao * nao;
+  double *Sf = c.d_Sfull.ensure(nn);
+  double *ao9 = c.d_ao9.ensure(nn * 9);
+  int g = grid_for((int64_t)nn);
+  S2G_LAUNCH(k_unpack, g, 256, 0, s, Sf, pk, nao, 0);
+  for (int q = 0; q < 9; ++q)
+    S2G_LAUNCH(k_unpack, g, 256, 0, s, ao9 + nn * q, pk + npk * (1 + q), nao, q < 3 ? 0 : 1);
+  S2G_CUDA(cudaStreamSynchronize(s));
+  c.sqrtS_ready = false;
+  c.loaded = true;
+}
+
+// A dynamic-polarizability request (lresp, linear_response.f:23-192).
+struct RespReq {
+  const double *omega;
+  int n;
+  double *alpha;   // [n*9]
+  double *resid;   // [n] or NULL
+};
+
+// (A-B)^-1 by Cholesky (ssptrf/ssptri, linear_response.f:89-95), then per omega
+// [(A+B) - w^2 (A-B)^-1] (X+Y) = -2 mu (linear_response.f:104-131) and
+// alpha_xy = -2 sum_j mu_x,j (X+Y)_y,j (linear_response.f:153-171).
+static void response(Ctx &c, double *Apb, double *Amb, int nci, const double *musel,
+                     const RespReq &rq) {
+  cudaStream_t s = c.stream;
+  const size_t n2 = (size_t)nci * nci;
+  int *info = c.w_info.ensure(1);
+  int h_info = 0;
+  auto check_info = [&](int code, const char *what) {
+    S2G_CUDA(cudaMemcpyAsync(&h_info, info, sizeof(int), cudaMemcpyDeviceToHost, s));
+    S2G_CUDA(cudaStreamSynchronize(s));
+    if (h_info != 0) throw Error{code, std::string(what) + " info " + std::to_string(h_info)};
+  };
+  double *Ainv = c.w_Ambh.ensure(n2);
+  S2G_CUDA(cudaMemcpyAsync(Ainv, Amb, sizeof(double) * n2, cudaMemcpyDeviceToDevice, s));
+  int lwork = 0;
+  S2G_CUSOLVER(cusolverDnDpotrf_bufferSize(c.solver, CUBLAS_FILL_MODE_LOWER, nci, Ainv, nci, &lwork));
+  int lw2 = 0;
+  S2G_CUSOLVER(cusolverDnDpotri_bufferSize(c.solver, CUBLAS_FILL_MODE_LOWER, nci, Ainv, nci, &lw2));
+  int lw3 = 0;
+  S2G_CUSOLVER(cusolverDnDgetrf_bufferSize(c.solver, nci, nci, Ainv, nci, &lw3));
+  double *work = c.w_work.ensure((size_t)std::max(lwork, std::max(lw2, lw3)) + 1);
+  S2G_CUSOLVER(cusolverDnDpotrf(c.solver, CUBLAS_FILL_MODE_LOWER, nci, Ainv, nci, work, lwork, info));
+  check_info(STD2G_EAMB_NOT_PD, "A-B Cholesky");
+  S2G_CUSOLVER(cusolverDnDpotri(c.solver, CUBLAS_FILL_MODE_LOWER, nci, Ainv, nci, work, lw2, info));
+  check_info(STD2G_EAMB_NOT_PD, "A-B inverse");
+  S2G_LAUNCH(k_symmetrize_lower, grid_for((int64_t)n2), 256, 0, s, Ainv, (int64_t)nci);
+  double *Mw = c.w_M.ensure(n2);
+  double *B = c.w_TL.ensure((size_t)nci * 3 * 3);
+  double *Xs = B + (size_t)nci * 3;
+  double *R = Xs + (size_t)nci * 3;
+  int *ipiv = c.w_tmpi.ensure(std::max<size_t>(nci, 1));
+  double *a9 = c.w_props.ensure(16);
+  for (int w = 0; w < rq.n; ++w) {
+    double om = rq.omega[w];
+    S2G_LAUNCH(k_axpby_mat, grid_for((int64_t)n2), 256, 0, s, Mw, Apb, Ainv, (int64_t)n2, -om * om);
+    // B = -2 mu_L ; Xs = B
+    S2G_LAUNCH(k_scale_copy, grid_for((int64_t)nci * 3), 256, 0, s, B, musel, (int64_t)nci * 3, -2.0);
+    S2G_CUDA(cudaMemcpyAsync(Xs, B, sizeof(double) * nci * 3, cudaMemcpyDeviceToDevice, s));
+    double *F = c.w_Apb.get() == Apb ? c.w_Kx.ensure(n2) : c.w_Kx.ensure(n2);
+    S2G_CUDA(cudaMemcpyAsync(F, Mw, sizeof(double) * n2, cudaMemcpyDeviceToDevice, s));
+    S2G_CUSOLVER(cusolverDnDpotrf(c.solver, CUBLAS_FILL_MODE_LOWER, nci, F, nci, work, lwork, info));
+    S2G_CUDA(cudaMemcpyAsync(&h_info, info, sizeof(int), cudaMemcpyDeviceToHost, s));
+    S2G_CUDA(cudaStreamSynchronize(s));
+    if (h_info == 0) {
+      S2G_CUSOLVER(cusolverDnDpotrs(c.solver, CUBLAS_FILL_MODE_LOWER, nci, 3, F, nci, Xs, nci, info));
+    } else {
+      // omega above the lowest excitation: indefinite, use LU (ssptrf is Bunch-Kaufman)
+      S2G_CUDA(cudaMemcpyAsync(F, Mw, sizeof(double) * n2, cudaMemcpyDeviceToDevice, s));
+      S2G_CUSOLVER(cusolverDnDgetrf(c.solver, nci, nci, F, nci, work, ipiv, info));
+      check_info(STD2G_ENOCONV, "response LU");
+      S2G_CUSOLVER(cusolverDnDgetrs(c.solver, CUBLAS_OP_N, nci, 3, F, nci, ipiv, Xs, nci, info));
+    }
+    check_info(STD2G_ENOCONV, "response solve");
+    // residual R = B - M X
+    S2G_CUDA(cudaMemcpyAsync(R, B, sizeof(double) * nci * 3, cudaMemcpyDeviceToDevice, s));
+    gemm(c, CUBLAS_OP_N, CUBLAS_OP_N, nci, 3, nci, -1.0, Mw, nci, Xs, nci, 1.0, R, nci);
+    // alpha = -2 mu^T (X+Y): a9[x + 3y]
+    gemm(c, CUBLAS_OP_T, CUBLAS_OP_N, 3, 3, nci, -2.0, musel, nci, Xs, nci, 0.0, a9, 3);
+    S2G_LAUNCH(k_resid_ratio, 1, 256, 0, s, R, B, nci, 3, a9 + 9);
+    double h[10];
+    S2G_CUDA(cudaMemcpyAsync(h, a9, sizeof(double) * 10, cudaMemcpyDeviceToHost, s));
+    S2G_CUDA(cudaStreamSynchronize(s));
+    for (int x = 0; x < 3; ++x)
+      for (int y = 0; y < 3; ++y) rq.alpha[(size_t)w * 9 + 3 * x + y] = h[x + 3 * y];
+    if (rq.resid) rq.resid[w] = h[9];
+  }
+}
+
+// --------------------------------------------------------------------------
+static void solve(Ctx &c, const std2g_params &p_in, std2g_result *res, const RespReq *resp) {
+  if (!c.loaded) throw Error{STD2G_ESTATE, "solve before load"};
+  std2g_params p = p_in;
+  if (resp) {
+    if (p.triplet) throw Error{STD2G_EINVAL, "response: triplet not available"};
+    p.rpa = 1;
+    p.velcorr = 0;
+  }
+  cudaStream_t s = c.stream;
+  const int N = c.ncent, nao = c.nao;
+  const bool mixed = c.opts.precision == 1;
+  record(c, PH_SETUP);
+  const double thr = p.e_thr_ev / kEh2eV_in;
+  const double fthr = p.fthr_ev < 1.79e308 ? p.fthr_ev / kEh2eV_in : INFINITY;
+  const double ak = p.triplet ? 0.0 : 2.0;
+  const double beta_j = p.beta_j >= -99.0 ? p.beta_j : 0.20 + 1.830 * p.ax;
+  const double alpha_k = p.alpha_k >= -99.0 ? p.alpha_k : 1.420 + 0.480 * p.ax;
+
+  // ---- orbital window and energy sort (stda.f:145-192, 261-308, 333) ----
+  const double deps = 2.0 * (1.0 + 0.8 * p.ax) * thr;
+  double omax = -1e42, vmin = 1e42;
+  for (int i = 0; i < c.nmo; ++i) {
+    if (c.h_occ[i] > 1.990 && c.h_eps[i] > omax) omax = c.h_eps[i];
+    if (c.h_occ[i] < 0.010 && c.h_eps[i] < vmin) vmin = c.h_eps[i];
+  }
+  std::vector<int> oidx, vidx;
+  for (int i = 0; i < c.nmo; ++i) {
+    if (c.h_occ[i] > 1.990 && c.h_eps[i] > vmin - deps) oidx.push_back(i);
+    if (c.h_occ[i] < 0.010 && c.h_eps[i] < omax + deps) vidx.push_back(i);
+  }
+  auto by_eps = [&](int a, int b) { return c.h_eps[a] < c.h_eps[b]; };
+  std::stable_sort(oidx.begin(), oidx.end(), by_eps);
+  std::stable_sort(vidx.begin(), vidx.end(), by_eps);
+  const int no = (int)oidx.size(), nv = (int)vidx.size(), moci = no + nv;
+  if (no == 0 || nv == 0) throw Error{STD2G_ENOCSF, "no CSF, increase energy threshold"};
+  std::vector<int> act(oidx);
+  act.insert(act.end(), vidx.begin(), vidx.end());
+  std::vector<double> eps_act(moci);
+  for (int m = 0; m < moci; ++m) eps_act[m] = c.h_eps[act[m]];
+  S2G_CUDA(cudaMemcpyAsync(c.w_act_idx.ensure(moci), act.data(), sizeof(int) * moci,
+                           cudaMemcpyHostToDevice, s));
+  S2G_CUDA(cudaMemcpyAsync(c.d_eps_act.ensure(moci), eps_act.data(), sizeof(double) * moci,
+                           cudaMemcpyHostToDevice, s));
+  double *Cact = c.w_Cact.ensure((size_t)nao * moci);
+  S2G_LAUNCH(k_gather_cols, grid_for((int64_t)nao * moci), 256, 0, s, Cact, c.d_C.get(),
+             (int64_t)nao, c.w_act_idx.get(), (int64_t)moci, (int64_t)nao);
+
+  // ---- S^1/2 (makel stda.f:1615-1691), once per load ----
+  record(c, PH_SQRTS);
+  if (!c.sqrtS_ready) {
+    size_t nn = (size_t)nao * nao;
+    double *U = c.w_tmp.ensure(nn * 2);
+    S2G_CUDA(cudaMemcpyAsync(U, c.d_Sfull.get(), sizeof(double) * nn, cudaMemcpyDeviceToDevice, s));
+    double *w = c.w_eval.ensure(std::max(nao, 16));
+    dense_eig_full(c, U, nao, w);
+    double wmin = 0;
+    S2G_CUDA(cudaMemcpyAsync(&wmin, w, sizeof(double), cudaMemcpyDeviceToHost, s));
+    S2G_CUDA(cudaStreamSynchronize(s));
+    if (wmin < 0) throw Error{STD2G_ES_NOT_PD, "negative overlap eigenvalue (S^1/2)"};
+    sym_sqrt(c, U, w, nao, c.d_sqrtS.ensure(nn), U + nn);
+    c.sqrtS_ready = true;
+  }
+  double *Clow = c.w_Clow.ensure((size_t)nao * moci);
+  gemm(c, CUBLAS_OP_N, CUBLAS_OP_N, nao, moci, nao, 1.0, c.d_sqrtS.get(), nao, Cact, nao, 0.0,
+       Clow, nao);
+  int *status = c.w_status.ensure(4);
+  S2G_CUDA(cudaMemsetAsync(status, 0, sizeof(int) * 4, s));
+  S2G_LAUNCH(k_colnorm_check, moci, 256, 0, s, Clow, nao, moci, status);
+
+  // ---- MO property integrals, occ-virt block (ONETRI, stda.f:351-412) ----
+  record(c, PH_MOINT);
+  {
+    size_t nn = (size_t)nao * nao;
+    double *T = c.w_T.ensure((size_t)nao * nv * 9);
+    double *mu = c.w_mu_ov.ensure((size_t)no * nv * 9);
+    double one = 1.0, zero = 0.0;
+    S2G_CUBLAS(cublasDgemmStridedBatched(c.blas, CUBLAS_OP_N, CUBLAS_OP_N, nao, nv, nao, &one,
+                                         c.d_ao9.get(), nao, (long long)nn, Cact + (size_t)nao * no,
+                                         nao, 0, &zero, T, nao, (long long)nao * nv, 9));
+    S2G_CUBLAS(cublasDgemmStridedBatched(c.blas, CUBLAS_OP_T, CUBLAS_OP_N, no, nv, nao, &one,
+                                         Cact, nao, 0, T, nao, (long long)nao * nv, &zero, mu, no,
+                                         (long long)no * nv, 9));
+  }
+
+  // ---- gamma and charges (stda.f:465-479, 509-532, 558-590, 728-763) ----
+  record(c, PH_CHARGES);
+  double *gj = c.w_gj.ensure((size_t)N * N), *gk = c.w_gk.ensure((size_t)N * N);
+  S2G_LAUNCH(k_gamma, grid_for((int64_t)N * N), 256, 0, s, c.d_xyz.get(), c.d_eta.get(), N, p.ax,
+             alpha_k, beta_j, gj, gk);
+  const int64_t nov = (int64_t)no * nv;
+  double *Qii = c.w_Qii.ensure((size_t)N * no), *Qaa = c.w_Qaa.ensure((size_t)N * nv);
+  double *Qia = c.w_Qia.ensure((size_t)N * nov), *Pia = c.w_Pia.ensure((size_t)N * nov);
+  double *Qoo = c.w_Qoo.ensure((size_t)N * no * no), *Poo = c.w_Poo.ensure((size_t)N * no * no);
+  double *Qvv = c.w_Qvv.ensure((size_t)N * nv * nv);
+  const int *aop = c.d_ao_ptr.get(), *aol = c.d_ao_list.get();
+  S2G_LAUNCH(k_charges_block, grid_for((int64_t)N * no), 256, 0, s, Qii, Clow, nao, N, aop, aol,
+             0, no, 0, no, 1);
+  S2G_LAUNCH(k_charges_block, grid_for((int64_t)N * nv), 256, 0, s, Qaa, Clow, nao, N, aop, aol,
+             no, nv, no, nv, 1);
+  S2G_LAUNCH(k_charges_block, grid_for((int64_t)N * nov), 256, 0, s, Qia, Clow, nao, N, aop, aol,
+             0, no, no, nv, 0);
+  S2G_LAUNCH(k_charges_block, grid_for((int64_t)N * no * no), 256, 0, s, Qoo, Clow, nao, N, aop,
+             aol, 0, no, 0, no, 0);
+  S2G_LAUNCH(k_charges_block, grid_for((int64_t)N * nv * nv), 256, 0, s, Qvv, Clow, nao, N, aop,
+             aol, no, nv, no, nv, 0);
+  // p = gamma q (ssymm, stda.f:558-590, 742-743)
+  double *Pii = c.w_Pii.ensure((size_t)N * no), *uci = c.w_uci.ensure((size_t)nv * no);
+  gemm(c, CUBLAS_OP_N, CUBLAS_OP_N, N, no, N, 1.0, gj, N, Qii, N, 0.0, Pii, N);
+  gemm(c, CUBLAS_OP_T, CUBLAS_OP_N, nv, no, N, 1.0, Qaa, N, Pii, N, 0.0, uci, nv);
+  gemm(c, CUBLAS_OP_N, CUBLAS_OP_N, N, (int)nov, N, 1.0, gk, N, Qia, N, 0.0, Pia, N);
+  gemm(c, CUBLAS_OP_N, CUBLAS_OP_N, N, no * no, N, 1.0, gj, N, Qoo, N, 0.0, Poo, N);
+
+  // ---- diagonal + energy screen (stda.f:593-668) ----
+  record(c, PH_SCREEN);
+  double *de = c.w_de.ensure(nov), *ek = c.w_ek.ensure(nov);
+  int *flag = c.w_flag.ensure(nov);
+  S2G_LAUNCH(k_diag_screen, grid_for(nov * 32), 256, 0, s, Pia, Qia, N, no, nv,
+             c.d_eps_act.get(), uci, ak, p.kshift, p.shftmax * 0.036749320,
+             p.shftwidth * 0.036749320, p.shftsteep, thr, fthr, de, ek, flag);
+  std::vector<int> h_flag(nov);
+  int h_status[4];
+  S2G_CUDA(cudaMemcpyAsync(h_flag.data(), flag, sizeof(int) * nov, cudaMemcpyDeviceToHost, s));
+  S2G_CUDA(cudaMemcpyAsync(h_status, status, sizeof(int) * 4, cudaMemcpyDeviceToHost, s));
+  S2G_CUDA(cudaStreamSynchronize(s));
+  if (h_status[0] != 0) throw Error{STD2G_EMONORM, "internal MO norm error"};
+  std::vector<int> pk_unsorted, ck;
+  for (int64_t k = 0; k < nov; ++k) {
+    if (h_flag[k] == 1) pk_unsorted.push_back((int)k);
+    else if (h_flag[k] == 2) ck.push_back((int)k);
+  }
+  const int nex = (int)pk_unsorted.size(), nexpt = (int)ck.size();
+  if (nex < 1) throw Error{STD2G_ENOCSF, "no CSF, increase energy threshold"};
+  // energy sort of primaries, stable in (i,a) enumeration order (stda.f:651-668)
+  std::vector<int> pk(nex);
+  std::vector<double> ed(nex);
+  {
+    int *d_in = c.w_tmpi.ensure(2 * (size_t)nex);
+    S2G_CUDA(cudaMemcpyAsync(d_in, pk_unsorted.data(), sizeof(int) * nex, cudaMemcpyHostToDevice, s));
+    double *keys_in = c.w_ed.ensure(2 * (size_t)nex);
+    // gather keys on device
+    S2G_LAUNCH(k_gather_cols, grid_for(nex), 256, 0, s, keys_in, de, (int64_t)1, d_in,
+               (int64_t)nex, (int64_t)1);
+    size_t tmpb = 0;
+    S2G_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmpb, keys_in, keys_in + nex, d_in,
+                                             d_in + nex, nex, 0, 64, s));
+    char *tmp = c.w_cub.ensure(tmpb + 16);
+    S2G_CUDA(cub::DeviceRadixSort::SortPairs(tmp, tmpb, keys_in, keys_in + nex, d_in, d_in + nex,
+                                             nex, 0, 64, s));
+    S2G_CUDA(cudaMemcpyAsync(pk.data(), d_in + nex, sizeof(int) * nex, cudaMemcpyDeviceToHost, s));
+    S2G_CUDA(cudaMemcpyAsync(ed.data(), keys_in + nex, sizeof(double) * nex,
+                             cudaMemcpyDeviceToHost, s));
+    S2G_CUDA(cudaStreamSynchronize(s));
+  }
+
+  // ---- PT selection (ptselect, stda.f:1773-1863) ----
+  record(c, PH_PT);
+  std::vector<int> newk;
+  std::vector<double> ed_lowered(ed);
+  if (nexpt > 0) {
+    // occupied / virtual sets spanned by the primaries
+    std::vector<int> omap(no, -1), vmap(nv, -1), OP, VP, pj(nex), pb(nex);
+    for (int q = 0; q < nex; ++q) {
+      pj[q] = pk[q] / nv;
+      pb[q] = pk[q] % nv;
+      omap[pj[q]] = 1;
+      vmap[pb[q]] = 1;
+    }
+    for (int i = 0; i < no; ++i)
+      if (omap[i] >= 0) { omap[i] = (int)OP.size(); OP.push_back(i); }
+    for (int a = 0; a < nv; ++a)
+      if (vmap[a] >= 0) { vmap[a] = (int)VP.size(); VP.push_back(a); }
+    const int nop = (int)OP.size(), nvp = (int)VP.size();
+    auto up = [&](DBuf<int> &b, const std::vector<int> &v) {
+      int *d = b.ensure(v.size());
+      S2G_CUDA(cudaMemcpyAsync(d, v.data(), sizeof(int) * v.size(), cudaMemcpyHostToDevice, s));
+      return d;
+    };
+    int *d_pk = up(c.w_pk, pk), *d_ck = up(c.w_ck, ck), *d_pj = up(c.w_pj, pj),
+        *d_pb = up(c.w_pb, pb), *d_omap = up(c.w_omap, omap), *d_vmap = up(c.w_vmap, vmap),
+        *d_OP = up(c.w_OP, OP), *d_VP = up(c.w_VP, VP);
+    double *d_ed = c.w_edsorted.ensure(nex);
+    S2G_CUDA(cudaMemcpyAsync(d_ed, ed.data(), sizeof(double) * nex, cudaMemcpyHostToDevice, s));
+    // primaries' charges and the virtual-pair factor
+    double *Qp = c.w_Qp.ensure((size_t)N * nex);
+    S2G_LAUNCH(k_gather_cols, grid_for((int64_t)N * nex), 256, 0, s, Qp, Qia, (int64_t)N, d_pk,
+               (int64_t)nex, (int64_t)N);
+    double *QvvP = c.w_QvvP.ensure((size_t)N * nv * nvp);
+    S2G_LAUNCH(k_gather_virt_pairs, grid_for((int64_t)N * nv * nvp), 256, 0, s, QvvP, Qvv, N, nv,
+               d_VP, nvp);
+    // chunk candidates by occupied index (candidates are in (i,a) order)
+    const int64_t ldj = (int64_t)nv * nvp;
+    const double budget = 6.0e9;   // bytes of K/J buffers per chunk
+    const double per_occ = 8.0 * ((double)nex * nv + (double)ldj * nop + (double)N * (nv + nop));
+    int occ_chunk = std::max(1, (int)std::min<double>(no, budget / per_occ));
+    std::vector<int> first_of_occ(no + 1, nexpt);
+    {
+      int q = 0;
+      for (int i = 0; i <= no; ++i) {
+        while (q < nexpt && ck[q] / nv < i) ++q;
+        first_of_occ[i] = q;
+      }
+    }
+    int nchunk = (int)div_up(no, occ_chunk);
+    double *colpart = c.w_colpart.ensure((size_t)nchunk * nex);
+    unsigned char *sel = c.w_sel.ensure(nexpt);
+    double *pert = c.w_pert.ensure(nexpt);
+    for (int q = 0; q < nchunk; ++q) {
+      int i0 = q * occ_chunk, i1 = std::min(no, i0 + occ_chunk), ni = i1 - i0;
+      int r0 = first_of_occ[i0], r1 = first_of_occ[i1], nr = r1 - r0;
+      if (nr == 0) {
+        S2G_CUDA(cudaMemsetAsync(colpart + (size_t)q * nex, 0, sizeof(double) * nex, s));
+        continue;
+      }
+      double *Pc = c.w_Pc.ensure((size_t)N * nr);
+      S2G_LAUNCH(k_gather_cols, grid_for((int64_t)N * nr), 256, 0, s, Pc, Pia, (int64_t)N,
+                 d_ck + r0, (int64_t)nr, (int64_t)N);
+      double *W = c.w_W.ensure((size_t)N * ni * nop);
+      S2G_LAUNCH(k_gather_occ_pairs, grid_for((int64_t)N * ni * nop), 256, 0, s, W, Poo, N, no,
+                 i0, ni, d_OP, nop);
+      if (!mixed) {
+        double *Kb = c.w_Kbuf.ensure((size_t)nex * nr);
+        double *Jb = c.w_Jbuf.ensure((size_t)ldj * ni * nop);
+        gemm(c, CUBLAS_OP_T, CUBLAS_OP_N, nex, nr, N, 1.0, Qp, N, Pc, N, 0.0, Kb, nex);
+        gemm(c, CUBLAS_OP_T, CUBLAS_OP_N, (int)ldj, ni * nop, N, 1.0, QvvP, N, W, N, 0.0, Jb,
+             (int)ldj);
+        S2G_LAUNCH((k_pt_rows<double, double>), nr, 256, 0, s, Kb, Jb, ldj, nex, nvp, nop, nr,
+                   d_ck + r0, nv, i0, de, d_pj, d_pb, d_omap, d_vmap, d_ed, ak, p.thrp,
+                   pert + r0, sel + r0);
+        S2G_LAUNCH((k_pt_cols<double, double>), (int)div_up(nex, 128), 128, 0, s, Kb, Jb, ldj,
+                   nex, nvp, nop, nr, d_ck + r0, nv, i0, de, d_pj, d_pb, d_omap, d_vmap, d_ed, ak,
+                   sel + r0, colpart + (size_t)q * nex);
+      } else {
+        mixed_pt_chunk(c.mixed, s, Qp, Pc, QvvP, W, N, nex, nr, (int)ldj, ni * nop);
+        S2G_LAUNCH((k_pt_rows<float, float>), nr, 256, 0, s, c.mixed.K.get(), c.mixed.J.get(),
+                   ldj, nex, nvp, nop, nr, d_ck + r0, nv, i0, de, d_pj, d_pb, d_omap, d_vmap,
+                   d_ed, ak, p.thrp, pert + r0, sel + r0);
+        // rows whose PT sum lies near the threshold are decided in FP64
+        mixed_pt_recheck(c.mixed, s, pert + r0, sel + r0, nr, p.thrp, Qp, Pc, QvvP, W, N, nex,
+                         (int)ldj, ni * nop, d_ck + r0, nv, i0, de, d_pj, d_pb, d_omap, d_vmap,
+                         d_ed, ak, nvp, nop);
+        S2G_LAUNCH((k_pt_cols<float, float>), (int)div_up(nex, 128), 128, 0, s, c.mixed.K.get(),
+                   c.mixed.J.get(), ldj, nex, nvp, nop, nr, d_ck + r0, nv, i0, de, d_pj, d_pb,
+                   d_omap, d_vmap, d_ed, ak, sel + r0, colpart + (size_t)q * nex);
+      }
+    }
+    double *pt2 = c.w_pt2.ensure(nex), *edp = c.w_edp.ensure(nex);
+    S2G_LAUNCH(k_pt2_finish, (int)div_up(nex, 128), 128, 0, s, colpart, nchunk, nex, d_ed, pt2,
+               edp);
+    std::vector<unsigned char> h_sel(nexpt);
+    S2G_CUDA(cudaMemcpyAsync(h_sel.data(), sel, nexpt, cudaMemcpyDeviceToHost, s));
+    S2G_CUDA(cudaMemcpyAsync(ed_lowered.data(), edp, sizeof(double) * nex, cudaMemcpyDeviceToHost,
+                             s));
+    S2G_CUDA(cudaStreamSynchronize(s));
+    for (int q = 0; q < nexpt; ++q)
+      if (h_sel[q]) newk.push_back(ck[q]);
+  }
+  const int nnew = (int)newk.size();
+  const int nci = nex + nnew;
+  std::vector<int> allk(pk);
+  allk.insert(allk.end(), newk.begin(), newk.end());
+  std::vector<int> ci(nci), ca(nci);
+  for (int u = 0; u < nci; ++u) {
+    ci[u] = allk[u] / nv;
+    ca[u] = allk[u] % nv;
+  }
+  std::vector<double> ed_all(ed_lowered);
+  if (nnew > 0) {
+    int *d_new = c.w_tmpi.ensure(std::max<size_t>(2 * (size_t)nex, nnew));
+    S2G_CUDA(cudaMemcpyAsync(d_new, newk.data(), sizeof(int) * nnew, cudaMemcpyHostToDevice, s));
+    double *d_denew = c.w_pert.ensure(std::max<size_t>(nexpt, nnew));
+    S2G_LAUNCH(k_gather_cols, grid_for(nnew), 256, 0, s, d_denew, de, (int64_t)1, d_new,
+               (int64_t)nnew, (int64_t)1);
+    std::vector<double> h_de(nnew);
+    S2G_CUDA(cudaMemcpyAsync(h_de.data(), d_denew, sizeof(double) * nnew, cudaMemcpyDeviceToHost, s));
+    S2G_CUDA(cudaStreamSynchronize(s));
+    ed_all.insert(ed_all.end(), h_de.begin(), h_de.end());
+  }
+
+  // ---- A / A+-B build (rtdamat stda.f:2010-2056, rrpamat stda.f:1870-2004) ----
+  record(c, PH_BUILD);
+  auto up = [&](DBuf<int> &b, const std::vector<int> &v) {
+    int *d = b.ensure(v.size());
+    S2G_CUDA(cudaMemcpyAsync(d, v.data(), sizeof(int) * v.size(), cudaMemcpyHostToDevice, s));
+    return d;
+  };
+  int *d_ci = up(c.w_ci, ci), *d_ca = up(c.w_ca, ca), *d_allk = up(c.w_allk, allk);
+  double *d_edall = c.w_ed.ensure(std::max<size_t>(2 * (size_t)nex, nci));
+  S2G_CUDA(cudaMemcpyAsync(d_edall, ed_all.data(), sizeof(double) * nci, cudaMemcpyHostToDevice, s));
+  const size_t n2 = (size_t)nci * nci;
+  double *Qs = c.w_Qs.ensure((size_t)N * nci), *Ps = c.w_Ps.ensure((size_t)N * nci);
+  S2G_LAUNCH(k_gather_cols, grid_for((int64_t)N * nci), 256, 0, s, Qs, Qia, (int64_t)N, d_allk,
+             (int64_t)nci, (int64_t)N);
+  S2G_LAUNCH(k_gather_cols, grid_for((int64_t)N * nci), 256, 0, s, Ps, Pia, (int64_t)N, d_allk,
+             (int64_t)nci, (int64_t)N);
+  double *ekd = c.w_tmp.ensure(std::max<size_t>(nci, (size_t)2 * nao * nao));
+  S2G_LAUNCH(k_gather_cols, grid_for(nci), 256, 0, s, ekd, ek, (int64_t)1, d_allk, (int64_t)nci,
+             (int64_t)1);
+  double *K = c.w_K.ensure(n2), *J = c.w_J.ensure(n2);
+  gemm(c, CUBLAS_OP_T, CUBLAS_OP_N, nci, nci, N, 1.0, Ps, N, Qs, N, 0.0, K, nci);
+  S2G_LAUNCH(k_pairdot, grid_for(n2 * 32), 256, 0, s, J, (int64_t)nci, d_ci, d_ca, nci, Poo, Qvv,
+             N, no, nv, 0);
+  const bool need_kx = p.rpa || p.velcorr;
+  double *Kx = nullptr;
+  if (need_kx) {
+    Kx = c.w_Kx.ensure(n2);
+    S2G_LAUNCH(k_pairdot, grid_for(n2 * 32), 256, 0, s, Kx, (int64_t)nci, d_ci, d_ca, nci, Pia,
+               Qia, N, no, nv, 1);
+  }
+  int nroot = 0;
+  double *X = nullptr, *Yv = nullptr, *om = nullptr;
+  double *Bh = nullptr;
+  if (!p.rpa) {
+    double *A = c.w_A.ensure(n2);
+    S2G_LAUNCH(k_combine_tda, grid_for(n2), 256, 0, s, A, K, J, (int64_t)nci, ak, d_edall);
+    if (p.velcorr) {
+      Bh = c.w_Bh.ensure(n2);
+      S2G_LAUNCH(k_combine_rpa, grid_for(n2), 256, 0, s, (double *)nullptr, (double *)nullptr, Bh,
+                 K, Kx, J, (int64_t)nci, ak, p.ax, d_edall, ekd);
+    }
+    record(c, PH_EIGEN);
+    om = c.w_eval.ensure(std::max(nci, nao));
+    if (mixed && p.nroots > 0 && nci > 256) {
+      nroot = mixed_davidson(c.mixed, c.blas, s, A, nci, p.nroots, p.conv_tol, om,
+                             c.w_X.ensure((size_t)nci * p.nroots));
+      X = c.w_X.get();
+    } else {
+      nroot = dense_eig(c, A, nci, 0.0, thr, p.nroots, om);
+      X = A;
+    }
+    if (nroot < 1) throw Error{STD2G_ENOROOT, "no root below the energy threshold"};
+  } else {
+    double *Apb = c.w_Apb.ensure(n2), *Amb = c.w_Amb.ensure(n2);
+    // J holds (ij|ab); A+B and A-B from K, Kx, J
+    S2G_LAUNCH(k_combine_rpa, grid_for(n2), 256, 0, s, Apb, Amb, (double *)nullptr, K, Kx, J,
+               (int64_t)nci, ak, p.ax, d_edall, ekd);
+    if (resp) {
+      record(c, PH_EIGEN);
+      record(c, PH_PROPS);
+      record(c, PH_RESPONSE);
+      double *musel = c.w_musel.ensure((size_t)nci * 9);
+      S2G_LAUNCH(k_gather_mu, grid_for((int64_t)nci * 9), 256, 0, s, musel, c.w_mu_ov.get(), no,
+                 nv, d_ci, d_ca, nci);
+      response(c, Apb, Amb, nci, musel, *resp);
+      record(c, PH_COUNT);
+      S2G_CUDA(cudaStreamSynchronize(s));
+      for (int q = 0; q < PH_COUNT; ++q) {
+        float ms = 0;
+        cudaEventElapsedTime(&ms, c.ev[q], c.ev[q + 1]);
+        c.ph_ms[q] = ms;
+      }
+      float tot = 0;
+      cudaEventElapsedTime(&tot, c.ev[PH_SETUP], c.ev[PH_COUNT]);
+      (void)cudaGetLastError();
+      c.last_nci = nci;
+      c.last_nroot = 0;
+      c.last_no = no;
+      c.last_nv = nv;
+      c.last_rpa = true;
+      if (res) {
+        res->nroot = 0;
+        res->no = no;
+        res->nv = nv;
+        res->nex = nex;
+        res->nexpt = nexpt;
+        res->new_pt = nnew;
+        res->nci = nci;
+        res->ms_total = tot;
+        res->csf_hash = fnv1a(ci, ca);
+      }
+      return;
+    }
+    record(c, PH_EIGEN);
+    // (A-B)^1/2 (smatpow srpapack.f:201-256)
+    double *U = c.w_Ambh.ensure(n2);
+    S2G_CUDA(cudaMemcpyAsync(U, Amb, sizeof(double) * n2, cudaMemcpyDeviceToDevice, s));
+    double *w = c.w_eval.ensure(std::max(nci, nao));
+    dense_eig_full(c, U, nci, w);
+    double wmin = 0;
+    S2G_CUDA(cudaMemcpyAsync(&wmin, w, sizeof(double), cudaMemcpyDeviceToHost, s));
+    S2G_CUDA(cudaStreamSynchronize(s));
+    if (wmin < 0) throw Error{STD2G_EAMB_NOT_PD, "matrix power impossible (A-B)"};
+    double *Ambh = c.w_M.ensure(n2);
+    double *tmp2 = c.w_Kx.ensure(n2);   // Kx no longer needed
+    sym_sqrt(c, U, w, nci, Ambh, tmp2);
+    // M = (A-B)^1/2 (A+B) (A-B)^1/2 (srpapack.f:58-71)
+    gemm(c, CUBLAS_OP_N, CUBLAS_OP_N, nci, nci, nci, 1.0, Apb, nci, Ambh, nci, 0.0, tmp2, nci);
+    double *Mm = U;
+    gemm(c, CUBLAS_OP_N, CUBLAS_OP_N, nci, nci, nci, 1.0, Ambh, nci, tmp2, nci, 0.0, Mm, nci);
+    om = c.w_eval.ensure(std::max(nci, nao));
+    nroot = dense_eig(c, Mm, nci, 0.0, thr * thr, p.nroots, om);
+    if (nroot < 1) throw Error{STD2G_ENOROOT, "RPA diag failed"};
+    S2G_LAUNCH(k_sqrt_inplace, (int)div_up(nroot, 128), 128, 0, s, om, nroot);
+    // X+Y = (A-B)^1/2 Z / sqrt(w); X-Y = (A+B)(X+Y)/w (srpapack.f:108-143)
+    X = c.w_X.ensure((size_t)nci * nroot);
+    Yv = c.w_Y.ensure((size_t)nci * nroot);
+    gemm(c, CUBLAS_OP_N, CUBLAS_OP_N, nci, nroot, nci, 1.0, Ambh, nci, Mm, nci, 0.0, X, nci);
+    S2G_LAUNCH(k_scale_columns, grid_for((int64_t)nci * nroot), 256, 0, s, X, (int64_t)nci, nroot,
+               om, 0);
+    gemm(c, CUBLAS_OP_N, CUBLAS_OP_N, nci, nroot, nci, 1.0, Apb, nci, X, nci, 0.0, Yv, nci);
+    S2G_LAUNCH(k_scale_columns, grid_for((int64_t)nci * nroot), 256, 0, s, Yv, (int64_t)nci,
+               nroot, om, 1);
+  }
+
+  // ---- properties (stda.f:1207-1289, apbtrafo.f:23-243) ----
+  record(c, PH_PROPS);
+  double *musel = c.w_musel.ensure((size_t)nci * 9);
+  S2G_LAUNCH(k_gather_mu, grid_for((int64_t)nci * 9), 256, 0, s, musel, c.w_mu_ov.get(), no, nv,
+             d_ci, d_ca, nci);
+  double *TL = c.w_TL.ensure((size_t)nroot * 9), *TVM = c.w_TVM.ensure((size_t)nroot * 9);
+  double *props = c.w_props.ensure((size_t)nroot * 4 + 8);
+  double *T2 = nullptr;
+  if (!p.rpa) {
+    gemm(c, CUBLAS_OP_T, CUBLAS_OP_N, nroot, 9, nci, 1.0, X, nci, musel, nci, 0.0, TL, nroot);
+    S2G_CUDA(cudaMemcpyAsync(TVM, TL, sizeof(double) * nroot * 9, cudaMemcpyDeviceToDevice, s));
+    if (p.velcorr) {
+      // X_new = (B/2) X / w (apbtrafo.f:51-65)
+      double *Xn = c.w_Y.ensure((size_t)nci * nroot);
+      gemm(c, CUBLAS_OP_N, CUBLAS_OP_N, nci, nroot, nci, 1.0, Bh, nci, X, nci, 0.0, Xn, nci);
+      S2G_LAUNCH(k_scale_columns, grid_for((int64_t)nci * nroot), 256, 0, s, Xn, (int64_t)nci,
+                 nroot, om, 2);
+      T2 = c.w_T2.ensure((size_t)nroot * 9);
+      gemm(c, CUBLAS_OP_T, CUBLAS_OP_N, nroot, 9, nci, 1.0, Xn, nci, musel, nci, 0.0, T2, nroot);
+    }
+  } else {
+    // uu = X+Y for the length form, pp = X-Y for velocity / magnetic
+    gemm(c, CUBLAS_OP_T, CUBLAS_OP_N, nroot, 9, nci, 1.0, X, nci, musel, nci, 0.0, TL, nroot);
+    gemm(c, CUBLAS_OP_T, CUBLAS_OP_N, nroot, 9, nci, 1.0, Yv, nci, musel, nci, 0.0, TVM, nroot);
+    int64_t tot = (int64_t)nci * nroot;
+    S2G_LAUNCH(k_xy_from_sums, grid_for(tot), 256, 0, s, X, Yv, tot);
+  }
+  S2G_LAUNCH(k_properties, (int)div_up(nroot, 128), 128, 0, s, TL, TVM, T2, nroot, nroot, om, ak,
+             (!p.rpa && p.velcorr) ? 1 : 0, props, props + nroot, props + 2 * nroot,
+             props + 3 * nroot);
+  S2G_LAUNCH(k_alpha0, 1, 128, 0, s, TL, nroot, nroot, om, ak, props + 4 * nroot);
+  record(c, PH_RESPONSE);
+  record(c, PH_COUNT);
+
+  // ---- results ----
+  std::vector<double> h_props((size_t)nroot * 4 + 6), h_om(nroot);
+  S2G_CUDA(cudaMemcpyAsync(h_props.data(), props, sizeof(double) * (nroot * 4 + 6),
+                           cudaMemcpyDeviceToHost, s));
+  S2G_CUDA(cudaMemcpyAsync(h_om.data(), om, sizeof(double) * nroot, cudaMemcpyDeviceToHost, s));
+  S2G_CUDA(cudaStreamSynchronize(s));
+  for (int q = 0; q < PH_COUNT; ++q) {
+    float ms = 0;
+    cudaEventElapsedTime(&ms, c.ev[q], c.ev[q + 1]);
+    c.ph_ms[q] = ms;
+  }
+  float tot = 0;
+  cudaEventElapsedTime(&tot, c.ev[PH_SETUP], c.ev[PH_COUNT]);
+  (void)cudaGetLastError();
+  c.last_nci = nci;
+  c.last_nroot = nroot;
+  c.last_no = no;
+  c.last_nv = nv;
+  c.last_rpa = p.rpa;
+  if (res) {
+    res->nroot = nroot;
+    res->no = no;
+    res->nv = nv;
+    res->nex = nex;
+    res->nexpt = nexpt;
+    res->new_pt = nnew;
+    res->nci = nci;
+    res->ms_total = tot;
+    res->csf_hash = fnv1a(ci, ca);
+    int m = std::min(nroot, res->cap);
+    for (int r = 0; r < m; ++r) {
+      if (res->omega) res->omega[r] = h_om[r];
+      if (res->fL) res->fL[r] = h_props[r];
+      if (res->fV) res->fV[r] = h_props[nroot + r];
+      if (res->RL) res->RL[r] = h_props[2 * nroot + r];
+      if (res->RV) res->RV[r] = h_props[3 * nroot + r];
+      if (res->resid) res->resid[r] = 0.0;
+    }
+    for (int q = 0; q < 6; ++q) res->alpha0[q] = h_props[4 * nroot + q];
+    if (nroot > res->cap) throw Error{STD2G_ECAP, "result capacity too small"};
+  }
+}
+
+}  // namespace std2g
+
+// ============================ C boundary =================================
+using std2g::Ctx;
+using std2g::Error;
+
+static thread_local std::string g_last_error;
+
+static int guard(const std::function<void()> &f) {
+  try {
+    f();
+    return STD2G_OK;
+  } catch (const Error &e) {
+    g_last_error = e.msg;
+    return e.code;
+  } catch (const std::bad_alloc &) {
+    g_last_error = "host allocation failed";
+    return STD2G_ENOMEM;
+  } catch (...) {
+    g_last_error = "unknown error";
+    return STD2G_ECUDA;
+  }
+}
+
+extern "C" {
+
+int std2g_create(void **ctx, const std2g_opts *opts) {
+  if (!ctx) return STD2G_EINVAL;
+  return guard([&] {
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+      throw Error{STD2G_ENODEV, "no CUDA device"};
+    std2g_opts o{};
+    if (opts) o = *opts;
+    if (o.device < 0 || o.device >= ndev) throw Error{STD2G_EINVAL, "bad device ordinal"};
+    cudaDeviceProp prop;
+    S2G_CUDA(cudaGetDeviceProperties(&prop, o.device));
+    if (prop.major != 10) throw Error{STD2G_ENODEV, "an sm_100 (B200) device is required"};
+    S2G_CUDA(cudaSetDevice(o.device));
+    auto *c = new Ctx();
+    c->opts = o;
+    S2G_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    S2G_CUBLAS(cublasCreate(&c->blas));
+    S2G_CUBLAS(cublasSetStream(c->blas, c->stream));
+    S2G_CUSOLVER(cusolverDnCreate(&c->solver));
+    S2G_CUSOLVER(cusolverDnSetStream(c->solver, c->stream));
+    for (auto &e : c->ev) S2G_CUDA(cudaEventCreate(&e));
+    *ctx = c;
+  });
+}
+
+int std2g_load(void *ctx, int ncent, int nmo, int nao, const double *xyz, const double *C,
+               const double *eps, const double *occ, const int *iaoat, const double *S,
+               const double *mu_L, const double *mu_V, const double *mu_M) {
+  if (!ctx) return STD2G_EINVAL;
+  auto *c = (Ctx *)ctx;
+  return guard([&] {
+    S2G_CUDA(cudaSetDevice(c->opts.device));
+    std2g::load(*c, ncent, nmo, nao, xyz, C, eps, occ, iaoat, S, mu_L, mu_V, mu_M);
+  });
+}
+
+int std2g_solve(void *ctx, const std2g_params *par, std2g_result *res) {
+  if (!ctx || !par) return STD2G_EINVAL;
+  auto *c = (Ctx *)ctx;
+  return guard([&] {
+    S2G_CUDA(cudaSetDevice(c->opts.device));
+    if (par->e_thr_ev <= 0) throw Error{STD2G_EINVAL, "e_thr_ev must be positive"};
+    std2g::solve(*c, *par, res, nullptr);
+  });
+}
+
+int std2g_polarizability(void *ctx, const std2g_params *par, const double *omega, int nomega,
+                         double *alpha, double *resid) {
+  if (!ctx || !par || !omega || nomega <= 0 || !alpha) return STD2G_EINVAL;
+  auto *c = (Ctx *)ctx;
+  return guard([&] {
+    S2G_CUDA(cudaSetDevice(c->opts.device));
+    std2g::RespReq rq{omega, nomega, alpha, resid};
+    std2g::solve(*c, *par, nullptr, &rq);
+  });
+}
+
+int std2g_get_csf(void *ctx, int *iconf, double *ed, int cap, int *nci) {
+  if (!ctx || !nci) return STD2G_EINVAL;
+  auto *c = (Ctx *)ctx;
+  return guard([&] {
+    int n = c->last_nci;
+    *nci = n;
+    if (n == 0) throw Error{STD2G_ESTATE, "no solve yet"};
+    if (cap < n) throw Error{STD2G_ECAP, "capacity too small"};
+    std::vector<int> ci(n), ca(n);
+    std::vector<double> h_ed(n);
+    S2G_CUDA(cudaMemcpy(ci.data(), c->w_ci.get(), sizeof(int) * n, cudaMemcpyDeviceToHost));
+    S2G_CUDA(cudaMemcpy(ca.data(), c->w_ca.get(), sizeof(int) * n, cudaMemcpyDeviceToHost));
+    S2G_CUDA(cudaMemcpy(h_ed.data(), c->w_ed.get(), sizeof(double) * n, cudaMemcpyDeviceToHost));
+    for (int u = 0; u < n; ++u) {
+      if (iconf) {
+        iconf[2 * u] = ci[u] + 1;
+        iconf[2 * u + 1] = c->last_no + ca[u] + 1;
+      }
+      if (ed) ed[u] = h_ed[u];
+    }
+  });
+}
+
+int std2g_get_vectors(void *ctx, double *X, double *Y, int cap, int *nroot, int *nci) {
+  if (!ctx || !nroot || !nci) return STD2G_EINVAL;
+  auto *c = (Ctx *)ctx;
+  return guard([&] {
+    *nroot = c->last_nroot;
+    *nci = c->last_nci;
+    if (c->last_nci == 0) throw Error{STD2G_ESTATE, "no solve yet"};
+    if (cap < c->last_nroot) throw Error{STD2G_ECAP, "capacity too small"};
+    size_t bytes = sizeof(double) * (size_t)c->last_nci * c->last_nroot;
+    const double *src = c->last_rpa ? c->w_X.get() : c->mixed.lastX ? c->mixed.lastX : c->w_A.get();
+    if (X) S2G_CUDA(cudaMemcpy(X, src, bytes, cudaMemcpyDeviceToHost));
+    if (Y && c->last_rpa) S2G_CUDA(cudaMemcpy(Y, c->w_Y.get(), bytes, cudaMemcpyDeviceToHost));
+  });
+}
+
+int std2g_phase_times(void *ctx, double *ms, int cap) {
+  if (!ctx) return 0;
+  auto *c = (Ctx *)ctx;
+  int n = std::min(cap, (int)std2g::PH_COUNT);
+  for (int q = 0; q < n; ++q) ms[q] = c->ph_ms[q];
+  return std2g::PH_COUNT;
+}
+
+const char *std2g_phase_name(int q) {
+  return (q >= 0 && q < std2g::PH_COUNT) ? std2g::kPhaseNames[q] : "";
+}
+
+int64_t std2g_kernel_launches(void *) { return std2g::g_launches; }
+
+const char *std2g_error_string(int status) {
+  switch (status) {
+    case STD2G_OK: return "ok";
+    case STD2G_EINVAL: return "invalid argument";
+    case STD2G_ECUDA: return g_last_error.empty() ? "CUDA error" : g_last_error.c_str();
+    case STD2G_ENOMEM: return "out of device memory";
+    case STD2G_ENOCSF: return "no CSF, increase energy threshold (-e option)";
+    case STD2G_ES_NOT_PD: return "S^1/2: overlap matrix not positive definite";
+    case STD2G_EMONORM: return "internal MO norm error";
+    case STD2G_ENOROOT: return "no root below the energy threshold";
+    case STD2G_ENOCONV: return "iterative solver did not converge";
+    case STD2G_EAMB_NOT_PD: return "matrix power impossible (A-B not positive definite)";
+    case STD2G_ESTATE: return "call order";
+    case STD2G_ECAP: return "caller buffer too small";
+    case STD2G_ENODEV: return "no sm_100 CUDA device";
+    case STD2G_ETIMEOUT: return "device wait timed out";
+    default: return "unknown status";
+  }
+}
+
+void std2g_destroy(void *ctx) {
+  if (!ctx) return;
+  auto *c = (Ctx *)ctx;
+  cudaSetDevice(c->opts.device);
+  cudaStreamSynchronize(c->stream);
+  for (auto &e : c->ev) cudaEventDestroy(e);
+  if (c->solver) cusolverDnDestroy(c->solver);
+  if (c->blas) cublasDestroy(c->blas);
+  delete c;   // buffers free themselves
+}
+
+}  // extern "C"

@@ -1,0 +1,286 @@
+"""Host-side binding of the std2g C ABI (``include/std2g.h``).
+
+This is the Python mirror of the reference's call ``stda(...)``
+(``stda.f:53-54``, called at ``main.f:928``): the same inputs (MOs, energies,
+occupations, AO->atom map, keyword values) and the same outputs (roots, f_L,
+f_V, R_L, R_V and ``tda.dat``).  All arithmetic happens in the CUDA library
+``libstd2g.so`` built in-tree; when that library is missing this module
+raises instead of computing anything on the CPU.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from .integrals import ao_integrals, pack_lower
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libstd2g.so")
+
+STATUS = {
+    0: "OK", 1: "EINVAL", 2: "ECUDA", 3: "ENOMEM", 4: "ENOCSF", 5: "ES_NOT_PD",
+    6: "EMONORM", 7: "ENOROOT", 8: "ENOCONV", 9: "EAMB_NOT_PD", 10: "ESTATE",
+    11: "ECAP", 12: "ENODEV", 13: "ETIMEOUT",
+}
+
+EXPORTS = [
+    "std2g_create", "std2g_load", "std2g_solve", "std2g_polarizability",
+    "std2g_get_csf", "std2g_get_vectors", "std2g_phase_times", "std2g_phase_name",
+    "std2g_kernel_launches", "std2g_error_string", "std2g_destroy",
+]
+
+
+class Std2gError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{STATUS.get(code, code)}: {msg}")
+        self.code = code
+        self.name = STATUS.get(code, str(code))
+
+
+class Opts(C.Structure):
+    _fields_ = [("device", C.c_int), ("precision", C.c_int), ("verbose", C.c_int),
+                ("reserved", C.c_int), ("max_device_bytes", C.c_int64)]
+
+
+class Params(C.Structure):
+    _fields_ = [("ax", C.c_double), ("e_thr_ev", C.c_double), ("thrp", C.c_double),
+                ("alpha_k", C.c_double), ("beta_j", C.c_double), ("fthr_ev", C.c_double),
+                ("triplet", C.c_int), ("rpa", C.c_int), ("velcorr", C.c_int), ("kshift", C.c_int),
+                ("shftmax", C.c_double), ("shftwidth", C.c_double), ("shftsteep", C.c_double),
+                ("nroots", C.c_int), ("solver", C.c_int), ("conv_tol", C.c_double)]
+
+
+class Result(C.Structure):
+    _fields_ = [("cap", C.c_int), ("nroot", C.c_int), ("no", C.c_int), ("nv", C.c_int),
+                ("nex", C.c_int), ("nexpt", C.c_int), ("new_pt", C.c_int), ("nci", C.c_int),
+                ("omega", C.POINTER(C.c_double)), ("fL", C.POINTER(C.c_double)),
+                ("fV", C.POINTER(C.c_double)), ("RL", C.POINTER(C.c_double)),
+                ("RV", C.POINTER(C.c_double)), ("resid", C.POINTER(C.c_double)),
+                ("alpha0", C.c_double * 6), ("csf_hash", C.c_uint64), ("ms_total", C.c_double)]
+
+
+_lib = None
+
+
+def library():
+    """Load ``libstd2g.so`` (built in-tree); raise if it is absent."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is not built; run stda_b200.build.build()")
+        lib = C.CDLL(LIB_PATH)
+        dp = C.POINTER(C.c_double)
+        ip = C.POINTER(C.c_int)
+        lib.std2g_create.argtypes = [C.POINTER(C.c_void_p), C.POINTER(Opts)]
+        lib.std2g_load.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, dp, dp, dp, dp, ip,
+                                   dp, dp, dp, dp]
+        lib.std2g_solve.argtypes = [C.c_void_p, C.POINTER(Params), C.POINTER(Result)]
+        lib.std2g_polarizability.argtypes = [C.c_void_p, C.POINTER(Params), dp, C.c_int, dp, dp]
+        lib.std2g_get_csf.argtypes = [C.c_void_p, ip, dp, C.c_int, ip]
+        lib.std2g_get_vectors.argtypes = [C.c_void_p, dp, dp, C.c_int, ip, ip]
+        lib.std2g_phase_times.argtypes = [C.c_void_p, dp, C.c_int]
+        lib.std2g_phase_name.argtypes = [C.c_int]
+        lib.std2g_phase_name.restype = C.c_char_p
+        lib.std2g_kernel_launches.argtypes = [C.c_void_p]
+        lib.std2g_kernel_launches.restype = C.c_int64
+        lib.std2g_error_string.argtypes = [C.c_int]
+        lib.std2g_error_string.restype = C.c_char_p
+        lib.std2g_destroy.argtypes = [C.c_void_p]
+        lib.std2g_destroy.restype = None
+        _lib = lib
+    return _lib
+
+
+def _dp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _check(code):
+    if code != 0:
+        raise Std2gError(code, library().std2g_error_string(code).decode())
+
+
+@dataclass
+class Keywords:
+    """std2 keywords of the sTDA path (``main.f:84-131``)."""
+    ax: float = 0.5
+    e_thr_ev: float = 7.0
+    thrp: float = 1e-4
+    alpha_k: float = -100.0
+    beta_j: float = -100.0
+    fthr_ev: float = 1.7976931348623157e308
+    triplet: bool = False
+    rpa: bool = False
+    velcorr: bool = True
+    kshift: bool = False
+    shftmax: float = 0.5
+    shftwidth: float = 0.1
+    shftsteep: float = 4.0
+    nroots: int = 0
+    solver: int = 0
+    conv_tol: float = 0.0
+
+    def to_c(self) -> Params:
+        return Params(self.ax, self.e_thr_ev, self.thrp, self.alpha_k, self.beta_j, self.fthr_ev,
+                      int(self.triplet), int(self.rpa), int(self.velcorr), int(self.kshift),
+                      self.shftmax, self.shftwidth, self.shftsteep, int(self.nroots),
+                      int(self.solver), float(self.conv_tol))
+
+
+@dataclass
+class Solution:
+    omega: np.ndarray
+    fL: np.ndarray
+    fV: np.ndarray
+    RL: np.ndarray
+    RV: np.ndarray
+    alpha0: np.ndarray
+    no: int
+    nv: int
+    nex: int
+    nexpt: int
+    new: int
+    nci: int
+    csf_hash: int
+    ms: float
+    velo: bool
+    xmolw: float = 0.0
+    extras: dict = field(default_factory=dict)
+
+
+@dataclass
+class BoundaryInputs:
+    """The arrays that cross the C ABI for one wavefunction."""
+    xyz4: np.ndarray     # (ncent, 4) rows x,y,z,Z == Fortran xyz(4,ncent)
+    C: np.ndarray        # Fortran-ordered (nao, nmo)
+    eps: np.ndarray
+    occ: np.ndarray
+    iaoat1: np.ndarray   # 1-based int32
+    S: np.ndarray        # packed
+    muL: np.ndarray      # (3, npk)
+    muV: np.ndarray
+    muM: np.ndarray
+
+    @property
+    def ncent(self):
+        return self.xyz4.shape[0]
+
+    @property
+    def nao(self):
+        return self.C.shape[0]
+
+    @property
+    def nmo(self):
+        return self.C.shape[1]
+
+
+def boundary_inputs(mol, ints=None) -> BoundaryInputs:
+    """Pack a molecule and its AO integrals into the boundary layout."""
+    S, L, V, M = ints if ints is not None else ao_integrals(mol)
+    xyz4 = np.ascontiguousarray(np.hstack([mol.xyz, mol.Z[:, None].astype(np.float64)]))
+    return BoundaryInputs(
+        xyz4=xyz4, C=np.asfortranarray(mol.C), eps=np.ascontiguousarray(mol.eps, dtype=np.float64),
+        occ=np.ascontiguousarray(mol.occ, dtype=np.float64),
+        iaoat1=np.ascontiguousarray(mol.iaoat() + 1, dtype=np.int32),
+        S=pack_lower(S), muL=np.ascontiguousarray(pack_lower(L)),
+        muV=np.ascontiguousarray(pack_lower(V)), muM=np.ascontiguousarray(pack_lower(M)))
+
+
+class Engine:
+    """One std2g context on one device (``precision`` 0: FP64, 1: mixed)."""
+
+    def __init__(self, device: int = 0, precision: int = 0, verbose: int = 0):
+        self.lib = library()
+        self.ctx = C.c_void_p()
+        opts = Opts(device, precision, verbose, 0, 0)
+        _check(self.lib.std2g_create(C.byref(self.ctx), C.byref(opts)))
+        self.precision = precision
+        self.inputs = None
+        self.xmolw = 0.0
+
+    def close(self):
+        if self.ctx:
+            self.lib.std2g_destroy(self.ctx)
+            self.ctx = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def load(self, b: BoundaryInputs):
+        self.inputs = b
+        from .tdadat import molecular_mass
+        self.xmolw = molecular_mass(b.xyz4[:, 3])
+        _check(self.lib.std2g_load(
+            self.ctx, b.ncent, b.nmo, b.nao, _dp(b.xyz4), _dp(b.C), _dp(b.eps), _dp(b.occ),
+            b.iaoat1.ctypes.data_as(C.POINTER(C.c_int)), _dp(b.S), _dp(b.muL), _dp(b.muV),
+            _dp(b.muM)))
+
+    def solve(self, kw: Keywords, cap: int = 4096) -> Solution:
+        bufs = [np.zeros(cap) for _ in range(6)]
+        res = Result()
+        res.cap = cap
+        res.omega, res.fL, res.fV, res.RL, res.RV, res.resid = (_dp(b) for b in bufs)
+        _check(self.lib.std2g_solve(self.ctx, C.byref(kw.to_c()), C.byref(res)))
+        n = res.nroot
+        return Solution(omega=bufs[0][:n].copy(), fL=bufs[1][:n].copy(), fV=bufs[2][:n].copy(),
+                        RL=bufs[3][:n].copy(), RV=bufs[4][:n].copy(),
+                        alpha0=np.array(res.alpha0[:]), no=res.no, nv=res.nv, nex=res.nex,
+                        nexpt=res.nexpt, new=res.new_pt, nci=res.nci, csf_hash=res.csf_hash,
+                        ms=res.ms_total, velo=(not kw.rpa) and kw.velcorr, xmolw=self.xmolw,
+                        extras=dict(resid=bufs[5][:n].copy()))
+
+    def polarizability(self, kw: Keywords, omegas):
+        om = np.ascontiguousarray(omegas, dtype=np.float64)
+        out = np.zeros(len(om) * 9)
+        resid = np.zeros(len(om))
+        _check(self.lib.std2g_polarizability(self.ctx, C.byref(kw.to_c()), _dp(om), len(om),
+                                             _dp(out), _dp(resid)))
+        return out.reshape(len(om), 3, 3), resid
+
+    def csf(self):
+        n = C.c_int()
+        _check_cap = self.lib.std2g_get_csf(self.ctx, None, None, 0, C.byref(n))
+        if _check_cap not in (0, 11):
+            _check(_check_cap)
+        iconf = np.zeros(2 * n.value, dtype=np.int32)
+        ed = np.zeros(n.value)
+        _check(self.lib.std2g_get_csf(self.ctx, iconf.ctypes.data_as(C.POINTER(C.c_int)),
+                                      _dp(ed), n.value, C.byref(n)))
+        return iconf.reshape(-1, 2), ed
+
+    def vectors(self, rpa=False):
+        nr, nci = C.c_int(), C.c_int()
+        code = self.lib.std2g_get_vectors(self.ctx, None, None, 0, C.byref(nr), C.byref(nci))
+        if code not in (0, 11):
+            _check(code)
+        X = np.zeros((nr.value, nci.value))
+        Y = np.zeros((nr.value, nci.value)) if rpa else None
+        _check(self.lib.std2g_get_vectors(self.ctx, _dp(X), _dp(Y) if rpa else None, nr.value,
+                                          C.byref(nr), C.byref(nci)))
+        return (X.T, Y.T) if rpa else X.T
+
+    def phase_times(self):
+        ms = np.zeros(16)
+        n = self.lib.std2g_phase_times(self.ctx, _dp(ms), 16)
+        return {self.lib.std2g_phase_name(q).decode(): ms[q] for q in range(n)}
+
+    def kernel_launches(self):
+        return int(self.lib.std2g_kernel_launches(self.ctx))
+
+
+def stda(mol, kw: Keywords, ints=None, device=0, precision=0):
+    """One-call mirror of ``call stda(...)``: returns (Solution, tda.dat text)."""
+    from .tdadat import tda_dat
+    eng = Engine(device, precision)
+    try:
+        eng.load(boundary_inputs(mol, ints))
+        sol = eng.solve(kw)
+    finally:
+        eng.close()
+    return sol, tda_dat(sol, kw)

