@@ -157,6 +157,13 @@ const char *std2g_phase_name(int phase);
 /* Number of kernels this library launched since the context was created. */
 int64_t std2g_kernel_launches(void *ctx);
 
+/* Tensor-core contraction statistics of the last solve: total device time
+   (ms), number of launches and algorithmic FLOPs (used for the roofline). */
+int std2g_kernel_stats(void *ctx, double *ms, int64_t *launches, double *flop);
+
+/* Davidson statistics of the last solve: iterations and sigma-vector count. */
+int std2g_solver_stats(void *ctx, int *iters, int64_t *matvecs);
+
 const char *std2g_error_string(int status);
 void std2g_destroy(void *ctx);
 

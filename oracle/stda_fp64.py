@@ -277,6 +277,19 @@ def stda(xyz4, C, eps, occ, iaoat, S, Lao, Vao, Mao, p: Params, want_A=True):
         J = J4[oinv1[:, None], oinv2[None, :], vinv1[:, None], vinv2[None, :]]
         return ak * K - J
 
+    def exchange(ks):
+        """(ib|ja) with gamma^K for CSF pairs u=(i,a), v=(j,b) (rrpamat stda.f:1943-1946)."""
+        i1, a1 = io_all[ks], ia_all[ks]
+        n = len(ks)
+        out = np.empty((n, n))
+        rb = max(1, int(3e7 // max(1, n * ncent)))
+        for r0 in range(0, n, rb):
+            r1 = min(n, r0 + rb)
+            kib = i1[r0:r1, None] * nv + a1[None, :]
+            kja = i1[None, :] * nv + a1[r0:r1, None]
+            out[r0:r1] = np.einsum("Auv,Auv->uv", pia[:, kib], qia[:, kja])
+        return out
+
     # PT selection (stda.f:1773-1863)
     pt2 = np.zeros(len(pk))
     incl = np.zeros(len(ck), dtype=bool)
@@ -306,16 +319,16 @@ def stda(xyz4, C, eps, occ, iaoat, S, Lao, Vao, Mao, p: Params, want_A=True):
     if not want_A:
         return res
 
-    # A matrix (rtdamat stda.f:2010-2056)
-    A = coupling(allk, allk)
+    # A matrix (rtdamat stda.f:2010-2056), built in row blocks to bound memory
+    A = np.empty((nci, nci))
+    rb = max(1, int(2e7 // max(1, nci)))
+    for r0 in range(0, nci, rb):
+        A[r0:r0 + rb] = coupling(allk[r0:r0 + rb], allk)
     np.fill_diagonal(A, ed)
 
     if p.rpa:
         # exchange-type (ib|ja) with gamma^K (rrpamat stda.f:1930-1963)
-        i1, a1 = io_all[allk], ia_all[allk]
-        kib = i1[:, None] * nv + a1[None, :]      # (ib): occ of row, virt of col
-        kja = i1[None, :] * nv + a1[:, None]      # (ja): occ of col, virt of row
-        Kx = np.einsum("Auv,Auv->uv", pia[:, kib], qia[:, kja])
+        Kx = exchange(allk)
         Kd = ek_all[allk]
         Kov = pia[:, allk].T @ qia[:, allk]
         Apb = 2.0 * ak * Kov - p.ax * Kx - (ak * Kov - A)       # 2ak(ia|jb) - ax(ib|ja) - (ij|ab)
@@ -366,10 +379,7 @@ def stda(xyz4, C, eps, occ, iaoat, S, Lao, Vao, Mao, p: Params, want_A=True):
 
     if (not p.rpa) and p.velcorr:
         # rtdacorr (apbtrafo.f:580-643) + apbtrafo (apbtrafo.f:23-300)
-        i1, a1 = io_all[allk], ia_all[allk]
-        kib = i1[:, None] * nv + a1[None, :]
-        kja = i1[None, :] * nv + a1[:, None]
-        Kx = np.einsum("Auv,Auv->uv", pia[:, kib], qia[:, kja])
+        Kx = exchange(allk)
         Kov = pia[:, allk].T @ qia[:, allk]
         Bh = 0.5 * ak * Kov - 0.5 * p.ax * Kx
         np.fill_diagonal(Bh, 0.5 * (ak * np.diag(Kov) - p.ax * np.diag(Kov)))
@@ -439,3 +449,99 @@ def read_tda_dat(text: str):
         if on and ln.strip():
             rows.append([float(t) for t in ln.split()])
     return np.array(rows)
+
+
+def stda_timed(xyz4, C, eps, occ, iaoat, S, Lao, Vao, Mao, p: Params, budget_s=15.0):
+    """Wall-clock estimate of one full FP64 CPU solve from a bounded sample.
+
+    Phases that are cheap run in full (window, MO integrals, S^1/2, charges,
+    gamma, screen).  The PT selection runs on leading candidate blocks until
+    about half the budget is used and is scaled linearly to all candidates;
+    the A build is timed on a row block of the primary space and scaled to
+    nci^2; the dense diagonalisation (ssyevr in the reference) is timed on a
+    min(nci, 1500)-sized matrix and scaled as n^3.  Used only as the reported
+    CPU baseline, never as a result.
+    """
+    import os
+    import time
+    t_all = time.perf_counter()
+    thr = p.e_thr_ev / EH2EV_IN
+    oidx, vidx = select_window(eps, occ, p.ax, thr)
+    no, nv = len(oidx), len(vidx)
+    Cact = C[:, np.concatenate([oidx, vidx])]
+    Co, Cv = Cact[:, :no], Cact[:, no:]
+    for mat in (Lao, Vao, Mao):
+        for d in range(3):
+            mo_ov(mat[d], Co, Cv)
+    Clow = lowdin_orthogonal_mos(S, Cact)
+    epsi = np.concatenate([eps[oidx], eps[vidx]])
+    ak = 0.0 if p.triplet else 2.0
+    alpha_k, beta_j = default_alpha_beta(p)
+    gj, gk = gamma_matrices(xyz4, p.ax, alpha_k, beta_j)
+    ncent = xyz4.shape[1]
+    io_all, ia_all = np.meshgrid(np.arange(no), np.arange(nv), indexing="ij")
+    io_all, ia_all = io_all.ravel(), ia_all.ravel()
+    qii = charges(Clow, iaoat, ncent, np.arange(no), np.arange(no))
+    qaa = charges(Clow, iaoat, ncent, no + np.arange(nv), no + np.arange(nv))
+    uci = qaa.T @ (gj @ qii)
+    qia = charges(Clow, iaoat, ncent, io_all, no + ia_all)
+    pia = gk @ qia
+    ek_all = np.einsum("Ak,Ak->k", pia, qia)
+    de_all = (epsi[no + ia_all] - epsi[io_all]) - uci[ia_all, io_all] + ak * ek_all
+    pk = np.nonzero(de_all <= thr)[0]
+    ck = np.nonzero(de_all > thr)[0]
+    pk = pk[np.argsort(de_all[pk], kind="stable")]
+    ed = de_all[pk]
+    ii, jj = np.meshgrid(np.arange(no), np.arange(no), indexing="ij")
+    qoo = charges(Clow, iaoat, ncent, ii.ravel(), jj.ravel()).reshape(ncent, no, no)
+    aa, bb = np.meshgrid(np.arange(nv), np.arange(nv), indexing="ij")
+    qvv = charges(Clow, iaoat, ncent, no + aa.ravel(), no + bb.ravel()).reshape(ncent, nv, nv)
+    poo = np.einsum("AB,Bij->Aij", gj, qoo)
+    t_setup = time.perf_counter() - t_all
+
+    def coupling(krow, kcol):
+        i1, a1 = io_all[krow], ia_all[krow]
+        i2, a2 = io_all[kcol], ia_all[kcol]
+        K = pia[:, krow].T @ qia[:, kcol]
+        ou1, oinv1 = np.unique(i1, return_inverse=True)
+        ou2, oinv2 = np.unique(i2, return_inverse=True)
+        vu1, vinv1 = np.unique(a1, return_inverse=True)
+        vu2, vinv2 = np.unique(a2, return_inverse=True)
+        P = poo[:, ou1][:, :, ou2].reshape(ncent, -1)
+        Q = qvv[:, vu1][:, :, vu2].reshape(ncent, -1)
+        J4 = (P.T @ Q).reshape(len(ou1), len(ou2), len(vu1), len(vu2))
+        return ak * K - J4[oinv1[:, None], oinv2[None, :], vinv1[:, None], vinv2[None, :]]
+
+    # PT selection on a leading sample of candidates
+    t0 = time.perf_counter()
+    done, nsel = 0, 0
+    blk = max(1, int(2e6 // max(1, len(pk))))
+    while done < len(ck) and time.perf_counter() - t0 < 0.5 * budget_s:
+        kk = ck[done:done + blk]
+        amat = coupling(kk, pk)
+        pert = (amat ** 2 / (de_all[kk][:, None] - ed[None, :] + 1e-10)).sum(axis=1)
+        nsel += int((pert > p.thrp).sum())
+        done += len(kk)
+    t_pt = (time.perf_counter() - t0) * len(ck) / max(1, done)
+    nci = len(pk) + int(round(nsel * len(ck) / max(1, done)))
+    # A build on a row block of the primaries, scaled to nci^2
+    t0 = time.perf_counter()
+    rows = pk[:min(len(pk), 256)]
+    coupling(rows, pk)
+    t_a = (time.perf_counter() - t0) * (nci / max(1, len(rows))) * (nci / max(1, len(pk)))
+    # dense diagonalisation scaled as n^3
+    n_s = min(nci, 1500)
+    rng = np.random.default_rng(0)
+    Mx = rng.standard_normal((n_s, n_s))
+    Mx = Mx + Mx.T
+    t0 = time.perf_counter()
+    np.linalg.eigh(Mx)
+    t_eig = (time.perf_counter() - t0) * (nci / n_s) ** 3
+    est = t_setup + t_pt + t_a + t_eig
+    threads = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    sample = (f"full window/S^1/2/charges/screen ({t_setup:.1f}s); PT on {done} of {len(ck)} "
+              f"candidates x {len(pk)} primaries scaled linearly ({t_pt:.1f}s est.); A build "
+              f"{len(rows)} rows scaled to nci={nci} ({t_a:.1f}s est.); dense eigh {n_s}^3 "
+              f"scaled to nci^3 ({t_eig:.1f}s est.)")
+    return dict(est_total_s=est, setup_s=t_setup, pt_s=t_pt, a_s=t_a, eig_s=t_eig, nci=nci,
+                threads=threads, sample=sample)

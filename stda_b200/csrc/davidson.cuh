@@ -1,0 +1,202 @@
+// Blocked Davidson eigensolver for the lowest k roots of the sTDA matrix A.
+//
+// The reference diagonalises A completely with LAPACK ssyevr and keeps the
+// roots in (0, E_thr] (stda.f:1133-1150).  For large CSF spaces this engine
+// finds the requested lowest roots iteratively: sigma = A V products through a
+// caller-supplied operator (matrix-free, matfree.cuh), and an FP64
+// Rayleigh-Ritz projection, FP64 orthogonalisation (classical Gram-Schmidt,
+// applied twice) and FP64 residuals.  The preconditioner is the diagonal
+// (Davidson) one, (theta - A_ii)^-1.  A few buffer roots beyond the wanted
+// ones are carried along so that near-degeneracies at the edge of the wanted
+// set do not stall convergence.
+#pragma once
+
+#include <algorithm>
+#include <functional>
+#include <numeric>
+#include <vector>
+
+#include "common.cuh"
+
+namespace std2g {
+
+// T[:, j] = R[:, cols[j]] / (theta - diag), guarded away from zero
+__global__ void k_dav_precond(double *__restrict__ T, const double *__restrict__ R,
+                              const double *__restrict__ diag, const double *__restrict__ theta,
+                              const int *__restrict__ cols, int n, int nc) {
+  int64_t total = (int64_t)n * nc;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    int j = (int)(t / n), i = (int)(t - (int64_t)j * n);
+    int c = cols[j];
+    double d = theta[c] - diag[i];
+    if (fabs(d) < 1e-4) d = d < 0 ? -1e-4 : 1e-4;
+    T[t] = R[i + (int64_t)n * c] / d;
+  }
+}
+
+// R[:, j] -= theta_j X[:, j]; rnorm[j] = ||R[:, j]||  (one block per column)
+__global__ void k_dav_resid(double *__restrict__ R, const double *__restrict__ X,
+                            const double *__restrict__ theta, int n, double *__restrict__ rnorm) {
+  int j = blockIdx.x;
+  double th = theta[j];
+  double s = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    int64_t o = i + (int64_t)n * j;
+    double r = R[o] - th * X[o];
+    R[o] = r;
+    s += r * r;
+  }
+  __shared__ double red[256];
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) rnorm[j] = sqrt(red[0]);
+}
+
+// column norm of v (one block), result to out[0]
+__global__ void k_norm(const double *__restrict__ v, int n, double *__restrict__ out) {
+  double s = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) s += v[i] * v[i];
+  __shared__ double red[256];
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[0] = sqrt(red[0]);
+}
+
+__global__ void k_scale_vec(double *__restrict__ v, int n, const double *__restrict__ nrm) {
+  double f = 1.0 / nrm[0];
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) v[i] *= f;
+}
+
+__global__ void k_unit_vectors(double *__restrict__ V, int n, const int *__restrict__ idx, int k) {
+  int64_t total = (int64_t)n * k;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    int j = (int)(t / n), i = (int)(t - (int64_t)j * n);
+    V[t] = (i == idx[j]) ? 1.0 : 0.0;
+  }
+}
+
+struct DavidsonWork {
+  DBuf<double> V, W, Hs, theta, X, R, T, tmp, rn, proj;
+  DBuf<int> cols, idx, info;
+  DBuf<double> work;
+  int iters = 0;
+  int64_t matvecs = 0;
+  double max_resid = 0;
+};
+
+using MatVec = std::function<void(const double *V, int nb, double *W)>;
+
+// Returns the number of converged wanted roots (== k on success).  `mv` forms
+// W = A V for nb column vectors (n x nb, column-major); `diag` is diag(A).
+inline int davidson(DavidsonWork &dw, cublasHandle_t blas, cusolverDnHandle_t sol,
+                    cudaStream_t s, const MatVec &mv, const double *diag, int n, int k,
+                    double tol, int max_iter, double *omega_out, double *X_out) {
+  if (k > n) k = n;
+  const int kwant = k;
+  k = std::min(n, k + std::max(4, k / 2));
+  const int mmax = std::min(n, std::max(4 * k, k + 32));
+  const int grid = 148 * 4;
+  double *V = dw.V.ensure((size_t)n * mmax), *W = dw.W.ensure((size_t)n * mmax);
+  double *Hs = dw.Hs.ensure((size_t)mmax * mmax);
+  double *theta = dw.theta.ensure(mmax), *X = dw.X.ensure((size_t)n * k);
+  double *R = dw.R.ensure((size_t)n * k), *T = dw.T.ensure((size_t)n * k);
+  double *tmp = dw.tmp.ensure((size_t)n * k), *rn = dw.rn.ensure(k + 2);
+  double *proj = dw.proj.ensure((size_t)mmax + 4);
+  int *cols = dw.cols.ensure(k), *info = dw.info.ensure(1);
+  const double one = 1.0, zero = 0.0, mone = -1.0;
+
+  // initial guess: unit vectors on the k lowest diagonal elements
+  std::vector<double> h_diag(n);
+  S2G_CUDA(cudaMemcpyAsync(h_diag.data(), diag, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+  S2G_CUDA(cudaStreamSynchronize(s));
+  std::vector<int> order(n);
+  std::iota(order.begin(), order.end(), 0);
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return h_diag[a] < h_diag[b]; });
+  int *idx = dw.idx.ensure(k);
+  S2G_CUDA(cudaMemcpyAsync(idx, order.data(), sizeof(int) * k, cudaMemcpyHostToDevice, s));
+  S2G_LAUNCH(k_unit_vectors, grid, 256, 0, s, V, n, idx, k);
+  int m = 0, nb = k;
+  int lwork = 0;
+  S2G_CUSOLVER(cusolverDnDsyevd_bufferSize(sol, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER,
+                                           mmax, Hs, mmax, theta, &lwork));
+  double *work = dw.work.ensure((size_t)lwork + 1);
+  std::vector<double> h_rn(k);
+  int nconv = 0;
+  dw.iters = 0;
+  dw.matvecs = 0;
+  for (int it = 0; it < max_iter; ++it) {
+    dw.iters = it + 1;
+    mv(V + (size_t)n * m, nb, W + (size_t)n * m);
+    dw.matvecs += nb;
+    m += nb;
+    // H = V^T W (m x m), Ritz pairs in FP64
+    S2G_CUBLAS(cublasDgemm(blas, CUBLAS_OP_T, CUBLAS_OP_N, m, m, n, &one, V, n, W, n, &zero, Hs, m));
+    S2G_CUSOLVER(cusolverDnDsyevd(sol, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, m, Hs, m,
+                                  theta, work, lwork, info));
+    // Ritz vectors X = V Y_k, residuals R = W Y_k - X theta
+    S2G_CUBLAS(cublasDgemm(blas, CUBLAS_OP_N, CUBLAS_OP_N, n, k, m, &one, V, n, Hs, m, &zero, X, n));
+    S2G_CUBLAS(cublasDgemm(blas, CUBLAS_OP_N, CUBLAS_OP_N, n, k, m, &one, W, n, Hs, m, &zero, R, n));
+    S2G_LAUNCH(k_dav_resid, k, 256, 0, s, R, X, theta, n, rn);
+    S2G_CUDA(cudaMemcpyAsync(h_rn.data(), rn, sizeof(double) * k, cudaMemcpyDeviceToHost, s));
+    S2G_CUDA(cudaStreamSynchronize(s));
+    std::vector<int> unc;
+    int nunc_wanted = 0;
+    for (int j = 0; j < k; ++j)
+      if (!(h_rn[j] < tol)) {
+        unc.push_back(j);
+        if (j < kwant) ++nunc_wanted;
+      }
+    nconv = kwant - nunc_wanted;
+    dw.max_resid = *std::max_element(h_rn.begin(), h_rn.begin() + kwant);
+    if (nunc_wanted == 0) break;
+    int nc = (int)unc.size();
+    S2G_CUDA(cudaMemcpyAsync(cols, unc.data(), sizeof(int) * nc, cudaMemcpyHostToDevice, s));
+    S2G_LAUNCH(k_dav_precond, grid, 256, 0, s, T, R, diag, theta, cols, n, nc);
+    if (m + nc > mmax) {
+      // restart with the current Ritz vectors: V <- X, W <- W Y_k
+      S2G_CUBLAS(cublasDgemm(blas, CUBLAS_OP_N, CUBLAS_OP_N, n, k, m, &one, W, n, Hs, m, &zero,
+                             tmp, n));
+      S2G_CUDA(cudaMemcpyAsync(W, tmp, sizeof(double) * n * k, cudaMemcpyDeviceToDevice, s));
+      S2G_CUDA(cudaMemcpyAsync(V, X, sizeof(double) * n * k, cudaMemcpyDeviceToDevice, s));
+      m = k;
+    }
+    // normalise each correction, orthogonalise against V (CGS applied twice), append
+    nb = 0;
+    for (int j = 0; j < nc; ++j) {
+      double *t = T + (size_t)n * j;
+      S2G_LAUNCH(k_norm, 1, 256, 0, s, t, n, rn + k);
+      S2G_LAUNCH(k_scale_vec, 64, 256, 0, s, t, n, rn + k);
+      for (int pass = 0; pass < 2; ++pass) {
+        int mc = m + nb;
+        S2G_CUBLAS(cublasDgemv(blas, CUBLAS_OP_T, n, mc, &one, V, n, t, 1, &zero, proj, 1));
+        S2G_CUBLAS(cublasDgemv(blas, CUBLAS_OP_N, n, mc, &mone, V, n, proj, 1, &one, t, 1));
+      }
+      S2G_LAUNCH(k_norm, 1, 256, 0, s, t, n, rn + k);
+      double h_nrm = 0;
+      S2G_CUDA(cudaMemcpyAsync(&h_nrm, rn + k, sizeof(double), cudaMemcpyDeviceToHost, s));
+      S2G_CUDA(cudaStreamSynchronize(s));
+      if (!(h_nrm > 1e-6)) continue;   // linearly dependent on the current space
+      S2G_LAUNCH(k_scale_vec, 64, 256, 0, s, t, n, rn + k);
+      S2G_CUDA(cudaMemcpyAsync(V + (size_t)n * (m + nb), t, sizeof(double) * n,
+                               cudaMemcpyDeviceToDevice, s));
+      ++nb;
+    }
+    if (nb == 0) break;
+  }
+  S2G_CUDA(cudaMemcpyAsync(omega_out, theta, sizeof(double) * kwant, cudaMemcpyDeviceToDevice, s));
+  S2G_CUDA(cudaMemcpyAsync(X_out, X, sizeof(double) * n * kwant, cudaMemcpyDeviceToDevice, s));
+  S2G_CUDA(cudaStreamSynchronize(s));
+  return nconv;
+}
+
+}  // namespace std2g

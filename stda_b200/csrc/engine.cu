@@ -18,6 +18,8 @@
 
 #include "common.cuh"
 #include "kernels_fp64.cuh"
+#include "davidson.cuh"
+#include "matfree.cuh"
 #include "mixed.cuh"
 
 namespace std2g {
@@ -58,7 +60,8 @@ struct Ctx {
   std::vector<double> h_eps, h_occ, h_xyz;
   // device inputs
   DBuf<double> d_xyz, d_C, d_eps_act, d_eta, d_Sfull, d_sqrtS, d_ao9;
-  DBuf<int> d_ao_ptr, d_ao_list, d_iaoat;
+  DBuf<int> d_ao_ptr, d_ao_list, d_iaoat, d_slot_ao;
+  int maxa = 1;
   bool sqrtS_ready = false;
   // work buffers
   DBuf<double> w_Cact, w_Clow, w_T, w_mu_ov, w_gj, w_gk, w_Qii, w_Qaa, w_Pii, w_uci;
@@ -74,6 +77,13 @@ struct Ctx {
   DBuf<int> w_info;
   DBuf<char> w_cub;
   MixedWork mixed;
+  DavidsonWork dav;
+  MatFree mf;
+  // tensor-core contraction statistics of the last solve
+  double tc_ms = 0, tc_flop = 0;
+  int64_t tc_launches = 0;
+  int dav_iters = 0;
+  int64_t dav_matvecs = 0;
   // last results
   int last_nci = 0, last_nroot = 0, last_no = 0, last_nv = 0;
   bool last_rpa = false;
@@ -99,7 +109,12 @@ static void record(Ctx &c, int ph) { S2G_CUDA(cudaEventRecord(c.ev[ph], c.stream
 // Dense symmetric eigen-decomposition with an eigenvalue window (vl, vu]
 // (ssyevr 'V' range, stda.f:1143-1147) or the lowest k (range 'I').
 // A (n x n) is overwritten by the eigenvectors; returns the number found.
+static void dense_eig_full(Ctx &c, double *A, int n, double *w);
 static int dense_eig(Ctx &c, double *A, int n, double vl, double vu, int kmax, double *w) {
+  if (kmax > 0) {   // lowest kmax roots: full decomposition, eigenvectors in the leading columns
+    dense_eig_full(c, A, n, w);
+    return std::min(kmax, n);
+  }
   int meig = 0, lwork = 0;
   cusolverEigRange_t range = kmax > 0 ? CUSOLVER_EIG_RANGE_I : CUSOLVER_EIG_RANGE_V;
   int il = 1, iu = kmax > 0 ? std::min(kmax, n) : n;
@@ -181,8 +196,16 @@ static void load(Ctx &c, int ncent, int nmo, int nao, const double *xyz, const d
   for (int a = 0; a < ncent; ++a) ptr[a + 1] = ptr[a] + cnt[a];
   std::vector<int> fill(ptr.begin(), ptr.end() - 1);
   for (int k = 0; k < nao; ++k) list[fill[iaoat[k] - 1]++] = k;
+  int maxa = 1;
+  for (int a = 0; a < ncent; ++a) maxa = std::max(maxa, cnt[a]);
+  std::vector<int> slot((size_t)ncent * maxa, -1);
+  for (int a = 0; a < ncent; ++a)
+    for (int q = 0; q < cnt[a]; ++q) slot[(size_t)a * maxa + q] = list[ptr[a] + q];
+  c.maxa = maxa;
   size_t npk = (size_t)nao * (nao + 1) / 2;
   cudaStream_t s = c.stream;
+  S2G_CUDA(cudaMemcpyAsync(c.d_slot_ao.ensure(slot.size()), slot.data(), sizeof(int) * slot.size(),
+                           cudaMemcpyHostToDevice, s));
   S2G_CUDA(cudaMemcpyAsync(c.d_xyz.ensure(4 * ncent), xyz, sizeof(double) * 4 * ncent,
                            cudaMemcpyHostToDevice, s));
   S2G_CUDA(cudaMemcpyAsync(c.d_eta.ensure(ncent), eta.data(), sizeof(double) * ncent,
@@ -301,6 +324,11 @@ static void solve(Ctx &c, const std2g_params &p_in, std2g_result *res, const Res
   cudaStream_t s = c.stream;
   const int N = c.ncent, nao = c.nao;
   const bool mixed = c.opts.precision == 1;
+  c.tc_ms = 0;
+  c.tc_flop = 0;
+  c.tc_launches = 0;
+  c.dav_iters = 0;
+  c.dav_matvecs = 0;
   record(c, PH_SETUP);
   const double thr = p.e_thr_ev / kEh2eV_in;
   const double fthr = p.fthr_ev < 1.79e308 ? p.fthr_ev / kEh2eV_in : INFINITY;
@@ -449,11 +477,19 @@ static void solve(Ctx &c, const std2g_params &p_in, std2g_result *res, const Res
   std::vector<int> newk;
   std::vector<double> ed_lowered(ed);
   if (nexpt > 0) {
+    // The PT kernels see the primaries in (j,b) enumeration order so that
+    // their couplings are read contiguously; pt2 is mapped back to the
+    // energy order afterwards.
+    const std::vector<int> &pko = pk_unsorted;
+    std::vector<int> kpos(nov, -1);
+    for (int q = 0; q < nex; ++q) kpos[pk[q]] = q;
+    std::vector<double> edo(nex);
+    for (int q = 0; q < nex; ++q) edo[q] = ed[kpos[pko[q]]];
     // occupied / virtual sets spanned by the primaries
     std::vector<int> omap(no, -1), vmap(nv, -1), OP, VP, pj(nex), pb(nex);
     for (int q = 0; q < nex; ++q) {
-      pj[q] = pk[q] / nv;
-      pb[q] = pk[q] % nv;
+      pj[q] = pko[q] / nv;
+      pb[q] = pko[q] % nv;
       omap[pj[q]] = 1;
       vmap[pb[q]] = 1;
     }
@@ -467,11 +503,11 @@ static void solve(Ctx &c, const std2g_params &p_in, std2g_result *res, const Res
       S2G_CUDA(cudaMemcpyAsync(d, v.data(), sizeof(int) * v.size(), cudaMemcpyHostToDevice, s));
       return d;
     };
-    int *d_pk = up(c.w_pk, pk), *d_ck = up(c.w_ck, ck), *d_pj = up(c.w_pj, pj),
+    int *d_pk = up(c.w_pk, pko), *d_ck = up(c.w_ck, ck), *d_pj = up(c.w_pj, pj),
         *d_pb = up(c.w_pb, pb), *d_omap = up(c.w_omap, omap), *d_vmap = up(c.w_vmap, vmap),
         *d_OP = up(c.w_OP, OP), *d_VP = up(c.w_VP, VP);
     double *d_ed = c.w_edsorted.ensure(nex);
-    S2G_CUDA(cudaMemcpyAsync(d_ed, ed.data(), sizeof(double) * nex, cudaMemcpyHostToDevice, s));
+    S2G_CUDA(cudaMemcpyAsync(d_ed, edo.data(), sizeof(double) * nex, cudaMemcpyHostToDevice, s));
     // primaries' charges and the virtual-pair factor
     double *Qp = c.w_Qp.ensure((size_t)N * nex);
     S2G_LAUNCH(k_gather_cols, grid_for((int64_t)N * nex), 256, 0, s, Qp, Qia, (int64_t)N, d_pk,
@@ -482,7 +518,8 @@ static void solve(Ctx &c, const std2g_params &p_in, std2g_result *res, const Res
     // chunk candidates by occupied index (candidates are in (i,a) order)
     const int64_t ldj = (int64_t)nv * nvp;
     const double budget = 6.0e9;   // bytes of K/J buffers per chunk
-    const double per_occ = 8.0 * ((double)nex * nv + (double)ldj * nop + (double)N * (nv + nop));
+    const double per_occ = (mixed ? 4.0 : 8.0) * ((double)nex * nv + (double)ldj * nop) +
+                           8.0 * (double)N * (nv + nop) + (mixed ? 4.0 * 64 * (nv + nop) : 0.0);
     int occ_chunk = std::max(1, (int)std::min<double>(no, budget / per_occ));
     std::vector<int> first_of_occ(no + 1, nexpt);
     {
@@ -491,6 +528,13 @@ static void solve(Ctx &c, const std2g_params &p_in, std2g_result *res, const Res
         while (q < nexpt && ck[q] / nv < i) ++q;
         first_of_occ[i] = q;
       }
+    }
+    bool mixed_ready = false;
+    if (mixed) {
+      c.mixed.tc.ms = 0;
+      c.mixed.tc.flop = 0;
+      c.mixed.tc.launches = 0;
+      c.mixed.rechecked = 0;
     }
     int nchunk = (int)div_up(no, occ_chunk);
     double *colpart = c.w_colpart.ensure((size_t)nchunk * nex);
@@ -515,23 +559,27 @@ static void solve(Ctx &c, const std2g_params &p_in, std2g_result *res, const Res
         gemm(c, CUBLAS_OP_T, CUBLAS_OP_N, nex, nr, N, 1.0, Qp, N, Pc, N, 0.0, Kb, nex);
         gemm(c, CUBLAS_OP_T, CUBLAS_OP_N, (int)ldj, ni * nop, N, 1.0, QvvP, N, W, N, 0.0, Jb,
              (int)ldj);
-        S2G_LAUNCH((k_pt_rows<double, double>), nr, 256, 0, s, Kb, Jb, ldj, nex, nvp, nop, nr,
-                   d_ck + r0, nv, i0, de, d_pj, d_pb, d_omap, d_vmap, d_ed, ak, p.thrp,
-                   pert + r0, sel + r0);
+        S2G_LAUNCH((k_pt_rows<double, double>), nr, 256, 0, s, Kb, Jb, ldj, (int64_t)nex, nex,
+                   nvp, nop, nr, d_ck + r0, nv, i0, de, d_pj, d_pb, d_omap, d_vmap, d_ed, ak,
+                   p.thrp, pert + r0, sel + r0);
         S2G_LAUNCH((k_pt_cols<double, double>), (int)div_up(nex, 128), 128, 0, s, Kb, Jb, ldj,
-                   nex, nvp, nop, nr, d_ck + r0, nv, i0, de, d_pj, d_pb, d_omap, d_vmap, d_ed, ak,
-                   sel + r0, colpart + (size_t)q * nex);
+                   (int64_t)nex, nex, nvp, nop, nr, d_ck + r0, nv, i0, de, d_pj, d_pb, d_omap,
+                   d_vmap, d_ed, ak, sel + r0, colpart + (size_t)q * nex);
       } else {
-        mixed_pt_chunk(c.mixed, s, Qp, Pc, QvvP, W, N, nex, nr, (int)ldj, ni * nop);
-        S2G_LAUNCH((k_pt_rows<float, float>), nr, 256, 0, s, c.mixed.K.get(), c.mixed.J.get(),
-                   ldj, nex, nvp, nop, nr, d_ck + r0, nv, i0, de, d_pj, d_pb, d_omap, d_vmap,
-                   d_ed, ak, p.thrp, pert + r0, sel + r0);
-        // rows whose PT sum lies near the threshold are decided in FP64
-        mixed_pt_recheck(c.mixed, s, pert + r0, sel + r0, nr, p.thrp, Qp, Pc, QvvP, W, N, nex,
-                         (int)ldj, ni * nop, d_ck + r0, nv, i0, de, d_pj, d_pb, d_omap, d_vmap,
-                         d_ed, ak, nvp, nop);
-        S2G_LAUNCH((k_pt_cols<float, float>), (int)div_up(nex, 128), 128, 0, s, c.mixed.K.get(),
-                   c.mixed.J.get(), ldj, nex, nvp, nop, nr, d_ck + r0, nv, i0, de, d_pj, d_pb,
+        if (!mixed_ready) {
+          mixed_pt_prepare(c.mixed, s, Qp, QvvP, N, nex, ldj);
+          mixed_ready = true;
+        }
+        mixed_pt_chunk(c.mixed, s, Pc, W, N, nex, nr, ldj, ni * nop);
+        const float *Kf = c.mixed.K.get(), *Jf = c.mixed.J.get();
+        S2G_LAUNCH((k_pt_rows<float, float>), nr, 256, 0, s, Kf, Jf, c.mixed.ldJ, c.mixed.ldK, nex,
+                   nvp, nop, nr, d_ck + r0, nv, i0, de, d_pj, d_pb, d_omap, d_vmap, d_ed, ak,
+                   p.thrp, pert + r0, sel + r0);
+        // candidates whose PT sum lies near the threshold are decided in FP64
+        mixed_pt_recheck(c.mixed, s, pert + r0, sel + r0, nr, p.thrp, d_ck + r0, d_pk, nex, Pia,
+                         Qia, Poo, Qvv, N, no, nv, de, d_ed, ak);
+        S2G_LAUNCH((k_pt_cols<float, float>), (int)div_up(nex, 128), 128, 0, s, Kf, Jf,
+                   c.mixed.ldJ, c.mixed.ldK, nex, nvp, nop, nr, d_ck + r0, nv, i0, de, d_pj, d_pb,
                    d_omap, d_vmap, d_ed, ak, sel + r0, colpart + (size_t)q * nex);
       }
     }
@@ -539,10 +587,16 @@ static void solve(Ctx &c, const std2g_params &p_in, std2g_result *res, const Res
     S2G_LAUNCH(k_pt2_finish, (int)div_up(nex, 128), 128, 0, s, colpart, nchunk, nex, d_ed, pt2,
                edp);
     std::vector<unsigned char> h_sel(nexpt);
+    std::vector<double> h_edp(nex);
     S2G_CUDA(cudaMemcpyAsync(h_sel.data(), sel, nexpt, cudaMemcpyDeviceToHost, s));
-    S2G_CUDA(cudaMemcpyAsync(ed_lowered.data(), edp, sizeof(double) * nex, cudaMemcpyDeviceToHost,
-                             s));
+    S2G_CUDA(cudaMemcpyAsync(h_edp.data(), edp, sizeof(double) * nex, cudaMemcpyDeviceToHost, s));
     S2G_CUDA(cudaStreamSynchronize(s));
+    for (int q = 0; q < nex; ++q) ed_lowered[kpos[pko[q]]] = h_edp[q];
+    if (mixed) {
+      c.tc_ms = c.mixed.tc.ms;
+      c.tc_flop = c.mixed.tc.flop;
+      c.tc_launches = c.mixed.tc.launches;
+    }
     for (int q = 0; q < nexpt; ++q)
       if (h_sel[q]) newk.push_back(ck[q]);
   }
@@ -587,21 +641,68 @@ static void solve(Ctx &c, const std2g_params &p_in, std2g_result *res, const Res
   double *ekd = c.w_tmp.ensure(std::max<size_t>(nci, (size_t)2 * nao * nao));
   S2G_LAUNCH(k_gather_cols, grid_for(nci), 256, 0, s, ekd, ek, (int64_t)1, d_allk, (int64_t)nci,
              (int64_t)1);
-  double *K = c.w_K.ensure(n2), *J = c.w_J.ensure(n2);
-  gemm(c, CUBLAS_OP_T, CUBLAS_OP_N, nci, nci, N, 1.0, Ps, N, Qs, N, 0.0, K, nci);
-  S2G_LAUNCH(k_pairdot, grid_for(n2 * 32), 256, 0, s, J, (int64_t)nci, d_ci, d_ca, nci, Poo, Qvv,
-             N, no, nv, 0);
-  const bool need_kx = p.rpa || p.velcorr;
-  double *Kx = nullptr;
-  if (need_kx) {
-    Kx = c.w_Kx.ensure(n2);
-    S2G_LAUNCH(k_pairdot, grid_for(n2 * 32), 256, 0, s, Kx, (int64_t)nci, d_ci, d_ca, nci, Pia,
-               Qia, N, no, nv, 1);
+  // Large TDA problems with a root count use the matrix-free operators and the
+  // blocked Davidson solver; everything else builds the matrices explicitly.
+  const bool use_mf = !p.rpa && p.nroots > 0 && (p.solver == 2 || (p.solver == 0 && nci > 1024));
+  double *K = nullptr, *J = nullptr, *Kx = nullptr;
+  if (!use_mf) {
+    K = c.w_K.ensure(n2);
+    J = c.w_J.ensure(n2);
+    gemm(c, CUBLAS_OP_T, CUBLAS_OP_N, nci, nci, N, 1.0, Ps, N, Qs, N, 0.0, K, nci);
+    S2G_LAUNCH(k_pairdot, grid_for(n2 * 32), 256, 0, s, J, (int64_t)nci, d_ci, d_ca, nci, Poo,
+               Qvv, N, no, nv, 0);
+    if (p.rpa || p.velcorr) {
+      Kx = c.w_Kx.ensure(n2);
+      S2G_LAUNCH(k_pairdot, grid_for(n2 * 32), 256, 0, s, Kx, (int64_t)nci, d_ci, d_ca, nci, Pia,
+                 Qia, N, no, nv, 1);
+    }
+  } else {
+    // matrix-free operators (matfree.cuh): padded Loewdin MOs, atom-major P
+    MatFree &mf = c.mf;
+    mf.N = N;
+    mf.maxa = c.maxa;
+    mf.no = no;
+    mf.nv = nv;
+    mf.nci = nci;
+    mf.nao = nao;
+    const int rows = N * c.maxa;
+    S2G_LAUNCH(k_mf_pad_rows, grid_for((int64_t)rows * nv), 256, 0, s,
+               mf.CvP.ensure((size_t)rows * nv), Clow, nao, c.d_slot_ao.get(), rows, no, nv);
+    S2G_LAUNCH(k_mf_pad_rows, grid_for((int64_t)rows * no), 256, 0, s,
+               mf.CoP.ensure((size_t)rows * no), Clow, nao, c.d_slot_ao.get(), rows, 0, no);
+    S2G_LAUNCH(k_pair_to_atom_major, grid_for((int64_t)N * no * no), 256, 0, s,
+               mf.PooA.ensure((size_t)N * no * no), Poo, N, no, no);
+    if (p.velcorr)
+      S2G_LAUNCH(k_pair_to_atom_major, grid_for((int64_t)N * nov), 256, 0, s,
+                 mf.PovA.ensure((size_t)N * nov), Pia, N, no, nv);
+    mf.Qs = Qs;
+    mf.Ps = Ps;
+    mf.ci = d_ci;
+    mf.ca = d_ca;
+    S2G_LAUNCH(k_mf_diag, (int)div_up(nci, 128), 128, 0, s, mf.dA.ensure(nci), d_edall, ekd, uci,
+               d_ci, d_ca, nci, nv, ak);
   }
   int nroot = 0;
   double *X = nullptr, *Yv = nullptr, *om = nullptr;
   double *Bh = nullptr;
-  if (!p.rpa) {
+  if (!p.rpa && use_mf) {
+    record(c, PH_EIGEN);
+    om = c.w_eval.ensure(std::max(nci, nao));
+    const double tol = p.conv_tol > 0 ? p.conv_tol : 1e-6;
+    double *Xd = c.w_X.ensure((size_t)nci * p.nroots);
+    MatVec mv = [&](const double *V, int nb, double *W) {
+      mf_apply(c.mf, c.blas, s, V, nb, W, ak, -1.0, 0.0, c.mf.dA.get());
+    };
+    int conv = davidson(c.dav, c.blas, c.solver, s, mv, d_edall, nci, p.nroots, tol, 300, om, Xd);
+    c.dav_iters = c.dav.iters;
+    c.dav_matvecs = c.dav.matvecs;
+    if (conv < std::min(p.nroots, nci))
+      throw Error{STD2G_ENOCONV, "Davidson: " + std::to_string(conv) + " of " +
+                                     std::to_string(p.nroots) + " roots converged"};
+    nroot = std::min(p.nroots, nci);
+    X = Xd;
+    c.mixed.lastX = X;
+  } else if (!p.rpa) {
     double *A = c.w_A.ensure(n2);
     S2G_LAUNCH(k_combine_tda, grid_for(n2), 256, 0, s, A, K, J, (int64_t)nci, ak, d_edall);
     if (p.velcorr) {
@@ -611,14 +712,9 @@ static void solve(Ctx &c, const std2g_params &p_in, std2g_result *res, const Res
     }
     record(c, PH_EIGEN);
     om = c.w_eval.ensure(std::max(nci, nao));
-    if (mixed && p.nroots > 0 && nci > 256) {
-      nroot = mixed_davidson(c.mixed, c.blas, s, A, nci, p.nroots, p.conv_tol, om,
-                             c.w_X.ensure((size_t)nci * p.nroots));
-      X = c.w_X.get();
-    } else {
-      nroot = dense_eig(c, A, nci, 0.0, thr, p.nroots, om);
-      X = A;
-    }
+    nroot = dense_eig(c, A, nci, 0.0, thr, p.nroots, om);
+    X = A;
+    c.mixed.lastX = X;
     if (nroot < 1) throw Error{STD2G_ENOROOT, "no root below the energy threshold"};
   } else {
     double *Apb = c.w_Apb.ensure(n2), *Amb = c.w_Amb.ensure(n2);
@@ -707,7 +803,10 @@ static void solve(Ctx &c, const std2g_params &p_in, std2g_result *res, const Res
     if (p.velcorr) {
       // X_new = (B/2) X / w (apbtrafo.f:51-65)
       double *Xn = c.w_Y.ensure((size_t)nci * nroot);
-      gemm(c, CUBLAS_OP_N, CUBLAS_OP_N, nci, nroot, nci, 1.0, Bh, nci, X, nci, 0.0, Xn, nci);
+      if (use_mf)
+        mf_apply(c.mf, c.blas, s, X, nroot, Xn, 0.5 * ak, 0.0, -0.5 * p.ax, nullptr);
+      else
+        gemm(c, CUBLAS_OP_N, CUBLAS_OP_N, nci, nroot, nci, 1.0, Bh, nci, X, nci, 0.0, Xn, nci);
       S2G_LAUNCH(k_scale_columns, grid_for((int64_t)nci * nroot), 256, 0, s, Xn, (int64_t)nci,
                  nroot, om, 2);
       T2 = c.w_T2.ensure((size_t)nroot * 9);
@@ -885,7 +984,7 @@ int std2g_get_vectors(void *ctx, double *X, double *Y, int cap, int *nroot, int 
     if (c->last_nci == 0) throw Error{STD2G_ESTATE, "no solve yet"};
     if (cap < c->last_nroot) throw Error{STD2G_ECAP, "capacity too small"};
     size_t bytes = sizeof(double) * (size_t)c->last_nci * c->last_nroot;
-    const double *src = c->last_rpa ? c->w_X.get() : c->mixed.lastX ? c->mixed.lastX : c->w_A.get();
+    const double *src = c->last_rpa ? c->w_X.get() : c->mixed.lastX;
     if (X) S2G_CUDA(cudaMemcpy(X, src, bytes, cudaMemcpyDeviceToHost));
     if (Y && c->last_rpa) S2G_CUDA(cudaMemcpy(Y, c->w_Y.get(), bytes, cudaMemcpyDeviceToHost));
   });
@@ -904,6 +1003,23 @@ const char *std2g_phase_name(int q) {
 }
 
 int64_t std2g_kernel_launches(void *) { return std2g::g_launches; }
+
+int std2g_kernel_stats(void *ctx, double *ms, int64_t *launches, double *flop) {
+  if (!ctx) return STD2G_EINVAL;
+  auto *c = (Ctx *)ctx;
+  if (ms) *ms = c->tc_ms;
+  if (launches) *launches = c->tc_launches;
+  if (flop) *flop = c->tc_flop;
+  return STD2G_OK;
+}
+
+int std2g_solver_stats(void *ctx, int *iters, int64_t *matvecs) {
+  if (!ctx) return STD2G_EINVAL;
+  auto *c = (Ctx *)ctx;
+  if (iters) *iters = c->dav_iters;
+  if (matvecs) *matvecs = c->dav_matvecs;
+  return STD2G_OK;
+}
 
 const char *std2g_error_string(int status) {
   switch (status) {

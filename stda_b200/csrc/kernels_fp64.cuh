@@ -188,12 +188,12 @@ __global__ void k_gather_virt_pairs(double *__restrict__ V, const double *__rest
 //   amat = ak*(ia|jb) - (ij|ab),  pt = amat^2 / (E_k - E_j + 1e-10)
 // K: Kbuf[c + nex*r]; J: Jbuf[(a*nvp + vmap[b]) + ldj*((i-i0)*nop + omap[j])]
 template <typename TK, typename TJ>
-__device__ __forceinline__ double pt_term(const TK *Kbuf, const TJ *Jbuf, int64_t ldj, int nex,
+__device__ __forceinline__ double pt_term(const TK *Kbuf, const TJ *Jbuf, int64_t ldj, int64_t ldk,
                                           int nvp, int nop, int r, int c, int iloc, int a,
                                           double de_r, const int *pj, const int *pb,
                                           const int *omap, const int *vmap,
                                           const double *ed, double ak) {
-  double kv = (double)Kbuf[(int64_t)c + (int64_t)nex * r];
+  double kv = (double)Kbuf[(int64_t)c + ldk * r];
   double jv = (double)Jbuf[((int64_t)a * nvp + vmap[pb[c]]) +
                            ldj * ((int64_t)iloc * nop + omap[pj[c]])];
   double amat = ak * kv - jv;
@@ -203,7 +203,7 @@ __device__ __forceinline__ double pt_term(const TK *Kbuf, const TJ *Jbuf, int64_
 // Row pass: pert[r] = sum_j pt(r, j) and the selection pert > thrp.
 template <typename TK, typename TJ>
 __global__ void k_pt_rows(const TK *__restrict__ Kbuf, const TJ *__restrict__ Jbuf, int64_t ldj,
-                          int nex, int nvp, int nop, int nrows, const int *__restrict__ cand_k,
+                          int64_t ldk, int nex, int nvp, int nop, int nrows, const int *__restrict__ cand_k,
                           int nv, int i0, const double *__restrict__ de_all,
                           const int *__restrict__ pj, const int *__restrict__ pb,
                           const int *__restrict__ omap, const int *__restrict__ vmap,
@@ -216,7 +216,7 @@ __global__ void k_pt_rows(const TK *__restrict__ Kbuf, const TJ *__restrict__ Jb
   double de_r = de_all[k];
   double s = 0.0;
   for (int c = threadIdx.x; c < nex; c += blockDim.x)
-    s += pt_term(Kbuf, Jbuf, ldj, nex, nvp, nop, r, c, i - i0, a, de_r, pj, pb, omap, vmap, ed, ak);
+    s += pt_term(Kbuf, Jbuf, ldj, ldk, nvp, nop, r, c, i - i0, a, de_r, pj, pb, omap, vmap, ed, ak);
   __shared__ double red[256];
   red[threadIdx.x] = s;
   __syncthreads();
@@ -233,7 +233,7 @@ __global__ void k_pt_rows(const TK *__restrict__ Kbuf, const TJ *__restrict__ Jb
 // Column pass: colpart[c] = sum over non-selected rows r (in order) of pt(r, c).
 template <typename TK, typename TJ>
 __global__ void k_pt_cols(const TK *__restrict__ Kbuf, const TJ *__restrict__ Jbuf, int64_t ldj,
-                          int nex, int nvp, int nop, int nrows, const int *__restrict__ cand_k,
+                          int64_t ldk, int nex, int nvp, int nop, int nrows, const int *__restrict__ cand_k,
                           int nv, int i0, const double *__restrict__ de_all,
                           const int *__restrict__ pj, const int *__restrict__ pb,
                           const int *__restrict__ omap, const int *__restrict__ vmap,
@@ -246,7 +246,7 @@ __global__ void k_pt_cols(const TK *__restrict__ Kbuf, const TJ *__restrict__ Jb
     if (sel[r]) continue;
     int k = cand_k[r];
     int i = k / nv, a = k - i * nv;
-    s += pt_term(Kbuf, Jbuf, ldj, nex, nvp, nop, r, c, i - i0, a, de_all[k], pj, pb, omap, vmap,
+    s += pt_term(Kbuf, Jbuf, ldj, ldk, nvp, nop, r, c, i - i0, a, de_all[k], pj, pb, omap, vmap,
                  ed, ak);
   }
   colpart[c] = s;

@@ -1,30 +1,143 @@
-// Mixed-precision form of the contractions (declarations; filled in by the
-// tensor-core kernels).
+// Mixed-precision form of the PT-selection contractions.
+//
+// The two coupling contractions of ptselect (stda.f:1812-1819) run on the
+// tensor cores with split-BF16 operands (tc_gemm.cuh) into FP32 buffers; the
+// selection decision of every candidate whose PT sum lies within a relative
+// band of the threshold is re-made in FP64 (k_pt_recheck), so the selected CSF
+// set is the one the FP64 arithmetic gives.
 #pragma once
 
+#include <cmath>
+#include <vector>
+
 #include "common.cuh"
+#include "tc_gemm.cuh"
 
 namespace std2g {
 
+constexpr double kRecheckBand = 2e-3;   // relative band around thrp decided in FP64
+
 struct MixedWork {
+  TcGemm tc;
+  DBuf<__nv_bfloat16> bq_hi, bq_lo, bv_hi, bv_lo, a_hi, a_lo, w_hi, w_lo;
   DBuf<float> K, J;
+  DBuf<int> recheck;
   double *lastX = nullptr;
+  int Kpad = 0;
+  int64_t ldK = 0, ldJ = 0;
+  int64_t rechecked = 0;
 };
 
-inline void mixed_pt_chunk(MixedWork &, cudaStream_t, const double *, const double *,
-                           const double *, const double *, int, int, int, int, int) {
-  throw Error{STD2G_EINVAL, "mixed form not available in this build"};
+inline int64_t round_up4(int64_t x) { return (x + 3) / 4 * 4; }
+
+inline void split_operand(MixedWork &mw, cudaStream_t s, DBuf<__nv_bfloat16> &h,
+                          DBuf<__nv_bfloat16> &l, const double *src, int N, int64_t ncols) {
+  const int Kp = mw.Kpad;
+  __nv_bfloat16 *ph = h.ensure((size_t)ncols * Kp), *pl = l.ensure((size_t)ncols * Kp);
+  int64_t tot = ncols * Kp;
+  int g = (int)std::min<int64_t>(div_up(tot, 256), 148 * 32);
+  S2G_LAUNCH(k_split_bf16, g, 256, 0, s, ph, pl, src, (int64_t)N, (const int *)nullptr, ncols, N,
+             Kp);
 }
-inline void mixed_pt_recheck(MixedWork &, cudaStream_t, double *, unsigned char *, int, double,
-                             const double *, const double *, const double *, const double *, int,
-                             int, int, int, const int *, int, int, const double *, const int *,
-                             const int *, const int *, const int *, const double *, double, int,
-                             int) {
-  throw Error{STD2G_EINVAL, "mixed form not available in this build"};
+
+// B operands of the PT contractions, once per solve: primaries' q (nex x N)
+// and the virtual-pair factor q_ab for b in the primaries' virtual set.
+inline void mixed_pt_prepare(MixedWork &mw, cudaStream_t s, const double *Qp, const double *QvvP,
+                             int N, int nex, int64_t nvcols) {
+  mw.Kpad = (int)div_up(N, 64) * 64;
+  split_operand(mw, s, mw.bq_hi, mw.bq_lo, Qp, N, nex);
+  split_operand(mw, s, mw.bv_hi, mw.bv_lo, QvvP, N, nvcols);
+  mw.ldK = round_up4(nex);
+  mw.ldJ = round_up4(nvcols);
 }
-inline int mixed_davidson(MixedWork &, cublasHandle_t, cudaStream_t, const double *, int, int,
-                          double, double *, double *) {
-  throw Error{STD2G_EINVAL, "mixed form not available in this build"};
+
+// One candidate chunk: K[r, c] = p_r . q_c  (nr x nex) and the J box
+// J[(i,j), (a,b)] = p_ij . q_ab  ((ni*nop) x (nv*nvp)).
+inline void mixed_pt_chunk(MixedWork &mw, cudaStream_t s, const double *Pc, const double *W, int N,
+                           int nex, int nr, int64_t nvcols, int nwcols) {
+  const int Kp = mw.Kpad;
+  split_operand(mw, s, mw.a_hi, mw.a_lo, Pc, N, nr);
+  split_operand(mw, s, mw.w_hi, mw.w_lo, W, N, nwcols);
+  float *K = mw.K.ensure((size_t)nr * mw.ldK);
+  float *J = mw.J.ensure((size_t)nwcols * mw.ldJ);
+  const int maxrows = 65535 * tc::BM;   // grid y extent of one launch
+  for (int r0 = 0; r0 < nr; r0 += maxrows) {
+    int rr = std::min(maxrows, nr - r0);
+    mw.tc.run(s, mw.a_hi.get() + (size_t)r0 * Kp, mw.a_lo.get() + (size_t)r0 * Kp, mw.bq_hi.get(),
+              mw.bq_lo.get(), rr, nex, Kp, K + (size_t)r0 * mw.ldK, mw.ldK,
+              2.0 * rr * (double)nex * N);
+  }
+  for (int r0 = 0; r0 < nwcols; r0 += maxrows) {
+    int rr = std::min(maxrows, nwcols - r0);
+    mw.tc.run(s, mw.w_hi.get() + (size_t)r0 * Kp, mw.w_lo.get() + (size_t)r0 * Kp, mw.bv_hi.get(),
+              mw.bv_lo.get(), rr, (int)nvcols, Kp, J + (size_t)r0 * mw.ldJ, mw.ldJ,
+              2.0 * rr * (double)nvcols * N);
+  }
+}
+
+// FP64 PT sum for candidate rows near the threshold (ptselect stda.f:1805-1834),
+// one block per row, couplings as gathered FP64 dot products over atoms.
+__global__ void k_pt_recheck(const int *__restrict__ rows, int nrc, const int *__restrict__ cand_k,
+                             const int *__restrict__ pk, int nex, const double *__restrict__ Pia,
+                             const double *__restrict__ Qia, const double *__restrict__ Poo,
+                             const double *__restrict__ Qvv, int N, int no, int nv,
+                             const double *__restrict__ de_all, const double *__restrict__ ed,
+                             double ak, double thrp, double *__restrict__ pert_out,
+                             unsigned char *__restrict__ sel) {
+  int q = blockIdx.x;
+  if (q >= nrc) return;
+  int r = rows[q];
+  int k = cand_k[r];
+  int i = k / nv, a = k - i * nv;
+  double de_r = de_all[k];
+  double s = 0.0;
+  const double *pr = Pia + (int64_t)N * k;
+  for (int c = threadIdx.x; c < nex; c += blockDim.x) {
+    int kc = pk[c];
+    int j = kc / nv, b = kc - j * nv;
+    const double *qc = Qia + (int64_t)N * kc;
+    const double *pij = Poo + (int64_t)N * ((int64_t)i * no + j);
+    const double *qab = Qvv + (int64_t)N * ((int64_t)a * nv + b);
+    double kv = 0.0, jv = 0.0;
+    for (int A = 0; A < N; ++A) {
+      kv += pr[A] * qc[A];
+      jv += pij[A] * qab[A];
+    }
+    double amat = ak * kv - jv;
+    s += amat * amat / (de_r - ed[c] + 1e-10);
+  }
+  __shared__ double red[256];
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    pert_out[r] = red[0];
+    sel[r] = red[0] > thrp ? 1 : 0;
+  }
+}
+
+// Rows whose mixed-precision PT sum lies within kRecheckBand of thrp get their
+// decision from FP64 arithmetic.
+inline void mixed_pt_recheck(MixedWork &mw, cudaStream_t s, double *pert, unsigned char *sel,
+                             int nr, double thrp, const int *cand_k, const int *pk, int nex,
+                             const double *Pia, const double *Qia, const double *Poo,
+                             const double *Qvv, int N, int no, int nv, const double *de_all,
+                             const double *ed, double ak) {
+  std::vector<double> h(nr);
+  S2G_CUDA(cudaMemcpyAsync(h.data(), pert, sizeof(double) * nr, cudaMemcpyDeviceToHost, s));
+  S2G_CUDA(cudaStreamSynchronize(s));
+  std::vector<int> rows;
+  for (int r = 0; r < nr; ++r)
+    if (std::fabs(h[r] - thrp) <= kRecheckBand * thrp) rows.push_back(r);
+  if (rows.empty()) return;
+  int *d = mw.recheck.ensure(rows.size());
+  S2G_CUDA(cudaMemcpyAsync(d, rows.data(), sizeof(int) * rows.size(), cudaMemcpyHostToDevice, s));
+  S2G_LAUNCH(k_pt_recheck, (int)rows.size(), 256, 0, s, d, (int)rows.size(), cand_k, pk, nex, Pia,
+             Qia, Poo, Qvv, N, no, nv, de_all, ed, ak, thrp, pert, sel);
+  mw.rechecked += (int64_t)rows.size();
 }
 
 }  // namespace std2g

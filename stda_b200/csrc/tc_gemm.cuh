@@ -1,0 +1,342 @@
+// Tensor-core (tcgen05 / TMEM / TMA) contraction for sm_100a with split-BF16
+// operands:
+//
+//   D[m, n] (FP32, row-major, ldd) = sum_k A[m, k] * B[n, k]
+//
+// A and B are given as BF16 pairs (hi, lo) with x ~= hi + lo, stored K-major
+// (row-major with K contiguous, K padded to a multiple of 64 with zeros).
+// Three MMAs per K step (hi*hi + hi*lo + lo*hi) into one FP32 TMEM
+// accumulator recover ~16 mantissa bits of each operand, i.e. products close
+// to FP32 accuracy at BF16 tensor-core rate.
+//
+// This is the contraction over atoms behind the sTDA couplings
+// (ptselect stda.f:1812-1819; rtdamat stda.f:2040-2046):
+//   (ia|jb) = sum_A p_ia^A q_jb^A    and    (ij|ab) = sum_A p_ij^A q_ab^A.
+//
+// One CTA computes one 128 x 128 tile: warp 0 issues TMA loads into a
+// 3-stage shared-memory ring, warp 1 issues tcgen05.mma from one thread,
+// warp 2 owns the TMEM allocation, warps 4-7 drain the accumulator
+// (tcgen05.ld) and store to global memory.  Every mbarrier wait is bounded by
+// a ~2 s wall-clock limit; on expiry the CTA records the failure in *err and
+// leaves without touching memory further.
+#pragma once
+
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cudaTypedefs.h>
+
+#include "common.cuh"
+
+namespace std2g {
+
+namespace tc {
+
+constexpr int BM = 128;
+constexpr int BN = 128;
+constexpr int BK = 64;          // 64 BF16 = 128 bytes = one 128B swizzle row
+constexpr int STAGES = 3;
+constexpr int TILE_A = BM * BK * 2;   // bytes per operand tile
+constexpr int TILE_B = BN * BK * 2;
+constexpr int STAGE_BYTES = 2 * TILE_A + 2 * TILE_B;
+constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256;
+constexpr unsigned long long kWaitNs = 2000000000ull;   // 2 s per wait
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ unsigned long long globaltimer() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// bounded wait; returns false (and flags *err) when the limit expires
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int *err, int code) {
+  if (mbar_try_wait(bar, parity)) return true;
+  unsigned long long t0 = globaltimer();
+  while (true) {
+    for (int q = 0; q < 256; ++q)
+      if (mbar_try_wait(bar, parity)) return true;
+    if (globaltimer() - t0 > kWaitNs) {
+      atomicExch(err, code);
+      return false;
+    }
+    if (*(volatile int *)err) return false;
+  }
+}
+
+__device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, uint64_t *bar,
+                                            int x, int y) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%3, %4}], [%2];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(x), "r"(y)
+      : "memory");
+}
+
+// UMMA shared-memory descriptor: K-major, 128B swizzle, 8-row groups 1024 B apart
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr >> 4) & 0x3FFF);          // start address
+  d |= (uint64_t)1 << 16;                          // leading byte offset (unused, 1)
+  d |= (uint64_t)(1024 >> 4) << 32;                // stride byte offset
+  d |= (uint64_t)1 << 46;                          // descriptor version (sm_100)
+  d |= (uint64_t)2 << 61;                          // SWIZZLE_128B
+  return d;
+}
+
+// instruction descriptor: BF16 x BF16 -> FP32, both K-major, M=128, N=BN
+constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) |
+                            ((uint32_t)(BM >> 4) << 24);
+
+__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t da, uint64_t db,
+                                          uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(
+          tmem_d),
+      "l"(da), "l"(db), "r"(kIdesc), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0));
+}
+
+__device__ __forceinline__ void umma_commit(uint64_t *bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                   smem_u32(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float *v) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,"
+      "%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+        "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int q = 0; q < 16; ++q) v[q] = __uint_as_float(r[q]);
+}
+
+}  // namespace tc
+
+__global__ void __launch_bounds__(256, 1)
+k_tc_gemm_bf16x3(const __grid_constant__ CUtensorMap mAh, const __grid_constant__ CUtensorMap mAl,
+                 const __grid_constant__ CUtensorMap mBh, const __grid_constant__ CUtensorMap mBl,
+                 float *__restrict__ D, int64_t ldd, int M, int N, int Kpad, int *err) {
+  using namespace tc;
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  unsigned char *base = (unsigned char *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  uint64_t *full = (uint64_t *)(base + STAGES * STAGE_BYTES);
+  uint64_t *empty = full + STAGES;
+  uint64_t *done = empty + STAGES;
+  uint32_t *tmem_slot = (uint32_t *)(done + 1);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
+  const int nk = Kpad / BK;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    mbar_init(done, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  if (warp == 2) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(tmem_slot)),
+                 "r"(BN));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *(volatile uint32_t *)tmem_slot;
+
+  if (warp == 0 && lane == 0) {
+    // ---- TMA producer ----
+    for (int kb = 0; kb < nk; ++kb) {
+      const int s = kb % STAGES;
+      if (kb >= STAGES && !mbar_wait(&empty[s], ((kb / STAGES) - 1) & 1, err, 1)) break;
+      unsigned char *st = base + s * STAGE_BYTES;
+      mbar_expect_tx(&full[s], STAGE_BYTES);
+      tma_load_2d(st, &mAh, &full[s], kb * BK, m0);
+      tma_load_2d(st + TILE_A, &mAl, &full[s], kb * BK, m0);
+      tma_load_2d(st + 2 * TILE_A, &mBh, &full[s], kb * BK, n0);
+      tma_load_2d(st + 2 * TILE_A + TILE_B, &mBl, &full[s], kb * BK, n0);
+    }
+  } else if (warp == 1 && lane == 0) {
+    // ---- MMA issuer ----
+    bool ok = true;
+    for (int kb = 0; kb < nk && ok; ++kb) {
+      const int s = kb % STAGES;
+      if (!mbar_wait(&full[s], (kb / STAGES) & 1, err, 2)) {
+        ok = false;
+        break;
+      }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const uint32_t st = smem_u32(base + s * STAGE_BYTES);
+      const uint32_t ah = st, al = st + TILE_A, bh = st + 2 * TILE_A, bl = st + 2 * TILE_A + TILE_B;
+#pragma unroll
+      for (int kk = 0; kk < BK / 16; ++kk) {
+        const uint32_t off = kk * 32;   // 16 BF16 = 32 bytes along K
+        const uint32_t acc0 = (kb > 0 || kk > 0) ? 1u : 0u;
+        umma_bf16(tmem, tc::umma_desc(ah + off), tc::umma_desc(bh + off), acc0);
+        umma_bf16(tmem, tc::umma_desc(ah + off), tc::umma_desc(bl + off), 1u);
+        umma_bf16(tmem, tc::umma_desc(al + off), tc::umma_desc(bh + off), 1u);
+      }
+      umma_commit(&empty[s]);   // stage reusable once these MMAs have read it
+    }
+    if (ok) umma_commit(done);
+  } else if (warp >= 4) {
+    // ---- epilogue: TMEM -> registers -> global ----
+    const int wq = warp - 4;                 // TMEM lanes 32*wq .. 32*wq+31
+    const bool ok = mbar_wait(done, 0, err, 3);
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (ok) {
+      const int row = m0 + wq * 32 + lane;
+      float v[16];
+#pragma unroll 1
+      for (int c = 0; c < BN; c += 16) {
+        tc::tmem_ld16(tmem + ((uint32_t)(wq * 32) << 16) + c, v);
+        if (row < M) {
+          float *dst = D + (int64_t)row * ldd + n0 + c;
+          if (n0 + c + 16 <= N) {
+#pragma unroll
+            for (int q = 0; q < 16; q += 4)
+              *(float4 *)(dst + q) = make_float4(v[q], v[q + 1], v[q + 2], v[q + 3]);
+          } else {
+            for (int q = 0; q < 16; ++q)
+              if (n0 + c + q < N) dst[q] = v[q];
+          }
+        }
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 2) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(BN));
+  }
+}
+
+// x (FP64, column c at src + ld*idx[c] (or ld*c), length Nk) -> hi/lo BF16 rows of Kpad
+__global__ void k_split_bf16(__nv_bfloat16 *__restrict__ hi, __nv_bfloat16 *__restrict__ lo,
+                             const double *__restrict__ src, int64_t ld, const int *__restrict__ idx,
+                             int64_t ncols, int Nk, int Kpad) {
+  int64_t total = ncols * Kpad;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    int64_t c = t / Kpad;
+    int k = (int)(t - c * Kpad);
+    double x = 0.0;
+    if (k < Nk) x = src[(idx ? (int64_t)idx[c] : c) * ld + k];
+    __nv_bfloat16 h = __double2bfloat16(x);
+    __nv_bfloat16 l = __double2bfloat16(x - (double)__bfloat162float(h));
+    hi[t] = h;
+    lo[t] = l;
+  }
+}
+
+// ---------------------------------------------------------------- host side
+struct TcGemm {
+  PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+  DBuf<int> err;
+  bool ready = false;
+  double ms = 0, flop = 0;
+  int64_t launches = 0;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+
+  void init() {
+    if (ready) return;
+    cudaDriverEntryPointQueryResult q;
+    void *fn = nullptr;
+    S2G_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q));
+    if (!fn || q != cudaDriverEntryPointSuccess)
+      throw Error{STD2G_ECUDA, "cuTensorMapEncodeTiled unavailable"};
+    encode = (PFN_cuTensorMapEncodeTiled_v12000)fn;
+    S2G_CUDA(cudaFuncSetAttribute(k_tc_gemm_bf16x3, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  tc::SMEM_BYTES));
+    S2G_CUDA(cudaEventCreate(&e0));
+    S2G_CUDA(cudaEventCreate(&e1));
+    ready = true;
+  }
+
+  CUtensorMap map(const __nv_bfloat16 *p, int64_t rows, int Kpad, int box_rows) {
+    CUtensorMap m;
+    cuuint64_t dims[2] = {(cuuint64_t)Kpad, (cuuint64_t)rows};
+    cuuint64_t strides[1] = {(cuuint64_t)Kpad * 2};
+    cuuint32_t box[2] = {(cuuint32_t)tc::BK, (cuuint32_t)box_rows};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = encode(&m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, (void *)p, dims, strides, box,
+                        estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                        CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS)
+      throw Error{STD2G_ECUDA, "cuTensorMapEncodeTiled failed " + std::to_string((int)r)};
+    return m;
+  }
+
+  // D (M x N, row-major ldd) = A (M x Kpad) B (N x Kpad)^T, split-BF16 operands.
+  // nflop: algorithmic FLOPs credited to this launch (2 M N K_true).
+  void run(cudaStream_t s, const __nv_bfloat16 *Ah, const __nv_bfloat16 *Al,
+           const __nv_bfloat16 *Bh, const __nv_bfloat16 *Bl, int M, int N, int Kpad, float *D,
+           int64_t ldd, double nflop) {
+    init();
+    if (M <= 0 || N <= 0) return;
+    if (Kpad % tc::BK != 0) throw Error{STD2G_EINVAL, "tc_gemm: K not padded to 64"};
+    if (((uintptr_t)Ah | (uintptr_t)Al | (uintptr_t)Bh | (uintptr_t)Bl) & 15)
+      throw Error{STD2G_EINVAL, "tc_gemm: operands not 16-byte aligned"};
+    if ((ldd % 4) != 0 || ((uintptr_t)D & 15))
+      throw Error{STD2G_EINVAL, "tc_gemm: output not 16-byte aligned"};
+    CUtensorMap ah = map(Ah, M, Kpad, tc::BM), al = map(Al, M, Kpad, tc::BM);
+    CUtensorMap bh = map(Bh, N, Kpad, tc::BN), bl = map(Bl, N, Kpad, tc::BN);
+    int *e = err.ensure(1);
+    S2G_CUDA(cudaMemsetAsync(e, 0, sizeof(int), s));
+    dim3 grid((unsigned)div_up(N, tc::BN), (unsigned)div_up(M, tc::BM));
+    if (grid.y > 65535) throw Error{STD2G_EINVAL, "tc_gemm: M too large for one launch"};
+    S2G_CUDA(cudaEventRecord(e0, s));
+    S2G_LAUNCH(k_tc_gemm_bf16x3, grid, 256, tc::SMEM_BYTES, s, ah, al, bh, bl, D, ldd, M, N,
+               Kpad, e);
+    S2G_CUDA(cudaEventRecord(e1, s));
+    int h_err = 0;
+    S2G_CUDA(cudaMemcpyAsync(&h_err, e, sizeof(int), cudaMemcpyDeviceToHost, s));
+    S2G_CUDA(cudaStreamSynchronize(s));
+    if (h_err)
+      throw Error{STD2G_ETIMEOUT, "tc_gemm: bounded wait expired (" + std::to_string(h_err) + ")"};
+    float t = 0;
+    S2G_CUDA(cudaEventElapsedTime(&t, e0, e1));
+    ms += t;
+    flop += nflop;
+    ++launches;
+  }
+};
+
+}  // namespace std2g

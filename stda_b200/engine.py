@@ -29,7 +29,8 @@ STATUS = {
 EXPORTS = [
     "std2g_create", "std2g_load", "std2g_solve", "std2g_polarizability",
     "std2g_get_csf", "std2g_get_vectors", "std2g_phase_times", "std2g_phase_name",
-    "std2g_kernel_launches", "std2g_error_string", "std2g_destroy",
+    "std2g_kernel_launches", "std2g_kernel_stats", "std2g_solver_stats", "std2g_error_string",
+    "std2g_destroy",
 ]
 
 
@@ -86,6 +87,8 @@ def library():
         lib.std2g_phase_name.restype = C.c_char_p
         lib.std2g_kernel_launches.argtypes = [C.c_void_p]
         lib.std2g_kernel_launches.restype = C.c_int64
+        lib.std2g_kernel_stats.argtypes = [C.c_void_p, dp, C.POINTER(C.c_int64), dp]
+        lib.std2g_solver_stats.argtypes = [C.c_void_p, ip, C.POINTER(C.c_int64)]
         lib.std2g_error_string.argtypes = [C.c_int]
         lib.std2g_error_string.restype = C.c_char_p
         lib.std2g_destroy.argtypes = [C.c_void_p]
@@ -269,6 +272,19 @@ class Engine:
         ms = np.zeros(16)
         n = self.lib.std2g_phase_times(self.ctx, _dp(ms), 16)
         return {self.lib.std2g_phase_name(q).decode(): ms[q] for q in range(n)}
+
+    def kernel_stats(self):
+        """Tensor-core contraction time / launches / algorithmic FLOPs of the last solve."""
+        ms, fl = C.c_double(), C.c_double()
+        n = C.c_int64()
+        _check(self.lib.std2g_kernel_stats(self.ctx, C.byref(ms), C.byref(n), C.byref(fl)))
+        return {"tc_ms": ms.value, "tc_launches": n.value, "tc_flop": fl.value}
+
+    def solver_stats(self):
+        it = C.c_int()
+        mv = C.c_int64()
+        _check(self.lib.std2g_solver_stats(self.ctx, C.byref(it), C.byref(mv)))
+        return {"davidson_iters": it.value, "sigma_vectors": mv.value}
 
     def kernel_launches(self):
         return int(self.lib.std2g_kernel_launches(self.ctx))

@@ -137,3 +137,59 @@ def test_error_paths(water):
     # the context stays usable after errors
     sol = eng.solve(Keywords(ax=1.0, e_thr_ev=20.0))
     assert len(sol.omega) == 4
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_matrix_free_davidson_vs_oracle(benzene, precision):
+    """Lowest roots by the matrix-free blocked Davidson vs the oracle's dense
+    diagonalisation, including the velocity-corrected rotatory strengths."""
+    mol, ints = benzene
+    kw = dict(ax=0.5, e_thr_ev=10.0)
+    eng, sol, iconf, ed = _run(mol, ints, precision=precision, nroots=12, solver=2,
+                               conv_tol=1e-8, **kw)
+    ref = _oracle(mol, ints, **kw)
+    assert _same_csf(ref, iconf)
+    assert np.abs(sol.omega - ref.omega[:12]).max() < 1e-9
+    assert np.allclose(sol.fL, ref.fL[:12], rtol=1e-5, atol=1e-8)
+    assert np.allclose(sol.fV, ref.fV[:12], rtol=1e-5, atol=1e-8)
+    assert np.allclose(sol.RV, ref.RV[:12], rtol=1e-4, atol=1e-6)
+
+
+def test_matrix_free_larger_cluster():
+    from stda_b200 import synth
+    mol, ints = synth.random_molecule(36, seed=11, with_ints=True)
+    kw = dict(ax=0.5, e_thr_ev=8.0)
+    eng, sol, iconf, ed = _run(mol, ints, nroots=20, solver=2, conv_tol=1e-8, **kw)
+    ref = _oracle(mol, ints, **kw)
+    assert _same_csf(ref, iconf)
+    n = min(20, len(ref.omega))
+    assert n >= 10
+    assert np.abs(sol.omega[:n] - ref.omega[:n]).max() < 1e-9
+    assert np.allclose(sol.fL[:n], ref.fL[:n], rtol=1e-5, atol=1e-8)
+    assert np.allclose(sol.RV[:n], ref.RV[:n], rtol=1e-4, atol=1e-6)
+
+
+def test_mixed_form_pt_selection_matches_fp64(benzene):
+    """Tensor-core (split-BF16) PT selection: same CSF set as the FP64 oracle,
+    roots within 1e-4 eV and oscillator strengths within 1e-4 relative."""
+    mol, ints = benzene
+    kw = dict(ax=0.5, e_thr_ev=10.0)
+    eng, sol, iconf, ed = _run(mol, ints, precision=1, **kw)
+    ref = _oracle(mol, ints, **kw)
+    assert _same_csf(ref, iconf)
+    assert np.abs(sol.omega - ref.omega).max() * 27.21139 < 1e-4
+    big = ref.fL > 1e-3
+    assert np.all(np.abs(sol.fL[big] - ref.fL[big]) / ref.fL[big] < 1e-4)
+    assert eng.kernel_stats()["tc_launches"] > 0
+
+
+@pytest.mark.parametrize("natoms,seed", [(30, 3), (40, 4)])
+def test_mixed_form_clusters(natoms, seed):
+    from stda_b200 import synth
+    mol, ints = synth.random_molecule(natoms, seed=seed, with_ints=True)
+    kw = dict(ax=0.5, e_thr_ev=8.0)
+    eng, sol, iconf, ed = _run(mol, ints, precision=1, nroots=10, solver=2, conv_tol=1e-7, **kw)
+    ref = _oracle(mol, ints, **kw)
+    assert _same_csf(ref, iconf)
+    n = min(10, len(ref.omega))
+    assert np.abs(sol.omega[:n] - ref.omega[:n]).max() * 27.21139 < 1e-4
