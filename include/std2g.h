@@ -164,6 +164,31 @@ int std2g_kernel_stats(void *ctx, double *ms, int64_t *launches, double *flop);
 /* Davidson statistics of the last solve: iterations and sigma-vector count. */
 int std2g_solver_stats(void *ctx, int *iters, int64_t *matvecs);
 
+/* Diagonal screen without any device allocation.  This entry point has no
+   counterpart in the reference.  It is for callers that cannot allocate device
+   memory: hosts whose GPU memory is owned by another allocator (a framework
+   that has reserved it for its own pool), or that must not call cudaMalloc at
+   this point because it synchronises the device.  They pass device buffers
+   they already own:
+     d_xyz   [4*ncent]        x,y,z (Bohr), Z (1..94) per atom
+     d_iaoat [nao]            AO -> atom, 1-based
+     d_clow  [nao*(no+nv)]    Loewdin-orthogonalised MOs of the active window,
+                              occupied then virtual, each block energy-sorted
+     d_eps   [no+nv]          their orbital energies (Eh)
+   and receive, for k = i*nv + a (0-based i < no, a < nv),
+     d_de    [no*nv]          diagonal element of A ((e_a-e_i) - (ii|aa) + ak (ia|ia))
+     d_flag  [no*nv]          1 primary (<= E_thr), 2 PT candidate, 0 neither
+   from par: ax, e_thr_ev, alpha_k, beta_j, fthr_ev, triplet, kshift(+shift).
+   Work arrays live in one fixed 64 MiB __device__ array that every GPU using
+   this library keeps until the process exits; sizes with
+   2N^2 + N(2no + nv) + 2 N no nv > 8 Mi doubles return STD2G_ECAP.  The first
+   call on a device looks up that array's address (make it before any stream
+   capture).  All calls share the array, so calls whose kernels overlap on the
+   GPU race.  Kernels are queued on `stream` (a cudaStream_t, NULL = default). */
+int std2g_screen_noalloc(int device, int ncent, int nao, int no, int nv, const double *d_xyz,
+                         const int *d_iaoat, const double *d_clow, const double *d_eps,
+                         const std2g_params *par, double *d_de, int *d_flag, void *stream);
+
 const char *std2g_error_string(int status);
 void std2g_destroy(void *ctx);
 

@@ -30,7 +30,7 @@ EXPORTS = [
     "std2g_create", "std2g_load", "std2g_solve", "std2g_polarizability",
     "std2g_get_csf", "std2g_get_vectors", "std2g_phase_times", "std2g_phase_name",
     "std2g_kernel_launches", "std2g_kernel_stats", "std2g_solver_stats", "std2g_error_string",
-    "std2g_destroy",
+    "std2g_destroy", "std2g_screen_noalloc",
 ]
 
 
@@ -89,6 +89,10 @@ def library():
         lib.std2g_kernel_launches.restype = C.c_int64
         lib.std2g_kernel_stats.argtypes = [C.c_void_p, dp, C.POINTER(C.c_int64), dp]
         lib.std2g_solver_stats.argtypes = [C.c_void_p, ip, C.POINTER(C.c_int64)]
+        lib.std2g_screen_noalloc.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                              C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                              C.POINTER(Params), C.c_void_p, C.c_void_p,
+                                              C.c_void_p]
         lib.std2g_error_string.argtypes = [C.c_int]
         lib.std2g_error_string.restype = C.c_char_p
         lib.std2g_destroy.argtypes = [C.c_void_p]
