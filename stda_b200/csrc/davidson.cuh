@@ -85,8 +85,34 @@ __global__ void k_unit_vectors(double *__restrict__ V, int n, const int *__restr
   }
 }
 
+// column norms of T (one block per column)
+__global__ void k_colnorms(const double *__restrict__ T, int n, double *__restrict__ out) {
+  const double *t = T + (int64_t)n * blockIdx.x;
+  double s = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) s += t[i] * t[i];
+  __shared__ double red[256];
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[blockIdx.x] = sqrt(red[0]);
+}
+
+// T[:, j] *= f(s[j]) with mode 0: 1/s, mode 1: 1/sqrt(s)
+__global__ void k_scale_by(double *__restrict__ T, int n, int ncol, const double *__restrict__ sv,
+                           int mode) {
+  int64_t total = (int64_t)n * ncol;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    double v = sv[t / n];
+    T[t] *= mode == 0 ? (v > 0 ? 1.0 / v : 0.0) : (v > 0 ? 1.0 / sqrt(v) : 0.0);
+  }
+}
+
 struct DavidsonWork {
-  DBuf<double> V, W, Hs, theta, X, R, T, tmp, rn, proj;
+  DBuf<double> V, W, Hs, theta, X, R, T, tmp, rn, proj, G, lam, work2;
   DBuf<int> cols, idx, info;
   DBuf<double> work;
   int iters = 0;
@@ -111,7 +137,7 @@ inline int davidson(DavidsonWork &dw, cublasHandle_t blas, cusolverDnHandle_t so
   double *theta = dw.theta.ensure(mmax), *X = dw.X.ensure((size_t)n * k);
   double *R = dw.R.ensure((size_t)n * k), *T = dw.T.ensure((size_t)n * k);
   double *tmp = dw.tmp.ensure((size_t)n * k), *rn = dw.rn.ensure(k + 2);
-  double *proj = dw.proj.ensure((size_t)mmax + 4);
+  double *proj = dw.proj.ensure((size_t)mmax * k + 4);
   int *cols = dw.cols.ensure(k), *info = dw.info.ensure(1);
   const double one = 1.0, zero = 0.0, mone = -1.0;
 
@@ -170,26 +196,55 @@ inline int davidson(DavidsonWork &dw, cublasHandle_t blas, cusolverDnHandle_t so
       S2G_CUDA(cudaMemcpyAsync(V, X, sizeof(double) * n * k, cudaMemcpyDeviceToDevice, s));
       m = k;
     }
-    // normalise each correction, orthogonalise against V (CGS applied twice), append
+    // block orthogonalisation of the corrections: normalise, project out V twice
+    // (classical Gram-Schmidt as GEMMs), then orthonormalise the block through
+    // the eigen-decomposition of its Gram matrix, dropping dependent directions
     nb = 0;
-    for (int j = 0; j < nc; ++j) {
-      double *t = T + (size_t)n * j;
-      S2G_LAUNCH(k_norm, 1, 256, 0, s, t, n, rn + k);
-      S2G_LAUNCH(k_scale_vec, 64, 256, 0, s, t, n, rn + k);
-      for (int pass = 0; pass < 2; ++pass) {
-        int mc = m + nb;
-        S2G_CUBLAS(cublasDgemv(blas, CUBLAS_OP_T, n, mc, &one, V, n, t, 1, &zero, proj, 1));
-        S2G_CUBLAS(cublasDgemv(blas, CUBLAS_OP_N, n, mc, &mone, V, n, proj, 1, &one, t, 1));
+    {
+      double *G = dw.G.ensure((size_t)k * k), *lam = dw.lam.ensure(k);
+      S2G_LAUNCH(k_colnorms, nc, 256, 0, s, T, n, lam);
+      S2G_LAUNCH(k_scale_by, grid, 256, 0, s, T, n, nc, lam, 0);
+      double *Tb = T;
+      int ncur = nc;
+      for (int round = 0; round < 2 && ncur > 0; ++round) {
+        for (int pass = 0; pass < 2; ++pass) {
+          S2G_CUBLAS(cublasDgemm(blas, CUBLAS_OP_T, CUBLAS_OP_N, m, ncur, n, &one, V, n, Tb, n,
+                                 &zero, proj, m));
+          S2G_CUBLAS(cublasDgemm(blas, CUBLAS_OP_N, CUBLAS_OP_N, n, ncur, m, &mone, V, n, proj, m,
+                                 &one, Tb, n));
+        }
+        // G = Tb^T Tb, eigenpairs ascending
+        S2G_CUBLAS(cublasDgemm(blas, CUBLAS_OP_T, CUBLAS_OP_N, ncur, ncur, n, &one, Tb, n, Tb, n,
+                               &zero, G, ncur));
+        int lw2 = 0;
+        S2G_CUSOLVER(cusolverDnDsyevd_bufferSize(sol, CUSOLVER_EIG_MODE_VECTOR,
+                                                 CUBLAS_FILL_MODE_LOWER, ncur, G, ncur, lam, &lw2));
+        double *work2 = dw.work2.ensure((size_t)lw2 + 1);
+        S2G_CUSOLVER(cusolverDnDsyevd(sol, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, ncur,
+                                      G, ncur, lam, work2, lw2, info));
+        std::vector<double> h_lam(ncur);
+        S2G_CUDA(cudaMemcpyAsync(h_lam.data(), lam, sizeof(double) * ncur, cudaMemcpyDeviceToHost,
+                                 s));
+        S2G_CUDA(cudaStreamSynchronize(s));
+        int first = 0;   // keep eigenvalues above the dependence threshold
+        const double cut = round == 0 ? 1e-10 : 1e-14;
+        while (first < ncur && !(h_lam[first] > cut)) ++first;
+        int nkeep = ncur - first;
+        if (nkeep == 0) {
+          ncur = 0;
+          break;
+        }
+        // new block = Tb U_keep diag(lam_keep)^-1/2, written into V after column m
+        double *dst = V + (size_t)n * m;
+        S2G_CUBLAS(cublasDgemm(blas, CUBLAS_OP_N, CUBLAS_OP_N, n, nkeep, ncur, &one, Tb, n,
+                               G + (size_t)ncur * first, ncur, &zero, tmp, n));
+        S2G_LAUNCH(k_scale_by, grid, 256, 0, s, tmp, n, nkeep, lam + first, 1);
+        S2G_CUDA(cudaMemcpyAsync(dst, tmp, sizeof(double) * n * nkeep, cudaMemcpyDeviceToDevice,
+                                 s));
+        Tb = dst;   // second round re-orthogonalises the appended block in place
+        ncur = nkeep;
       }
-      S2G_LAUNCH(k_norm, 1, 256, 0, s, t, n, rn + k);
-      double h_nrm = 0;
-      S2G_CUDA(cudaMemcpyAsync(&h_nrm, rn + k, sizeof(double), cudaMemcpyDeviceToHost, s));
-      S2G_CUDA(cudaStreamSynchronize(s));
-      if (!(h_nrm > 1e-6)) continue;   // linearly dependent on the current space
-      S2G_LAUNCH(k_scale_vec, 64, 256, 0, s, t, n, rn + k);
-      S2G_CUDA(cudaMemcpyAsync(V + (size_t)n * (m + nb), t, sizeof(double) * n,
-                               cudaMemcpyDeviceToDevice, s));
-      ++nb;
+      nb = ncur;
     }
     if (nb == 0) break;
   }

@@ -537,16 +537,24 @@ static void solve(Ctx &c, const std2g_params &p_in, std2g_result *res, const Res
       c.mixed.rechecked = 0;
     }
     int nchunk = (int)div_up(no, occ_chunk);
-    double *colpart = c.w_colpart.ensure((size_t)nchunk * nex);
+    // column sums of the PT terms by segments of candidate rows (deterministic order)
+    const int kSeg = 2048;
+    std::vector<int> seg_off(nchunk + 1, 0);
+    for (int q = 0; q < nchunk; ++q) {
+      int a0 = q * occ_chunk, a1 = std::min(no, a0 + occ_chunk);
+      int nrq = first_of_occ[a1] - first_of_occ[a0];
+      seg_off[q + 1] = seg_off[q] + (int)div_up(nrq, kSeg);
+    }
+    const int nseg_total = std::max(1, seg_off[nchunk]);
+    double *colpart = c.w_colpart.ensure((size_t)nseg_total * nex);
     unsigned char *sel = c.w_sel.ensure(nexpt);
     double *pert = c.w_pert.ensure(nexpt);
     for (int q = 0; q < nchunk; ++q) {
       int i0 = q * occ_chunk, i1 = std::min(no, i0 + occ_chunk), ni = i1 - i0;
       int r0 = first_of_occ[i0], r1 = first_of_occ[i1], nr = r1 - r0;
-      if (nr == 0) {
-        S2G_CUDA(cudaMemsetAsync(colpart + (size_t)q * nex, 0, sizeof(double) * nex, s));
-        continue;
-      }
+      if (nr == 0) continue;
+      const dim3 cgrid((unsigned)div_up(nex, 128), (unsigned)(seg_off[q + 1] - seg_off[q]));
+      double *cpart = colpart + (size_t)seg_off[q] * nex;
       double *Pc = c.w_Pc.ensure((size_t)N * nr);
       S2G_LAUNCH(k_gather_cols, grid_for((int64_t)N * nr), 256, 0, s, Pc, Pia, (int64_t)N,
                  d_ck + r0, (int64_t)nr, (int64_t)N);
@@ -562,9 +570,9 @@ static void solve(Ctx &c, const std2g_params &p_in, std2g_result *res, const Res
         S2G_LAUNCH((k_pt_rows<double, double>), nr, 256, 0, s, Kb, Jb, ldj, (int64_t)nex, nex,
                    nvp, nop, nr, d_ck + r0, nv, i0, de, d_pj, d_pb, d_omap, d_vmap, d_ed, ak,
                    p.thrp, pert + r0, sel + r0);
-        S2G_LAUNCH((k_pt_cols<double, double>), (int)div_up(nex, 128), 128, 0, s, Kb, Jb, ldj,
-                   (int64_t)nex, nex, nvp, nop, nr, d_ck + r0, nv, i0, de, d_pj, d_pb, d_omap,
-                   d_vmap, d_ed, ak, sel + r0, colpart + (size_t)q * nex);
+        S2G_LAUNCH((k_pt_cols<double, double>), cgrid, 128, 0, s, Kb, Jb, ldj, (int64_t)nex, nex,
+                   nvp, nop, nr, d_ck + r0, nv, i0, de, d_pj, d_pb, d_omap, d_vmap, d_ed, ak,
+                   sel + r0, cpart, kSeg);
       } else {
         if (!mixed_ready) {
           mixed_pt_prepare(c.mixed, s, Qp, QvvP, N, nex, ldj);
@@ -578,13 +586,14 @@ static void solve(Ctx &c, const std2g_params &p_in, std2g_result *res, const Res
         // candidates whose PT sum lies near the threshold are decided in FP64
         mixed_pt_recheck(c.mixed, s, pert + r0, sel + r0, nr, p.thrp, d_ck + r0, d_pk, nex, Pia,
                          Qia, Poo, Qvv, N, no, nv, de, d_ed, ak);
-        S2G_LAUNCH((k_pt_cols<float, float>), (int)div_up(nex, 128), 128, 0, s, Kf, Jf,
-                   c.mixed.ldJ, c.mixed.ldK, nex, nvp, nop, nr, d_ck + r0, nv, i0, de, d_pj, d_pb,
-                   d_omap, d_vmap, d_ed, ak, sel + r0, colpart + (size_t)q * nex);
+        S2G_LAUNCH((k_pt_cols<float, float>), cgrid, 128, 0, s, Kf, Jf, c.mixed.ldJ, c.mixed.ldK,
+                   nex, nvp, nop, nr, d_ck + r0, nv, i0, de, d_pj, d_pb, d_omap, d_vmap, d_ed, ak,
+                   sel + r0, cpart, kSeg);
       }
     }
     double *pt2 = c.w_pt2.ensure(nex), *edp = c.w_edp.ensure(nex);
-    S2G_LAUNCH(k_pt2_finish, (int)div_up(nex, 128), 128, 0, s, colpart, nchunk, nex, d_ed, pt2,
+    if (seg_off[nchunk] == 0) S2G_CUDA(cudaMemsetAsync(colpart, 0, sizeof(double) * nex, s));
+    S2G_LAUNCH(k_pt2_finish, (int)div_up(nex, 128), 128, 0, s, colpart, nseg_total, nex, d_ed, pt2,
                edp);
     std::vector<unsigned char> h_sel(nexpt);
     std::vector<double> h_edp(nex);

@@ -238,11 +238,17 @@ __global__ void k_pt_cols(const TK *__restrict__ Kbuf, const TJ *__restrict__ Jb
                           const int *__restrict__ pj, const int *__restrict__ pb,
                           const int *__restrict__ omap, const int *__restrict__ vmap,
                           const double *__restrict__ ed, double ak,
-                          const unsigned char *__restrict__ sel, double *__restrict__ colpart) {
+                          const unsigned char *__restrict__ sel, double *__restrict__ colpart,
+                          int seg_rows) {
+  // grid: x over primaries, y over segments of seg_rows candidate rows;
+  // colpart[y*nex + c] holds the segment's sum (reduced in fixed order later)
   int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= nex) return;
+  const int rbeg = blockIdx.y * seg_rows;
+  const int rend = min(nrows, rbeg + seg_rows);
+  colpart += (int64_t)blockIdx.y * nex;
   double s = 0.0;
-  for (int r = 0; r < nrows; ++r) {
+  for (int r = rbeg; r < rend; ++r) {
     if (sel[r]) continue;
     int k = cand_k[r];
     int i = k / nv, a = k - i * nv;
