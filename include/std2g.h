@@ -161,8 +161,11 @@ int64_t std2g_kernel_launches(void *ctx);
    (ms), number of launches and algorithmic FLOPs (used for the roofline). */
 int std2g_kernel_stats(void *ctx, double *ms, int64_t *launches, double *flop);
 
-/* Davidson statistics of the last solve: iterations and sigma-vector count. */
-int std2g_solver_stats(void *ctx, int *iters, int64_t *matvecs);
+/* Statistics of the last solve: Davidson iterations, sigma vectors formed
+   with tensor-core (mixed) products and with FP64 products, and the number of
+   PT candidates whose selection was re-decided in FP64 (mixed form). */
+int std2g_solver_stats(void *ctx, int *iters, int64_t *matvecs, int64_t *matvecs_fp64,
+                       int64_t *pt_rechecked);
 
 /* Diagonal screen without any device allocation.  This entry point has no
    counterpart in the reference.  It is for callers that cannot allocate device

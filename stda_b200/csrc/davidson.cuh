@@ -111,8 +111,14 @@ __global__ void k_scale_by(double *__restrict__ T, int n, int ncol, const double
   }
 }
 
+// d[j] = A[j + lda*j]
+__global__ void k_diag_of(const double *__restrict__ A, int lda, int n, double *__restrict__ d) {
+  int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j < n) d[j] = A[j + (int64_t)lda * j];
+}
+
 struct DavidsonWork {
-  DBuf<double> V, W, Hs, theta, X, R, T, tmp, rn, proj, G, lam, work2;
+  DBuf<double> V, W, Hs, theta, X, R, T, tmp, rn, proj, G, Gc, lam, work2;
   DBuf<int> cols, idx, info;
   DBuf<double> work;
   int iters = 0;
@@ -124,14 +130,18 @@ using MatVec = std::function<void(const double *V, int nb, double *W)>;
 
 // Returns the number of converged wanted roots (== k on success).  `mv` forms
 // W = A V for nb column vectors (n x nb, column-major); `diag` is diag(A).
+// With `warm`, the first block is the k Ritz vectors left in dw.X by a
+// previous call on the same problem (orthonormal), instead of unit vectors.
 inline int davidson(DavidsonWork &dw, cublasHandle_t blas, cusolverDnHandle_t sol,
                     cudaStream_t s, const MatVec &mv, const double *diag, int n, int k,
-                    double tol, int max_iter, double *omega_out, double *X_out) {
+                    double tol, int max_iter, double *omega_out, double *X_out,
+                    bool warm = false) {
   if (k > n) k = n;
   const int kwant = k;
   k = std::min(n, k + std::max(4, k / 2));
   const int mmax = std::min(n, std::max(4 * k, k + 32));
   const int grid = 148 * 4;
+  if (warm && dw.X.n < (size_t)n * k) warm = false;
   double *V = dw.V.ensure((size_t)n * mmax), *W = dw.W.ensure((size_t)n * mmax);
   double *Hs = dw.Hs.ensure((size_t)mmax * mmax);
   double *theta = dw.theta.ensure(mmax), *X = dw.X.ensure((size_t)n * k);
@@ -149,8 +159,12 @@ inline int davidson(DavidsonWork &dw, cublasHandle_t blas, cusolverDnHandle_t so
   std::iota(order.begin(), order.end(), 0);
   std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return h_diag[a] < h_diag[b]; });
   int *idx = dw.idx.ensure(k);
-  S2G_CUDA(cudaMemcpyAsync(idx, order.data(), sizeof(int) * k, cudaMemcpyHostToDevice, s));
-  S2G_LAUNCH(k_unit_vectors, grid, 256, 0, s, V, n, idx, k);
+  if (warm) {
+    S2G_CUDA(cudaMemcpyAsync(V, X, sizeof(double) * n * k, cudaMemcpyDeviceToDevice, s));
+  } else {
+    S2G_CUDA(cudaMemcpyAsync(idx, order.data(), sizeof(int) * k, cudaMemcpyHostToDevice, s));
+    S2G_LAUNCH(k_unit_vectors, grid, 256, 0, s, V, n, idx, k);
+  }
   int m = 0, nb = k;
   int lwork = 0;
   S2G_CUSOLVER(cusolverDnDsyevd_bufferSize(sol, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER,
@@ -213,9 +227,41 @@ inline int davidson(DavidsonWork &dw, cublasHandle_t blas, cusolverDnHandle_t so
           S2G_CUBLAS(cublasDgemm(blas, CUBLAS_OP_N, CUBLAS_OP_N, n, ncur, m, &mone, V, n, proj, m,
                                  &one, Tb, n));
         }
-        // G = Tb^T Tb, eigenpairs ascending
+        // G = Tb^T Tb; Cholesky QR when G is safely positive definite
         S2G_CUBLAS(cublasDgemm(blas, CUBLAS_OP_T, CUBLAS_OP_N, ncur, ncur, n, &one, Tb, n, Tb, n,
                                &zero, G, ncur));
+        {
+          double *Gc = dw.Gc.ensure((size_t)k * k);
+          S2G_CUDA(cudaMemcpyAsync(Gc, G, sizeof(double) * ncur * ncur, cudaMemcpyDeviceToDevice,
+                                   s));
+          int lwp = 0;
+          S2G_CUSOLVER(cusolverDnDpotrf_bufferSize(sol, CUBLAS_FILL_MODE_LOWER, ncur, Gc, ncur,
+                                                   &lwp));
+          double *wp = dw.work2.ensure((size_t)lwp + 1);
+          S2G_CUSOLVER(cusolverDnDpotrf(sol, CUBLAS_FILL_MODE_LOWER, ncur, Gc, ncur, wp, lwp,
+                                        info));
+          S2G_LAUNCH(k_diag_of, (int)div_up(ncur, 128), 128, 0, s, Gc, ncur, ncur, lam);
+          int h_info = 0;
+          std::vector<double> h_d(ncur);
+          S2G_CUDA(cudaMemcpyAsync(&h_info, info, sizeof(int), cudaMemcpyDeviceToHost, s));
+          S2G_CUDA(cudaMemcpyAsync(h_d.data(), lam, sizeof(double) * ncur, cudaMemcpyDeviceToHost,
+                                   s));
+          S2G_CUDA(cudaStreamSynchronize(s));
+          double dmin = 1e300;
+          for (double v : h_d) dmin = std::min(dmin, v);
+          if (h_info == 0 && dmin * dmin > 1e-8) {
+            double *dst = V + (size_t)n * m;
+            if (Tb != dst)
+              S2G_CUDA(cudaMemcpyAsync(dst, Tb, sizeof(double) * n * ncur,
+                                       cudaMemcpyDeviceToDevice, s));
+            // dst <- dst L^-T
+            S2G_CUBLAS(cublasDtrsm(blas, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_T,
+                                   CUBLAS_DIAG_NON_UNIT, n, ncur, &one, Gc, ncur, dst, n));
+            Tb = dst;
+            continue;
+          }
+        }
+        // eigenpairs of G ascending: drop dependent directions
         int lw2 = 0;
         S2G_CUSOLVER(cusolverDnDsyevd_bufferSize(sol, CUSOLVER_EIG_MODE_VECTOR,
                                                  CUBLAS_FILL_MODE_LOWER, ncur, G, ncur, lam, &lw2));

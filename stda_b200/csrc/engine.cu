@@ -83,7 +83,7 @@ struct Ctx {
   double tc_ms = 0, tc_flop = 0;
   int64_t tc_launches = 0;
   int dav_iters = 0;
-  int64_t dav_matvecs = 0;
+  int64_t dav_matvecs = 0, dav_fp64_matvecs = 0;
   // last results
   int last_nci = 0, last_nroot = 0, last_no = 0, last_nv = 0;
   bool last_rpa = false;
@@ -329,6 +329,7 @@ static void solve(Ctx &c, const std2g_params &p_in, std2g_result *res, const Res
   c.tc_launches = 0;
   c.dav_iters = 0;
   c.dav_matvecs = 0;
+  c.dav_fp64_matvecs = 0;
   record(c, PH_SETUP);
   const double thr = p.e_thr_ev / kEh2eV_in;
   const double fthr = p.fthr_ev < 1.79e308 ? p.fthr_ev / kEh2eV_in : INFINITY;
@@ -674,18 +675,11 @@ static void solve(Ctx &c, const std2g_params &p_in, std2g_result *res, const Res
     mf.nv = nv;
     mf.nci = nci;
     mf.nao = nao;
-    const int rows = N * c.maxa;
-    S2G_LAUNCH(k_mf_pad_rows, grid_for((int64_t)rows * nv), 256, 0, s,
-               mf.CvP.ensure((size_t)rows * nv), Clow, nao, c.d_slot_ao.get(), rows, no, nv);
-    S2G_LAUNCH(k_mf_pad_rows, grid_for((int64_t)rows * no), 256, 0, s,
-               mf.CoP.ensure((size_t)rows * no), Clow, nao, c.d_slot_ao.get(), rows, 0, no);
-    S2G_LAUNCH(k_pair_to_atom_major, grid_for((int64_t)N * no * no), 256, 0, s,
-               mf.PooA.ensure((size_t)N * no * no), Poo, N, no, no);
-    if (p.velcorr)
-      S2G_LAUNCH(k_pair_to_atom_major, grid_for((int64_t)N * nov), 256, 0, s,
-                 mf.PovA.ensure((size_t)N * nov), Pia, N, no, nv);
-    mf.Qs = Qs;
-    mf.Ps = Ps;
+    mf.f32 = mixed;
+    if (mixed)
+      mf_setup_ops<float>(mf, mf.f, s, Clow, c.d_slot_ao.get(), Poo, Pia, Qs, Ps, p.velcorr);
+    else
+      mf_setup_ops<double>(mf, mf.d, s, Clow, c.d_slot_ao.get(), Poo, Pia, Qs, Ps, p.velcorr);
     mf.ci = d_ci;
     mf.ca = d_ca;
     S2G_LAUNCH(k_mf_diag, (int)div_up(nci, 128), 128, 0, s, mf.dA.ensure(nci), d_edall, ekd, uci,
@@ -702,9 +696,25 @@ static void solve(Ctx &c, const std2g_params &p_in, std2g_result *res, const Res
     MatVec mv = [&](const double *V, int nb, double *W) {
       mf_apply(c.mf, c.blas, s, V, nb, W, ak, -1.0, 0.0, c.mf.dA.get());
     };
-    int conv = davidson(c.dav, c.blas, c.solver, s, mv, d_edall, nci, p.nroots, tol, 300, om, Xd);
-    c.dav_iters = c.dav.iters;
-    c.dav_matvecs = c.dav.matvecs;
+    int conv = 0;
+    if (mixed) {
+      // stage 1: tensor-core (split-BF16 FP32) products; stage 2: FP64 products
+      // from those Ritz vectors until the FP64 residuals meet tol
+      davidson(c.dav, c.blas, c.solver, s, mv, d_edall, nci, p.nroots, tol, 300, om, Xd);
+      c.dav_iters = c.dav.iters;
+      c.dav_matvecs = c.dav.matvecs;
+      mf_setup_ops<double>(c.mf, c.mf.d, s, Clow, c.d_slot_ao.get(), Poo, Pia, Qs, Ps, p.velcorr);
+      c.mf.f32 = false;
+      conv = davidson(c.dav, c.blas, c.solver, s, mv, d_edall, nci, p.nroots, tol, 100, om, Xd,
+                      true);
+      c.dav_iters += c.dav.iters;
+      c.dav_fp64_matvecs = c.dav.matvecs;   // B X of the velocity correction also in FP64
+    } else {
+      conv = davidson(c.dav, c.blas, c.solver, s, mv, d_edall, nci, p.nroots, tol, 300, om, Xd);
+      c.dav_iters = c.dav.iters;
+      c.dav_matvecs = 0;
+      c.dav_fp64_matvecs = c.dav.matvecs;
+    }
     if (conv < std::min(p.nroots, nci))
       throw Error{STD2G_ENOCONV, "Davidson: " + std::to_string(conv) + " of " +
                                      std::to_string(p.nroots) + " roots converged"};
@@ -922,6 +932,11 @@ int std2g_create(void **ctx, const std2g_opts *opts) {
     S2G_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
     S2G_CUBLAS(cublasCreate(&c->blas));
     S2G_CUBLAS(cublasSetStream(c->blas, c->stream));
+    // FP32 GEMMs of this handle (the mixed form's matrix-free products) run on
+    // the tensor cores as split-BF16 products (FP32 emulation); FP64 GEMMs are
+    // unaffected
+    S2G_CUBLAS(cublasSetMathMode(c->blas, CUBLAS_FP32_EMULATED_BF16X9_MATH));
+    S2G_CUBLAS(cublasSetEmulationStrategy(c->blas, CUBLAS_EMULATION_STRATEGY_EAGER));
     S2G_CUSOLVER(cusolverDnCreate(&c->solver));
     S2G_CUSOLVER(cusolverDnSetStream(c->solver, c->stream));
     for (auto &e : c->ev) S2G_CUDA(cudaEventCreate(&e));
@@ -1022,11 +1037,14 @@ int std2g_kernel_stats(void *ctx, double *ms, int64_t *launches, double *flop) {
   return STD2G_OK;
 }
 
-int std2g_solver_stats(void *ctx, int *iters, int64_t *matvecs) {
+int std2g_solver_stats(void *ctx, int *iters, int64_t *matvecs, int64_t *matvecs_fp64,
+                       int64_t *pt_rechecked) {
   if (!ctx) return STD2G_EINVAL;
   auto *c = (Ctx *)ctx;
   if (iters) *iters = c->dav_iters;
   if (matvecs) *matvecs = c->dav_matvecs;
+  if (matvecs_fp64) *matvecs_fp64 = c->dav_fp64_matvecs;
+  if (pt_rechecked) *pt_rechecked = c->opts.precision == 1 ? c->mixed.rechecked : 0;
   return STD2G_OK;
 }
 

@@ -15,7 +15,7 @@
 
 namespace std2g {
 
-constexpr double kRecheckBand = 2e-3;   // relative band around thrp decided in FP64
+constexpr double kRecheckBand = 2e-4;   // relative band around thrp decided in FP64
 
 struct MixedWork {
   TcGemm tc;
@@ -90,32 +90,35 @@ __global__ void k_pt_recheck(const int *__restrict__ rows, int nrc, const int *_
   int k = cand_k[r];
   int i = k / nv, a = k - i * nv;
   double de_r = de_all[k];
-  double s = 0.0;
   const double *pr = Pia + (int64_t)N * k;
-  for (int c = threadIdx.x; c < nex; c += blockDim.x) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarp = blockDim.x >> 5;
+  double s = 0.0;   // meaningful in lane 0 of each warp
+  for (int c = warp; c < nex; c += nwarp) {
     int kc = pk[c];
     int j = kc / nv, b = kc - j * nv;
     const double *qc = Qia + (int64_t)N * kc;
     const double *pij = Poo + (int64_t)N * ((int64_t)i * no + j);
     const double *qab = Qvv + (int64_t)N * ((int64_t)a * nv + b);
     double kv = 0.0, jv = 0.0;
-    for (int A = 0; A < N; ++A) {
+    for (int A = lane; A < N; A += 32) {
       kv += pr[A] * qc[A];
       jv += pij[A] * qab[A];
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      kv += __shfl_xor_sync(0xffffffffu, kv, o);
+      jv += __shfl_xor_sync(0xffffffffu, jv, o);
     }
     double amat = ak * kv - jv;
     s += amat * amat / (de_r - ed[c] + 1e-10);
   }
-  __shared__ double red[256];
-  red[threadIdx.x] = s;
+  __shared__ double red[32];
+  if (lane == 0) red[warp] = s;
   __syncthreads();
-  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
-    if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
-    __syncthreads();
-  }
   if (threadIdx.x == 0) {
-    pert_out[r] = red[0];
-    sel[r] = red[0] > thrp ? 1 : 0;
+    double t = 0.0;
+    for (int w = 0; w < nwarp; ++w) t += red[w];
+    pert_out[r] = t;
+    sel[r] = t > thrp ? 1 : 0;
   }
 }
 

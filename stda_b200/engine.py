@@ -88,7 +88,8 @@ def library():
         lib.std2g_kernel_launches.argtypes = [C.c_void_p]
         lib.std2g_kernel_launches.restype = C.c_int64
         lib.std2g_kernel_stats.argtypes = [C.c_void_p, dp, C.POINTER(C.c_int64), dp]
-        lib.std2g_solver_stats.argtypes = [C.c_void_p, ip, C.POINTER(C.c_int64)]
+        lib.std2g_solver_stats.argtypes = [C.c_void_p, ip, C.POINTER(C.c_int64),
+                                            C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
         lib.std2g_screen_noalloc.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                                               C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                               C.POINTER(Params), C.c_void_p, C.c_void_p,
@@ -286,9 +287,11 @@ class Engine:
 
     def solver_stats(self):
         it = C.c_int()
-        mv = C.c_int64()
-        _check(self.lib.std2g_solver_stats(self.ctx, C.byref(it), C.byref(mv)))
-        return {"davidson_iters": it.value, "sigma_vectors": mv.value}
+        mv, mv64, rc = C.c_int64(), C.c_int64(), C.c_int64()
+        _check(self.lib.std2g_solver_stats(self.ctx, C.byref(it), C.byref(mv), C.byref(mv64),
+                                           C.byref(rc)))
+        return {"davidson_iters": it.value, "sigma_vectors_mixed": mv.value,
+                "sigma_vectors_fp64": mv64.value, "pt_rechecked_fp64": rc.value}
 
     def kernel_launches(self):
         return int(self.lib.std2g_kernel_launches(self.ctx))
