@@ -20,6 +20,7 @@
 #include "kernels_fp64.cuh"
 #include "davidson.cuh"
 #include "matfree.cuh"
+#include "matfree_tc.cuh"
 #include "mixed.cuh"
 
 namespace std2g {
@@ -79,6 +80,7 @@ struct Ctx {
   MixedWork mixed;
   DavidsonWork dav;
   MatFree mf;
+  MatFreeTc mftc;
   // tensor-core contraction statistics of the last solve
   double tc_ms = 0, tc_flop = 0;
   int64_t tc_launches = 0;
@@ -675,11 +677,23 @@ static void solve(Ctx &c, const std2g_params &p_in, std2g_result *res, const Res
     mf.nv = nv;
     mf.nci = nci;
     mf.nao = nao;
-    mf.f32 = mixed;
-    if (mixed)
-      mf_setup_ops<float>(mf, mf.f, s, Clow, c.d_slot_ao.get(), Poo, Pia, Qs, Ps, p.velcorr);
-    else
+    mf.f32 = false;
+    if (mixed) {
+      // tensor-core products for the first Davidson stage
+      MatFreeTc &w = c.mftc;
+      w.N = N;
+      w.maxa = c.maxa;
+      w.no = no;
+      w.nv = nv;
+      w.nci = nci;
+      w.Qs = Qs;
+      w.Ps = Ps;
+      w.ci = d_ci;
+      w.ca = d_ca;
+      mftc_setup(w, s, Clow, nao, c.d_slot_ao.get(), Poo);
+    } else {
       mf_setup_ops<double>(mf, mf.d, s, Clow, c.d_slot_ao.get(), Poo, Pia, Qs, Ps, p.velcorr);
+    }
     mf.ci = d_ci;
     mf.ca = d_ca;
     S2G_LAUNCH(k_mf_diag, (int)div_up(nci, 128), 128, 0, s, mf.dA.ensure(nci), d_edall, ekd, uci,
@@ -700,7 +714,10 @@ static void solve(Ctx &c, const std2g_params &p_in, std2g_result *res, const Res
     if (mixed) {
       // stage 1: tensor-core (split-BF16 FP32) products; stage 2: FP64 products
       // from those Ritz vectors until the FP64 residuals meet tol
-      davidson(c.dav, c.blas, c.solver, s, mv, d_edall, nci, p.nroots, tol, 300, om, Xd);
+      MatVec mv_tc = [&](const double *V, int nb, double *W) {
+        mftc_apply(c.mftc, c.blas, s, V, nb, W, ak, -1.0, c.mf.dA.get());
+      };
+      davidson(c.dav, c.blas, c.solver, s, mv_tc, d_edall, nci, p.nroots, tol, 300, om, Xd);
       c.dav_iters = c.dav.iters;
       c.dav_matvecs = c.dav.matvecs;
       mf_setup_ops<double>(c.mf, c.mf.d, s, Clow, c.d_slot_ao.get(), Poo, Pia, Qs, Ps, p.velcorr);

@@ -22,6 +22,7 @@ struct MixedWork {
   DBuf<__nv_bfloat16> bq_hi, bq_lo, bv_hi, bv_lo, a_hi, a_lo, w_hi, w_lo;
   DBuf<float> K, J;
   DBuf<int> recheck;
+  DBuf<double> recheck_part;
   double *lastX = nullptr;
   int Kpad = 0;
   int64_t ldK = 0, ldJ = 0;
@@ -82,8 +83,8 @@ __global__ void k_pt_recheck(const int *__restrict__ rows, int nrc, const int *_
                              const double *__restrict__ Qia, const double *__restrict__ Poo,
                              const double *__restrict__ Qvv, int N, int no, int nv,
                              const double *__restrict__ de_all, const double *__restrict__ ed,
-                             double ak, double thrp, double *__restrict__ pert_out,
-                             unsigned char *__restrict__ sel) {
+                             double ak, double *__restrict__ part) {
+  // grid (nrc, nsplit): block (q, y) sums couplings c = y*8 + warp (+ nsplit*8 ...)
   int q = blockIdx.x;
   if (q >= nrc) return;
   int r = rows[q];
@@ -93,7 +94,7 @@ __global__ void k_pt_recheck(const int *__restrict__ rows, int nrc, const int *_
   const double *pr = Pia + (int64_t)N * k;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarp = blockDim.x >> 5;
   double s = 0.0;   // meaningful in lane 0 of each warp
-  for (int c = warp; c < nex; c += nwarp) {
+  for (int c = blockIdx.y * nwarp + warp; c < nex; c += gridDim.y * nwarp) {
     int kc = pk[c];
     int j = kc / nv, b = kc - j * nv;
     const double *qc = Qia + (int64_t)N * kc;
@@ -117,9 +118,20 @@ __global__ void k_pt_recheck(const int *__restrict__ rows, int nrc, const int *_
   if (threadIdx.x == 0) {
     double t = 0.0;
     for (int w = 0; w < nwarp; ++w) t += red[w];
-    pert_out[r] = t;
-    sel[r] = t > thrp ? 1 : 0;
+    part[(int64_t)q * gridDim.y + blockIdx.y] = t;
   }
+}
+
+// pert[rows[q]] = sum_y part[q][y] (fixed order); selection pert > thrp
+__global__ void k_pt_recheck_finish(const int *__restrict__ rows, int nrc, int nsplit,
+                                    const double *__restrict__ part, double thrp,
+                                    double *__restrict__ pert_out, unsigned char *__restrict__ sel) {
+  int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= nrc) return;
+  double t = 0.0;
+  for (int y = 0; y < nsplit; ++y) t += part[(int64_t)q * nsplit + y];
+  pert_out[rows[q]] = t;
+  sel[rows[q]] = t > thrp ? 1 : 0;
 }
 
 // Rows whose mixed-precision PT sum lies within kRecheckBand of thrp get their
@@ -138,8 +150,13 @@ inline void mixed_pt_recheck(MixedWork &mw, cudaStream_t s, double *pert, unsign
   if (rows.empty()) return;
   int *d = mw.recheck.ensure(rows.size());
   S2G_CUDA(cudaMemcpyAsync(d, rows.data(), sizeof(int) * rows.size(), cudaMemcpyHostToDevice, s));
-  S2G_LAUNCH(k_pt_recheck, (int)rows.size(), 256, 0, s, d, (int)rows.size(), cand_k, pk, nex, Pia,
-             Qia, Poo, Qvv, N, no, nv, de_all, ed, ak, thrp, pert, sel);
+  const int nrc = (int)rows.size();
+  const int nsplit = (int)std::max<int64_t>(1, std::min<int64_t>(div_up(nex, 64), 128));
+  double *part = mw.recheck_part.ensure((size_t)nrc * nsplit);
+  S2G_LAUNCH(k_pt_recheck, dim3((unsigned)nrc, (unsigned)nsplit), 256, 0, s, d, nrc, cand_k, pk,
+             nex, Pia, Qia, Poo, Qvv, N, no, nv, de_all, ed, ak, part);
+  S2G_LAUNCH(k_pt_recheck_finish, (int)div_up(nrc, 128), 128, 0, s, d, nrc, nsplit, part, thrp,
+             pert, sel);
   mw.rechecked += (int64_t)rows.size();
 }
 

@@ -88,12 +88,14 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int *e
   }
 }
 
-__device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, uint64_t *bar,
-                                            int x, int y) {
+// 3-D tiled TMA load (x = K offset, y = row, z = batch); x is a multiple of 64
+// elements, i.e. 128-byte aligned
+__device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, uint64_t *bar,
+                                            int x, int y, int z) {
   asm volatile(
-      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes"
-      " [%0], [%1, {%3, %4}], [%2];" ::"r"(smem_u32(dst)),
-      "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(x), "r"(y)
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%3, %4, %5}], [%2];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(x), "r"(y), "r"(z)
       : "memory");
 }
 
@@ -147,7 +149,8 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float *v) {
 __global__ void __launch_bounds__(256, 1)
 k_tc_gemm_bf16x3(const __grid_constant__ CUtensorMap mAh, const __grid_constant__ CUtensorMap mAl,
                  const __grid_constant__ CUtensorMap mBh, const __grid_constant__ CUtensorMap mBl,
-                 float *__restrict__ D, int64_t ldd, int M, int N, int Kpad, int *err) {
+                 float *__restrict__ D, int64_t ldd, int64_t bstride_d, int M, int N, int Kpad,
+                 int b_batched, int *err) {
   using namespace tc;
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char *base = (unsigned char *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
@@ -158,6 +161,8 @@ k_tc_gemm_bf16x3(const __grid_constant__ CUtensorMap mAh, const __grid_constant_
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
+  const int za = blockIdx.z, zb = b_batched ? (int)blockIdx.z : 0;
+  D += (int64_t)blockIdx.z * bstride_d;
   const int nk = Kpad / BK;
 
   if (threadIdx.x == 0) {
@@ -187,10 +192,10 @@ k_tc_gemm_bf16x3(const __grid_constant__ CUtensorMap mAh, const __grid_constant_
       if (kb >= STAGES && !mbar_wait(&empty[s], ((kb / STAGES) - 1) & 1, err, 1)) break;
       unsigned char *st = base + s * STAGE_BYTES;
       mbar_expect_tx(&full[s], STAGE_BYTES);
-      tma_load_2d(st, &mAh, &full[s], kb * BK, m0);
-      tma_load_2d(st + TILE_A, &mAl, &full[s], kb * BK, m0);
-      tma_load_2d(st + 2 * TILE_A, &mBh, &full[s], kb * BK, n0);
-      tma_load_2d(st + 2 * TILE_A + TILE_B, &mBl, &full[s], kb * BK, n0);
+      tma_load_3d(st, &mAh, &full[s], kb * BK, m0, za);
+      tma_load_3d(st + TILE_A, &mAl, &full[s], kb * BK, m0, za);
+      tma_load_3d(st + 2 * TILE_A, &mBh, &full[s], kb * BK, n0, zb);
+      tma_load_3d(st + 2 * TILE_A + TILE_B, &mBl, &full[s], kb * BK, n0, zb);
     }
   } else if (warp == 1 && lane == 0) {
     // ---- MMA issuer ----
@@ -273,6 +278,7 @@ struct TcGemm {
   bool ready = false;
   double ms = 0, flop = 0;
   int64_t launches = 0;
+  bool armed = false;
   cudaEvent_t e0 = nullptr, e1 = nullptr;
 
   void init() {
@@ -290,13 +296,14 @@ struct TcGemm {
     ready = true;
   }
 
-  CUtensorMap map(const __nv_bfloat16 *p, int64_t rows, int Kpad, int box_rows) {
+  // rows x Kpad BF16 matrices, `batch` of them `rows*Kpad` elements apart
+  CUtensorMap map(const __nv_bfloat16 *p, int64_t rows, int Kpad, int box_rows, int batch = 1) {
     CUtensorMap m;
-    cuuint64_t dims[2] = {(cuuint64_t)Kpad, (cuuint64_t)rows};
-    cuuint64_t strides[1] = {(cuuint64_t)Kpad * 2};
-    cuuint32_t box[2] = {(cuuint32_t)tc::BK, (cuuint32_t)box_rows};
-    cuuint32_t estr[2] = {1, 1};
-    CUresult r = encode(&m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, (void *)p, dims, strides, box,
+    cuuint64_t dims[3] = {(cuuint64_t)Kpad, (cuuint64_t)rows, (cuuint64_t)batch};
+    cuuint64_t strides[2] = {(cuuint64_t)Kpad * 2, (cuuint64_t)rows * Kpad * 2};
+    cuuint32_t box[3] = {(cuuint32_t)tc::BK, (cuuint32_t)box_rows, 1};
+    cuuint32_t estr[3] = {1, 1, 1};
+    CUresult r = encode(&m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, (void *)p, dims, strides, box,
                         estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
                         CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS)
@@ -304,11 +311,13 @@ struct TcGemm {
     return m;
   }
 
-  // D (M x N, row-major ldd) = A (M x Kpad) B (N x Kpad)^T, split-BF16 operands.
-  // nflop: algorithmic FLOPs credited to this launch (2 M N K_true).
+  // D (M x N, row-major ldd) = A (M x Kpad) B (N x Kpad)^T, split-BF16 operands,
+  // for `batch` independent problems (A, D batched; B batched when b_batched).
+  // nflop: algorithmic FLOPs credited to this launch (2 M N K_true per problem).
   void run(cudaStream_t s, const __nv_bfloat16 *Ah, const __nv_bfloat16 *Al,
            const __nv_bfloat16 *Bh, const __nv_bfloat16 *Bl, int M, int N, int Kpad, float *D,
-           int64_t ldd, double nflop) {
+           int64_t ldd, double nflop, int batch = 1, bool b_batched = false,
+           int64_t bstride_d = 0, bool sync = true) {
     init();
     if (M <= 0 || N <= 0) return;
     if (Kpad % tc::BK != 0) throw Error{STD2G_EINVAL, "tc_gemm: K not padded to 64"};
@@ -316,26 +325,41 @@ struct TcGemm {
       throw Error{STD2G_EINVAL, "tc_gemm: operands not 16-byte aligned"};
     if ((ldd % 4) != 0 || ((uintptr_t)D & 15))
       throw Error{STD2G_EINVAL, "tc_gemm: output not 16-byte aligned"};
-    CUtensorMap ah = map(Ah, M, Kpad, tc::BM), al = map(Al, M, Kpad, tc::BM);
-    CUtensorMap bh = map(Bh, N, Kpad, tc::BN), bl = map(Bl, N, Kpad, tc::BN);
+    if (batch < 1 || batch > 65535) throw Error{STD2G_EINVAL, "tc_gemm: bad batch"};
+    if (batch > 1 && ((bstride_d % 4) != 0)) throw Error{STD2G_EINVAL, "tc_gemm: batch stride"};
+    CUtensorMap ah = map(Ah, M, Kpad, tc::BM, batch), al = map(Al, M, Kpad, tc::BM, batch);
+    CUtensorMap bh = map(Bh, N, Kpad, tc::BN, b_batched ? batch : 1);
+    CUtensorMap bl = map(Bl, N, Kpad, tc::BN, b_batched ? batch : 1);
     int *e = err.ensure(1);
-    S2G_CUDA(cudaMemsetAsync(e, 0, sizeof(int), s));
-    dim3 grid((unsigned)div_up(N, tc::BN), (unsigned)div_up(M, tc::BM));
+    if (!armed) {
+      S2G_CUDA(cudaMemsetAsync(e, 0, sizeof(int), s));
+      armed = true;
+    }
+    dim3 grid((unsigned)div_up(N, tc::BN), (unsigned)div_up(M, tc::BM), (unsigned)batch);
     if (grid.y > 65535) throw Error{STD2G_EINVAL, "tc_gemm: M too large for one launch"};
-    S2G_CUDA(cudaEventRecord(e0, s));
-    S2G_LAUNCH(k_tc_gemm_bf16x3, grid, 256, tc::SMEM_BYTES, s, ah, al, bh, bl, D, ldd, M, N,
-               Kpad, e);
-    S2G_CUDA(cudaEventRecord(e1, s));
+    if (sync) S2G_CUDA(cudaEventRecord(e0, s));
+    S2G_LAUNCH(k_tc_gemm_bf16x3, grid, 256, tc::SMEM_BYTES, s, ah, al, bh, bl, D, ldd, bstride_d,
+               M, N, Kpad, b_batched ? 1 : 0, e);
+    ++launches;
+    flop += nflop * batch;
+    if (sync) {
+      S2G_CUDA(cudaEventRecord(e1, s));
+      check(s);
+      float t = 0;
+      S2G_CUDA(cudaEventElapsedTime(&t, e0, e1));
+      ms += t;
+    }
+  }
+
+  // read the error flag of the launches since the last check (synchronises)
+  void check(cudaStream_t s) {
+    if (!armed) return;
     int h_err = 0;
-    S2G_CUDA(cudaMemcpyAsync(&h_err, e, sizeof(int), cudaMemcpyDeviceToHost, s));
+    S2G_CUDA(cudaMemcpyAsync(&h_err, err.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
     S2G_CUDA(cudaStreamSynchronize(s));
+    armed = false;
     if (h_err)
       throw Error{STD2G_ETIMEOUT, "tc_gemm: bounded wait expired (" + std::to_string(h_err) + ")"};
-    float t = 0;
-    S2G_CUDA(cudaEventElapsedTime(&t, e0, e1));
-    ms += t;
-    flop += nflop;
-    ++launches;
   }
 };
 
