@@ -89,10 +89,11 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def build_workload():
+def build_workload(n=8):
+    """Flake C_{6n^2}H_{6n}; n = 8 is the benchmark workload (C384H48)."""
     from stda_b200 import synth
     from stda_b200.engine import boundary_inputs
-    mol, ints = synth.graphene_flake(8, with_ints=True)
+    mol, ints = synth.graphene_flake(n, with_ints=True)
     return mol, ints, boundary_inputs(mol, ints)
 
 
@@ -108,7 +109,7 @@ def cpu_sample(mol, ints, budget_s=15.0):
 def run_reference(args):
     if int(os.environ.get("RANK", "0")) != 0:
         return
-    mol, ints, _ = build_workload()
+    mol, ints, _ = build_workload(args.flake)
     times, info = [], None
     for step in range(args.warmup + args.steps):
         info = cpu_sample(mol, ints, budget_s=args.cpu_budget)
@@ -138,6 +139,9 @@ def main():
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64-form comparison")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--cpu-budget", type=float, default=15.0)
+    ap.add_argument("--flake", type=int, default=8,
+                    help="flake size n of C_{6n^2}H_{6n}; 8 = the benchmark workload, smaller "
+                         "values are profiling cases")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     if args.impl == "reference":
@@ -156,7 +160,7 @@ def main():
         dist = dist_
 
     from stda_b200.engine import Engine, Keywords
-    mol, ints, b = build_workload()
+    mol, ints, b = build_workload(args.flake)
     prec = 1 if args.precision == "mixed" else 0
     kw = Keywords(**KW)
     eng = Engine(local, prec)
@@ -215,7 +219,8 @@ def main():
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
            "dtype": "bf16x3->f32 contractions, f64 screen/RR" if prec else "f64",
            "data": "synthetic",
-           "config": {"workload": WORKLOAD, "nci": sol.nci, "nex": sol.nex, "nexpt": sol.nexpt,
+           "config": {"workload": WORKLOAD if args.flake == 8 else f"flake n={args.flake} (profiling case)",
+                      "nci": sol.nci, "nex": sol.nex, "nexpt": sol.nexpt,
                       "new_pt": sol.new, "no": sol.no, "nv": sol.nv, "nroots": len(sol.omega),
                       "parallelism": f"replicas x{world}",
                       "l2": "inputs > L2: per-solve charge/PT buffers are GBs"},

@@ -111,6 +111,22 @@ __global__ void k_scale_by(double *__restrict__ T, int n, int ncol, const double
   }
 }
 
+// H[c + ld*r] = H[r + ld*c] for rows r < m of the new columns c in [m, m+nb)
+__global__ void k_mirror_cols(double *__restrict__ H, int ld, int m, int nb) {
+  int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= (int64_t)m * nb) return;
+  int c = m + (int)(t / m), r = (int)(t % m);
+  H[c + (int64_t)ld * r] = H[r + (int64_t)ld * c];
+}
+
+// H[0:k, 0:k] = diag(theta)
+__global__ void k_diag_matrix(double *__restrict__ H, int ld, int k, const double *__restrict__ th) {
+  int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= (int64_t)k * k) return;
+  int c = (int)(t / k), r = (int)(t % k);
+  H[r + (int64_t)ld * c] = r == c ? th[r] : 0.0;
+}
+
 // d[j] = A[j + lda*j]
 __global__ void k_diag_of(const double *__restrict__ A, int lda, int n, double *__restrict__ d) {
   int j = blockIdx.x * blockDim.x + threadIdx.x;
@@ -118,7 +134,7 @@ __global__ void k_diag_of(const double *__restrict__ A, int lda, int n, double *
 }
 
 struct DavidsonWork {
-  DBuf<double> V, W, Hs, theta, X, R, T, tmp, rn, proj, G, Gc, lam, work2;
+  DBuf<double> V, W, H, Hs, theta, X, R, T, tmp, rn, proj, G, Gc, lam, work2;
   DBuf<int> cols, idx, info;
   DBuf<double> work;
   int iters = 0;
@@ -135,15 +151,16 @@ using MatVec = std::function<void(const double *V, int nb, double *W)>;
 inline int davidson(DavidsonWork &dw, cublasHandle_t blas, cusolverDnHandle_t sol,
                     cudaStream_t s, const MatVec &mv, const double *diag, int n, int k,
                     double tol, int max_iter, double *omega_out, double *X_out,
-                    bool warm = false) {
+                    bool warm = false, bool buffer_roots = true) {
   if (k > n) k = n;
   const int kwant = k;
-  k = std::min(n, k + std::max(4, k / 2));
+  if (buffer_roots) k = std::min(n, k + std::max(4, k / 2));
   const int mmax = std::min(n, std::max(4 * k, k + 32));
   const int grid = 148 * 4;
   if (warm && dw.X.n < (size_t)n * k) warm = false;
   double *V = dw.V.ensure((size_t)n * mmax), *W = dw.W.ensure((size_t)n * mmax);
   double *Hs = dw.Hs.ensure((size_t)mmax * mmax);
+  double *H = dw.H.ensure((size_t)mmax * mmax);   // V^T W, kept across iterations (ld mmax)
   double *theta = dw.theta.ensure(mmax), *X = dw.X.ensure((size_t)n * k);
   double *R = dw.R.ensure((size_t)n * k), *T = dw.T.ensure((size_t)n * k);
   double *tmp = dw.tmp.ensure((size_t)n * k), *rn = dw.rn.ensure(k + 2);
@@ -178,9 +195,15 @@ inline int davidson(DavidsonWork &dw, cublasHandle_t blas, cusolverDnHandle_t so
     dw.iters = it + 1;
     mv(V + (size_t)n * m, nb, W + (size_t)n * m);
     dw.matvecs += nb;
+    // H = V^T W (ld mmax): only the new columns are formed; the new rows
+    // follow from the symmetry of A
+    S2G_CUBLAS(cublasDgemm(blas, CUBLAS_OP_T, CUBLAS_OP_N, m + nb, nb, n, &one, V, n,
+                           W + (size_t)n * m, n, &zero, H + (size_t)mmax * m, mmax));
+    if (m > 0)
+      S2G_LAUNCH(k_mirror_cols, (int)div_up((int64_t)m * nb, 256), 256, 0, s, H, mmax, m, nb);
     m += nb;
-    // H = V^T W (m x m), Ritz pairs in FP64
-    S2G_CUBLAS(cublasDgemm(blas, CUBLAS_OP_T, CUBLAS_OP_N, m, m, n, &one, V, n, W, n, &zero, Hs, m));
+    S2G_CUDA(cudaMemcpy2DAsync(Hs, sizeof(double) * m, H, sizeof(double) * mmax,
+                               sizeof(double) * m, m, cudaMemcpyDeviceToDevice, s));
     S2G_CUSOLVER(cusolverDnDsyevd(sol, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, m, Hs, m,
                                   theta, work, lwork, info));
     // Ritz vectors X = V Y_k, residuals R = W Y_k - X theta
@@ -209,6 +232,8 @@ inline int davidson(DavidsonWork &dw, cublasHandle_t blas, cusolverDnHandle_t so
       S2G_CUDA(cudaMemcpyAsync(W, tmp, sizeof(double) * n * k, cudaMemcpyDeviceToDevice, s));
       S2G_CUDA(cudaMemcpyAsync(V, X, sizeof(double) * n * k, cudaMemcpyDeviceToDevice, s));
       m = k;
+      // H restricted to the Ritz vectors is diag(theta)
+      S2G_LAUNCH(k_diag_matrix, (int)div_up((int64_t)k * k, 256), 256, 0, s, H, mmax, k, theta);
     }
     // block orthogonalisation of the corrections: normalise, project out V twice
     // (classical Gram-Schmidt as GEMMs), then orthonormalise the block through

@@ -723,7 +723,7 @@ static void solve(Ctx &c, const std2g_params &p_in, std2g_result *res, const Res
       mf_setup_ops<double>(c.mf, c.mf.d, s, Clow, c.d_slot_ao.get(), Poo, Pia, Qs, Ps, p.velcorr);
       c.mf.f32 = false;
       conv = davidson(c.dav, c.blas, c.solver, s, mv, d_edall, nci, p.nroots, tol, 100, om, Xd,
-                      true);
+                      true, false);
       c.dav_iters += c.dav.iters;
       c.dav_fp64_matvecs = c.dav.matvecs;   // B X of the velocity correction also in FP64
     } else {
