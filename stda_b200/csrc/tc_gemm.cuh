@@ -13,10 +13,10 @@
 // (ptselect stda.f:1812-1819; rtdamat stda.f:2040-2046):
 //   (ia|jb) = sum_A p_ia^A q_jb^A    and    (ij|ab) = sum_A p_ij^A q_ab^A.
 //
-// One CTA computes one 128 x 128 tile: warp 0 issues TMA loads into a
-// 3-stage shared-memory ring, warp 1 issues tcgen05.mma from one thread,
-// warp 2 owns the TMEM allocation, warps 4-7 drain the accumulator
-// (tcgen05.ld) and store to global memory.  Every mbarrier wait is bounded by
+// Persistent CTAs (one per SM) walk 128 x 128 tiles: warp 0 issues TMA loads
+// into a 3-stage shared-memory ring, warp 1 issues tcgen05.mma from one thread
+// into one of two TMEM accumulators, warp 2 owns the TMEM allocation, warps
+// 4-7 drain the other accumulator (tcgen05.ld) and store to global memory.  Every mbarrier wait is bounded by
 // a ~2 s wall-clock limit; on expiry the CTA records the failure in *err and
 // leaves without touching memory further.
 #pragma once
@@ -38,7 +38,7 @@ constexpr int STAGES = 3;
 constexpr int TILE_A = BM * BK * 2;   // bytes per operand tile
 constexpr int TILE_B = BN * BK * 2;
 constexpr int STAGE_BYTES = 2 * TILE_A + 2 * TILE_B;
-constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256;
+constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256;   // ring + barriers + slack
 constexpr unsigned long long kWaitNs = 2000000000ull;   // 2 s per wait
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
@@ -146,38 +146,50 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float *v) {
 
 }  // namespace tc
 
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(tc::smem_u32(bar)) : "memory");
+}
+
+// Persistent kernel: CTA b handles tiles b, b + gridDim.x, ... of the
+// (batch, M/128, N/128) tile space.  The TMEM accumulator is double-buffered
+// (2 x BN columns) so that the epilogue of one tile overlaps the MMAs of the
+// next; the TMA producer runs ahead across tile boundaries through the
+// 3-stage shared-memory ring.
 __global__ void __launch_bounds__(256, 1)
 k_tc_gemm_bf16x3(const __grid_constant__ CUtensorMap mAh, const __grid_constant__ CUtensorMap mAl,
                  const __grid_constant__ CUtensorMap mBh, const __grid_constant__ CUtensorMap mBl,
                  float *__restrict__ D, int64_t ldd, int64_t bstride_d, int M, int N, int Kpad,
-                 int b_batched, int *err) {
+                 int b_batched, int batch, int *err) {
   using namespace tc;
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char *base = (unsigned char *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   uint64_t *full = (uint64_t *)(base + STAGES * STAGE_BYTES);
   uint64_t *empty = full + STAGES;
-  uint64_t *done = empty + STAGES;
-  uint32_t *tmem_slot = (uint32_t *)(done + 1);
+  uint64_t *acc_full = empty + STAGES;     // [2]
+  uint64_t *acc_empty = acc_full + 2;      // [2]
+  uint32_t *tmem_slot = (uint32_t *)(acc_empty + 2);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
-  const int za = blockIdx.z, zb = b_batched ? (int)blockIdx.z : 0;
-  D += (int64_t)blockIdx.z * bstride_d;
   const int nk = Kpad / BK;
+  const int tiles_n = (N + BN - 1) / BN, tiles_m = (M + BM - 1) / BM;
+  const int64_t ntiles = (int64_t)tiles_n * tiles_m * batch;
 
   if (threadIdx.x == 0) {
-    for (int s = 0; s < STAGES; ++s) {
-      mbar_init(&full[s], 1);
-      mbar_init(&empty[s], 1);
+    for (int q = 0; q < STAGES; ++q) {
+      mbar_init(&full[q], 1);
+      mbar_init(&empty[q], 1);
     }
-    mbar_init(done, 1);
+    for (int q = 0; q < 2; ++q) {
+      mbar_init(&acc_full[q], 1);
+      mbar_init(&acc_empty[q], 128);   // every epilogue thread arrives
+    }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   }
   if (warp == 2) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
                      smem_u32(tmem_slot)),
-                 "r"(BN));
+                 "r"(2 * BN));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -187,52 +199,78 @@ k_tc_gemm_bf16x3(const __grid_constant__ CUtensorMap mAh, const __grid_constant_
 
   if (warp == 0 && lane == 0) {
     // ---- TMA producer ----
-    for (int kb = 0; kb < nk; ++kb) {
-      const int s = kb % STAGES;
-      if (kb >= STAGES && !mbar_wait(&empty[s], ((kb / STAGES) - 1) & 1, err, 1)) break;
-      unsigned char *st = base + s * STAGE_BYTES;
-      mbar_expect_tx(&full[s], STAGE_BYTES);
-      tma_load_3d(st, &mAh, &full[s], kb * BK, m0, za);
-      tma_load_3d(st + TILE_A, &mAl, &full[s], kb * BK, m0, za);
-      tma_load_3d(st + 2 * TILE_A, &mBh, &full[s], kb * BK, n0, zb);
-      tma_load_3d(st + 2 * TILE_A + TILE_B, &mBl, &full[s], kb * BK, n0, zb);
+    int64_t it = 0;
+    bool ok = true;
+    for (int64_t t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
+      const int tn = (int)(t % tiles_n);
+      const int64_t rest = t / tiles_n;
+      const int tm = (int)(rest % tiles_m), z = (int)(rest / tiles_m);
+      const int zb = b_batched ? z : 0;
+      for (int kb = 0; kb < nk; ++kb, ++it) {
+        const int s = (int)(it % STAGES);
+        if (it >= STAGES && !mbar_wait(&empty[s], (uint32_t)(((it / STAGES) - 1) & 1), err, 1)) {
+          ok = false;
+          break;
+        }
+        unsigned char *st = base + s * STAGE_BYTES;
+        mbar_expect_tx(&full[s], STAGE_BYTES);
+        tma_load_3d(st, &mAh, &full[s], kb * BK, tm * BM, z);
+        tma_load_3d(st + TILE_A, &mAl, &full[s], kb * BK, tm * BM, z);
+        tma_load_3d(st + 2 * TILE_A, &mBh, &full[s], kb * BK, tn * BN, zb);
+        tma_load_3d(st + 2 * TILE_A + TILE_B, &mBl, &full[s], kb * BK, tn * BN, zb);
+      }
     }
   } else if (warp == 1 && lane == 0) {
     // ---- MMA issuer ----
+    int64_t it = 0, lt = 0;
     bool ok = true;
-    for (int kb = 0; kb < nk && ok; ++kb) {
-      const int s = kb % STAGES;
-      if (!mbar_wait(&full[s], (kb / STAGES) & 1, err, 2)) {
-        ok = false;
-        break;
-      }
+    for (int64_t t = blockIdx.x; t < ntiles && ok; t += gridDim.x, ++lt) {
+      const int ab = (int)(lt & 1);
+      if (lt >= 2 && !mbar_wait(&acc_empty[ab], (uint32_t)(((lt >> 1) - 1) & 1), err, 4)) break;
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      const uint32_t st = smem_u32(base + s * STAGE_BYTES);
-      const uint32_t ah = st, al = st + TILE_A, bh = st + 2 * TILE_A, bl = st + 2 * TILE_A + TILE_B;
+      const uint32_t dacc = tmem + (uint32_t)(ab * BN);
+      for (int kb = 0; kb < nk; ++kb, ++it) {
+        const int s = (int)(it % STAGES);
+        if (!mbar_wait(&full[s], (uint32_t)((it / STAGES) & 1), err, 2)) {
+          ok = false;
+          break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint32_t st = smem_u32(base + s * STAGE_BYTES);
+        const uint32_t ah = st, al = st + TILE_A, bh = st + 2 * TILE_A,
+                       bl = st + 2 * TILE_A + TILE_B;
 #pragma unroll
-      for (int kk = 0; kk < BK / 16; ++kk) {
-        const uint32_t off = kk * 32;   // 16 BF16 = 32 bytes along K
-        const uint32_t acc0 = (kb > 0 || kk > 0) ? 1u : 0u;
-        umma_bf16(tmem, tc::umma_desc(ah + off), tc::umma_desc(bh + off), acc0);
-        umma_bf16(tmem, tc::umma_desc(ah + off), tc::umma_desc(bl + off), 1u);
-        umma_bf16(tmem, tc::umma_desc(al + off), tc::umma_desc(bh + off), 1u);
+        for (int kk = 0; kk < BK / 16; ++kk) {
+          const uint32_t off = kk * 32;   // 16 BF16 = 32 bytes along K
+          const uint32_t acc0 = (kb > 0 || kk > 0) ? 1u : 0u;
+          umma_bf16(dacc, tc::umma_desc(ah + off), tc::umma_desc(bh + off), acc0);
+          umma_bf16(dacc, tc::umma_desc(ah + off), tc::umma_desc(bl + off), 1u);
+          umma_bf16(dacc, tc::umma_desc(al + off), tc::umma_desc(bh + off), 1u);
+        }
+        umma_commit(&empty[s]);   // stage reusable once these MMAs have read it
       }
-      umma_commit(&empty[s]);   // stage reusable once these MMAs have read it
+      if (ok) umma_commit(&acc_full[ab]);   // accumulator complete
     }
-    if (ok) umma_commit(done);
   } else if (warp >= 4) {
     // ---- epilogue: TMEM -> registers -> global ----
     const int wq = warp - 4;                 // TMEM lanes 32*wq .. 32*wq+31
-    const bool ok = mbar_wait(done, 0, err, 3);
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    if (ok) {
+    int64_t lt = 0;
+    for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x, ++lt) {
+      const int ab = (int)(lt & 1);
+      if (!mbar_wait(&acc_full[ab], (uint32_t)((lt >> 1) & 1), err, 3)) break;
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const int tn = (int)(t % tiles_n);
+      const int64_t rest = t / tiles_n;
+      const int tm = (int)(rest % tiles_m), z = (int)(rest / tiles_m);
+      const int m0 = tm * BM, n0 = tn * BN;
+      float *Dz = D + (int64_t)z * bstride_d;
       const int row = m0 + wq * 32 + lane;
       float v[16];
 #pragma unroll 1
       for (int c = 0; c < BN; c += 16) {
-        tc::tmem_ld16(tmem + ((uint32_t)(wq * 32) << 16) + c, v);
+        tc::tmem_ld16(tmem + ((uint32_t)(wq * 32) << 16) + (uint32_t)(ab * BN + c), v);
         if (row < M) {
-          float *dst = D + (int64_t)row * ldd + n0 + c;
+          float *dst = Dz + (int64_t)row * ldd + n0 + c;
           if (n0 + c + 16 <= N) {
 #pragma unroll
             for (int q = 0; q < 16; q += 4)
@@ -243,13 +281,17 @@ k_tc_gemm_bf16x3(const __grid_constant__ CUtensorMap mAh, const __grid_constant_
           }
         }
       }
+      // this thread's reads of the accumulator are complete
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      mbar_arrive(&acc_empty[ab]);
     }
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   if (warp == 2) {
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(BN));
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(2 * BN));
   }
 }
 
@@ -279,6 +321,7 @@ struct TcGemm {
   double ms = 0, flop = 0;
   int64_t launches = 0;
   bool armed = false;
+  int nsm = 148;
   cudaEvent_t e0 = nullptr, e1 = nullptr;
 
   void init() {
@@ -293,6 +336,9 @@ struct TcGemm {
                                   tc::SMEM_BYTES));
     S2G_CUDA(cudaEventCreate(&e0));
     S2G_CUDA(cudaEventCreate(&e1));
+    int dev = 0;
+    S2G_CUDA(cudaGetDevice(&dev));
+    S2G_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
     ready = true;
   }
 
@@ -335,11 +381,11 @@ struct TcGemm {
       S2G_CUDA(cudaMemsetAsync(e, 0, sizeof(int), s));
       armed = true;
     }
-    dim3 grid((unsigned)div_up(N, tc::BN), (unsigned)div_up(M, tc::BM), (unsigned)batch);
-    if (grid.y > 65535) throw Error{STD2G_EINVAL, "tc_gemm: M too large for one launch"};
+    const int64_t ntiles = div_up(N, tc::BN) * div_up(M, tc::BM) * (int64_t)batch;
+    const int grid = (int)std::min<int64_t>(ntiles, nsm);
     if (sync) S2G_CUDA(cudaEventRecord(e0, s));
     S2G_LAUNCH(k_tc_gemm_bf16x3, grid, 256, tc::SMEM_BYTES, s, ah, al, bh, bl, D, ldd, bstride_d,
-               M, N, Kpad, b_batched ? 1 : 0, e);
+               M, N, Kpad, b_batched ? 1 : 0, batch, e);
     ++launches;
     flop += nflop * batch;
     if (sync) {
