@@ -12,6 +12,7 @@
 #pragma once
 
 #include <algorithm>
+#include <chrono>
 #include <functional>
 #include <numeric>
 #include <vector>
@@ -36,25 +37,61 @@ __global__ void k_dav_precond(double *__restrict__ T, const double *__restrict__
 }
 
 // R[:, j] -= theta_j X[:, j]; rnorm[j] = ||R[:, j]||  (one block per column)
-__global__ void k_dav_resid(double *__restrict__ R, const double *__restrict__ X,
-                            const double *__restrict__ theta, int n, double *__restrict__ rnorm) {
-  int j = blockIdx.x;
-  double th = theta[j];
-  double s = 0.0;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
-    int64_t o = i + (int64_t)n * j;
-    double r = R[o] - th * X[o];
-    R[o] = r;
-    s += r * r;
-  }
-  __shared__ double red[256];
+// Column norms are reduced in two fixed-order stages so that a block of
+// columns spreads over the whole GPU: grid (kColSplit, ncol) writes partial
+// sums of squares, k_colnorm_finish adds them in order and takes the root.
+constexpr int kColSplit = 16;
+
+__device__ __forceinline__ double block_sum256(double s, double *red) {
   red[threadIdx.x] = s;
   __syncthreads();
   for (int o = blockDim.x / 2; o > 0; o >>= 1) {
     if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
     __syncthreads();
   }
-  if (threadIdx.x == 0) rnorm[j] = sqrt(red[0]);
+  return red[0];
+}
+
+// R[:, j] -= theta[j] X[:, j]; part[j*gridDim.x + b] = partial |R[:, j]|^2
+__global__ void k_dav_resid(double *__restrict__ R, const double *__restrict__ X,
+                            const double *__restrict__ theta, int n, double *__restrict__ part) {
+  const int j = blockIdx.y;
+  const double th = theta[j];
+  const int64_t chunk = (n + gridDim.x - 1) / gridDim.x;
+  const int64_t i0 = chunk * blockIdx.x, i1 = min((int64_t)n, i0 + chunk);
+  double s = 0.0;
+  for (int64_t i = i0 + threadIdx.x; i < i1; i += blockDim.x) {
+    int64_t o = i + (int64_t)n * j;
+    double r = R[o] - th * X[o];
+    R[o] = r;
+    s += r * r;
+  }
+  __shared__ double red[256];
+  s = block_sum256(s, red);
+  if (threadIdx.x == 0) part[(int64_t)j * gridDim.x + blockIdx.x] = s;
+}
+
+// part[j*gridDim.x + b] = partial |T[:, j]|^2
+__global__ void k_colnorm_part(const double *__restrict__ T, int n, double *__restrict__ part) {
+  const int j = blockIdx.y;
+  const int64_t chunk = (n + gridDim.x - 1) / gridDim.x;
+  const int64_t i0 = chunk * blockIdx.x, i1 = min((int64_t)n, i0 + chunk);
+  const double *t = T + (int64_t)n * j;
+  double s = 0.0;
+  for (int64_t i = i0 + threadIdx.x; i < i1; i += blockDim.x) s += t[i] * t[i];
+  __shared__ double red[256];
+  s = block_sum256(s, red);
+  if (threadIdx.x == 0) part[(int64_t)j * gridDim.x + blockIdx.x] = s;
+}
+
+// out[j] = sqrt(sum_b part[j*nsplit + b]), in order
+__global__ void k_colnorm_finish(const double *__restrict__ part, int nsplit, int ncol,
+                                 double *__restrict__ out) {
+  int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= ncol) return;
+  double s = 0.0;
+  for (int b = 0; b < nsplit; ++b) s += part[(int64_t)j * nsplit + b];
+  out[j] = sqrt(s);
 }
 
 // column norm of v (one block), result to out[0]
@@ -86,20 +123,6 @@ __global__ void k_unit_vectors(double *__restrict__ V, int n, const int *__restr
 }
 
 // column norms of T (one block per column)
-__global__ void k_colnorms(const double *__restrict__ T, int n, double *__restrict__ out) {
-  const double *t = T + (int64_t)n * blockIdx.x;
-  double s = 0.0;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) s += t[i] * t[i];
-  __shared__ double red[256];
-  red[threadIdx.x] = s;
-  __syncthreads();
-  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
-    if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) out[blockIdx.x] = sqrt(red[0]);
-}
-
 // T[:, j] *= f(s[j]) with mode 0: 1/s, mode 1: 1/sqrt(s)
 __global__ void k_scale_by(double *__restrict__ T, int n, int ncol, const double *__restrict__ sv,
                            int mode) {
@@ -134,12 +157,37 @@ __global__ void k_diag_of(const double *__restrict__ A, int lda, int n, double *
 }
 
 struct DavidsonWork {
-  DBuf<double> V, W, H, Hs, theta, X, R, T, tmp, rn, proj, G, Gc, lam, work2;
+  DBuf<double> V, W, H, Hs, theta, X, R, T, tmp, rn, proj, G, Gc, lam, work2, part;
   DBuf<int> cols, idx, info;
   DBuf<double> work;
   int iters = 0;
   int64_t matvecs = 0;
   double max_resid = 0;
+  // optional section timing (synchronises at every section boundary):
+  // [0] sigma products, [1] projected matrix, [2] its eigen-decomposition,
+  // [3] Ritz vectors + residuals, [4] orthogonalisation
+  bool profile = false;
+  double sec_ms[5] = {0, 0, 0, 0, 0};
+};
+
+// host wall-clock section timer used when DavidsonWork::profile is set
+struct SectionClock {
+  DavidsonWork &dw;
+  cudaStream_t s;
+  std::chrono::steady_clock::time_point t0;
+  SectionClock(DavidsonWork &w, cudaStream_t st) : dw(w), s(st) {
+    if (dw.profile) {
+      S2G_CUDA(cudaStreamSynchronize(s));
+      t0 = std::chrono::steady_clock::now();
+    }
+  }
+  void tick(int slot) {
+    if (!dw.profile) return;
+    S2G_CUDA(cudaStreamSynchronize(s));
+    auto t1 = std::chrono::steady_clock::now();
+    dw.sec_ms[slot] += std::chrono::duration<double, std::milli>(t1 - t0).count();
+    t0 = t1;
+  }
 };
 
 using MatVec = std::function<void(const double *V, int nb, double *W)>;
@@ -191,10 +239,12 @@ inline int davidson(DavidsonWork &dw, cublasHandle_t blas, cusolverDnHandle_t so
   int nconv = 0;
   dw.iters = 0;
   dw.matvecs = 0;
+  SectionClock clk(dw, s);
   for (int it = 0; it < max_iter; ++it) {
     dw.iters = it + 1;
     mv(V + (size_t)n * m, nb, W + (size_t)n * m);
     dw.matvecs += nb;
+    clk.tick(0);
     // H = V^T W (ld mmax): only the new columns are formed; the new rows
     // follow from the symmetry of A
     S2G_CUBLAS(cublasDgemm(blas, CUBLAS_OP_T, CUBLAS_OP_N, m + nb, nb, n, &one, V, n,
@@ -204,12 +254,18 @@ inline int davidson(DavidsonWork &dw, cublasHandle_t blas, cusolverDnHandle_t so
     m += nb;
     S2G_CUDA(cudaMemcpy2DAsync(Hs, sizeof(double) * m, H, sizeof(double) * mmax,
                                sizeof(double) * m, m, cudaMemcpyDeviceToDevice, s));
+    clk.tick(1);
     S2G_CUSOLVER(cusolverDnDsyevd(sol, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, m, Hs, m,
                                   theta, work, lwork, info));
+    clk.tick(2);
     // Ritz vectors X = V Y_k, residuals R = W Y_k - X theta
     S2G_CUBLAS(cublasDgemm(blas, CUBLAS_OP_N, CUBLAS_OP_N, n, k, m, &one, V, n, Hs, m, &zero, X, n));
     S2G_CUBLAS(cublasDgemm(blas, CUBLAS_OP_N, CUBLAS_OP_N, n, k, m, &one, W, n, Hs, m, &zero, R, n));
-    S2G_LAUNCH(k_dav_resid, k, 256, 0, s, R, X, theta, n, rn);
+    {
+      double *part = dw.part.ensure((size_t)k * kColSplit);
+      S2G_LAUNCH(k_dav_resid, dim3(kColSplit, (unsigned)k), 256, 0, s, R, X, theta, n, part);
+      S2G_LAUNCH(k_colnorm_finish, (int)div_up(k, 128), 128, 0, s, part, kColSplit, k, rn);
+    }
     S2G_CUDA(cudaMemcpyAsync(h_rn.data(), rn, sizeof(double) * k, cudaMemcpyDeviceToHost, s));
     S2G_CUDA(cudaStreamSynchronize(s));
     std::vector<int> unc;
@@ -221,6 +277,7 @@ inline int davidson(DavidsonWork &dw, cublasHandle_t blas, cusolverDnHandle_t so
       }
     nconv = kwant - nunc_wanted;
     dw.max_resid = *std::max_element(h_rn.begin(), h_rn.begin() + kwant);
+    clk.tick(3);
     if (nunc_wanted == 0) break;
     int nc = (int)unc.size();
     S2G_CUDA(cudaMemcpyAsync(cols, unc.data(), sizeof(int) * nc, cudaMemcpyHostToDevice, s));
@@ -235,23 +292,25 @@ inline int davidson(DavidsonWork &dw, cublasHandle_t blas, cusolverDnHandle_t so
       // H restricted to the Ritz vectors is diag(theta)
       S2G_LAUNCH(k_diag_matrix, (int)div_up((int64_t)k * k, 256), 256, 0, s, H, mmax, k, theta);
     }
-    // block orthogonalisation of the corrections: normalise, project out V twice
-    // (classical Gram-Schmidt as GEMMs), then orthonormalise the block through
-    // the eigen-decomposition of its Gram matrix, dropping dependent directions
+    // block orthogonalisation of the corrections (BCGS2): normalise, then two
+    // rounds of one block classical Gram-Schmidt projection against V (GEMMs)
+    // followed by Cholesky QR of the block, or, when its Gram matrix is not
+    // safely positive definite, orthonormalisation through the Gram matrix's
+    // eigen-decomposition that drops dependent directions
     nb = 0;
     {
       double *G = dw.G.ensure((size_t)k * k), *lam = dw.lam.ensure(k);
-      S2G_LAUNCH(k_colnorms, nc, 256, 0, s, T, n, lam);
+      double *part = dw.part.ensure((size_t)k * kColSplit);
+      S2G_LAUNCH(k_colnorm_part, dim3(kColSplit, (unsigned)nc), 256, 0, s, T, n, part);
+      S2G_LAUNCH(k_colnorm_finish, (int)div_up(nc, 128), 128, 0, s, part, kColSplit, nc, lam);
       S2G_LAUNCH(k_scale_by, grid, 256, 0, s, T, n, nc, lam, 0);
       double *Tb = T;
       int ncur = nc;
       for (int round = 0; round < 2 && ncur > 0; ++round) {
-        for (int pass = 0; pass < 2; ++pass) {
-          S2G_CUBLAS(cublasDgemm(blas, CUBLAS_OP_T, CUBLAS_OP_N, m, ncur, n, &one, V, n, Tb, n,
-                                 &zero, proj, m));
-          S2G_CUBLAS(cublasDgemm(blas, CUBLAS_OP_N, CUBLAS_OP_N, n, ncur, m, &mone, V, n, proj, m,
-                                 &one, Tb, n));
-        }
+        S2G_CUBLAS(cublasDgemm(blas, CUBLAS_OP_T, CUBLAS_OP_N, m, ncur, n, &one, V, n, Tb, n,
+                               &zero, proj, m));
+        S2G_CUBLAS(cublasDgemm(blas, CUBLAS_OP_N, CUBLAS_OP_N, n, ncur, m, &mone, V, n, proj, m,
+                               &one, Tb, n));
         // G = Tb^T Tb; Cholesky QR when G is safely positive definite
         S2G_CUBLAS(cublasDgemm(blas, CUBLAS_OP_T, CUBLAS_OP_N, ncur, ncur, n, &one, Tb, n, Tb, n,
                                &zero, G, ncur));
@@ -317,6 +376,7 @@ inline int davidson(DavidsonWork &dw, cublasHandle_t blas, cusolverDnHandle_t so
       }
       nb = ncur;
     }
+    clk.tick(4);
     if (nb == 0) break;
   }
   S2G_CUDA(cudaMemcpyAsync(omega_out, theta, sizeof(double) * kwant, cudaMemcpyDeviceToDevice, s));

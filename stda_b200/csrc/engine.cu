@@ -577,21 +577,27 @@ static void solve(Ctx &c, const std2g_params &p_in, std2g_result *res, const Res
                    nvp, nop, nr, d_ck + r0, nv, i0, de, d_pj, d_pb, d_omap, d_vmap, d_ed, ak,
                    sel + r0, cpart, kSeg);
       } else {
+        MixedWork &mw = c.mixed;
         if (!mixed_ready) {
-          mixed_pt_prepare(c.mixed, s, Qp, QvvP, N, nex, ldj);
+          mixed_pt_prepare(mw, s, Qp, QvvP, N, nex, ldj);
+          const int ncol4 = (int)round_up4(nex);
+          S2G_LAUNCH(k_pt_colinfo, (int)div_up(ncol4, 128), 128, 0, s, nex, ncol4, d_pj, d_pb,
+                     d_omap, d_vmap, mw.ldJ, d_ed, mw.jcol.ensure(ncol4), mw.eh.ensure(ncol4),
+                     mw.el.ensure(ncol4));
           mixed_ready = true;
         }
-        mixed_pt_chunk(c.mixed, s, Pc, W, N, nex, nr, ldj, ni * nop);
-        const float *Kf = c.mixed.K.get(), *Jf = c.mixed.J.get();
-        S2G_LAUNCH((k_pt_rows<float, float>), nr, 256, 0, s, Kf, Jf, c.mixed.ldJ, c.mixed.ldK, nex,
-                   nvp, nop, nr, d_ck + r0, nv, i0, de, d_pj, d_pb, d_omap, d_vmap, d_ed, ak,
-                   p.thrp, pert + r0, sel + r0);
+        mixed_pt_chunk(mw, s, Pc, W, N, nex, nr, ldj, ni * nop);
+        const float *Kf = mw.K.get(), *Jf = mw.J.get();
+        int64_t *roff = mw.roff.ensure(nr);
+        float *rhl = mw.rhl.ensure((size_t)2 * nr);
+        S2G_LAUNCH(k_pt_rows32, (int)div_up(nr, kRowWarps), 256, 0, s, Kf, Jf, mw.ldJ, mw.ldK,
+                   nex, nvp, nop, nr, d_ck + r0, nv, i0, de, mw.jcol.get(), mw.eh.get(),
+                   mw.el.get(), (float)ak, p.thrp, pert + r0, sel + r0, roff, rhl);
         // candidates whose PT sum lies near the threshold are decided in FP64
-        mixed_pt_recheck(c.mixed, s, pert + r0, sel + r0, nr, p.thrp, d_ck + r0, d_pk, nex, Pia,
-                         Qia, Poo, Qvv, N, no, nv, de, d_ed, ak);
-        S2G_LAUNCH((k_pt_cols<float, float>), cgrid, 128, 0, s, Kf, Jf, c.mixed.ldJ, c.mixed.ldK,
-                   nex, nvp, nop, nr, d_ck + r0, nv, i0, de, d_pj, d_pb, d_omap, d_vmap, d_ed, ak,
-                   sel + r0, cpart, kSeg);
+        mixed_pt_recheck(mw, s, pert + r0, sel + r0, nr, p.thrp, d_ck + r0, d_pk, nex, Pia, Qia,
+                         Poo, Qvv, N, no, nv, de, d_ed, ak);
+        S2G_LAUNCH(k_pt_cols32, cgrid, 128, 0, s, Kf, Jf, mw.ldK, nex, nr, mw.jcol.get(),
+                   mw.eh.get(), mw.el.get(), (float)ak, sel + r0, roff, rhl, cpart, kSeg);
       }
     }
     double *pt2 = c.w_pt2.ensure(nex), *edp = c.w_edp.ensure(nex);
@@ -717,15 +723,34 @@ static void solve(Ctx &c, const std2g_params &p_in, std2g_result *res, const Res
       MatVec mv_tc = [&](const double *V, int nb, double *W) {
         mftc_apply(c.mftc, c.blas, s, V, nb, W, ak, -1.0, c.mf.dA.get());
       };
+      c.dav.profile = c.opts.verbose >= 2;
+      for (double &v : c.dav.sec_ms) v = 0;
       davidson(c.dav, c.blas, c.solver, s, mv_tc, d_edall, nci, p.nroots, tol, 300, om, Xd);
       c.dav_iters = c.dav.iters;
       c.dav_matvecs = c.dav.matvecs;
+      if (c.dav.profile)
+        std::fprintf(stderr,
+                     "davidson stage 1: %d iters, sigma %.2f, H %.2f, eig %.2f, ritz %.2f, "
+                     "ortho %.2f ms\n",
+                     c.dav.iters, c.dav.sec_ms[0], c.dav.sec_ms[1], c.dav.sec_ms[2],
+                     c.dav.sec_ms[3], c.dav.sec_ms[4]);
+      for (double &v : c.dav.sec_ms) v = 0;
+      SectionClock sc(c.dav, s);
       mf_setup_ops<double>(c.mf, c.mf.d, s, Clow, c.d_slot_ao.get(), Poo, Pia, Qs, Ps, p.velcorr);
       c.mf.f32 = false;
+      sc.tick(0);
+      if (c.dav.profile) std::fprintf(stderr, "FP64 operator setup %.2f ms\n", c.dav.sec_ms[0]);
+      for (double &v : c.dav.sec_ms) v = 0;
       conv = davidson(c.dav, c.blas, c.solver, s, mv, d_edall, nci, p.nroots, tol, 100, om, Xd,
                       true, false);
       c.dav_iters += c.dav.iters;
       c.dav_fp64_matvecs = c.dav.matvecs;   // B X of the velocity correction also in FP64
+      if (c.dav.profile)
+        std::fprintf(stderr,
+                     "davidson stage 2: %d iters, sigma %.2f, H %.2f, eig %.2f, ritz %.2f, "
+                     "ortho %.2f ms\n",
+                     c.dav.iters, c.dav.sec_ms[0], c.dav.sec_ms[1], c.dav.sec_ms[2],
+                     c.dav.sec_ms[3], c.dav.sec_ms[4]);
     } else {
       conv = davidson(c.dav, c.blas, c.solver, s, mv, d_edall, nci, p.nroots, tol, 300, om, Xd);
       c.dav_iters = c.dav.iters;

@@ -142,6 +142,28 @@ __global__ void k_tcs_gather(double *__restrict__ out, const float *__restrict__
   }
 }
 
+// A second stream with its own cuBLAS handle, on which the FP64 exchange
+// part of the product runs concurrently with the tensor-core Coulomb part.
+struct SideStream {
+  cudaStream_t s = nullptr;
+  cublasHandle_t h = nullptr;
+  cudaEvent_t fork = nullptr, join = nullptr;
+  void init() {
+    if (s) return;
+    S2G_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    S2G_CUBLAS(cublasCreate(&h));
+    S2G_CUBLAS(cublasSetStream(h, s));
+    S2G_CUDA(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
+    S2G_CUDA(cudaEventCreateWithFlags(&join, cudaEventDisableTiming));
+  }
+  ~SideStream() {
+    if (h) cublasDestroy(h);
+    if (fork) cudaEventDestroy(fork);
+    if (join) cudaEventDestroy(join);
+    if (s) cudaStreamDestroy(s);
+  }
+};
+
 struct MatFreeTc {
   int N = 0, maxa = 0, no = 0, nv = 0, nci = 0, rows = 0;
   int Kv = 0, Ko = 0, KR = 0;
@@ -152,6 +174,7 @@ struct MatFreeTc {
   DBuf<__nv_bfloat16> xb_h, xb_l, zt_h, zt_l, tt_h, tt_l;
   DBuf<float> Z, T, Y;
   DBuf<double> G, Kt;
+  SideStream side;
 };
 
 // Operands fixed for the solve: Cv in both K-major orientations, P^A_oo rows.
@@ -183,15 +206,23 @@ inline void mftc_apply(MatFreeTc &w, cublasHandle_t h, cudaStream_t s, const dou
                        double *out, double cK, double cJ, const double *diag) {
   const int N = w.N, no = w.no, nv = w.nv, nci = w.nci, rows = w.rows, maxa = w.maxa;
   const int g = 148 * 8;
-  S2G_CUDA(cudaMemsetAsync(out, 0, sizeof(double) * nci * m, s));
-  if (cK != 0.0) {
+  // exchange part, out = cK Ps^T (Qs X), in FP64 on the side stream
+  const bool side = cK != 0.0;
+  if (side) {
+    w.side.init();
+    S2G_CUDA(cudaEventRecord(w.side.fork, s));
+    S2G_CUDA(cudaStreamWaitEvent(w.side.s, w.side.fork, 0));
     double *G = w.G.ensure((size_t)N * m);
     const double one = 1.0, zero = 0.0, ck = cK;
-    S2G_CUBLAS(cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, N, m, nci, &one, w.Qs, N, X, nci, &zero,
-                           G, N));
-    S2G_CUBLAS(cublasDgemm(h, CUBLAS_OP_T, CUBLAS_OP_N, nci, m, N, &ck, w.Ps, N, G, N, &one, out,
-                           nci));
+    S2G_CUBLAS(cublasDgemm(w.side.h, CUBLAS_OP_N, CUBLAS_OP_N, N, m, nci, &one, w.Qs, N, X, nci,
+                           &zero, G, N));
+    S2G_CUBLAS(cublasDgemm(w.side.h, CUBLAS_OP_T, CUBLAS_OP_N, nci, m, N, &ck, w.Ps, N, G, N,
+                           &zero, out, nci));
+    S2G_CUDA(cudaEventRecord(w.side.join, w.side.s));
+  } else {
+    S2G_CUDA(cudaMemsetAsync(out, 0, sizeof(double) * nci * m, s));
   }
+  (void)h;
   if (cJ != 0.0) {
     const int64_t mo = (int64_t)no * m;
     const int ldR = ld4(rows), ldo = ld4(no), ldv = ld4(nv);
@@ -223,8 +254,11 @@ inline void mftc_apply(MatFreeTc &w, cublasHandle_t h, cudaStream_t s, const dou
     float *Y = w.Y.ensure((size_t)mo * ldv);
     w.tc.run(s, th, tl, w.cv2_h.get(), w.cv2_l.get(), (int)mo, nv, w.KR, Y, ldv,
              2.0 * mo * nv * rows, 1, false, 0, false);
+    if (side) S2G_CUDA(cudaStreamWaitEvent(s, w.side.join, 0));
     S2G_LAUNCH(k_tcs_gather, g, 256, 0, s, out, Y, ldv, w.ci, w.ca, nci, no, m);
     w.tc.check(s);
+  } else if (side) {
+    S2G_CUDA(cudaStreamWaitEvent(s, w.side.join, 0));
   }
   if (diag) {
     const int64_t total = (int64_t)nci * m;

@@ -23,6 +23,8 @@ struct MixedWork {
   DBuf<float> K, J;
   DBuf<int> recheck;
   DBuf<double> recheck_part;
+  DBuf<int64_t> jcol, roff;
+  DBuf<float> eh, el, rhl;
   double *lastX = nullptr;
   int Kpad = 0;
   int64_t ldK = 0, ldJ = 0;
@@ -74,6 +76,134 @@ inline void mixed_pt_chunk(MixedWork &mw, cudaStream_t s, const double *Pc, cons
               mw.bv_lo.get(), rr, (int)nvcols, Kp, J + (size_t)r0 * mw.ldJ, mw.ldJ,
               2.0 * rr * (double)nvcols * N);
   }
+}
+
+// ---- PT sums over the FP32 coupling buffers (mixed form) ----
+// The couplings K, J carry the split-BF16 GEMM's ~1e-6 relative error, so the
+// terms (ak K - J)^2 / (E_r - E_c) are evaluated in FP32 and summed in FP64.
+// The energy difference of a candidate r and a primary c, which can cancel,
+// is formed from hi/lo FP32 pairs: (rh_r - eh_c) + (rl_r - el_c) keeps ~1e-7
+// relative accuracy.  Rows whose sum lands near thrp are re-decided in FP64
+// (k_pt_recheck), so the selection is the FP64 one.
+
+// Per primary c (PT order): J column offset and its energy as a hi/lo pair.
+// Entries nex <= c < ncol (padding to a multiple of 4) get offset 0 and zero
+// energies, so vector loads past the end stay in bounds.
+__global__ void k_pt_colinfo(int nex, int ncol, const int *__restrict__ pj,
+                             const int *__restrict__ pb, const int *__restrict__ omap,
+                             const int *__restrict__ vmap, int64_t ldj,
+                             const double *__restrict__ ed, int64_t *__restrict__ jcol,
+                             float *__restrict__ eh, float *__restrict__ el) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncol) return;
+  if (c >= nex) {
+    jcol[c] = 0;
+    eh[c] = 0.f;
+    el[c] = 0.f;
+    return;
+  }
+  jcol[c] = (int64_t)vmap[pb[c]] + ldj * (int64_t)omap[pj[c]];
+  double e = ed[c];
+  float h = (float)e;
+  eh[c] = h;
+  el[c] = (float)(e - (double)h);
+}
+
+__device__ __forceinline__ float pt_term32(float kv, float jv, float akf, float rh, float rl,
+                                           float ehc, float elc) {
+  float amat = akf * kv - jv;
+  float den = (rh - ehc) + (rl - elc);
+  return __fdividef(amat * amat, den);
+}
+
+// Row pass, one warp per candidate row: pert[r] = sum_c term(r, c) and
+// sel[r] = pert > thrp; also the row's J offset and energy pair for the column
+// pass.  Each lane takes 4 consecutive primaries per step (float4 loads of K,
+// ldk a multiple of 4); per-lane partial sums are reduced in a fixed order.
+constexpr int kRowWarps = 8;
+__global__ void __launch_bounds__(256)
+k_pt_rows32(const float *__restrict__ K, const float *__restrict__ J, int64_t ldj, int64_t ldk,
+            int nex, int nvp, int nop, int nrows, const int *__restrict__ cand_k, int nv, int i0,
+            const double *__restrict__ de_all, const int64_t *__restrict__ jcol,
+            const float *__restrict__ eh, const float *__restrict__ el, float akf, double thrp,
+            double *__restrict__ pert_out, unsigned char *__restrict__ sel,
+            int64_t *__restrict__ roff, float *__restrict__ rhl) {
+  const int lane = threadIdx.x & 31;
+  const int r = blockIdx.x * kRowWarps + (threadIdx.x >> 5);
+  if (r >= nrows) return;
+  const int k = cand_k[r];
+  const int i = k / nv, a = k - i * nv;
+  const int64_t off = (int64_t)a * nvp + ldj * (int64_t)(i - i0) * nop;
+  const double d = de_all[k] + 1e-10;
+  const float rh = (float)d, rl = (float)(d - (double)rh);
+  if (lane == 0) {
+    roff[r] = off;
+    rhl[2 * r] = rh;
+    rhl[2 * r + 1] = rl;
+  }
+  const float *Kr = K + (int64_t)r * ldk;
+  double acc = 0.0;
+#pragma unroll 2
+  for (int c = lane * 4; c < nex; c += 128) {
+    const float4 kv = *reinterpret_cast<const float4 *>(Kr + c);
+    const longlong2 j01 = *reinterpret_cast<const longlong2 *>(jcol + c);
+    const longlong2 j23 = *reinterpret_cast<const longlong2 *>(jcol + c + 2);
+    const float4 e_h = *reinterpret_cast<const float4 *>(eh + c);
+    const float4 e_l = *reinterpret_cast<const float4 *>(el + c);
+    const float jv0 = J[off + j01.x], jv1 = J[off + j01.y], jv2 = J[off + j23.x],
+                jv3 = J[off + j23.y];
+    float t = pt_term32(kv.x, jv0, akf, rh, rl, e_h.x, e_l.x);
+    if (c + 1 < nex) t += pt_term32(kv.y, jv1, akf, rh, rl, e_h.y, e_l.y);
+    if (c + 2 < nex) t += pt_term32(kv.z, jv2, akf, rh, rl, e_h.z, e_l.z);
+    if (c + 3 < nex) t += pt_term32(kv.w, jv3, akf, rh, rl, e_h.w, e_l.w);
+    acc += (double)t;
+  }
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if (lane == 0) {
+    pert_out[r] = acc;
+    sel[r] = acc > thrp ? 1 : 0;
+  }
+}
+
+// Column pass: colpart[y*nex + c] = sum over the non-selected rows of segment y
+// (in row order) of term(r, c).  Rows are taken 8 at a time with all loads
+// issued before the arithmetic.
+constexpr int kColUnroll = 8;
+__global__ void __launch_bounds__(128)
+k_pt_cols32(const float *__restrict__ K, const float *__restrict__ J, int64_t ldk, int nex,
+            int nrows, const int64_t *__restrict__ jcol, const float *__restrict__ eh,
+            const float *__restrict__ el, float akf, const unsigned char *__restrict__ sel,
+            const int64_t *__restrict__ roff, const float *__restrict__ rhl,
+            double *__restrict__ colpart, int seg_rows) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nex) return;
+  const int rbeg = blockIdx.y * seg_rows;
+  const int rend = min(nrows, rbeg + seg_rows);
+  const int64_t jc = jcol[c];
+  const float ehc = eh[c], elc = el[c];
+  double s = 0.0;
+  for (int r = rbeg; r < rend; r += kColUnroll) {
+    float kv[kColUnroll], jv[kColUnroll];
+    bool use[kColUnroll];
+#pragma unroll
+    for (int q = 0; q < kColUnroll; ++q) {
+      const int rr = r + q;
+      use[q] = rr < rend && !sel[rr];
+      kv[q] = 0.f;
+      jv[q] = 0.f;
+      if (use[q]) {
+        kv[q] = K[(int64_t)rr * ldk + c];
+        jv[q] = J[roff[rr] + jc];
+      }
+    }
+    float t = 0.f;
+#pragma unroll
+    for (int q = 0; q < kColUnroll; ++q)
+      if (use[q])
+        t += pt_term32(kv[q], jv[q], akf, rhl[2 * (r + q)], rhl[2 * (r + q) + 1], ehc, elc);
+    s += (double)t;
+  }
+  colpart[(int64_t)blockIdx.y * nex + c] = s;
 }
 
 // FP64 PT sum for candidate rows near the threshold (ptselect stda.f:1805-1834),
