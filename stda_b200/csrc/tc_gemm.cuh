@@ -16,7 +16,8 @@
 // Persistent CTAs (one per SM) walk 128 x 128 tiles: warp 0 issues TMA loads
 // into a 3-stage shared-memory ring, warp 1 issues tcgen05.mma from one thread
 // into one of two TMEM accumulators, warp 2 owns the TMEM allocation, warps
-// 4-7 drain the other accumulator (tcgen05.ld) and store to global memory.  Every mbarrier wait is bounded by
+// 4-7 drain the other accumulator (tcgen05.ld) through swizzled shared memory
+// and TMA bulk stores.  Every mbarrier wait is bounded by
 // a ~2 s wall-clock limit; on expiry the CTA records the failure in *err and
 // leaves without touching memory further.
 #pragma once
@@ -38,7 +39,12 @@ constexpr int STAGES = 3;
 constexpr int TILE_A = BM * BK * 2;   // bytes per operand tile
 constexpr int TILE_B = BN * BK * 2;
 constexpr int STAGE_BYTES = 2 * TILE_A + 2 * TILE_B;
-constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256;   // ring + barriers + slack
+// epilogue staging: per epilogue warp two 32 x 32 FP32 blocks (128B-swizzled)
+constexpr int EPI_COLS = 32;
+constexpr int EPI_BUF = 32 * EPI_COLS * 4;
+constexpr int EPI_BYTES = 4 * 2 * EPI_BUF;
+constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + EPI_BYTES + 1024 + 256;   // + barriers, slack
+static_assert(SMEM_BYTES <= 232448, "shared memory budget of one CTA");
 constexpr unsigned long long kWaitNs = 2000000000ull;   // 2 s per wait
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
@@ -144,6 +150,43 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float *v) {
   for (int q = 0; q < 16; ++q) v[q] = __uint_as_float(r[q]);
 }
 
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t *r) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,"
+      "%15,%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+        "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]),
+        "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]),
+        "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+// 3-D tiled TMA store (x = column, y = row, z = batch) from 128B-swizzled smem;
+// x is a multiple of 32 FP32 elements and never negative
+__device__ __forceinline__ void tma_store_3d(const CUtensorMap *map, const void *src, int x, int y,
+                                             int z) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.global.shared::cta.tile.bulk_group [%0, {%2, %3, %4}], [%1];" ::"l"(
+          reinterpret_cast<uint64_t>(map)),
+      "r"(smem_u32(src)), "r"(x), "r"(y), "r"(z)
+      : "memory");
+}
+
+__device__ __forceinline__ void bulk_commit() {
+  asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+}
+
+// wait until at most one committed store group still reads shared memory
+__device__ __forceinline__ void bulk_wait_read1() {
+  asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory");
+}
+
+__device__ __forceinline__ void bulk_wait_all() {
+  asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+}
+
 }  // namespace tc
 
 __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
@@ -158,12 +201,13 @@ __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
 __global__ void __launch_bounds__(256, 1)
 k_tc_gemm_bf16x3(const __grid_constant__ CUtensorMap mAh, const __grid_constant__ CUtensorMap mAl,
                  const __grid_constant__ CUtensorMap mBh, const __grid_constant__ CUtensorMap mBl,
-                 float *__restrict__ D, int64_t ldd, int64_t bstride_d, int M, int N, int Kpad,
-                 int b_batched, int batch, int *err) {
+                 const __grid_constant__ CUtensorMap mD, int M, int N, int Kpad, int b_batched,
+                 int batch, int *err) {
   using namespace tc;
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char *base = (unsigned char *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-  uint64_t *full = (uint64_t *)(base + STAGES * STAGE_BYTES);
+  unsigned char *epi = base + STAGES * STAGE_BYTES;   // 1024-aligned staging buffers
+  uint64_t *full = (uint64_t *)(epi + EPI_BYTES);
   uint64_t *empty = full + STAGES;
   uint64_t *acc_full = empty + STAGES;     // [2]
   uint64_t *acc_empty = acc_full + 2;      // [2]
@@ -252,9 +296,14 @@ k_tc_gemm_bf16x3(const __grid_constant__ CUtensorMap mAh, const __grid_constant_
       if (ok) umma_commit(&acc_full[ab]);   // accumulator complete
     }
   } else if (warp >= 4) {
-    // ---- epilogue: TMEM -> registers -> global ----
-    const int wq = warp - 4;                 // TMEM lanes 32*wq .. 32*wq+31
+    // ---- epilogue: TMEM -> registers -> swizzled smem -> TMA store ----
+    // Warp wq owns TMEM lanes (tile rows) 32*wq .. 32*wq+31 and writes them in
+    // 32-column blocks through two staging buffers; the store unit clips rows
+    // >= M and columns >= N.
+    const int wq = warp - 4;
+    unsigned char *stage0 = epi + (wq * 2) * EPI_BUF;
     int64_t lt = 0;
+    uint32_t nblk = 0;
     for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x, ++lt) {
       const int ab = (int)(lt & 1);
       if (!mbar_wait(&acc_full[ab], (uint32_t)((lt >> 1) & 1), err, 3)) break;
@@ -263,28 +312,34 @@ k_tc_gemm_bf16x3(const __grid_constant__ CUtensorMap mAh, const __grid_constant_
       const int64_t rest = t / tiles_n;
       const int tm = (int)(rest % tiles_m), z = (int)(rest / tiles_m);
       const int m0 = tm * BM, n0 = tn * BN;
-      float *Dz = D + (int64_t)z * bstride_d;
-      const int row = m0 + wq * 32 + lane;
-      float v[16];
 #pragma unroll 1
-      for (int c = 0; c < BN; c += 16) {
-        tc::tmem_ld16(tmem + ((uint32_t)(wq * 32) << 16) + (uint32_t)(ab * BN + c), v);
-        if (row < M) {
-          float *dst = Dz + (int64_t)row * ldd + n0 + c;
-          if (n0 + c + 16 <= N) {
+      for (int c = 0; c < BN; c += EPI_COLS, ++nblk) {
+        unsigned char *buf = stage0 + (nblk & 1) * EPI_BUF;
+        // the store that last used this buffer has finished reading it
+        if (lane == 0) tc::bulk_wait_read1();
+        __syncwarp();
+        uint32_t v[32];
+        tc::tmem_ld32(tmem + ((uint32_t)(wq * 32) << 16) + (uint32_t)(ab * BN + c), v);
+        // row `lane`: 16-byte chunk q goes to chunk q ^ (lane % 8) (128B swizzle)
+        unsigned char *rowp = buf + lane * 128;
 #pragma unroll
-            for (int q = 0; q < 16; q += 4)
-              *(float4 *)(dst + q) = make_float4(v[q], v[q + 1], v[q + 2], v[q + 3]);
-          } else {
-            for (int q = 0; q < 16; ++q)
-              if (n0 + c + q < N) dst[q] = v[q];
-          }
+        for (int q = 0; q < 8; ++q) {
+          uint4 w = make_uint4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+          *reinterpret_cast<uint4 *>(rowp + ((q ^ (lane & 7)) << 4)) = w;
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncwarp();
+        if (lane == 0) {
+          tc::tma_store_3d(&mD, buf, n0 + c, m0 + wq * 32, z);
+          tc::bulk_commit();
         }
       }
       // this thread's reads of the accumulator are complete
       asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
       mbar_arrive(&acc_empty[ab]);
     }
+    if (lane == 0) tc::bulk_wait_all();
+    __syncwarp();
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
@@ -357,6 +412,23 @@ struct TcGemm {
     return m;
   }
 
+  // FP32 output D (rows x cols, row stride ldd elements, `batch` matrices
+  // bstride elements apart) stored in 32 x 32 blocks from 128B-swizzled smem
+  CUtensorMap map_out(float *p, int64_t rows, int64_t cols, int64_t ldd, int batch,
+                      int64_t bstride) {
+    CUtensorMap m;
+    cuuint64_t dims[3] = {(cuuint64_t)cols, (cuuint64_t)rows, (cuuint64_t)batch};
+    cuuint64_t strides[2] = {(cuuint64_t)ldd * 4, (cuuint64_t)bstride * 4};
+    cuuint32_t box[3] = {(cuuint32_t)tc::EPI_COLS, 32, 1};
+    cuuint32_t estr[3] = {1, 1, 1};
+    CUresult r = encode(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, (void *)p, dims, strides, box,
+                        estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                        CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS)
+      throw Error{STD2G_ECUDA, "cuTensorMapEncodeTiled (output) failed " + std::to_string((int)r)};
+    return m;
+  }
+
   // D (M x N, row-major ldd) = A (M x Kpad) B (N x Kpad)^T, split-BF16 operands,
   // for `batch` independent problems (A, D batched; B batched when b_batched).
   // nflop: algorithmic FLOPs credited to this launch (2 M N K_true per problem).
@@ -376,6 +448,7 @@ struct TcGemm {
     CUtensorMap ah = map(Ah, M, Kpad, tc::BM, batch), al = map(Al, M, Kpad, tc::BM, batch);
     CUtensorMap bh = map(Bh, N, Kpad, tc::BN, b_batched ? batch : 1);
     CUtensorMap bl = map(Bl, N, Kpad, tc::BN, b_batched ? batch : 1);
+    CUtensorMap dm = map_out(D, M, N, ldd, batch, batch > 1 ? bstride_d : (int64_t)M * ldd);
     int *e = err.ensure(1);
     if (!armed) {
       S2G_CUDA(cudaMemsetAsync(e, 0, sizeof(int), s));
@@ -384,8 +457,8 @@ struct TcGemm {
     const int64_t ntiles = div_up(N, tc::BN) * div_up(M, tc::BM) * (int64_t)batch;
     const int grid = (int)std::min<int64_t>(ntiles, nsm);
     if (sync) S2G_CUDA(cudaEventRecord(e0, s));
-    S2G_LAUNCH(k_tc_gemm_bf16x3, grid, 256, tc::SMEM_BYTES, s, ah, al, bh, bl, D, ldd, bstride_d,
-               M, N, Kpad, b_batched ? 1 : 0, batch, e);
+    S2G_LAUNCH(k_tc_gemm_bf16x3, grid, 256, tc::SMEM_BYTES, s, ah, al, bh, bl, dm, M, N, Kpad,
+               b_batched ? 1 : 0, batch, e);
     ++launches;
     flop += nflop * batch;
     if (sync) {
