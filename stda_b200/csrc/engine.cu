@@ -22,6 +22,7 @@
 #include "matfree.cuh"
 #include "matfree_tc.cuh"
 #include "mixed.cuh"
+#include "response_mixed.cuh"
 
 namespace std2g {
 
@@ -56,6 +57,8 @@ struct Ctx {
   cudaStream_t stream = nullptr;
   cublasHandle_t blas = nullptr;
   cusolverDnHandle_t solver = nullptr;
+  cusolverDnParams_t solver_params = nullptr;   // 64-bit cuSOLVER API (large n)
+  std::vector<char> host_work;
   bool loaded = false;
   int ncent = 0, nmo = 0, nao = 0;
   std::vector<double> h_eps, h_occ, h_xyz;
@@ -78,6 +81,12 @@ struct Ctx {
   DBuf<int> w_info;
   DBuf<char> w_cub;
   MixedWork mixed;
+  struct RespWork {
+    DBuf<float> Apb32, Amb32, dp, dm, yu, yv, ru, rv, zu, zv, pu, pv, qu, qv, cu, cv;
+    DBuf<double> B1, U, V, PU, MV, R1, R2, pa, pb, wcol, rz, alpha, beta, rr, nrm, nrm2;
+    DBuf<unsigned> flag;
+    int outer = 0, inner = 0;
+  } rw;
   DavidsonWork dav;
   MatFree mf;
   MatFreeTc mftc;
@@ -135,15 +144,21 @@ static int dense_eig(Ctx &c, double *A, int n, double vl, double vu, int kmax, d
   return meig;
 }
 
-// Full symmetric eigen-decomposition (makel stda.f:1615-1691, smatpow srpapack.f:201-256)
+// Full symmetric eigen-decomposition (makel stda.f:1615-1691, smatpow srpapack.f:201-256),
+// through the 64-bit cuSOLVER interface: the workspace of n >~ 11000 exceeds
+// 2^31 bytes.
 static void dense_eig_full(Ctx &c, double *A, int n, double *w) {
-  int lwork = 0;
-  S2G_CUSOLVER(cusolverDnDsyevd_bufferSize(c.solver, CUSOLVER_EIG_MODE_VECTOR,
-                                           CUBLAS_FILL_MODE_LOWER, n, A, n, w, &lwork));
-  double *work = c.w_work.ensure((size_t)lwork + 1);
+  if (!c.solver_params) S2G_CUSOLVER(cusolverDnCreateParams(&c.solver_params));
+  size_t dbytes = 0, hbytes = 0;
+  S2G_CUSOLVER(cusolverDnXsyevd_bufferSize(c.solver, c.solver_params, CUSOLVER_EIG_MODE_VECTOR,
+                                           CUBLAS_FILL_MODE_LOWER, n, CUDA_R_64F, A, n,
+                                           CUDA_R_64F, w, CUDA_R_64F, &dbytes, &hbytes));
+  double *work = c.w_work.ensure(dbytes / sizeof(double) + 1);
+  if (c.host_work.size() < hbytes + 1) c.host_work.resize(hbytes + 1);
   int *info = c.w_info.ensure(1);
-  S2G_CUSOLVER(cusolverDnDsyevd(c.solver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, n, A,
-                                n, w, work, lwork, info));
+  S2G_CUSOLVER(cusolverDnXsyevd(c.solver, c.solver_params, CUSOLVER_EIG_MODE_VECTOR,
+                                CUBLAS_FILL_MODE_LOWER, n, CUDA_R_64F, A, n, CUDA_R_64F, w,
+                                CUDA_R_64F, work, dbytes, c.host_work.data(), hbytes, info));
   int h_info = 0;
   S2G_CUDA(cudaMemcpyAsync(&h_info, info, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
   S2G_CUDA(cudaStreamSynchronize(c.stream));
@@ -311,6 +326,156 @@ static void response(Ctx &c, double *Apb, double *Amb, int nci, const double *mu
     for (int x = 0; x < 3; ++x)
       for (int y = 0; y < 3; ++y) rq.alpha[(size_t)w * 9 + 3 * x + y] = h[x + 3 * y];
     if (rq.resid) rq.resid[w] = h[9];
+  }
+}
+
+// Mixed-precision response (response_mixed.cuh): FP64 iterative refinement of
+// the coupled (u, v) equations around FP32 preconditioned conjugate gradients
+// on the same system.  Frequencies whose system is not positive definite are
+// returned in `fallback` (their alpha entries are left untouched).
+static void response_mixed(Ctx &c, const double *Apb, const double *Amb, int n,
+                           const double *musel, const RespReq &rq, std::vector<int> &fallback) {
+  cudaStream_t s = c.stream;
+  auto &w = c.rw;
+  const int nw = rq.n, ncol = 3 * nw;
+  if (ncol > 32) throw Error{STD2G_EINVAL, "response: at most 10 frequencies per call"};
+  const size_t n2 = (size_t)n * n, nc = (size_t)n * ncol;
+  const int g = grid_for((int64_t)nc);
+  const double tol = 1e-10;   // relative FP64 residual of every right-hand side
+  const int kMaxOuter = 12, kMaxInner = 400;
+  const float one = 1.f, zero = 0.f;
+  const double done = 1.0, dzero = 0.0;
+  const bool prof = c.opts.verbose >= 2;
+  const auto t0 = std::chrono::steady_clock::now();
+  std::vector<double> hw(ncol);
+  for (int j = 0; j < ncol; ++j) hw[j] = rq.omega[j / 3];
+  double *wcol = w.wcol.ensure(ncol);
+  S2G_CUDA(cudaMemcpyAsync(wcol, hw.data(), sizeof(double) * ncol, cudaMemcpyHostToDevice, s));
+  // FP32 copies of A+B and A-B and their diagonals
+  float *Apb32 = w.Apb32.ensure(n2), *Amb32 = w.Amb32.ensure(n2);
+  S2G_LAUNCH(k_d2f, grid_for((int64_t)n2), 256, 0, s, Apb32, Apb, (int64_t)n2);
+  S2G_LAUNCH(k_d2f, grid_for((int64_t)n2), 256, 0, s, Amb32, Amb, (int64_t)n2);
+  float *dp = w.dp.ensure(n), *dm = w.dm.ensure(n);
+  S2G_LAUNCH(k_resp_diags, (int)div_up(n, 256), 256, 0, s, Apb, Amb, n, dp, dm);
+  double *B1 = w.B1.ensure(nc), *U = w.U.ensure(nc), *V = w.V.ensure(nc);
+  double *PU = w.PU.ensure(nc), *MV = w.MV.ensure(nc), *R1 = w.R1.ensure(nc),
+         *R2 = w.R2.ensure(nc);
+  double *pa = w.pa.ensure((size_t)ncol * kRespSplit), *pb = w.pb.ensure((size_t)ncol * kRespSplit);
+  double *nrm = w.nrm.ensure(ncol), *nrm2 = w.nrm2.ensure(ncol);
+  S2G_LAUNCH(k_resp_rhs, g, 256, 0, s, B1, musel, n, nw);
+  S2G_CUDA(cudaMemsetAsync(U, 0, sizeof(double) * nc, s));
+  S2G_CUDA(cudaMemsetAsync(V, 0, sizeof(double) * nc, s));
+  const dim3 rgrid(kRespSplit, (unsigned)ncol);
+  const int sgrid = (int)div_up(ncol, 32);
+  auto coldot64 = [&](const double *a, const double *b, double *out) {
+    S2G_LAUNCH(k_resp_dot64, rgrid, 256, 0, s, a, b, n, pa);
+    S2G_LAUNCH(k_resp_sum, sgrid, 32, 0, s, pa, kRespSplit, ncol, out);
+  };
+  std::vector<double> hb(ncol), hr(ncol), hr2(ncol), hrel(ncol, 1.0);
+  coldot64(B1, B1, nrm);
+  S2G_CUDA(cudaMemcpyAsync(hb.data(), nrm, sizeof(double) * ncol, cudaMemcpyDeviceToHost, s));
+  // FP32 CG vectors, halves (u, v)
+  float *yu = w.yu.ensure(nc), *yv = w.yv.ensure(nc), *ru = w.ru.ensure(nc), *rv = w.rv.ensure(nc),
+        *zu = w.zu.ensure(nc), *zv = w.zv.ensure(nc), *pu = w.pu.ensure(nc), *pv = w.pv.ensure(nc),
+        *qu = w.qu.ensure(nc), *qv = w.qv.ensure(nc), *cu = w.cu.ensure(nc), *cv = w.cv.ensure(nc);
+  double *rz = w.rz.ensure(ncol), *al = w.alpha.ensure(ncol), *be = w.beta.ensure(ncol),
+         *rr = w.rr.ensure(ncol);
+  unsigned *flag = w.flag.ensure(1);
+  S2G_CUDA(cudaMemsetAsync(flag, 0, sizeof(unsigned), s));
+  cublasHandle_t h = c.blas;
+  auto pcg = [&]() {
+    S2G_LAUNCH(k_pcg2_init, rgrid, 256, 0, s, yu, yv, ru, rv, zu, zv, pu, pv, cu, cv, dp, dm, wcol,
+               n, pa, pb);
+    S2G_LAUNCH(k_pcg_beta, sgrid, 32, 0, s, pa, pb, kRespSplit, ncol, rz, be, rr, 1);
+    std::vector<double> rr0(ncol), rrn(ncol);
+    S2G_CUDA(cudaMemcpyAsync(rr0.data(), rr, sizeof(double) * ncol, cudaMemcpyDeviceToHost, s));
+    S2G_CUDA(cudaStreamSynchronize(s));
+    for (int it = 1; it <= kMaxInner; ++it) {
+      S2G_CUBLAS(cublasSgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, n, ncol, n, &one, Apb32, n, pu, n,
+                             &zero, qu, n));
+      S2G_CUBLAS(cublasSgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, n, ncol, n, &one, Amb32, n, pv, n,
+                             &zero, qv, n));
+      S2G_LAUNCH(k_pcg2_pq, rgrid, 256, 0, s, qu, qv, pu, pv, wcol, n, pa);
+      S2G_LAUNCH(k_pcg_alpha, sgrid, 32, 0, s, pa, kRespSplit, ncol, rz, al, flag);
+      S2G_LAUNCH(k_pcg2_update, rgrid, 256, 0, s, yu, yv, ru, rv, zu, zv, pu, pv, qu, qv, dp, dm,
+                 wcol, al, n, pa, pb);
+      S2G_LAUNCH(k_pcg_beta, sgrid, 32, 0, s, pa, pb, kRespSplit, ncol, rz, be, rr, 0);
+      S2G_LAUNCH(k_pcg2_dir, g, 256, 0, s, pu, pv, zu, zv, be, n, ncol);
+      ++w.inner;
+      if (it % 8 == 0) {
+        S2G_CUDA(cudaMemcpyAsync(rrn.data(), rr, sizeof(double) * ncol, cudaMemcpyDeviceToHost,
+                                 s));
+        S2G_CUDA(cudaStreamSynchronize(s));
+        bool done_all = true;
+        for (int j = 0; j < ncol; ++j)
+          if (rrn[j] > 1e-11 * rr0[j]) done_all = false;
+        if (done_all) break;
+      }
+    }
+  };
+  w.outer = w.inner = 0;
+  for (int outer = 0; outer <= kMaxOuter; ++outer) {
+    // FP64 residuals of the coupled equations
+    S2G_CUBLAS(cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, n, ncol, n, &done, Apb, n, U, n, &dzero,
+                           PU, n));
+    S2G_CUBLAS(cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, n, ncol, n, &done, Amb, n, V, n, &dzero,
+                           MV, n));
+    S2G_LAUNCH(k_resp_resid, g, 256, 0, s, R1, R2, B1, U, V, PU, MV, wcol, n, ncol);
+    coldot64(R1, R1, nrm);
+    coldot64(R2, R2, nrm2);
+    S2G_CUDA(cudaMemcpyAsync(hr.data(), nrm, sizeof(double) * ncol, cudaMemcpyDeviceToHost, s));
+    S2G_CUDA(cudaMemcpyAsync(hr2.data(), nrm2, sizeof(double) * ncol, cudaMemcpyDeviceToHost, s));
+    unsigned hflag = 0;
+    S2G_CUDA(cudaMemcpyAsync(&hflag, flag, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+    S2G_CUDA(cudaStreamSynchronize(s));
+    double worst = 0.0;
+    for (int j = 0; j < ncol; ++j) {
+      hrel[j] = hb[j] > 0 ? std::sqrt((hr[j] + hr2[j]) / hb[j]) : 0.0;
+      if (!(hflag >> j & 1u)) worst = std::max(worst, hrel[j]);
+    }
+    w.outer = outer;
+    if (worst <= tol || outer == kMaxOuter) {
+      // a frequency with negative curvature in any column, or not converged,
+      // goes to the FP64 form
+      for (int fw = 0; fw < nw; ++fw) {
+        bool bad = false;
+        for (int x = 0; x < 3; ++x) {
+          const int j = 3 * fw + x;
+          bad |= (hflag >> j & 1u) != 0 || hrel[j] > tol;
+        }
+        if (bad) fallback.push_back(fw);
+      }
+      break;
+    }
+    // correction from the FP32 solve of the same system with the residual
+    S2G_LAUNCH(k_d2f, g, 256, 0, s, cu, R1, (int64_t)nc);
+    S2G_LAUNCH(k_d2f, g, 256, 0, s, cv, R2, (int64_t)nc);
+    pcg();
+    S2G_LAUNCH(k_resp_accum, g, 256, 0, s, U, V, yu, yv, (int64_t)nc);
+  }
+  if (prof) {
+    S2G_CUDA(cudaStreamSynchronize(s));
+    std::fprintf(stderr, "response (mixed): %d refinement steps, %d CG steps, %.2f ms\n",
+                 w.outer, w.inner,
+                 std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0)
+                     .count());
+  }
+  // alpha = -2 mu^T (X+Y) per frequency
+  double *a9 = c.w_props.ensure(16);
+  for (int fw = 0; fw < nw; ++fw) {
+    if (std::find(fallback.begin(), fallback.end(), fw) != fallback.end()) continue;
+    gemm(c, CUBLAS_OP_T, CUBLAS_OP_N, 3, 3, n, -2.0, musel, n, U + (size_t)n * 3 * fw, n, 0.0,
+         a9, 3);
+    double ha[9];
+    S2G_CUDA(cudaMemcpyAsync(ha, a9, sizeof(double) * 9, cudaMemcpyDeviceToHost, s));
+    S2G_CUDA(cudaStreamSynchronize(s));
+    for (int x = 0; x < 3; ++x)
+      for (int yy = 0; yy < 3; ++yy) rq.alpha[(size_t)fw * 9 + 3 * x + yy] = ha[x + 3 * yy];
+    if (rq.resid) {
+      double wf = 0;
+      for (int x = 0; x < 3; ++x) wf = std::max(wf, hrel[3 * fw + x]);
+      rq.resid[fw] = wf;
+    }
   }
 }
 
@@ -789,7 +954,23 @@ static void solve(Ctx &c, const std2g_params &p_in, std2g_result *res, const Res
       double *musel = c.w_musel.ensure((size_t)nci * 9);
       S2G_LAUNCH(k_gather_mu, grid_for((int64_t)nci * 9), 256, 0, s, musel, c.w_mu_ov.get(), no,
                  nv, d_ci, d_ca, nci);
-      response(c, Apb, Amb, nci, musel, *resp);
+      if (mixed) {
+        std::vector<int> fb;
+        response_mixed(c, Apb, Amb, nci, musel, *resp, fb);
+        if (!fb.empty()) {
+          // frequencies above the first excitation: the FP64 form's factorisations
+          std::vector<double> om(fb.size()), al(fb.size() * 9), rs(fb.size());
+          for (size_t q = 0; q < fb.size(); ++q) om[q] = resp->omega[fb[q]];
+          RespReq sub{om.data(), (int)fb.size(), al.data(), rs.data()};
+          response(c, Apb, Amb, nci, musel, sub);
+          for (size_t q = 0; q < fb.size(); ++q) {
+            std::copy(al.begin() + 9 * q, al.begin() + 9 * q + 9, resp->alpha + 9 * fb[q]);
+            if (resp->resid) resp->resid[fb[q]] = rs[q];
+          }
+        }
+      } else {
+        response(c, Apb, Amb, nci, musel, *resp);
+      }
       record(c, PH_COUNT);
       S2G_CUDA(cudaStreamSynchronize(s));
       for (int q = 0; q < PH_COUNT; ++q) {
@@ -1116,6 +1297,7 @@ void std2g_destroy(void *ctx) {
   cudaSetDevice(c->opts.device);
   cudaStreamSynchronize(c->stream);
   for (auto &e : c->ev) cudaEventDestroy(e);
+  if (c->solver_params) cusolverDnDestroyParams(c->solver_params);
   if (c->solver) cusolverDnDestroy(c->solver);
   if (c->blas) cublasDestroy(c->blas);
   delete c;   // buffers free themselves

@@ -108,6 +108,42 @@ def test_benzene_rpa_and_polarizability(benzene):
     assert resid.max() < 1e-10
 
 
+def test_polarizability_mixed_refinement(benzene):
+    """Mixed form of alpha(w): FP32 conjugate gradients inside FP64 iterative
+    refinement.  Below the first excitation the FP64 residual must reach 1e-8
+    and alpha must match the oracle to 1e-4 relative (it does to ~1e-9); a
+    frequency above the first excitation goes through the FP64 form and must
+    match it as well."""
+    from stda_b200.engine import Keywords
+    mol, ints = benzene
+    kw = dict(ax=0.5, e_thr_ev=10.0)
+    ref = _oracle(mol, ints, rpa=True, **kw)
+    eng = _engine(1)
+    from stda_b200.engine import boundary_inputs
+    eng.load(boundary_inputs(mol, ints))
+    above = float(ref.omega[0]) * 1.05           # just above the lowest root
+    om = [0.0, 0.03, 0.06, 0.09, above]
+    alpha, resid = eng.polarizability(Keywords(**kw), om)
+    aref = dynamic_polarizability(ref, om)
+    scale = np.abs(aref).max(axis=(1, 2))
+    rel = np.abs(alpha - aref).max(axis=(1, 2)) / scale
+    assert rel.max() < 1e-4, rel
+    assert resid.max() < 1e-8, resid
+    # the mixed and FP64 forms agree on a larger molecule
+    from stda_b200 import synth
+    mol2, ints2 = synth.random_molecule(40, seed=11, with_ints=True)
+    kw2 = Keywords(ax=0.5, e_thr_ev=9.0)
+    out = []
+    for prec in (0, 1):
+        e = _engine(prec)
+        e.load(boundary_inputs(mol2, ints2))
+        out.append(e.polarizability(kw2, [0.0, 0.05, 0.1]))
+    (a0, r0), (a1, r1) = out
+    rel2 = np.abs(a1 - a0).max(axis=(1, 2)) / np.abs(a0).max(axis=(1, 2))
+    assert rel2.max() < 1e-4, rel2
+    assert r1.max() < 1e-8
+
+
 def test_random_cluster_triplet_and_kshift():
     from stda_b200 import synth
     mol, ints = synth.random_molecule(24, seed=5, with_ints=True)
