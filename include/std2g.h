@@ -192,6 +192,52 @@ int std2g_screen_noalloc(int device, int ncent, int nao, int no, int nv, const d
                          const int *d_iaoat, const double *d_clow, const double *d_eps,
                          const std2g_params *par, double *d_de, int *d_flag, void *stream);
 
+/* ---- served / batched form ---------------------------------------------
+   Many molecules through a pool of contexts (continuous batching).  The
+   reference runs one molecule per process (main.f:928-929); this layer has no
+   counterpart there.  A request is admitted when one of `slots` contexts is
+   free and its estimated device footprint fits `hbm_budget` beside the
+   requests in flight (FIFO; a request that alone exceeds the budget runs when
+   nothing else does).  Requests that arrive while others run start as soon as
+   a slot and memory free up; their kernels overlap on the device.  Each
+   context keeps its device work buffers between requests.  The server owns
+   one host thread per slot; submit / wait / poll are thread-safe. */
+typedef struct {
+  int device;
+  int precision;        /* as std2g_opts.precision, for every slot */
+  int slots;            /* concurrent solves (1..64) */
+  int reserved;
+  int64_t hbm_budget;   /* bytes the admitted requests may use (0: 80 % of free memory) */
+} std2g_server_opts;
+
+typedef struct {
+  int ncent, nmo, nao;  /* as std2g_load; every array is copied at submit */
+  const double *xyz, *C, *eps, *occ;
+  const int *iaoat;
+  const double *S, *mu_L, *mu_V, *mu_M;
+  std2g_params params;  /* the excitation solve (std2g_solve) */
+  int nomega;           /* > 0: also alpha(omega) (std2g_polarizability) */
+  const double *omega;  /* [nomega] Eh */
+} std2g_request;
+
+int std2g_server_create(void **srv, const std2g_server_opts *opts);
+/* Queue one request; *ticket identifies it for poll / wait. */
+int std2g_server_submit(void *srv, const std2g_request *rq, int64_t *ticket);
+/* *done = 1 once the request has finished (successfully or not). */
+int std2g_server_poll(void *srv, int64_t ticket, int *done);
+/* Block until the request has finished; returns its status and, on success,
+   fills res (caller arrays of res->cap), alpha [nomega*9], alpha_resid
+   [nomega] and timing_ms [3] = queued, running, total (submit to finish).
+   The ticket is released. */
+int std2g_server_wait(void *srv, int64_t ticket, std2g_result *res, double *alpha,
+                      double *alpha_resid, double *timing_ms);
+/* stats[7]: submitted, completed, in flight, peak in flight, bytes in flight
+   (estimated), peak bytes in flight, budget. */
+int std2g_server_stats(void *srv, int64_t *stats);
+/* Stop the workers after their current requests (queued ones are dropped) and
+   free the contexts; call after the last wait. */
+void std2g_server_destroy(void *srv);
+
 const char *std2g_error_string(int status);
 void std2g_destroy(void *ctx);
 

@@ -7,6 +7,7 @@
 #include <cusolverDn.h>
 
 #include <cstdint>
+#include <atomic>
 #include <cstdio>
 #include <string>
 #include <vector>
@@ -56,7 +57,7 @@ struct Error {
 
 // Launch counter shared by all kernels of this library (the number reported
 // by std2g_kernel_launches).
-extern int64_t g_launches;
+extern std::atomic<int64_t> g_launches;
 
 #define S2G_LAUNCH(kernel, grid, block, smem, stream, ...)                       \
   do {                                                                           \

@@ -26,7 +26,7 @@
 
 namespace std2g {
 
-int64_t g_launches = 0;
+std::atomic<int64_t> g_launches{0};
 
 static const double kEta[94] = {
     0.472592880, 0.922033910, 0.174528880, 0.257007330, 0.339490860, 0.421954120, 0.504381930,
@@ -1249,7 +1249,7 @@ const char *std2g_phase_name(int q) {
   return (q >= 0 && q < std2g::PH_COUNT) ? std2g::kPhaseNames[q] : "";
 }
 
-int64_t std2g_kernel_launches(void *) { return std2g::g_launches; }
+int64_t std2g_kernel_launches(void *) { return std2g::g_launches.load(); }
 
 int std2g_kernel_stats(void *ctx, double *ms, int64_t *launches, double *flop) {
   if (!ctx) return STD2G_EINVAL;

@@ -1,0 +1,306 @@
+// Served form of the sTDA / sTD-DFT path: a request loop with continuous
+// batching over a pool of engine contexts.
+//
+// The reference is a single-shot program (one molecule per process, main.f);
+// serving many molecules is this engine's own layer on top of the C ABI.
+// Design:
+//   * `slots` contexts (std2g_create), each with its own CUDA stream, cuBLAS /
+//     cuSOLVER handles and grow-only device work buffers that stay resident
+//     between requests (charges, gamma products, PT buffers, Davidson subspace);
+//   * one worker thread per slot; a request is admitted when a slot is free
+//     and its estimated device footprint fits the HBM budget beside the
+//     requests already in flight (or nothing else is in flight), in FIFO
+//     order, so requests that arrive while others run start as soon as slots
+//     and memory free up and their kernels overlap on the device;
+//   * inputs are copied at submit, results are kept until std2g_server_wait.
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <memory>
+#include <mutex>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/std2g.h"
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+struct Job {
+  int64_t ticket = 0;
+  int ncent = 0, nmo = 0, nao = 0;
+  std::vector<double> xyz, C, eps, occ, S, muL, muV, muM, omega;
+  std::vector<int> iaoat;
+  std2g_params par{};
+  int64_t footprint = 0;
+  Clock::time_point t_submit, t_start, t_end;
+  // results
+  bool done = false;
+  int status = STD2G_OK;
+  std2g_result res{};
+  std::vector<double> om, fL, fV, RL, RV, resid, alpha, alpha_resid;
+};
+
+struct Server {
+  std2g_server_opts opts{};
+  int64_t budget = 0;
+  std::vector<void *> ctxs;
+  std::vector<std::thread> workers;
+  std::mutex mu;
+  std::condition_variable cv_queue, cv_done;
+  std::deque<std::shared_ptr<Job>> queue;
+  std::unordered_map<int64_t, std::shared_ptr<Job>> jobs;
+  int64_t next_ticket = 1;
+  int64_t inflight_bytes = 0;
+  int inflight = 0;
+  bool stop = false;
+  int64_t submitted = 0, completed = 0, peak_bytes = 0;
+  int peak_inflight = 0;
+};
+
+// Estimated device bytes of one solve from the input sizes alone (the CSF
+// count is not known before the screen): charge and gamma-product tensors
+// over the largest possible window (all occupied x all virtual MOs), AO-basis
+// work arrays, and the PT coupling buffers up to their chunk budget.
+int64_t footprint_estimate(const Job &j) {
+  int64_t nocc = 0;
+  for (double o : j.occ)
+    if (o > 1e-8) ++nocc;
+  const int64_t nvir = j.nmo - nocc, N = j.ncent, nao = j.nao;
+  const int64_t pairs = nocc * nvir;
+  int64_t b = 8 * (3 * N * pairs + 2 * N * nocc * nocc + 2 * N * nvir * nvir);
+  b += 8 * (16 * nao * nao + 12 * (int64_t)j.nmo * nao);
+  b += std::min<int64_t>(6000000000LL, 8 * pairs * std::min<int64_t>(pairs, 4096));
+  const int64_t nci = std::min<int64_t>(pairs, 20000);
+  if (nci <= 1024 || j.par.rpa || !j.omega.empty())
+    b += 8 * 8 * nci * nci;   // dense A / A+B / A-B and their work copies
+  return b;
+}
+
+void run_job(void *ctx, Job &j) {
+  j.t_start = Clock::now();
+  int st = std2g_load(ctx, j.ncent, j.nmo, j.nao, j.xyz.data(), j.C.data(), j.eps.data(),
+                      j.occ.data(), j.iaoat.data(), j.S.data(), j.muL.data(), j.muV.data(),
+                      j.muM.data());
+  if (st == STD2G_OK) {
+    const int cap = j.par.nroots > 0 ? j.par.nroots : 20000;
+    j.om.assign(cap, 0.0);
+    j.fL.assign(cap, 0.0);
+    j.fV.assign(cap, 0.0);
+    j.RL.assign(cap, 0.0);
+    j.RV.assign(cap, 0.0);
+    j.resid.assign(cap, 0.0);
+    j.res = std2g_result{};
+    j.res.cap = cap;
+    j.res.omega = j.om.data();
+    j.res.fL = j.fL.data();
+    j.res.fV = j.fV.data();
+    j.res.RL = j.RL.data();
+    j.res.RV = j.RV.data();
+    j.res.resid = j.resid.data();
+    st = std2g_solve(ctx, &j.par, &j.res);
+  }
+  if (st == STD2G_OK && !j.omega.empty()) {
+    j.alpha.assign(9 * j.omega.size(), 0.0);
+    j.alpha_resid.assign(j.omega.size(), 0.0);
+    st = std2g_polarizability(ctx, &j.par, j.omega.data(), (int)j.omega.size(), j.alpha.data(),
+                              j.alpha_resid.data());
+  }
+  j.status = st;
+  j.t_end = Clock::now();
+}
+
+bool can_admit(const Server &s) {
+  if (s.queue.empty()) return false;
+  return s.inflight == 0 || s.inflight_bytes + s.queue.front()->footprint <= s.budget;
+}
+
+void worker(Server *s, int slot) {
+  void *ctx = s->ctxs[slot];
+  for (;;) {
+    std::shared_ptr<Job> job;
+    {
+      std::unique_lock<std::mutex> lk(s->mu);
+      s->cv_queue.wait(lk, [&] { return s->stop || can_admit(*s); });
+      if (s->stop) return;
+      job = s->queue.front();
+      s->queue.pop_front();
+      s->inflight_bytes += job->footprint;
+      ++s->inflight;
+      s->peak_inflight = std::max(s->peak_inflight, s->inflight);
+      s->peak_bytes = std::max(s->peak_bytes, s->inflight_bytes);
+    }
+    run_job(ctx, *job);
+    {
+      std::lock_guard<std::mutex> lk(s->mu);
+      s->inflight_bytes -= job->footprint;
+      --s->inflight;
+      ++s->completed;
+      job->done = true;
+    }
+    s->cv_done.notify_all();
+    s->cv_queue.notify_all();
+  }
+}
+
+template <typename T>
+std::vector<T> copy_of(const T *p, size_t n) {
+  return std::vector<T>(p, p + n);
+}
+
+}  // namespace
+
+extern "C" {
+
+int std2g_server_create(void **srv, const std2g_server_opts *o) {
+  if (!srv || !o || o->slots < 1 || o->slots > 64) return STD2G_EINVAL;
+  auto s = std::make_unique<Server>();
+  s->opts = *o;
+  if (cudaSetDevice(o->device) != cudaSuccess) return STD2G_ENODEV;
+  size_t free_b = 0, total_b = 0;
+  if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) return STD2G_ECUDA;
+  s->budget = o->hbm_budget > 0 ? o->hbm_budget : (int64_t)(0.8 * (double)free_b);
+  for (int k = 0; k < o->slots; ++k) {
+    std2g_opts eo{};
+    eo.device = o->device;
+    eo.precision = o->precision;
+    eo.verbose = 0;
+    void *ctx = nullptr;
+    int st = std2g_create(&ctx, &eo);
+    if (st != STD2G_OK) {
+      for (void *c : s->ctxs) std2g_destroy(c);
+      return st;
+    }
+    s->ctxs.push_back(ctx);
+  }
+  for (int k = 0; k < o->slots; ++k) s->workers.emplace_back(worker, s.get(), k);
+  *srv = s.release();
+  return STD2G_OK;
+}
+
+int std2g_server_submit(void *srv, const std2g_request *rq, int64_t *ticket) {
+  if (!srv || !rq || !ticket || rq->ncent <= 0 || rq->nmo <= 0 || rq->nao <= 0 || !rq->xyz ||
+      !rq->C || !rq->eps || !rq->occ || !rq->iaoat || !rq->S || !rq->mu_L || !rq->mu_V ||
+      !rq->mu_M || rq->nomega < 0 || (rq->nomega > 0 && !rq->omega))
+    return STD2G_EINVAL;
+  auto *s = (Server *)srv;
+  auto j = std::make_shared<Job>();
+  const size_t npk = (size_t)rq->nao * (rq->nao + 1) / 2;
+  j->ncent = rq->ncent;
+  j->nmo = rq->nmo;
+  j->nao = rq->nao;
+  j->xyz = copy_of(rq->xyz, 4 * (size_t)rq->ncent);
+  j->C = copy_of(rq->C, (size_t)rq->nao * rq->nmo);
+  j->eps = copy_of(rq->eps, (size_t)rq->nmo);
+  j->occ = copy_of(rq->occ, (size_t)rq->nmo);
+  j->iaoat = copy_of(rq->iaoat, (size_t)rq->nao);
+  j->S = copy_of(rq->S, npk);
+  j->muL = copy_of(rq->mu_L, 3 * npk);
+  j->muV = copy_of(rq->mu_V, 3 * npk);
+  j->muM = copy_of(rq->mu_M, 3 * npk);
+  if (rq->nomega > 0) j->omega = copy_of(rq->omega, (size_t)rq->nomega);
+  j->par = rq->params;
+  j->footprint = footprint_estimate(*j);
+  j->t_submit = Clock::now();
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    j->ticket = s->next_ticket++;
+    s->jobs[j->ticket] = j;
+    s->queue.push_back(j);
+    ++s->submitted;
+  }
+  s->cv_queue.notify_all();
+  *ticket = j->ticket;
+  return STD2G_OK;
+}
+
+int std2g_server_poll(void *srv, int64_t ticket, int *done) {
+  if (!srv || !done) return STD2G_EINVAL;
+  auto *s = (Server *)srv;
+  std::lock_guard<std::mutex> lk(s->mu);
+  auto it = s->jobs.find(ticket);
+  if (it == s->jobs.end()) return STD2G_EINVAL;
+  *done = it->second->done ? 1 : 0;
+  return STD2G_OK;
+}
+
+int std2g_server_wait(void *srv, int64_t ticket, std2g_result *res, double *alpha,
+                      double *alpha_resid, double *timing_ms) {
+  if (!srv) return STD2G_EINVAL;
+  auto *s = (Server *)srv;
+  std::shared_ptr<Job> j;
+  {
+    std::unique_lock<std::mutex> lk(s->mu);
+    auto it = s->jobs.find(ticket);
+    if (it == s->jobs.end()) return STD2G_EINVAL;
+    j = it->second;
+    s->cv_done.wait(lk, [&] { return j->done; });
+    s->jobs.erase(ticket);
+  }
+  if (timing_ms) {
+    auto ms = [](Clock::time_point a, Clock::time_point b) {
+      return std::chrono::duration<double, std::milli>(b - a).count();
+    };
+    timing_ms[0] = ms(j->t_submit, j->t_start);   // queued
+    timing_ms[1] = ms(j->t_start, j->t_end);      // running
+    timing_ms[2] = ms(j->t_submit, j->t_end);     // latency
+  }
+  if (j->status != STD2G_OK) return j->status;
+  if (res) {
+    const int n = j->res.nroot;
+    if (res->cap < n) return STD2G_ECAP;
+    double *dst[6] = {res->omega, res->fL, res->fV, res->RL, res->RV, res->resid};
+    const std::vector<double> *src[6] = {&j->om, &j->fL, &j->fV, &j->RL, &j->RV, &j->resid};
+    for (int q = 0; q < 6; ++q)
+      if (dst[q]) std::copy(src[q]->begin(), src[q]->begin() + n, dst[q]);
+    const int cap = res->cap;
+    std2g_result keep = *res;
+    *res = j->res;
+    res->cap = cap;
+    res->omega = keep.omega;
+    res->fL = keep.fL;
+    res->fV = keep.fV;
+    res->RL = keep.RL;
+    res->RV = keep.RV;
+    res->resid = keep.resid;
+  }
+  if (alpha && !j->alpha.empty()) std::copy(j->alpha.begin(), j->alpha.end(), alpha);
+  if (alpha_resid && !j->alpha_resid.empty())
+    std::copy(j->alpha_resid.begin(), j->alpha_resid.end(), alpha_resid);
+  return STD2G_OK;
+}
+
+int std2g_server_stats(void *srv, int64_t *stats) {
+  if (!srv || !stats) return STD2G_EINVAL;
+  auto *s = (Server *)srv;
+  std::lock_guard<std::mutex> lk(s->mu);
+  stats[0] = s->submitted;
+  stats[1] = s->completed;
+  stats[2] = s->inflight;
+  stats[3] = s->peak_inflight;
+  stats[4] = s->inflight_bytes;
+  stats[5] = s->peak_bytes;
+  stats[6] = s->budget;
+  return STD2G_OK;
+}
+
+void std2g_server_destroy(void *srv) {
+  if (!srv) return;
+  auto *s = (Server *)srv;
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->stop = true;
+  }
+  s->cv_queue.notify_all();
+  for (auto &t : s->workers) t.join();
+  for (void *c : s->ctxs) std2g_destroy(c);
+  delete s;
+}
+
+}  // extern "C"

@@ -30,7 +30,8 @@ EXPORTS = [
     "std2g_create", "std2g_load", "std2g_solve", "std2g_polarizability",
     "std2g_get_csf", "std2g_get_vectors", "std2g_phase_times", "std2g_phase_name",
     "std2g_kernel_launches", "std2g_kernel_stats", "std2g_solver_stats", "std2g_error_string",
-    "std2g_destroy", "std2g_screen_noalloc",
+    "std2g_destroy", "std2g_screen_noalloc", "std2g_server_create", "std2g_server_submit",
+    "std2g_server_poll", "std2g_server_wait", "std2g_server_stats", "std2g_server_destroy",
 ]
 
 
@@ -52,6 +53,21 @@ class Params(C.Structure):
                 ("triplet", C.c_int), ("rpa", C.c_int), ("velcorr", C.c_int), ("kshift", C.c_int),
                 ("shftmax", C.c_double), ("shftwidth", C.c_double), ("shftsteep", C.c_double),
                 ("nroots", C.c_int), ("solver", C.c_int), ("conv_tol", C.c_double)]
+
+
+class ServerOpts(C.Structure):
+    _fields_ = [("device", C.c_int), ("precision", C.c_int), ("slots", C.c_int),
+                ("reserved", C.c_int), ("hbm_budget", C.c_int64)]
+
+
+class Request(C.Structure):
+    _fields_ = [("ncent", C.c_int), ("nmo", C.c_int), ("nao", C.c_int),
+                ("xyz", C.POINTER(C.c_double)), ("C", C.POINTER(C.c_double)),
+                ("eps", C.POINTER(C.c_double)), ("occ", C.POINTER(C.c_double)),
+                ("iaoat", C.POINTER(C.c_int)), ("S", C.POINTER(C.c_double)),
+                ("mu_L", C.POINTER(C.c_double)), ("mu_V", C.POINTER(C.c_double)),
+                ("mu_M", C.POINTER(C.c_double)), ("params", Params), ("nomega", C.c_int),
+                ("omega", C.POINTER(C.c_double))]
 
 
 class Result(C.Structure):
@@ -90,6 +106,14 @@ def library():
         lib.std2g_kernel_stats.argtypes = [C.c_void_p, dp, C.POINTER(C.c_int64), dp]
         lib.std2g_solver_stats.argtypes = [C.c_void_p, ip, C.POINTER(C.c_int64),
                                             C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
+        lib.std2g_server_create.argtypes = [C.POINTER(C.c_void_p), C.POINTER(ServerOpts)]
+        lib.std2g_server_submit.argtypes = [C.c_void_p, C.POINTER(Request),
+                                            C.POINTER(C.c_int64)]
+        lib.std2g_server_poll.argtypes = [C.c_void_p, C.c_int64, ip]
+        lib.std2g_server_wait.argtypes = [C.c_void_p, C.c_int64, C.POINTER(Result), dp, dp, dp]
+        lib.std2g_server_stats.argtypes = [C.c_void_p, C.POINTER(C.c_int64)]
+        lib.std2g_server_destroy.argtypes = [C.c_void_p]
+        lib.std2g_server_destroy.restype = None
         lib.std2g_screen_noalloc.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                                               C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                               C.POINTER(Params), C.c_void_p, C.c_void_p,
@@ -307,3 +331,78 @@ def stda(mol, kw: Keywords, ints=None, device=0, precision=0):
     finally:
         eng.close()
     return sol, tda_dat(sol, kw)
+
+
+class Server:
+    """Served form: a request loop with continuous batching over ``slots``
+    engine contexts on one device (``include/std2g.h``, served / batched form).
+
+    ``submit`` copies the inputs and returns a ticket at once; ``wait`` blocks
+    until that request has finished and returns its roots and properties,
+    alpha(omega) when requested, and its queued / running / total times (ms).
+    """
+
+    def __init__(self, device: int = 0, precision: int = 1, slots: int = 4,
+                 hbm_budget: int = 0):
+        self.lib = library()
+        self.srv = C.c_void_p()
+        _check(self.lib.std2g_server_create(C.byref(self.srv),
+                                            C.byref(ServerOpts(device, precision, slots, 0,
+                                                               int(hbm_budget)))))
+        self._nomega = {}
+
+    def submit(self, b: BoundaryInputs, kw: Keywords, omegas=None) -> int:
+        om = None if omegas is None else np.ascontiguousarray(omegas, dtype=np.float64)
+        rq = Request(b.ncent, b.nmo, b.nao, _dp(b.xyz4), _dp(b.C), _dp(b.eps), _dp(b.occ),
+                     b.iaoat1.ctypes.data_as(C.POINTER(C.c_int)), _dp(b.S), _dp(b.muL),
+                     _dp(b.muV), _dp(b.muM), kw.to_c(), 0 if om is None else len(om),
+                     None if om is None else _dp(om))
+        t = C.c_int64()
+        _check(self.lib.std2g_server_submit(self.srv, C.byref(rq), C.byref(t)))
+        self._nomega[t.value] = (0 if om is None else len(om), kw)
+        return t.value
+
+    def done(self, ticket: int) -> bool:
+        d = C.c_int()
+        _check(self.lib.std2g_server_poll(self.srv, ticket, C.byref(d)))
+        return bool(d.value)
+
+    def wait(self, ticket: int, cap: int = 4096):
+        nom, kw = self._nomega.pop(ticket)
+        bufs = [np.zeros(cap) for _ in range(6)]
+        res = Result()
+        res.cap = cap
+        res.omega, res.fL, res.fV, res.RL, res.RV, res.resid = (_dp(x) for x in bufs)
+        alpha = np.zeros(max(1, nom) * 9)
+        ares = np.zeros(max(1, nom))
+        timing = np.zeros(3)
+        _check(self.lib.std2g_server_wait(self.srv, ticket, C.byref(res), _dp(alpha), _dp(ares),
+                                          _dp(timing)))
+        n = res.nroot
+        sol = Solution(omega=bufs[0][:n].copy(), fL=bufs[1][:n].copy(), fV=bufs[2][:n].copy(),
+                       RL=bufs[3][:n].copy(), RV=bufs[4][:n].copy(),
+                       alpha0=np.array(res.alpha0[:]), no=res.no, nv=res.nv, nex=res.nex,
+                       nexpt=res.nexpt, new=res.new_pt, nci=res.nci, csf_hash=res.csf_hash,
+                       ms=res.ms_total, velo=(not kw.rpa) and kw.velcorr,
+                       extras=dict(resid=bufs[5][:n].copy()))
+        a = alpha[:nom * 9].reshape(nom, 3, 3) if nom else None
+        return sol, a, (ares[:nom] if nom else None), dict(
+            queued_ms=timing[0], run_ms=timing[1], latency_ms=timing[2])
+
+    def stats(self) -> dict:
+        st = (C.c_int64 * 7)()
+        _check(self.lib.std2g_server_stats(self.srv, st))
+        keys = ("submitted", "completed", "in_flight", "peak_in_flight", "bytes_in_flight",
+                "peak_bytes", "budget")
+        return dict(zip(keys, [int(x) for x in st]))
+
+    def close(self):
+        if self.srv:
+            self.lib.std2g_server_destroy(self.srv)
+            self.srv = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
