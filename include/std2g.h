@@ -82,7 +82,9 @@ typedef struct {
   double shftmax, shftwidth, shftsteep;   /* kshiftcommon, eV */
   int nroots;        /* 0: every root in (0, E_thr] as ssyevr's window does;
                         k > 0: the lowest k roots (Davidson) */
-  int solver;        /* 0 auto, 1 dense diagonalisation, 2 blocked Davidson */
+  int solver;        /* 0 auto, 1 dense diagonalisation, 2 iterative: blocked
+                        Davidson for roots, matrix-free refined solve for alpha(w)
+                        (auto uses it when the dense A+B, A-B would exceed ~24 GB) */
   double conv_tol;   /* Davidson residual norm tolerance (0: 1e-6) */
 } std2g_params;
 

@@ -82,8 +82,10 @@ struct Ctx {
   DBuf<char> w_cub;
   MixedWork mixed;
   struct RespWork {
-    DBuf<float> Apb32, Amb32, dp, dm, yu, yv, ru, rv, zu, zv, pu, pv, qu, qv, cu, cv;
-    DBuf<double> B1, U, V, PU, MV, R1, R2, pa, pb, wcol, rz, alpha, beta, rr, nrm, nrm2;
+    DBuf<float> Apb32, Amb32, dp, dm;
+    DBuf<double> B1, U, V, PU, MV, R1, R2, pa, pb, wcol, rz, alpha, beta, rr, nrm, nrm2, dmf, dpd,
+        dmd;
+    DBuf<char> vecs[12];
     DBuf<unsigned> flag;
     int outer = 0, inner = 0;
   } rw;
@@ -329,34 +331,30 @@ static void response(Ctx &c, double *Apb, double *Amb, int nci, const double *mu
   }
 }
 
-// Mixed-precision response (response_mixed.cuh): FP64 iterative refinement of
-// the coupled (u, v) equations around FP32 preconditioned conjugate gradients
-// on the same system.  Frequencies whose system is not positive definite are
-// returned in `fallback` (their alpha entries are left untouched).
-static void response_mixed(Ctx &c, const double *Apb, const double *Amb, int n,
-                           const double *musel, const RespReq &rq, std::vector<int> &fallback) {
+// Iterative refinement of the coupled (u, v) response equations
+// (response_mixed.cuh).  fp64(U, V, PU, MV) forms PU = (A+B) U and MV = (A-B) V
+// in FP64; inner(pu, pv, qu, qv) the same products for the CG vectors (type T)
+// in lower precision.  dp, dm: diagonals of A+B, A-B for the preconditioner.
+// Frequencies whose system is not positive definite (or that do not converge)
+// are returned in `fallback` (their alpha entries are left untouched).
+template <typename T, typename D, class Fp64Products, class InnerProducts>
+static void response_ir(Ctx &c, int n, const double *musel, const RespReq &rq,
+                        std::vector<int> &fallback, const D *dp, const D *dm,
+                        const Fp64Products &fp64, const InnerProducts &inner) {
   cudaStream_t s = c.stream;
   auto &w = c.rw;
   const int nw = rq.n, ncol = 3 * nw;
   if (ncol > 32) throw Error{STD2G_EINVAL, "response: at most 10 frequencies per call"};
-  const size_t n2 = (size_t)n * n, nc = (size_t)n * ncol;
+  const size_t nc = (size_t)n * ncol;
   const int g = grid_for((int64_t)nc);
   const double tol = 1e-10;   // relative FP64 residual of every right-hand side
   const int kMaxOuter = 12, kMaxInner = 400;
-  const float one = 1.f, zero = 0.f;
-  const double done = 1.0, dzero = 0.0;
   const bool prof = c.opts.verbose >= 2;
   const auto t0 = std::chrono::steady_clock::now();
   std::vector<double> hw(ncol);
   for (int j = 0; j < ncol; ++j) hw[j] = rq.omega[j / 3];
   double *wcol = w.wcol.ensure(ncol);
   S2G_CUDA(cudaMemcpyAsync(wcol, hw.data(), sizeof(double) * ncol, cudaMemcpyHostToDevice, s));
-  // FP32 copies of A+B and A-B and their diagonals
-  float *Apb32 = w.Apb32.ensure(n2), *Amb32 = w.Amb32.ensure(n2);
-  S2G_LAUNCH(k_d2f, grid_for((int64_t)n2), 256, 0, s, Apb32, Apb, (int64_t)n2);
-  S2G_LAUNCH(k_d2f, grid_for((int64_t)n2), 256, 0, s, Amb32, Amb, (int64_t)n2);
-  float *dp = w.dp.ensure(n), *dm = w.dm.ensure(n);
-  S2G_LAUNCH(k_resp_diags, (int)div_up(n, 256), 256, 0, s, Apb, Amb, n, dp, dm);
   double *B1 = w.B1.ensure(nc), *U = w.U.ensure(nc), *V = w.V.ensure(nc);
   double *PU = w.PU.ensure(nc), *MV = w.MV.ensure(nc), *R1 = w.R1.ensure(nc),
          *R2 = w.R2.ensure(nc);
@@ -374,33 +372,30 @@ static void response_mixed(Ctx &c, const double *Apb, const double *Amb, int n,
   std::vector<double> hb(ncol), hr(ncol), hr2(ncol), hrel(ncol, 1.0);
   coldot64(B1, B1, nrm);
   S2G_CUDA(cudaMemcpyAsync(hb.data(), nrm, sizeof(double) * ncol, cudaMemcpyDeviceToHost, s));
-  // FP32 CG vectors, halves (u, v)
-  float *yu = w.yu.ensure(nc), *yv = w.yv.ensure(nc), *ru = w.ru.ensure(nc), *rv = w.rv.ensure(nc),
-        *zu = w.zu.ensure(nc), *zv = w.zv.ensure(nc), *pu = w.pu.ensure(nc), *pv = w.pv.ensure(nc),
-        *qu = w.qu.ensure(nc), *qv = w.qv.ensure(nc), *cu = w.cu.ensure(nc), *cv = w.cv.ensure(nc);
+  // CG vectors, halves (u, v)
+  T *vec[12];
+  for (int q = 0; q < 12; ++q) vec[q] = (T *)w.vecs[q].ensure(nc * sizeof(T));
+  T *yu = vec[0], *yv = vec[1], *ru = vec[2], *rv = vec[3], *zu = vec[4], *zv = vec[5],
+    *pu = vec[6], *pv = vec[7], *qu = vec[8], *qv = vec[9], *cu = vec[10], *cv = vec[11];
   double *rz = w.rz.ensure(ncol), *al = w.alpha.ensure(ncol), *be = w.beta.ensure(ncol),
          *rr = w.rr.ensure(ncol);
   unsigned *flag = w.flag.ensure(1);
   S2G_CUDA(cudaMemsetAsync(flag, 0, sizeof(unsigned), s));
-  cublasHandle_t h = c.blas;
   auto pcg = [&]() {
-    S2G_LAUNCH(k_pcg2_init, rgrid, 256, 0, s, yu, yv, ru, rv, zu, zv, pu, pv, cu, cv, dp, dm, wcol,
-               n, pa, pb);
+    S2G_LAUNCH((k_pcg2_init<T, D>), rgrid, 256, 0, s, yu, yv, ru, rv, zu, zv, pu, pv, cu, cv, dp,
+               dm, wcol, n, pa, pb);
     S2G_LAUNCH(k_pcg_beta, sgrid, 32, 0, s, pa, pb, kRespSplit, ncol, rz, be, rr, 1);
     std::vector<double> rr0(ncol), rrn(ncol);
     S2G_CUDA(cudaMemcpyAsync(rr0.data(), rr, sizeof(double) * ncol, cudaMemcpyDeviceToHost, s));
     S2G_CUDA(cudaStreamSynchronize(s));
     for (int it = 1; it <= kMaxInner; ++it) {
-      S2G_CUBLAS(cublasSgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, n, ncol, n, &one, Apb32, n, pu, n,
-                             &zero, qu, n));
-      S2G_CUBLAS(cublasSgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, n, ncol, n, &one, Amb32, n, pv, n,
-                             &zero, qv, n));
-      S2G_LAUNCH(k_pcg2_pq, rgrid, 256, 0, s, qu, qv, pu, pv, wcol, n, pa);
+      inner(pu, pv, qu, qv);
+      S2G_LAUNCH(k_pcg2_pq<T>, rgrid, 256, 0, s, qu, qv, pu, pv, wcol, n, pa);
       S2G_LAUNCH(k_pcg_alpha, sgrid, 32, 0, s, pa, kRespSplit, ncol, rz, al, flag);
-      S2G_LAUNCH(k_pcg2_update, rgrid, 256, 0, s, yu, yv, ru, rv, zu, zv, pu, pv, qu, qv, dp, dm,
-                 wcol, al, n, pa, pb);
+      S2G_LAUNCH((k_pcg2_update<T, D>), rgrid, 256, 0, s, yu, yv, ru, rv, zu, zv, pu, pv, qu, qv,
+                 dp, dm, wcol, al, n, pa, pb);
       S2G_LAUNCH(k_pcg_beta, sgrid, 32, 0, s, pa, pb, kRespSplit, ncol, rz, be, rr, 0);
-      S2G_LAUNCH(k_pcg2_dir, g, 256, 0, s, pu, pv, zu, zv, be, n, ncol);
+      S2G_LAUNCH(k_pcg2_dir<T>, g, 256, 0, s, pu, pv, zu, zv, be, n, ncol);
       ++w.inner;
       if (it % 8 == 0) {
         S2G_CUDA(cudaMemcpyAsync(rrn.data(), rr, sizeof(double) * ncol, cudaMemcpyDeviceToHost,
@@ -416,10 +411,7 @@ static void response_mixed(Ctx &c, const double *Apb, const double *Amb, int n,
   w.outer = w.inner = 0;
   for (int outer = 0; outer <= kMaxOuter; ++outer) {
     // FP64 residuals of the coupled equations
-    S2G_CUBLAS(cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, n, ncol, n, &done, Apb, n, U, n, &dzero,
-                           PU, n));
-    S2G_CUBLAS(cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, n, ncol, n, &done, Amb, n, V, n, &dzero,
-                           MV, n));
+    fp64(U, V, PU, MV);
     S2G_LAUNCH(k_resp_resid, g, 256, 0, s, R1, R2, B1, U, V, PU, MV, wcol, n, ncol);
     coldot64(R1, R1, nrm);
     coldot64(R2, R2, nrm2);
@@ -435,8 +427,6 @@ static void response_mixed(Ctx &c, const double *Apb, const double *Amb, int n,
     }
     w.outer = outer;
     if (worst <= tol || outer == kMaxOuter) {
-      // a frequency with negative curvature in any column, or not converged,
-      // goes to the FP64 form
       for (int fw = 0; fw < nw; ++fw) {
         bool bad = false;
         for (int x = 0; x < 3; ++x) {
@@ -447,15 +437,20 @@ static void response_mixed(Ctx &c, const double *Apb, const double *Amb, int n,
       }
       break;
     }
-    // correction from the FP32 solve of the same system with the residual
-    S2G_LAUNCH(k_d2f, g, 256, 0, s, cu, R1, (int64_t)nc);
-    S2G_LAUNCH(k_d2f, g, 256, 0, s, cv, R2, (int64_t)nc);
+    // correction from the lower-precision solve of the same system
+    if (sizeof(T) == sizeof(float)) {
+      S2G_LAUNCH(k_d2f, g, 256, 0, s, (float *)cu, R1, (int64_t)nc);
+      S2G_LAUNCH(k_d2f, g, 256, 0, s, (float *)cv, R2, (int64_t)nc);
+    } else {
+      S2G_CUDA(cudaMemcpyAsync(cu, R1, sizeof(double) * nc, cudaMemcpyDeviceToDevice, s));
+      S2G_CUDA(cudaMemcpyAsync(cv, R2, sizeof(double) * nc, cudaMemcpyDeviceToDevice, s));
+    }
     pcg();
-    S2G_LAUNCH(k_resp_accum, g, 256, 0, s, U, V, yu, yv, (int64_t)nc);
+    S2G_LAUNCH(k_resp_accum<T>, g, 256, 0, s, U, V, yu, yv, (int64_t)nc);
   }
   if (prof) {
     S2G_CUDA(cudaStreamSynchronize(s));
-    std::fprintf(stderr, "response (mixed): %d refinement steps, %d CG steps, %.2f ms\n",
+    std::fprintf(stderr, "response (refined): %d refinement steps, %d CG steps, %.2f ms\n",
                  w.outer, w.inner,
                  std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0)
                      .count());
@@ -477,6 +472,68 @@ static void response_mixed(Ctx &c, const double *Apb, const double *Amb, int n,
       rq.resid[fw] = wf;
     }
   }
+}
+
+// Mixed form with the dense matrices: FP64 residual products with A+B, A-B,
+// FP32 copies of both for the CG products.
+static void response_mixed(Ctx &c, const double *Apb, const double *Amb, int n,
+                           const double *musel, const RespReq &rq, std::vector<int> &fallback) {
+  cudaStream_t s = c.stream;
+  auto &w = c.rw;
+  const size_t n2 = (size_t)n * n;
+  const int ncol = 3 * rq.n;
+  float *Apb32 = w.Apb32.ensure(n2), *Amb32 = w.Amb32.ensure(n2);
+  S2G_LAUNCH(k_d2f, grid_for((int64_t)n2), 256, 0, s, Apb32, Apb, (int64_t)n2);
+  S2G_LAUNCH(k_d2f, grid_for((int64_t)n2), 256, 0, s, Amb32, Amb, (int64_t)n2);
+  float *dp = w.dp.ensure(n), *dm = w.dm.ensure(n);
+  S2G_LAUNCH(k_resp_diags, (int)div_up(n, 256), 256, 0, s, Apb, Amb, n, dp, dm);
+  cublasHandle_t h = c.blas;
+  const float one = 1.f, zero = 0.f;
+  const double done = 1.0, dzero = 0.0;
+  auto fp64 = [&](const double *U, const double *V, double *PU, double *MV) {
+    S2G_CUBLAS(cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, n, ncol, n, &done, Apb, n, U, n, &dzero,
+                           PU, n));
+    S2G_CUBLAS(cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, n, ncol, n, &done, Amb, n, V, n, &dzero,
+                           MV, n));
+  };
+  auto inner = [&](const float *pu, const float *pv, float *qu, float *qv) {
+    S2G_CUBLAS(cublasSgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, n, ncol, n, &one, Apb32, n, pu, n, &zero,
+                           qu, n));
+    S2G_CUBLAS(cublasSgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, n, ncol, n, &one, Amb32, n, pv, n, &zero,
+                           qv, n));
+  };
+  response_ir<float, float>(c, n, musel, rq, fallback, dp, dm, fp64, inner);
+}
+
+// Matrix-free form (no n x n storage): products with A+B, A-B through the
+// Loewdin-MO operators of matfree.cuh (k_rpa_mf_diag), FP64 for the residuals
+// and, in the mixed form, FP32 operator products for the CG.
+static void response_matfree(Ctx &c, int n, const double *musel, const RespReq &rq,
+                             std::vector<int> &fallback, const double *ed, const double *ekd,
+                             const double *uci, double ak, double ax, bool mixed) {
+  cudaStream_t s = c.stream;
+  auto &w = c.rw;
+  const int ncol = 3 * rq.n;
+  double *d = w.dmf.ensure(n), *dpd = w.dpd.ensure(n), *dmd = w.dmd.ensure(n);
+  S2G_LAUNCH(k_rpa_mf_diag, (int)div_up(n, 128), 128, 0, s, d, dpd, dmd, ed, ekd, uci, c.mf.ci,
+             c.mf.ca, n, c.mf.nv, ak, ax);
+  const bool amb_diag = std::fabs(ax) < 1e-6;
+  auto products = [&](const double *U, const double *V, double *PU, double *MV, bool f32) {
+    c.mf.f32 = f32;
+    mf_apply(c.mf, c.blas, s, U, ncol, PU, 2.0 * ak, -1.0, -ax, d);
+    if (amb_diag)
+      S2G_LAUNCH(k_diag_mul, grid_for((int64_t)n * ncol), 256, 0, s, MV, dmd, V, n, ncol);
+    else
+      mf_apply(c.mf, c.blas, s, V, ncol, MV, 0.0, -1.0, ax, d);
+    c.mf.f32 = false;
+  };
+  auto fp64 = [&](const double *U, const double *V, double *PU, double *MV) {
+    products(U, V, PU, MV, false);
+  };
+  auto inner = [&](const double *pu, const double *pv, double *qu, double *qv) {
+    products(pu, pv, qu, qv, mixed);
+  };
+  response_ir<double, double>(c, n, musel, rq, fallback, dpd, dmd, fp64, inner);
 }
 
 // --------------------------------------------------------------------------
@@ -827,8 +884,13 @@ static void solve(Ctx &c, const std2g_params &p_in, std2g_result *res, const Res
   // Large TDA problems with a root count use the matrix-free operators and the
   // blocked Davidson solver; everything else builds the matrices explicitly.
   const bool use_mf = !p.rpa && p.nroots > 0 && (p.solver == 2 || (p.solver == 0 && nci > 1024));
+  // alpha(w) for CSF spaces whose dense A+B, A-B and their work copies would
+  // exceed ~24 GB: matrix-free operators and the refined iterative solve
+  // (or when the iterative solver is requested, solver == 2)
+  const bool resp_mf =
+      resp != nullptr && (p.solver == 2 || (double)nci * nci * 8.0 * 10.0 > 24e9);
   double *K = nullptr, *J = nullptr, *Kx = nullptr;
-  if (!use_mf) {
+  if (!use_mf && !resp_mf) {
     K = c.w_K.ensure(n2);
     J = c.w_J.ensure(n2);
     gemm(c, CUBLAS_OP_T, CUBLAS_OP_N, nci, nci, N, 1.0, Ps, N, Qs, N, 0.0, K, nci);
@@ -849,7 +911,10 @@ static void solve(Ctx &c, const std2g_params &p_in, std2g_result *res, const Res
     mf.nci = nci;
     mf.nao = nao;
     mf.f32 = false;
-    if (mixed) {
+    if (resp_mf) {
+      mf_setup_ops<double>(mf, mf.d, s, Clow, c.d_slot_ao.get(), Poo, Pia, Qs, Ps, true);
+      if (mixed) mf_setup_ops<float>(mf, mf.f, s, Clow, c.d_slot_ao.get(), Poo, Pia, Qs, Ps, true);
+    } else if (mixed) {
       // tensor-core products for the first Davidson stage
       MatFreeTc &w = c.mftc;
       w.N = N;
@@ -943,10 +1008,14 @@ static void solve(Ctx &c, const std2g_params &p_in, std2g_result *res, const Res
     c.mixed.lastX = X;
     if (nroot < 1) throw Error{STD2G_ENOROOT, "no root below the energy threshold"};
   } else {
-    double *Apb = c.w_Apb.ensure(n2), *Amb = c.w_Amb.ensure(n2);
-    // J holds (ij|ab); A+B and A-B from K, Kx, J
-    S2G_LAUNCH(k_combine_rpa, grid_for(n2), 256, 0, s, Apb, Amb, (double *)nullptr, K, Kx, J,
-               (int64_t)nci, ak, p.ax, d_edall, ekd);
+    double *Apb = nullptr, *Amb = nullptr;
+    if (!resp_mf) {
+      Apb = c.w_Apb.ensure(n2);
+      Amb = c.w_Amb.ensure(n2);
+      // J holds (ij|ab); A+B and A-B from K, Kx, J
+      S2G_LAUNCH(k_combine_rpa, grid_for(n2), 256, 0, s, Apb, Amb, (double *)nullptr, K, Kx, J,
+                 (int64_t)nci, ak, p.ax, d_edall, ekd);
+    }
     if (resp) {
       record(c, PH_EIGEN);
       record(c, PH_PROPS);
@@ -954,7 +1023,14 @@ static void solve(Ctx &c, const std2g_params &p_in, std2g_result *res, const Res
       double *musel = c.w_musel.ensure((size_t)nci * 9);
       S2G_LAUNCH(k_gather_mu, grid_for((int64_t)nci * 9), 256, 0, s, musel, c.w_mu_ov.get(), no,
                  nv, d_ci, d_ca, nci);
-      if (mixed) {
+      if (resp_mf) {
+        std::vector<int> fb;
+        response_matfree(c, nci, musel, *resp, fb, d_edall, ekd, uci, ak, p.ax, mixed);
+        if (!fb.empty())
+          throw Error{STD2G_ENOCONV,
+                      "alpha(w): a frequency above the first excitation needs the dense form, "
+                      "which does not fit for this CSF space"};
+      } else if (mixed) {
         std::vector<int> fb;
         response_mixed(c, Apb, Amb, nci, musel, *resp, fb);
         if (!fb.empty()) {

@@ -6,8 +6,9 @@
 // system in u = X+Y, v = X-Y
 //   (A+B) u - w v = -2 mu,     -w u + (A-B) v = 0,
 // by iterative refinement: residuals in FP64 from products with the FP64
-// A+B and A-B (no inverse is formed), corrections from FP32 preconditioned
-// conjugate gradients on the same 2n system.  For w below the first
+// A+B and A-B (no inverse is formed), corrections from preconditioned
+// conjugate gradients on the same 2n system with lower-precision products
+// (dense: FP32 copies of A+B, A-B; matrix-free: the FP32 operator).  For w below the first
 // excitation that system is positive definite (its Schur complement is the
 // reference's matrix).  The preconditioner is the exact inverse of each 2x2
 // block [[p_i, -w], [-w, m_i]] (p, m the diagonals of A+B and A-B).  All
@@ -88,7 +89,7 @@ __global__ void k_resp_sum(const double *__restrict__ part, int nsplit, int ncol
   out[j] = s;
 }
 
-// Diagonals of A+B and A-B (FP64)
+// Diagonals of A+B and A-B from the dense FP64 matrices
 __global__ void k_resp_diags(const double *__restrict__ Apb, const double *__restrict__ Amb, int n,
                              float *__restrict__ dp, float *__restrict__ dm) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -97,10 +98,38 @@ __global__ void k_resp_diags(const double *__restrict__ Apb, const double *__res
   dm[i] = (float)Amb[i + (int64_t)n * i];
 }
 
-// U += du ; V += dv (FP32 corrections into FP64 iterates)
+// Matrix-free A+B / A-B (rrpamat stda.f:1893-1928 in operator form): with the
+// operator parts K, J, Kx (their own diagonals included),
+//   (A+B) x = (2ak K - ax Kx - J) x + d o x,   (A-B) x = (ax Kx - J) x + d o x,
+//   d = ed - ak (ia|ia) + (ii|aa);
+// for ax = 0, A-B is the diagonal ed - ak (ia|ia).  Also the diagonals of
+// A+B and A-B for the preconditioner.
+__global__ void k_rpa_mf_diag(double *__restrict__ d, double *__restrict__ dpd,
+                              double *__restrict__ dmd, const double *__restrict__ ed,
+                              const double *__restrict__ ekd, const double *__restrict__ uci,
+                              const int *__restrict__ ci, const int *__restrict__ ca, int nci,
+                              int nv, double ak, double ax) {
+  int u = blockIdx.x * blockDim.x + threadIdx.x;
+  if (u >= nci) return;
+  const double e = ekd[u], jd = uci[ca[u] + (int64_t)nv * ci[u]];
+  d[u] = ed[u] - ak * e + jd;
+  dpd[u] = ed[u] - ax * e + ak * e;
+  dmd[u] = ed[u] - ak * e + ax * e;
+}
+
+// y[:, j] = d o x[:, j]
+__global__ void k_diag_mul(double *__restrict__ y, const double *__restrict__ d,
+                           const double *__restrict__ x, int n, int ncol) {
+  const int64_t total = (int64_t)n * ncol;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
+       t += (int64_t)gridDim.x * blockDim.x)
+    y[t] = d[t % n] * x[t];
+}
+
+// U += du ; V += dv (corrections into the FP64 iterates)
+template <typename T>
 __global__ void k_resp_accum(double *__restrict__ U, double *__restrict__ V,
-                             const float *__restrict__ du, const float *__restrict__ dv,
-                             int64_t total) {
+                             const T *__restrict__ du, const T *__restrict__ dv, int64_t total) {
   for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
        t += (int64_t)gridDim.x * blockDim.x) {
     U[t] += (double)du[t];
@@ -109,38 +138,40 @@ __global__ void k_resp_accum(double *__restrict__ U, double *__restrict__ V,
 }
 
 // ---- preconditioned CG on the 2n system, ncol independent systems in lockstep ----
-// Vectors come in halves (u, v), each n x ncol column-major.  Scalars per
-// column (FP64): rz, alpha, beta, rr; flag: bit j set on negative curvature.
+// Vectors (type T: FP32 for the dense mixed form, FP64 for the matrix-free
+// form) come in halves (u, v), each n x ncol column-major.  Scalars per column
+// (FP64): rz, alpha, beta, rr; flag: bit j set on negative curvature.
 
 // z = P r with P the inverse of the 2x2 blocks [[p, -w], [-w, m]]
-__device__ __forceinline__ void pcg2_prec(float ru, float rv, float p, float m, float w,
-                                          float &zu, float &zv) {
-  const float det = fmaxf(p * m - w * w, 1e-12f);
-  zu = (m * ru + w * rv) / det;
-  zv = (w * ru + p * rv) / det;
+template <typename T, typename D>
+__device__ __forceinline__ void pcg2_prec(T ru, T rv, D p, D m, T w, T &zu, T &zv) {
+  const T pp = (T)p, mm = (T)m;
+  T det = pp * mm - w * w;
+  det = det > (T)1e-12 ? det : (T)1e-12;
+  zu = (mm * ru + w * rv) / det;
+  zv = (w * ru + pp * rv) / det;
 }
 
 // y = 0, r = c, z = P r, p = z; partial r.z and r.r
-__global__ void k_pcg2_init(float *__restrict__ yu, float *__restrict__ yv,
-                            float *__restrict__ ru, float *__restrict__ rv,
-                            float *__restrict__ zu, float *__restrict__ zv,
-                            float *__restrict__ pu, float *__restrict__ pv,
-                            const float *__restrict__ cu, const float *__restrict__ cv,
-                            const float *__restrict__ dp, const float *__restrict__ dm,
-                            const double *__restrict__ wcol, int n,
+template <typename T, typename D>
+__global__ void k_pcg2_init(T *__restrict__ yu, T *__restrict__ yv, T *__restrict__ ru,
+                            T *__restrict__ rv, T *__restrict__ zu, T *__restrict__ zv,
+                            T *__restrict__ pu, T *__restrict__ pv, const T *__restrict__ cu,
+                            const T *__restrict__ cv, const D *__restrict__ dp,
+                            const D *__restrict__ dm, const double *__restrict__ wcol, int n,
                             double *__restrict__ part_rz, double *__restrict__ part_rr) {
   const int j = blockIdx.y;
-  const float w = (float)wcol[j];
+  const T w = (T)wcol[j];
   const int64_t chunk = (n + gridDim.x - 1) / gridDim.x;
   const int64_t i0 = chunk * blockIdx.x, i1 = min((int64_t)n, i0 + chunk);
   double srz = 0.0, srr = 0.0;
   for (int64_t i = i0 + threadIdx.x; i < i1; i += blockDim.x) {
     const int64_t o = i + (int64_t)n * j;
-    const float a = cu[o], b = cv[o];
-    float za, zb;
+    const T a = cu[o], b = cv[o];
+    T za, zb;
     pcg2_prec(a, b, dp[i], dm[i], w, za, zb);
-    yu[o] = 0.f;
-    yv[o] = 0.f;
+    yu[o] = (T)0;
+    yv[o] = (T)0;
     ru[o] = a;
     rv[o] = b;
     zu[o] = za;
@@ -162,17 +193,18 @@ __global__ void k_pcg2_init(float *__restrict__ yu, float *__restrict__ yv,
 
 // (qu, qv) = ((A+B) pu - w pv, (A-B) pv - w pu), the products given in (qu, qv);
 // partial p.q
-__global__ void k_pcg2_pq(float *__restrict__ qu, float *__restrict__ qv,
-                          const float *__restrict__ pu, const float *__restrict__ pv,
-                          const double *__restrict__ wcol, int n, double *__restrict__ part) {
+template <typename T>
+__global__ void k_pcg2_pq(T *__restrict__ qu, T *__restrict__ qv, const T *__restrict__ pu,
+                          const T *__restrict__ pv, const double *__restrict__ wcol, int n,
+                          double *__restrict__ part) {
   const int j = blockIdx.y;
-  const float w = (float)wcol[j];
+  const T w = (T)wcol[j];
   const int64_t chunk = (n + gridDim.x - 1) / gridDim.x;
   const int64_t i0 = chunk * blockIdx.x, i1 = min((int64_t)n, i0 + chunk);
   double s = 0.0;
   for (int64_t i = i0 + threadIdx.x; i < i1; i += blockDim.x) {
     const int64_t o = i + (int64_t)n * j;
-    const float a = qu[o] - w * pv[o], b = qv[o] - w * pu[o];
+    const T a = qu[o] - w * pv[o], b = qv[o] - w * pu[o];
     qu[o] = a;
     qv[o] = b;
     s += (double)pu[o] * a + (double)pv[o] * b;
@@ -201,16 +233,16 @@ __global__ void k_pcg_alpha(const double *__restrict__ part, int nsplit, int nco
 }
 
 // y += a p ; r -= a q ; z = P r ; partial r.z and r.r
-__global__ void k_pcg2_update(float *__restrict__ yu, float *__restrict__ yv,
-                              float *__restrict__ ru, float *__restrict__ rv,
-                              float *__restrict__ zu, float *__restrict__ zv,
-                              const float *__restrict__ pu, const float *__restrict__ pv,
-                              const float *__restrict__ qu, const float *__restrict__ qv,
-                              const float *__restrict__ dp, const float *__restrict__ dm,
+template <typename T, typename D>
+__global__ void k_pcg2_update(T *__restrict__ yu, T *__restrict__ yv, T *__restrict__ ru,
+                              T *__restrict__ rv, T *__restrict__ zu, T *__restrict__ zv,
+                              const T *__restrict__ pu, const T *__restrict__ pv,
+                              const T *__restrict__ qu, const T *__restrict__ qv,
+                              const D *__restrict__ dp, const D *__restrict__ dm,
                               const double *__restrict__ wcol, const double *__restrict__ alpha,
                               int n, double *__restrict__ part_rz, double *__restrict__ part_rr) {
   const int j = blockIdx.y;
-  const float a = (float)alpha[j], w = (float)wcol[j];
+  const T a = (T)alpha[j], w = (T)wcol[j];
   const int64_t chunk = (n + gridDim.x - 1) / gridDim.x;
   const int64_t i0 = chunk * blockIdx.x, i1 = min((int64_t)n, i0 + chunk);
   double srz = 0.0, srr = 0.0;
@@ -218,10 +250,10 @@ __global__ void k_pcg2_update(float *__restrict__ yu, float *__restrict__ yv,
     const int64_t o = i + (int64_t)n * j;
     yu[o] += a * pu[o];
     yv[o] += a * pv[o];
-    const float x = ru[o] - a * qu[o], y = rv[o] - a * qv[o];
+    const T x = ru[o] - a * qu[o], y = rv[o] - a * qv[o];
     ru[o] = x;
     rv[o] = y;
-    float za, zb;
+    T za, zb;
     pcg2_prec(x, y, dp[i], dm[i], w, za, zb);
     zu[o] = za;
     zv[o] = zb;
@@ -255,13 +287,14 @@ __global__ void k_pcg_beta(const double *__restrict__ part_rz, const double *__r
 }
 
 // p = z + beta p, both halves
-__global__ void k_pcg2_dir(float *__restrict__ pu, float *__restrict__ pv,
-                           const float *__restrict__ zu, const float *__restrict__ zv,
-                           const double *__restrict__ beta, int n, int ncol) {
+template <typename T>
+__global__ void k_pcg2_dir(T *__restrict__ pu, T *__restrict__ pv, const T *__restrict__ zu,
+                           const T *__restrict__ zv, const double *__restrict__ beta, int n,
+                           int ncol) {
   const int64_t total = (int64_t)n * ncol;
   for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
        t += (int64_t)gridDim.x * blockDim.x) {
-    const float b = (float)beta[t / n];
+    const T b = (T)beta[t / n];
     pu[t] = zu[t] + b * pu[t];
     pv[t] = zv[t] + b * pv[t];
   }

@@ -12,7 +12,10 @@
 //     requests already in flight (or nothing else is in flight), in FIFO
 //     order, so requests that arrive while others run start as soon as slots
 //     and memory free up and their kernels overlap on the device;
-//   * inputs are copied at submit, results are kept until std2g_server_wait.
+//   * inputs are copied at submit, results are kept until std2g_server_wait;
+//   * a slot that ran a large request (estimate above budget / (2 slots)) or
+//     ran out of memory gets a fresh context; a request that ran out of
+//     memory is retried once with the device to itself.
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
@@ -39,6 +42,7 @@ struct Job {
   std::vector<int> iaoat;
   std2g_params par{};
   int64_t footprint = 0;
+  bool exclusive = false;   // admitted only when nothing else is in flight
   Clock::time_point t_submit, t_start, t_end;
   // results
   bool done = false;
@@ -77,9 +81,11 @@ int64_t footprint_estimate(const Job &j) {
   int64_t b = 8 * (3 * N * pairs + 2 * N * nocc * nocc + 2 * N * nvir * nvir);
   b += 8 * (16 * nao * nao + 12 * (int64_t)j.nmo * nao);
   b += std::min<int64_t>(6000000000LL, 8 * pairs * std::min<int64_t>(pairs, 4096));
-  const int64_t nci = std::min<int64_t>(pairs, 20000);
+  const int64_t nci = std::min<int64_t>(pairs, 30000);
   if (nci <= 1024 || j.par.rpa || !j.omega.empty())
-    b += 8 * 8 * nci * nci;   // dense A / A+B / A-B and their work copies
+    b += 12 * 8 * nci * nci;   // dense K, J, Kx, A+B, A-B and their work copies
+  else
+    b += 4 * 8 * nci * 512;    // Davidson subspace and products
   return b;
 }
 
@@ -118,11 +124,25 @@ void run_job(void *ctx, Job &j) {
 
 bool can_admit(const Server &s) {
   if (s.queue.empty()) return false;
-  return s.inflight == 0 || s.inflight_bytes + s.queue.front()->footprint <= s.budget;
+  if (s.inflight == 0) return true;
+  const Job &j = *s.queue.front();
+  return !j.exclusive && s.inflight_bytes + j.footprint <= s.budget;
+}
+
+// Fresh context for a slot: releases every device buffer the old one held.
+bool renew_context(Server *s, int slot) {
+  std2g_destroy(s->ctxs[slot]);
+  s->ctxs[slot] = nullptr;
+  std2g_opts eo{};
+  eo.device = s->opts.device;
+  eo.precision = s->opts.precision;
+  void *ctx = nullptr;
+  if (std2g_create(&ctx, &eo) != STD2G_OK) return false;
+  s->ctxs[slot] = ctx;
+  return true;
 }
 
 void worker(Server *s, int slot) {
-  void *ctx = s->ctxs[slot];
   for (;;) {
     std::shared_ptr<Job> job;
     {
@@ -136,16 +156,31 @@ void worker(Server *s, int slot) {
       s->peak_inflight = std::max(s->peak_inflight, s->inflight);
       s->peak_bytes = std::max(s->peak_bytes, s->inflight_bytes);
     }
-    run_job(ctx, *job);
+    run_job(s->ctxs[slot], *job);
+    // Context buffers only grow; after a large request (or a failed one) the
+    // slot starts again from a fresh context so that idle slots do not hold
+    // memory the admission rule no longer counts.
+    const bool out_of_memory = job->status == STD2G_ENOMEM;
+    const bool large = job->footprint > s->budget / (2 * (int64_t)s->ctxs.size());
+    bool alive = true;
+    if (out_of_memory || large) alive = renew_context(s, slot);
+    bool retry = out_of_memory && !job->exclusive && alive;
     {
       std::lock_guard<std::mutex> lk(s->mu);
       s->inflight_bytes -= job->footprint;
       --s->inflight;
-      ++s->completed;
-      job->done = true;
+      if (retry) {   // once more, with the device to itself
+        job->exclusive = true;
+        job->status = STD2G_OK;
+        s->queue.push_front(job);
+      } else {
+        ++s->completed;
+        job->done = true;
+      }
     }
     s->cv_done.notify_all();
     s->cv_queue.notify_all();
+    if (!alive) return;   // this slot could not get a new context
   }
 }
 
@@ -299,7 +334,8 @@ void std2g_server_destroy(void *srv) {
   }
   s->cv_queue.notify_all();
   for (auto &t : s->workers) t.join();
-  for (void *c : s->ctxs) std2g_destroy(c);
+  for (void *c : s->ctxs)
+    if (c) std2g_destroy(c);
   delete s;
 }
 

@@ -142,6 +142,15 @@ def test_polarizability_mixed_refinement(benzene):
     rel2 = np.abs(a1 - a0).max(axis=(1, 2)) / np.abs(a0).max(axis=(1, 2))
     assert rel2.max() < 1e-4, rel2
     assert r1.max() < 1e-8
+    # matrix-free operators (no n x n storage), both forms, against the dense FP64 form
+    kw3 = Keywords(ax=0.5, e_thr_ev=9.0, solver=2)
+    for prec in (0, 1):
+        e = _engine(prec)
+        e.load(boundary_inputs(mol2, ints2))
+        a3, r3 = e.polarizability(kw3, [0.0, 0.05, 0.1])
+        rel3 = np.abs(a3 - a0).max(axis=(1, 2)) / np.abs(a0).max(axis=(1, 2))
+        assert rel3.max() < 1e-6, (prec, rel3)
+        assert r3.max() < 1e-8
 
 
 def test_random_cluster_triplet_and_kshift():
