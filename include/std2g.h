@@ -57,13 +57,18 @@ enum {
 };
 
 /* ---- engine options (per context) -------------------------------------- */
+/* Mixed form: tensor-core PT couplings and Davidson products at any problem
+   size (by default they are used from ~2.5e8 PT couplings and 16384 CSFs, below
+   which the solve is latency-bound and the FP64 GEMMs serve it). */
+#define STD2G_FLAG_TENSOR_ALWAYS 1
+
 typedef struct {
   int device;            /* CUDA device ordinal */
   int precision;         /* 0: FP64 form (all contractions FP64)
                             1: mixed form (BF16-split tensor-core contractions,
                                FP32 A storage, FP64 screen / Rayleigh-Ritz) */
   int verbose;           /* 0 silent; 1 per-phase timings to stderr */
-  int reserved;
+  int flags;             /* STD2G_FLAG_* */
   int64_t max_device_bytes; /* 0 = no limit */
 } std2g_opts;
 
@@ -83,8 +88,10 @@ typedef struct {
   int nroots;        /* 0: every root in (0, E_thr] as ssyevr's window does;
                         k > 0: the lowest k roots (Davidson) */
   int solver;        /* 0 auto, 1 dense diagonalisation, 2 iterative: blocked
-                        Davidson for roots, matrix-free refined solve for alpha(w)
-                        (auto uses it when the dense A+B, A-B would exceed ~24 GB) */
+                        Davidson for roots (in the mixed form with its tensor-core
+                        first stage at any size; auto uses that stage from 16384
+                        CSFs), matrix-free refined solve for alpha(w) (auto uses
+                        it when the dense A+B, A-B would exceed ~24 GB) */
   double conv_tol;   /* Davidson residual norm tolerance (0: 1e-6) */
 } std2g_params;
 

@@ -277,6 +277,9 @@ inline int davidson(DavidsonWork &dw, cublasHandle_t blas, cusolverDnHandle_t so
       }
     nconv = kwant - nunc_wanted;
     dw.max_resid = *std::max_element(h_rn.begin(), h_rn.begin() + kwant);
+    if (dw.profile)
+      std::fprintf(stderr, "  davidson iter %d: m %d, unconverged %d of %d, max residual %.3e\n",
+                   it + 1, m, nunc_wanted, kwant, dw.max_resid);
     clk.tick(3);
     if (nunc_wanted == 0) break;
     int nc = (int)unc.size();

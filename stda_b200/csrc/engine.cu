@@ -743,8 +743,13 @@ static void solve(Ctx &c, const std2g_params &p_in, std2g_result *res, const Res
     // chunk candidates by occupied index (candidates are in (i,a) order)
     const int64_t ldj = (int64_t)nv * nvp;
     const double budget = 6.0e9;   // bytes of K/J buffers per chunk
-    const double per_occ = (mixed ? 4.0 : 8.0) * ((double)nex * nv + (double)ldj * nop) +
-                           8.0 * (double)N * (nv + nop) + (mixed ? 4.0 * 64 * (nv + nop) : 0.0);
+    // Mixed form: the couplings go to the tensor cores once there are enough
+    // of them (candidates x primaries); smaller problems are latency-bound and
+    // use the FP64 GEMMs, which give the FP64 selection directly.
+    const bool tc_pt = mixed && ((c.opts.flags & STD2G_FLAG_TENSOR_ALWAYS) ||
+                                 (double)nexpt * (double)nex >= 2.5e8);
+    const double per_occ = (tc_pt ? 4.0 : 8.0) * ((double)nex * nv + (double)ldj * nop) +
+                           8.0 * (double)N * (nv + nop) + (tc_pt ? 4.0 * 64 * (nv + nop) : 0.0);
     int occ_chunk = std::max(1, (int)std::min<double>(no, budget / per_occ));
     std::vector<int> first_of_occ(no + 1, nexpt);
     {
@@ -786,7 +791,7 @@ static void solve(Ctx &c, const std2g_params &p_in, std2g_result *res, const Res
       double *W = c.w_W.ensure((size_t)N * ni * nop);
       S2G_LAUNCH(k_gather_occ_pairs, grid_for((int64_t)N * ni * nop), 256, 0, s, W, Poo, N, no,
                  i0, ni, d_OP, nop);
-      if (!mixed) {
+      if (!tc_pt) {
         double *Kb = c.w_Kbuf.ensure((size_t)nex * nr);
         double *Jb = c.w_Jbuf.ensure((size_t)ldj * ni * nop);
         gemm(c, CUBLAS_OP_T, CUBLAS_OP_N, nex, nr, N, 1.0, Qp, N, Pc, N, 0.0, Kb, nex);
@@ -884,6 +889,12 @@ static void solve(Ctx &c, const std2g_params &p_in, std2g_result *res, const Res
   // Large TDA problems with a root count use the matrix-free operators and the
   // blocked Davidson solver; everything else builds the matrices explicitly.
   const bool use_mf = !p.rpa && p.nroots > 0 && (p.solver == 2 || (p.solver == 0 && nci > 1024));
+  // Mixed form: the tensor-core first Davidson stage pays off once the
+  // products dominate; below kTcDavidsonMin CSFs (solver auto) the solve is
+  // latency-bound and runs the single FP64 stage.
+  constexpr int kTcDavidsonMin = 16384;
+  const bool tc_dav = mixed && (p.solver == 2 || (c.opts.flags & STD2G_FLAG_TENSOR_ALWAYS) ||
+                                nci >= kTcDavidsonMin);
   // alpha(w) for CSF spaces whose dense A+B, A-B and their work copies would
   // exceed ~24 GB: matrix-free operators and the refined iterative solve
   // (or when the iterative solver is requested, solver == 2)
@@ -914,7 +925,7 @@ static void solve(Ctx &c, const std2g_params &p_in, std2g_result *res, const Res
     if (resp_mf) {
       mf_setup_ops<double>(mf, mf.d, s, Clow, c.d_slot_ao.get(), Poo, Pia, Qs, Ps, true);
       if (mixed) mf_setup_ops<float>(mf, mf.f, s, Clow, c.d_slot_ao.get(), Poo, Pia, Qs, Ps, true);
-    } else if (mixed) {
+    } else if (tc_dav) {
       // tensor-core products for the first Davidson stage
       MatFreeTc &w = c.mftc;
       w.N = N;
@@ -941,13 +952,16 @@ static void solve(Ctx &c, const std2g_params &p_in, std2g_result *res, const Res
   if (!p.rpa && use_mf) {
     record(c, PH_EIGEN);
     om = c.w_eval.ensure(std::max(nci, nao));
+    // residual norm tolerance of the final (FP64) stage; the tensor-core stage
+    // stops at 1e-6 at the least, about as far as its FP32-accurate products reach
     const double tol = p.conv_tol > 0 ? p.conv_tol : 1e-6;
+    const double tol1 = std::max(tol, 1e-6);
     double *Xd = c.w_X.ensure((size_t)nci * p.nroots);
     MatVec mv = [&](const double *V, int nb, double *W) {
       mf_apply(c.mf, c.blas, s, V, nb, W, ak, -1.0, 0.0, c.mf.dA.get());
     };
     int conv = 0;
-    if (mixed) {
+    if (tc_dav) {
       // stage 1: tensor-core (split-BF16 FP32) products; stage 2: FP64 products
       // from those Ritz vectors until the FP64 residuals meet tol
       MatVec mv_tc = [&](const double *V, int nb, double *W) {
@@ -955,7 +969,7 @@ static void solve(Ctx &c, const std2g_params &p_in, std2g_result *res, const Res
       };
       c.dav.profile = c.opts.verbose >= 2;
       for (double &v : c.dav.sec_ms) v = 0;
-      davidson(c.dav, c.blas, c.solver, s, mv_tc, d_edall, nci, p.nroots, tol, 300, om, Xd);
+      davidson(c.dav, c.blas, c.solver, s, mv_tc, d_edall, nci, p.nroots, tol1, 300, om, Xd);
       c.dav_iters = c.dav.iters;
       c.dav_matvecs = c.dav.matvecs;
       if (c.dav.profile)

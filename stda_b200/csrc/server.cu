@@ -13,7 +13,7 @@
 //     order, so requests that arrive while others run start as soon as slots
 //     and memory free up and their kernels overlap on the device;
 //   * inputs are copied at submit, results are kept until std2g_server_wait;
-//   * a slot that ran a large request (estimate above budget / (2 slots)) or
+//   * a slot that ran a large request (estimate above budget / slots) or
 //     ran out of memory gets a fresh context; a request that ran out of
 //     memory is retried once with the device to itself.
 #include <algorithm>
@@ -161,7 +161,7 @@ void worker(Server *s, int slot) {
     // slot starts again from a fresh context so that idle slots do not hold
     // memory the admission rule no longer counts.
     const bool out_of_memory = job->status == STD2G_ENOMEM;
-    const bool large = job->footprint > s->budget / (2 * (int64_t)s->ctxs.size());
+    const bool large = job->footprint > s->budget / (int64_t)s->ctxs.size();
     bool alive = true;
     if (out_of_memory || large) alive = renew_context(s, slot);
     bool retry = out_of_memory && !job->exclusive && alive;

@@ -44,7 +44,10 @@ class Std2gError(RuntimeError):
 
 class Opts(C.Structure):
     _fields_ = [("device", C.c_int), ("precision", C.c_int), ("verbose", C.c_int),
-                ("reserved", C.c_int), ("max_device_bytes", C.c_int64)]
+                ("flags", C.c_int), ("max_device_bytes", C.c_int64)]
+
+
+FLAG_TENSOR_ALWAYS = 1
 
 
 class Params(C.Structure):
@@ -224,10 +227,10 @@ def boundary_inputs(mol, ints=None) -> BoundaryInputs:
 class Engine:
     """One std2g context on one device (``precision`` 0: FP64, 1: mixed)."""
 
-    def __init__(self, device: int = 0, precision: int = 0, verbose: int = 0):
+    def __init__(self, device: int = 0, precision: int = 0, verbose: int = 0, flags: int = 0):
         self.lib = library()
         self.ctx = C.c_void_p()
-        opts = Opts(device, precision, verbose, 0, 0)
+        opts = Opts(device, precision, verbose, flags, 0)
         _check(self.lib.std2g_create(C.byref(self.ctx), C.byref(opts)))
         self.precision = precision
         self.inputs = None

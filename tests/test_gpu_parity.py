@@ -20,8 +20,10 @@ EXPECTED = json.load(open(os.path.join(GOLDEN, "reference_expected.json")))
 
 
 def _engine(precision=0):
-    from stda_b200.engine import Engine
-    return Engine(0, precision)
+    """Mixed-form engines use the tensor-core paths at every size here, so that
+    the small test molecules exercise them."""
+    from stda_b200.engine import Engine, FLAG_TENSOR_ALWAYS
+    return Engine(0, precision, flags=FLAG_TENSOR_ALWAYS if precision == 1 else 0)
 
 
 def _oracle(mol, ints, **kw):
