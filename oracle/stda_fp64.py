@@ -184,6 +184,19 @@ def charges(Clow, iaoat, ncent, p_idx, q_idx):
     return out
 
 
+def charges_block(Clow, iaoat, ncent, P, Q):
+    """lo12pop (stda.f:1727-1744) for every pair of the MO blocks P x Q, pair
+    index k = p*len(Q) + q -> (ncent, len(P)*len(Q)); per atom the AO sum is one
+    small product C_A[:, P]^T C_A[:, Q] (same sums as ``charges``)."""
+    P, Q = np.asarray(P), np.asarray(Q)
+    out = np.zeros((ncent, len(P) * len(Q)))
+    for A in range(ncent):
+        rows = np.nonzero(iaoat == A)[0]
+        if len(rows):
+            out[A] = (Clow[np.ix_(rows, P)].T @ Clow[np.ix_(rows, Q)]).ravel()
+    return out
+
+
 def mo_ov(mat_ao, C_occ, C_virt):
     """ONETRI (onetri.f:20-55) restricted to the occ-virt block: C_i^T B C_a."""
     return C_occ.T @ mat_ao @ C_virt
@@ -235,7 +248,7 @@ def stda(xyz4, C, eps, occ, iaoat, S, Lao, Vao, Mao, p: Params, want_A=True):
     qii = charges(Clow, iaoat, ncent, np.arange(no), np.arange(no))
     qaa = charges(Clow, iaoat, ncent, no + np.arange(nv), no + np.arange(nv))
     uci = qaa.T @ (gj @ qii)                                  # (nv, no): (ii|aa)
-    qia = charges(Clow, iaoat, ncent, io_all, no + ia_all)    # (N, no*nv)
+    qia = charges_block(Clow, iaoat, ncent, np.arange(no), no + np.arange(nv))    # (N, no*nv)
     pia = gk @ qia
     ek_all = np.einsum("Ak,Ak->k", pia, qia)                  # (ia|ia)
     de_all = (epsi[no + ia_all] - epsi[io_all]) - uci[ia_all, io_all] + ak * ek_all
@@ -256,10 +269,10 @@ def stda(xyz4, C, eps, occ, iaoat, S, Lao, Vao, Mao, p: Params, want_A=True):
 
     # J-type charges for all occ pairs and virt pairs (stda.f:728-763)
     ii, jj = np.meshgrid(np.arange(no), np.arange(no), indexing="ij")
-    qoo = charges(Clow, iaoat, ncent, ii.ravel(), jj.ravel()).reshape(ncent, no, no)
+    qoo = charges_block(Clow, iaoat, ncent, np.arange(no), np.arange(no)).reshape(ncent, no, no)
     aa, bb = np.meshgrid(np.arange(nv), np.arange(nv), indexing="ij")
-    qvv = charges(Clow, iaoat, ncent, no + aa.ravel(), no + bb.ravel()).reshape(ncent, nv, nv)
-    poo = np.einsum("AB,Bij->Aij", gj, qoo)
+    qvv = charges_block(Clow, iaoat, ncent, no + np.arange(nv), no + np.arange(nv)).reshape(ncent, nv, nv)
+    poo = (gj @ qoo.reshape(ncent, -1)).reshape(qoo.shape)
 
     def coupling(krow, kcol):
         """ak*(ia|jb) - (ij|ab) for CSF index arrays (ravelled i*nv+a)."""
@@ -455,8 +468,9 @@ def stda_timed(xyz4, C, eps, occ, iaoat, S, Lao, Vao, Mao, p: Params, budget_s=1
     """Wall-clock estimate of one full FP64 CPU solve from a bounded sample.
 
     Phases that are cheap run in full (window, MO integrals, S^1/2, charges,
-    gamma, screen).  The PT selection runs on leading candidate blocks until
-    about half the budget is used and is scaled linearly to all candidates;
+    gamma, screen).  The PT selection runs on candidate blocks spread evenly
+    over the candidate list until about half the budget is used and is scaled
+    linearly to all candidates (also the estimate of the selected count);
     the A build is timed on a row block of the primary space and scaled to
     nci^2; the dense diagonalisation (ssyevr in the reference) is timed on a
     min(nci, 1500)-sized matrix and scaled as n^3.  Used only as the reported
@@ -484,7 +498,7 @@ def stda_timed(xyz4, C, eps, occ, iaoat, S, Lao, Vao, Mao, p: Params, budget_s=1
     qii = charges(Clow, iaoat, ncent, np.arange(no), np.arange(no))
     qaa = charges(Clow, iaoat, ncent, no + np.arange(nv), no + np.arange(nv))
     uci = qaa.T @ (gj @ qii)
-    qia = charges(Clow, iaoat, ncent, io_all, no + ia_all)
+    qia = charges_block(Clow, iaoat, ncent, np.arange(no), no + np.arange(nv))
     pia = gk @ qia
     ek_all = np.einsum("Ak,Ak->k", pia, qia)
     de_all = (epsi[no + ia_all] - epsi[io_all]) - uci[ia_all, io_all] + ak * ek_all
@@ -493,10 +507,10 @@ def stda_timed(xyz4, C, eps, occ, iaoat, S, Lao, Vao, Mao, p: Params, budget_s=1
     pk = pk[np.argsort(de_all[pk], kind="stable")]
     ed = de_all[pk]
     ii, jj = np.meshgrid(np.arange(no), np.arange(no), indexing="ij")
-    qoo = charges(Clow, iaoat, ncent, ii.ravel(), jj.ravel()).reshape(ncent, no, no)
+    qoo = charges_block(Clow, iaoat, ncent, np.arange(no), np.arange(no)).reshape(ncent, no, no)
     aa, bb = np.meshgrid(np.arange(nv), np.arange(nv), indexing="ij")
-    qvv = charges(Clow, iaoat, ncent, no + aa.ravel(), no + bb.ravel()).reshape(ncent, nv, nv)
-    poo = np.einsum("AB,Bij->Aij", gj, qoo)
+    qvv = charges_block(Clow, iaoat, ncent, no + np.arange(nv), no + np.arange(nv)).reshape(ncent, nv, nv)
+    poo = (gj @ qoo.reshape(ncent, -1)).reshape(qoo.shape)
     t_setup = time.perf_counter() - t_all
 
     def coupling(krow, kcol):
@@ -512,12 +526,17 @@ def stda_timed(xyz4, C, eps, occ, iaoat, S, Lao, Vao, Mao, p: Params, budget_s=1
         J4 = (P.T @ Q).reshape(len(ou1), len(ou2), len(vu1), len(vu2))
         return ak * K - J4[oinv1[:, None], oinv2[None, :], vinv1[:, None], vinv2[None, :]]
 
-    # PT selection on a leading sample of candidates
+    # PT selection on a sample of candidate blocks spread evenly over the
+    # candidate list (the selection rate varies along it), scaled linearly
     t0 = time.perf_counter()
     done, nsel = 0, 0
     blk = max(1, int(2e6 // max(1, len(pk))))
-    while done < len(ck) and time.perf_counter() - t0 < 0.5 * budget_s:
-        kk = ck[done:done + blk]
+    nblk_all = max(1, -(-len(ck) // blk))
+    order = np.argsort((np.arange(nblk_all) * 0.6180339887) % 1.0, kind="stable")
+    for b in order:
+        if time.perf_counter() - t0 >= 0.5 * budget_s:
+            break
+        kk = ck[b * blk:(b + 1) * blk]
         amat = coupling(kk, pk)
         pert = (amat ** 2 / (de_all[kk][:, None] - ed[None, :] + 1e-10)).sum(axis=1)
         nsel += int((pert > p.thrp).sum())
@@ -540,7 +559,8 @@ def stda_timed(xyz4, C, eps, occ, iaoat, S, Lao, Vao, Mao, p: Params, budget_s=1
     est = t_setup + t_pt + t_a + t_eig
     threads = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
     sample = (f"full window/S^1/2/charges/screen ({t_setup:.1f}s); PT on {done} of {len(ck)} "
-              f"candidates x {len(pk)} primaries scaled linearly ({t_pt:.1f}s est.); A build "
+              f"candidates (evenly spread blocks) x {len(pk)} primaries scaled linearly "
+              f"({t_pt:.1f}s est.); A build "
               f"{len(rows)} rows scaled to nci={nci} ({t_a:.1f}s est.); dense eigh {n_s}^3 "
               f"scaled to nci^3 ({t_eig:.1f}s est.)")
     return dict(est_total_s=est, setup_s=t_setup, pt_s=t_pt, a_s=t_a, eig_s=t_eig, nci=nci,
