@@ -891,10 +891,14 @@ static void solve(Ctx &c, const std2g_params &p_in, std2g_result *res, const Res
   const bool use_mf = !p.rpa && p.nroots > 0 && (p.solver == 2 || (p.solver == 0 && nci > 1024));
   // Mixed form: the tensor-core first Davidson stage pays off once the
   // products dominate; below kTcDavidsonMin CSFs (solver auto) the solve is
-  // latency-bound and runs the single FP64 stage.
+  // latency-bound and runs the single FP64 stage.  The tensor-core stage
+  // reaches residuals of ~1e-6; for tighter tolerances the FP64 second stage,
+  // restarted from the Ritz vectors alone, would do most of the work, so those
+  // also run the single FP64 stage.
   constexpr int kTcDavidsonMin = 16384;
-  const bool tc_dav = mixed && (p.solver == 2 || (c.opts.flags & STD2G_FLAG_TENSOR_ALWAYS) ||
-                                nci >= kTcDavidsonMin);
+  const bool tc_dav =
+      mixed && ((c.opts.flags & STD2G_FLAG_TENSOR_ALWAYS) ||
+                ((p.solver == 2 || nci >= kTcDavidsonMin) && !(p.conv_tol > 0 && p.conv_tol < 1e-6)));
   // alpha(w) for CSF spaces whose dense A+B, A-B and their work copies would
   // exceed ~24 GB: matrix-free operators and the refined iterative solve
   // (or when the iterative solver is requested, solver == 2)
