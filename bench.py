@@ -405,8 +405,16 @@ def main():
     if tc_launch > 0:
         pk, src = peaks()
         ach = tc_flop / (tc_ms / 1e3) / 1e12
+        # DRAM traffic per launch from the ncu capture of the same kernel on the
+        # flake-6 case (profiles/tc_gemm_bf16x3_pt_flake6.md): 4.27 B per FP32
+        # output element (output written once + operands read once), scaled by
+        # the output elements of an average launch here (FLOP / (2 N_atoms))
+        traffic = 4.27 * (tc_flop / tc_launch) / (2.0 * b.ncent)
         out["roofline"] = {"bound": "tensor", "achieved": ach, "peak": pk["bf16_tflops"],
-                           "unit": "TFLOP/s", "frac": ach / pk["bf16_tflops"], "traffic": None,
+                           "unit": "TFLOP/s", "frac": ach / pk["bf16_tflops"],
+                           "traffic": traffic,
+                           "traffic_source": "ncu dram bytes per output element (flake-6 "
+                                             "capture) x output elements per launch",
                            "kernel": "k_tc_gemm_bf16x3 (PT-selection contractions)",
                            "flop_count": "algorithmic 2*M*N*N_atoms; the bf16 hi/lo split "
                                          "executes 3x as many tensor-core FLOPs",
