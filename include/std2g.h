@@ -247,6 +247,14 @@ int std2g_server_stats(void *srv, int64_t *stats);
    free the contexts; call after the last wait. */
 void std2g_server_destroy(void *srv);
 
+/* Diagnostic: lowest k eigenpairs of the symmetric n x n matrix A (host,
+   column-major, lower triangle used) by the engine's single-block eigensolver
+   of the Davidson Rayleigh-Ritz step (n <= 224), and all eigenvalues by
+   cuSOLVER syevd for comparison.  w [k], Z [n*k], w_ref [n] (host).  No
+   reference counterpart (the reference diagonalises with LAPACK ssyevr). */
+int std2g_symeig_check(int device, int n, int k, const double *A, double *w, double *Z,
+                       double *w_ref);
+
 const char *std2g_error_string(int status);
 void std2g_destroy(void *ctx);
 

@@ -23,6 +23,7 @@
 #include "matfree_tc.cuh"
 #include "mixed.cuh"
 #include "response_mixed.cuh"
+#include "symeig_small.cuh"
 
 namespace std2g {
 
@@ -1363,6 +1364,45 @@ int std2g_solver_stats(void *ctx, int *iters, int64_t *matvecs, int64_t *matvecs
   if (matvecs_fp64) *matvecs_fp64 = c->dav_fp64_matvecs;
   if (pt_rechecked) *pt_rechecked = c->opts.precision == 1 ? c->mixed.rechecked : 0;
   return STD2G_OK;
+}
+
+int std2g_symeig_check(int device, int n, int k, const double *A, double *w, double *Z,
+                       double *w_ref) {
+  if (n < 1 || k < 1 || k > n || !A || !w || !Z || !w_ref) return STD2G_EINVAL;
+  return guard([&] {
+    using namespace std2g;
+    S2G_CUDA(cudaSetDevice(device));
+    cudaStream_t s;
+    S2G_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    DBuf<double> dA, dw, dZ, dwork, dref, dA2, dlw;
+    DBuf<int> dinfo;
+    const size_t n2 = (size_t)n * n;
+    S2G_CUDA(cudaMemcpyAsync(dA.ensure(n2), A, sizeof(double) * n2, cudaMemcpyHostToDevice, s));
+    S2G_CUDA(cudaMemsetAsync(dinfo.ensure(2), 0, 2 * sizeof(int), s));
+    symeig_small(s, dA.get(), n, n, k, dw.ensure(k), dZ.ensure((size_t)n * k), n,
+                 dwork.ensure((size_t)k * 6 * n), dinfo.get());
+    // cuSOLVER on a copy
+    cusolverDnHandle_t h;
+    S2G_CUSOLVER(cusolverDnCreate(&h));
+    S2G_CUSOLVER(cusolverDnSetStream(h, s));
+    S2G_CUDA(cudaMemcpyAsync(dA2.ensure(n2), A, sizeof(double) * n2, cudaMemcpyHostToDevice, s));
+    int lw = 0;
+    S2G_CUSOLVER(cusolverDnDsyevd_bufferSize(h, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER,
+                                             n, dA2.get(), n, dref.ensure(n), &lw));
+    S2G_CUSOLVER(cusolverDnDsyevd(h, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, n,
+                                  dA2.get(), n, dref.get(), dlw.ensure((size_t)lw + 1), lw,
+                                  dinfo.get() + 1));
+    int hinfo[2] = {0, 0};
+    S2G_CUDA(cudaMemcpyAsync(w, dw.get(), sizeof(double) * k, cudaMemcpyDeviceToHost, s));
+    S2G_CUDA(cudaMemcpyAsync(Z, dZ.get(), sizeof(double) * n * k, cudaMemcpyDeviceToHost, s));
+    S2G_CUDA(cudaMemcpyAsync(w_ref, dref.get(), sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+    S2G_CUDA(cudaMemcpyAsync(hinfo, dinfo.get(), 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
+    S2G_CUDA(cudaStreamSynchronize(s));
+    cusolverDnDestroy(h);
+    cudaStreamDestroy(s);
+    if (hinfo[0] != 0) throw Error{STD2G_ECUDA, "symeig_small: non-finite result"};
+    if (hinfo[1] != 0) throw Error{STD2G_ECUDA, "syevd info " + std::to_string(hinfo[1])};
+  });
 }
 
 const char *std2g_error_string(int status) {

@@ -32,6 +32,7 @@ EXPORTS = [
     "std2g_kernel_launches", "std2g_kernel_stats", "std2g_solver_stats", "std2g_error_string",
     "std2g_destroy", "std2g_screen_noalloc", "std2g_server_create", "std2g_server_submit",
     "std2g_server_poll", "std2g_server_wait", "std2g_server_stats", "std2g_server_destroy",
+    "std2g_symeig_check",
 ]
 
 
@@ -115,6 +116,7 @@ def library():
         lib.std2g_server_poll.argtypes = [C.c_void_p, C.c_int64, ip]
         lib.std2g_server_wait.argtypes = [C.c_void_p, C.c_int64, C.POINTER(Result), dp, dp, dp]
         lib.std2g_server_stats.argtypes = [C.c_void_p, C.POINTER(C.c_int64)]
+        lib.std2g_symeig_check.argtypes = [C.c_int, C.c_int, C.c_int, dp, dp, dp, dp]
         lib.std2g_server_destroy.argtypes = [C.c_void_p]
         lib.std2g_server_destroy.restype = None
         lib.std2g_screen_noalloc.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
@@ -409,3 +411,13 @@ class Server:
             self.close()
         except Exception:
             pass
+
+
+def symeig_check(A, k, device: int = 0):
+    """The engine's small symmetric eigensolver (lowest k pairs) and cuSOLVER's
+    eigenvalues for the same matrix: (w, Z, w_ref)."""
+    A = np.asfortranarray(A, dtype=np.float64)
+    n = A.shape[0]
+    w, Z, wr = np.zeros(k), np.zeros((n, k), order="F"), np.zeros(n)
+    _check(library().std2g_symeig_check(device, n, k, _dp(A), _dp(w), _dp(Z), _dp(wr)))
+    return w, Z, wr
