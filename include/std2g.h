@@ -247,6 +247,12 @@ int std2g_server_stats(void *srv, int64_t *stats);
    free the contexts; call after the last wait. */
 void std2g_server_destroy(void *srv);
 
+/* Cap the persistent tensor-core kernels of this context at max_sms CTAs (one
+   per SM; 0 = all SMs), so that several contexts sharing a device (the
+   request server's slots) leave SMs to each other's kernels.  No reference
+   counterpart. */
+int std2g_set_sm_limit(void *ctx, int max_sms);
+
 /* Diagnostic: lowest k eigenpairs of the symmetric n x n matrix A (host,
    column-major, lower triangle used) by the engine's single-block eigensolver
    of the Davidson Rayleigh-Ritz step (n <= 224), and all eigenvalues by

@@ -1346,6 +1346,14 @@ const char *std2g_phase_name(int q) {
 
 int64_t std2g_kernel_launches(void *) { return std2g::g_launches.load(); }
 
+int std2g_set_sm_limit(void *ctx, int max_sms) {
+  if (!ctx || max_sms < 0) return STD2G_EINVAL;
+  auto *c = (std2g::Ctx *)ctx;
+  c->mixed.tc.max_ctas = max_sms;
+  c->mftc.tc.max_ctas = max_sms;
+  return STD2G_OK;
+}
+
 int std2g_kernel_stats(void *ctx, double *ms, int64_t *launches, double *flop) {
   if (!ctx) return STD2G_EINVAL;
   auto *c = (Ctx *)ctx;

@@ -12,6 +12,9 @@
 //     requests already in flight (or nothing else is in flight), in FIFO
 //     order, so requests that arrive while others run start as soon as slots
 //     and memory free up and their kernels overlap on the device;
+//   * each slot's persistent tensor-core kernels use an equal share of the SMs
+//     (std2g_set_sm_limit), so a large request does not hold every SM while
+//     small ones wait;
 //   * inputs are copied at submit, results are kept until std2g_server_wait;
 //   * a slot that ran a large request (estimate above budget / slots) or
 //     ran out of memory gets a fresh context; a request that ran out of
@@ -130,6 +133,13 @@ bool can_admit(const Server &s) {
 }
 
 // Fresh context for a slot: releases every device buffer the old one held.
+// SMs for one slot's persistent tensor-core kernels: an equal share of the device
+int sm_share(const Server &s) {
+  int dev_sms = 148;
+  cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, s.opts.device);
+  return std::max(1, dev_sms / (int)s.ctxs.size());
+}
+
 bool renew_context(Server *s, int slot) {
   std2g_destroy(s->ctxs[slot]);
   s->ctxs[slot] = nullptr;
@@ -138,6 +148,7 @@ bool renew_context(Server *s, int slot) {
   eo.precision = s->opts.precision;
   void *ctx = nullptr;
   if (std2g_create(&ctx, &eo) != STD2G_OK) return false;
+  std2g_set_sm_limit(ctx, sm_share(*s));
   s->ctxs[slot] = ctx;
   return true;
 }
@@ -214,6 +225,8 @@ int std2g_server_create(void **srv, const std2g_server_opts *o) {
     }
     s->ctxs.push_back(ctx);
   }
+  const int share = sm_share(*s);
+  for (void *c : s->ctxs) std2g_set_sm_limit(c, share);
   for (int k = 0; k < o->slots; ++k) s->workers.emplace_back(worker, s.get(), k);
   *srv = s.release();
   return STD2G_OK;

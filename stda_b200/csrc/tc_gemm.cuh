@@ -377,6 +377,7 @@ struct TcGemm {
   int64_t launches = 0;
   bool armed = false;
   int nsm = 148;
+  int max_ctas = 0;   // > 0: at most this many persistent CTAs (SMs shared with other work)
   cudaEvent_t e0 = nullptr, e1 = nullptr;
 
   void init() {
@@ -455,7 +456,8 @@ struct TcGemm {
       armed = true;
     }
     const int64_t ntiles = div_up(N, tc::BN) * div_up(M, tc::BM) * (int64_t)batch;
-    const int grid = (int)std::min<int64_t>(ntiles, nsm);
+    const int cap = max_ctas > 0 ? std::min(max_ctas, nsm) : nsm;
+    const int grid = (int)std::min<int64_t>(ntiles, cap);
     if (sync) S2G_CUDA(cudaEventRecord(e0, s));
     S2G_LAUNCH(k_tc_gemm_bf16x3, grid, 256, tc::SMEM_BYTES, s, ah, al, bh, bl, dm, M, N, Kpad,
                b_batched ? 1 : 0, batch, e);

@@ -32,7 +32,7 @@ EXPORTS = [
     "std2g_kernel_launches", "std2g_kernel_stats", "std2g_solver_stats", "std2g_error_string",
     "std2g_destroy", "std2g_screen_noalloc", "std2g_server_create", "std2g_server_submit",
     "std2g_server_poll", "std2g_server_wait", "std2g_server_stats", "std2g_server_destroy",
-    "std2g_symeig_check",
+    "std2g_symeig_check", "std2g_set_sm_limit",
 ]
 
 
@@ -116,6 +116,7 @@ def library():
         lib.std2g_server_poll.argtypes = [C.c_void_p, C.c_int64, ip]
         lib.std2g_server_wait.argtypes = [C.c_void_p, C.c_int64, C.POINTER(Result), dp, dp, dp]
         lib.std2g_server_stats.argtypes = [C.c_void_p, C.POINTER(C.c_int64)]
+        lib.std2g_set_sm_limit.argtypes = [C.c_void_p, C.c_int]
         lib.std2g_symeig_check.argtypes = [C.c_int, C.c_int, C.c_int, dp, dp, dp, dp]
         lib.std2g_server_destroy.argtypes = [C.c_void_p]
         lib.std2g_server_destroy.restype = None
