@@ -67,6 +67,7 @@ struct Ctx {
   DBuf<double> d_xyz, d_C, d_eps_act, d_eta, d_Sfull, d_sqrtS, d_ao9;
   DBuf<int> d_ao_ptr, d_ao_list, d_iaoat, d_slot_ao;
   int maxa = 1;
+  int chunk_rows = 1;   // largest AO count of kChAtoms consecutive atoms
   bool sqrtS_ready = false;
   // work buffers
   DBuf<double> w_Cact, w_Clow, w_T, w_mu_ov, w_gj, w_gk, w_Qii, w_Qaa, w_Pii, w_uci;
@@ -222,6 +223,9 @@ static void load(Ctx &c, int ncent, int nmo, int nao, const double *xyz, const d
   for (int a = 0; a < ncent; ++a)
     for (int q = 0; q < cnt[a]; ++q) slot[(size_t)a * maxa + q] = list[ptr[a] + q];
   c.maxa = maxa;
+  c.chunk_rows = 1;
+  for (int a0 = 0; a0 < ncent; a0 += kChAtoms)
+    c.chunk_rows = std::max(c.chunk_rows, ptr[std::min(ncent, a0 + kChAtoms)] - ptr[a0]);
   size_t npk = (size_t)nao * (nao + 1) / 2;
   cudaStream_t s = c.stream;
   S2G_CUDA(cudaMemcpyAsync(c.d_slot_ao.ensure(slot.size()), slot.data(), sizeof(int) * slot.size(),
@@ -643,12 +647,23 @@ static void solve(Ctx &c, const std2g_params &p_in, std2g_result *res, const Res
              0, no, 0, no, 1);
   S2G_LAUNCH(k_charges_block, grid_for((int64_t)N * nv), 256, 0, s, Qaa, Clow, nao, N, aop, aol,
              no, nv, no, nv, 1);
-  S2G_LAUNCH(k_charges_block, grid_for((int64_t)N * nov), 256, 0, s, Qia, Clow, nao, N, aop, aol,
-             0, no, no, nv, 0);
-  S2G_LAUNCH(k_charges_block, grid_for((int64_t)N * no * no), 256, 0, s, Qoo, Clow, nao, N, aop,
-             aol, 0, no, 0, no, 0);
-  S2G_LAUNCH(k_charges_block, grid_for((int64_t)N * nv * nv), 256, 0, s, Qvv, Clow, nao, N, aop,
-             aol, no, nv, no, nv, 0);
+  {
+    // full MO blocks: ia, ij, ab pairs
+    const size_t shb = charges_tiled_smem(c.chunk_rows);
+    if (shb > 227 * 1024) throw Error{STD2G_EINVAL, "charges: too many AOs per atom"};
+    // the limit is a per-function setting shared by every context and thread:
+    // always the same (maximum) value, never a size of this molecule
+    S2G_CUDA(cudaFuncSetAttribute(k_charges_tiled, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  227 * 1024));
+    auto tiled = [&](double *out, int p0, int np, int q0, int nq) {
+      const dim3 g((unsigned)div_up(nq, kChTQ), (unsigned)div_up(np, kChTP));
+      S2G_LAUNCH(k_charges_tiled, g, 256, shb, s, out, Clow, nao, N, aop, aol, p0, np, q0, nq,
+                 c.chunk_rows);
+    };
+    tiled(Qia, 0, no, no, nv);
+    tiled(Qoo, 0, no, 0, no);
+    tiled(Qvv, no, nv, no, nv);
+  }
   // p = gamma q (ssymm, stda.f:558-590, 742-743)
   double *Pii = c.w_Pii.ensure((size_t)N * no), *uci = c.w_uci.ensure((size_t)nv * no);
   gemm(c, CUBLAS_OP_N, CUBLAS_OP_N, N, no, N, 1.0, gj, N, Qii, N, 0.0, Pii, N);

@@ -128,6 +128,63 @@ __global__ void k_charges_block(double *__restrict__ out, const double *__restri
   }
 }
 
+// Charges of a full MO block, q^A_(p,q) for p < np, q < nq (lo12pop
+// stda.f:1727-1744), out[(p*nq + q)*N + A].  One CTA per 8 x 32 tile of MO
+// pairs walks the atoms in chunks of kChAtoms: the chunk's AO rows of the
+// tile's 40 MO columns are staged in shared memory (so every C element is read
+// once per tile, not once per pair), each thread forms its pair's sums for the
+// chunk's atoms, and the results leave as contiguous 128-byte segments of the
+// [pair][atom] layout.  Write-bound.  Shared memory: 40*max_rows + 256*17 doubles.
+constexpr int kChTP = 8, kChTQ = 32, kChAtoms = 16;
+__global__ void __launch_bounds__(256)
+k_charges_tiled(double *__restrict__ out, const double *__restrict__ C, int nao, int N,
+                const int *__restrict__ ao_ptr, const int *__restrict__ ao_list, int p0, int np,
+                int q0, int nq, int max_rows) {
+  extern __shared__ double sh[];
+  double *cp = sh;                                 // [max_rows][kChTP]
+  double *cq = cp + (size_t)max_rows * kChTP;      // [max_rows][kChTQ]
+  double *st = cq + (size_t)max_rows * kChTQ;      // [256][kChAtoms + 1]
+  const int pt = blockIdx.y * kChTP, qt = blockIdx.x * kChTQ;
+  const int pi = threadIdx.x / kChTQ, qi = threadIdx.x % kChTQ;
+  constexpr int kCols = kChTP + kChTQ, kSt = kChAtoms + 1;
+  for (int A0 = 0; A0 < N; A0 += kChAtoms) {
+    const int A1 = min(N, A0 + kChAtoms);
+    const int r0 = ao_ptr[A0], nr = ao_ptr[A1] - r0;
+    __syncthreads();   // the previous chunk's staged results have been written
+    // stage C[rows of the chunk, tile columns]; consecutive threads take
+    // consecutive rows of one column
+    for (int t = threadIdx.x; t < nr * kCols; t += blockDim.x) {
+      const int c = t / nr, r = t - c * nr;
+      const int k = ao_list[r0 + r];
+      if (c < kChTP) {
+        const int p = pt + c;
+        cp[r * kChTP + c] = p < np ? C[k + (int64_t)nao * (p0 + p)] : 0.0;
+      } else {
+        const int q = qt + (c - kChTP);
+        cq[r * kChTQ + (c - kChTP)] = q < nq ? C[k + (int64_t)nao * (q0 + q)] : 0.0;
+      }
+    }
+    __syncthreads();
+    for (int a = A0; a < A1; ++a) {
+      double sum = 0.0;
+      const int ra = ao_ptr[a] - r0, rb = ao_ptr[a + 1] - r0;
+      for (int r = ra; r < rb; ++r) sum += cp[r * kChTP + pi] * cq[r * kChTQ + qi];
+      st[threadIdx.x * kSt + (a - A0)] = sum;
+    }
+    __syncthreads();
+    const int na = A1 - A0;
+    for (int t = threadIdx.x; t < kChTP * kChTQ * na; t += blockDim.x) {
+      const int pl = t / na, a = t - pl * na;
+      const int p = pt + pl / kChTQ, q = qt + pl % kChTQ;
+      if (p < np && q < nq) out[((int64_t)p * nq + q) * N + A0 + a] = st[pl * kSt + a];
+    }
+  }
+}
+
+inline size_t charges_tiled_smem(int max_rows) {
+  return sizeof(double) * ((size_t)max_rows * (kChTP + kChTQ) + 256 * (kChAtoms + 1));
+}
+
 // Diagonal of A and the energy screen (stda.f:593-668, kshift stda.f:1750-1768):
 //   ek = p_ia . q_ia,  de = (e_a - e_i) - (ii|aa) + ak*ek [+ kshift]
 //   flag = 1 primary (de <= thr), 2 PT candidate (thr < de < fthr), 0 neither
