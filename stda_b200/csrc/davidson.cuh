@@ -95,25 +95,6 @@ __global__ void k_colnorm_finish(const double *__restrict__ part, int nsplit, in
   out[j] = sqrt(s);
 }
 
-// column norm of v (one block), result to out[0]
-__global__ void k_norm(const double *__restrict__ v, int n, double *__restrict__ out) {
-  double s = 0.0;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) s += v[i] * v[i];
-  __shared__ double red[256];
-  red[threadIdx.x] = s;
-  __syncthreads();
-  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
-    if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) out[0] = sqrt(red[0]);
-}
-
-__global__ void k_scale_vec(double *__restrict__ v, int n, const double *__restrict__ nrm) {
-  double f = 1.0 / nrm[0];
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) v[i] *= f;
-}
-
 __global__ void k_unit_vectors(double *__restrict__ V, int n, const int *__restrict__ idx, int k) {
   int64_t total = (int64_t)n * k;
   for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;

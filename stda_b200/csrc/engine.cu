@@ -79,7 +79,6 @@ struct Ctx {
   DBuf<unsigned char> w_sel;
   DBuf<double> w_Qs, w_Ps, w_K, w_J, w_Kx, w_A, w_Apb, w_Amb, w_Bh, w_Ambh, w_M, w_eval, w_X,
       w_Y, w_tmp, w_musel, w_TL, w_TVM, w_T2, w_props, w_work;
-  DBuf<float> m_A;   // mixed-form FP32 A storage
   DBuf<int> w_info;
   DBuf<char> w_cub;
   MixedWork mixed;
@@ -511,8 +510,9 @@ static void response_mixed(Ctx &c, const double *Apb, const double *Amb, int n,
 }
 
 // Matrix-free form (no n x n storage): products with A+B, A-B through the
-// Loewdin-MO operators of matfree.cuh (k_rpa_mf_diag), FP64 for the residuals
-// and, in the mixed form, FP32 operator products for the CG.
+// Loewdin-MO operators (k_rpa_mf_diag), FP64 (matfree.cuh) for the residuals
+// and, in the mixed form, the split-BF16 tensor-core operators
+// (matfree_tc.cuh) for the CG.
 static void response_matfree(Ctx &c, int n, const double *musel, const RespReq &rq,
                              std::vector<int> &fallback, const double *ed, const double *ekd,
                              const double *uci, double ak, double ax, bool mixed) {
@@ -523,14 +523,17 @@ static void response_matfree(Ctx &c, int n, const double *musel, const RespReq &
   S2G_LAUNCH(k_rpa_mf_diag, (int)div_up(n, 128), 128, 0, s, d, dpd, dmd, ed, ekd, uci, c.mf.ci,
              c.mf.ca, n, c.mf.nv, ak, ax);
   const bool amb_diag = std::fabs(ax) < 1e-6;
-  auto products = [&](const double *U, const double *V, double *PU, double *MV, bool f32) {
-    c.mf.f32 = f32;
-    mf_apply(c.mf, c.blas, s, U, ncol, PU, 2.0 * ak, -1.0, -ax, d);
+  auto products = [&](const double *U, const double *V, double *PU, double *MV, bool tc) {
+    if (tc)
+      mftc_apply(c.mftc, c.blas, s, U, ncol, PU, 2.0 * ak, -1.0, -ax, d);
+    else
+      mf_apply(c.mf, c.blas, s, U, ncol, PU, 2.0 * ak, -1.0, -ax, d);
     if (amb_diag)
       S2G_LAUNCH(k_diag_mul, grid_for((int64_t)n * ncol), 256, 0, s, MV, dmd, V, n, ncol);
+    else if (tc)
+      mftc_apply(c.mftc, c.blas, s, V, ncol, MV, 0.0, -1.0, ax, d);
     else
       mf_apply(c.mf, c.blas, s, V, ncol, MV, 0.0, -1.0, ax, d);
-    c.mf.f32 = false;
   };
   auto fp64 = [&](const double *U, const double *V, double *PU, double *MV) {
     products(U, V, PU, MV, false);
@@ -915,11 +918,13 @@ static void solve(Ctx &c, const std2g_params &p_in, std2g_result *res, const Res
   const bool tc_dav =
       mixed && ((c.opts.flags & STD2G_FLAG_TENSOR_ALWAYS) ||
                 ((p.solver == 2 || nci >= kTcDavidsonMin) && !(p.conv_tol > 0 && p.conv_tol < 1e-6)));
-  // alpha(w) for CSF spaces whose dense A+B, A-B and their work copies would
-  // exceed ~24 GB: matrix-free operators and the refined iterative solve
-  // (or when the iterative solver is requested, solver == 2)
+  // alpha(w) through the matrix-free operators and the refined iterative solve:
+  // when requested (solver == 2), when the dense A+B, A-B and their work copies
+  // would exceed ~24 GB, and in the mixed form from 4096 CSFs (its tensor-core
+  // operator products beat the dense build there: 38 vs 80 ms for 12457 CSFs)
   const bool resp_mf =
-      resp != nullptr && (p.solver == 2 || (double)nci * nci * 8.0 * 10.0 > 24e9);
+      resp != nullptr && (p.solver == 2 || (double)nci * nci * 8.0 * 10.0 > 24e9 ||
+                          (mixed && p.solver == 0 && nci > 4096));
   double *K = nullptr, *J = nullptr, *Kx = nullptr;
   if (!use_mf && !resp_mf) {
     K = c.w_K.ensure(n2);
@@ -942,11 +947,9 @@ static void solve(Ctx &c, const std2g_params &p_in, std2g_result *res, const Res
     mf.nci = nci;
     mf.nao = nao;
     mf.f32 = false;
-    if (resp_mf) {
-      mf_setup_ops<double>(mf, mf.d, s, Clow, c.d_slot_ao.get(), Poo, Pia, Qs, Ps, true);
-      if (mixed) mf_setup_ops<float>(mf, mf.f, s, Clow, c.d_slot_ao.get(), Poo, Pia, Qs, Ps, true);
-    } else if (tc_dav) {
-      // tensor-core products for the first Davidson stage
+    if (resp_mf || tc_dav) {
+      // tensor-core products (mixed form): the first Davidson stage, the
+      // velocity correction and the CG products of the refined alpha(w) solve
       MatFreeTc &w = c.mftc;
       w.N = N;
       w.maxa = c.maxa;
@@ -957,7 +960,14 @@ static void solve(Ctx &c, const std2g_params &p_in, std2g_result *res, const Res
       w.Ps = Ps;
       w.ci = d_ci;
       w.ca = d_ca;
-      mftc_setup(w, s, Clow, nao, c.d_slot_ao.get(), Poo);
+    }
+    if (resp_mf) {
+      mf_setup_ops<double>(mf, mf.d, s, Clow, c.d_slot_ao.get(), Poo, Pia, Qs, Ps, true);
+      if (mixed) mftc_setup(c.mftc, s, Clow, nao, c.d_slot_ao.get(), Poo, Pia);
+    } else if (tc_dav) {
+      // tensor-core products for the first Davidson stage (and the velocity
+      // correction's exchange products)
+      mftc_setup(c.mftc, s, Clow, nao, c.d_slot_ao.get(), Poo, p.velcorr ? Pia : nullptr);
     } else {
       mf_setup_ops<double>(mf, mf.d, s, Clow, c.d_slot_ao.get(), Poo, Pia, Qs, Ps, p.velcorr);
     }
@@ -985,7 +995,7 @@ static void solve(Ctx &c, const std2g_params &p_in, std2g_result *res, const Res
       // stage 1: tensor-core (split-BF16 FP32) products; stage 2: FP64 products
       // from those Ritz vectors until the FP64 residuals meet tol
       MatVec mv_tc = [&](const double *V, int nb, double *W) {
-        mftc_apply(c.mftc, c.blas, s, V, nb, W, ak, -1.0, c.mf.dA.get());
+        mftc_apply(c.mftc, c.blas, s, V, nb, W, ak, -1.0, 0.0, c.mf.dA.get());
       };
       c.dav.profile = c.opts.verbose >= 2;
       for (double &v : c.dav.sec_ms) v = 0;
@@ -1000,7 +1010,9 @@ static void solve(Ctx &c, const std2g_params &p_in, std2g_result *res, const Res
                      c.dav.sec_ms[3], c.dav.sec_ms[4]);
       for (double &v : c.dav.sec_ms) v = 0;
       SectionClock sc(c.dav, s);
-      mf_setup_ops<double>(c.mf, c.mf.d, s, Clow, c.d_slot_ao.get(), Poo, Pia, Qs, Ps, p.velcorr);
+      // (the velocity correction uses the tensor-core exchange products, so the
+      // FP64 operators need no P^A_ov)
+      mf_setup_ops<double>(c.mf, c.mf.d, s, Clow, c.d_slot_ao.get(), Poo, Pia, Qs, Ps, false);
       c.mf.f32 = false;
       sc.tick(0);
       if (c.dav.profile) std::fprintf(stderr, "FP64 operator setup %.2f ms\n", c.dav.sec_ms[0]);
@@ -1155,7 +1167,9 @@ static void solve(Ctx &c, const std2g_params &p_in, std2g_result *res, const Res
     if (p.velcorr) {
       // X_new = (B/2) X / w (apbtrafo.f:51-65)
       double *Xn = c.w_Y.ensure((size_t)nci * nroot);
-      if (use_mf)
+      if (use_mf && tc_dav)   // mixed form: tensor-core exchange products
+        mftc_apply(c.mftc, c.blas, s, X, nroot, Xn, 0.5 * ak, 0.0, -0.5 * p.ax, nullptr);
+      else if (use_mf)
         mf_apply(c.mf, c.blas, s, X, nroot, Xn, 0.5 * ak, 0.0, -0.5 * p.ax, nullptr);
       else
         gemm(c, CUBLAS_OP_N, CUBLAS_OP_N, nci, nroot, nci, 1.0, Bh, nci, X, nci, 0.0, Xn, nci);

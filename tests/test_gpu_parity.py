@@ -201,10 +201,13 @@ def test_matrix_free_davidson_vs_oracle(benzene, precision):
         assert np.allclose(sol.fL, ref.fL[:12], rtol=1e-5, atol=1e-8)
         assert np.allclose(sol.fV, ref.fV[:12], rtol=1e-5, atol=1e-8)
         assert np.allclose(sol.RV, ref.RV[:12], rtol=1e-4, atol=1e-6)
-    else:   # tensor-core (TF32) products in the matrix-free operator
+    else:   # split-BF16 tensor-core products (first stage, velocity correction)
         assert np.abs(sol.omega - ref.omega[:12]).max() * 27.21139 < 1e-4
         big = ref.fL[:12] > 1e-3
         assert np.all(np.abs(sol.fL[big] - ref.fL[:12][big]) / ref.fL[:12][big] < 1e-4)
+        bigv = ref.fV[:12] > 1e-3   # f_V: velocity correction from the exchange products
+        assert np.all(np.abs(sol.fV[bigv] - ref.fV[:12][bigv]) / ref.fV[:12][bigv] < 1e-4)
+        assert np.allclose(sol.RV, ref.RV[:12], rtol=1e-3, atol=1e-6)
 
 
 def test_matrix_free_larger_cluster():
