@@ -54,8 +54,8 @@ class Clocks:
     """nvidia-smi sampling during the timed region."""
 
     def __init__(self, dev):
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
-        os.makedirs(os.path.dirname(self.path), exist_ok=True)
+        import tempfile
+        self.path = os.path.join(tempfile.gettempdir(), f"std2g_clocks_{os.getpid()}.csv")
         q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
