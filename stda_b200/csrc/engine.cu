@@ -659,7 +659,8 @@ static void solve(Ctx &c, const std2g_params &p_in, std2g_result *res, const Res
     S2G_CUDA(cudaFuncSetAttribute(k_charges_tiled, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   227 * 1024));
     auto tiled = [&](double *out, int p0, int np, int q0, int nq) {
-      const dim3 g((unsigned)div_up(nq, kChTQ), (unsigned)div_up(np, kChTP));
+      const dim3 g((unsigned)div_up(nq, kChTQ), (unsigned)div_up(np, kChTP),
+                   (unsigned)div_up(N, kChAtoms));
       S2G_LAUNCH(k_charges_tiled, g, 256, shb, s, out, Clow, nao, N, aop, aol, p0, np, q0, nq,
                  c.chunk_rows);
     };

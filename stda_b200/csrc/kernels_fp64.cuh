@@ -130,11 +130,12 @@ __global__ void k_charges_block(double *__restrict__ out, const double *__restri
 
 // Charges of a full MO block, q^A_(p,q) for p < np, q < nq (lo12pop
 // stda.f:1727-1744), out[(p*nq + q)*N + A].  One CTA per 8 x 32 tile of MO
-// pairs walks the atoms in chunks of kChAtoms: the chunk's AO rows of the
+// pairs and one chunk of kChAtoms atoms (grid z): the chunk's AO rows of the
 // tile's 40 MO columns are staged in shared memory (so every C element is read
-// once per tile, not once per pair), each thread forms its pair's sums for the
-// chunk's atoms, and the results leave as contiguous 128-byte segments of the
-// [pair][atom] layout.  Write-bound.  Shared memory: 40*max_rows + 256*17 doubles.
+// once per tile and chunk, not once per pair), each thread forms its pair's
+// sums for the chunk's atoms, and the results leave as contiguous 128-byte
+// segments of the [pair][atom] layout.  Write-bound.  Shared memory:
+// 40*max_rows + 256*17 doubles.
 constexpr int kChTP = 8, kChTQ = 32, kChAtoms = 16;
 __global__ void __launch_bounds__(256)
 k_charges_tiled(double *__restrict__ out, const double *__restrict__ C, int nao, int N,
@@ -147,10 +148,10 @@ k_charges_tiled(double *__restrict__ out, const double *__restrict__ C, int nao,
   const int pt = blockIdx.y * kChTP, qt = blockIdx.x * kChTQ;
   const int pi = threadIdx.x / kChTQ, qi = threadIdx.x % kChTQ;
   constexpr int kCols = kChTP + kChTQ, kSt = kChAtoms + 1;
-  for (int A0 = 0; A0 < N; A0 += kChAtoms) {
+  {
+    const int A0 = blockIdx.z * kChAtoms;
     const int A1 = min(N, A0 + kChAtoms);
     const int r0 = ao_ptr[A0], nr = ao_ptr[A1] - r0;
-    __syncthreads();   // the previous chunk's staged results have been written
     // stage C[rows of the chunk, tile columns]; consecutive threads take
     // consecutive rows of one column
     for (int t = threadIdx.x; t < nr * kCols; t += blockDim.x) {
