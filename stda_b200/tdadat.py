@@ -12,10 +12,22 @@ import numpy as np
 EH2EV_OUT = 27.21139
 EH2EV_IN = 27.211385050
 
-# atomic masses by nuclear charge (block.f:24-35); 0 where the table has none
-_AMS = {1: 1.00790, 2: 4.00260, 3: 6.94000, 4: 9.01218, 5: 10.81000, 6: 12.01100, 7: 14.00670,
-        8: 15.99940, 9: 18.99840, 10: 20.17900, 11: 22.98977, 12: 24.30500, 13: 26.98154,
-        14: 28.08550, 15: 30.97376, 16: 32.06000, 17: 35.45300, 18: 39.94800}
+# atomic masses by nuclear charge (block.f:24-38): Z = 1-56 and 72-83 carry a mass,
+# Z = 102 the hydrogen value; every other Z up to 107 contributes 0 to MMASS
+_MASS_1_56 = (
+    1.00790, 4.00260, 6.94000, 9.01218, 10.81000, 12.01100, 14.00670, 15.99940,
+    18.99840, 20.17900, 22.98977, 24.30500, 26.98154, 28.08550, 30.97376, 32.06000,
+    35.45300, 39.94800, 39.09830, 40.08000, 44.95590, 47.90000, 50.94150, 51.99600,
+    54.93800, 55.84700, 58.93320, 58.71000, 63.54600, 65.38000, 69.73500, 72.59000,
+    74.92160, 78.96000, 79.90400, 83.80000, 85.46780, 87.62000, 88.90590, 91.22000,
+    92.90640, 95.94000, 98.90620, 101.0700, 102.9055, 106.4000, 107.8680, 112.4100,
+    114.8200, 118.6900, 121.7500, 127.6000, 126.9045, 131.3000, 132.9054, 137.3300)
+_MASS_72_83 = (
+    178.4900, 180.9479, 183.8500, 186.2070, 190.2000, 192.2200, 195.0900, 196.9665,
+    200.5900, 204.3700, 207.2000, 208.9804)
+_AMS = {z: m for z, m in enumerate(_MASS_1_56, start=1)}
+_AMS.update({z: m for z, m in enumerate(_MASS_72_83, start=72)})
+_AMS[102] = 1.0079
 
 
 def molecular_mass(Z) -> float:
