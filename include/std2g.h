@@ -92,7 +92,8 @@ typedef struct {
                         first stage at any size; auto uses that stage from 16384
                         CSFs), matrix-free refined solve for alpha(w) (auto uses
                         it when the dense A+B, A-B would exceed ~24 GB, and in
-                        the mixed form from 4096 CSFs) */
+                        the mixed form from 4096 CSFs; the mixed form's inner
+                        products use the tensor cores from 1.5e6 atoms x CSFs) */
   double conv_tol;   /* Davidson residual norm tolerance (0: 1e-6) */
 } std2g_params;
 

@@ -926,6 +926,16 @@ static void solve(Ctx &c, const std2g_params &p_in, std2g_result *res, const Res
   const bool resp_mf =
       resp != nullptr && (p.solver == 2 || (double)nci * nci * 8.0 * 10.0 > 24e9 ||
                           (mixed && p.solver == 0 && nci > 4096));
+  // the mixed form's inner products of that solve go to the tensor cores once
+  // atoms x CSFs (the size of one operator product) reaches 1.5e6; below that
+  // the FP64 products are as fast or faster (measured alpha at 3 w: 7.5 vs 10.1
+  // ms for 20 atoms / 713 CSFs, 18.0 vs 18.4 ms for 90 / 13645, but 23.9 vs
+  // 30.7 ms for 130 / 23567 and 38 vs 77 ms for 200 / 12457) and the solve is
+  // the FP64 form's, which converges in its first refinement step
+  constexpr double kTcResponseMinWork = 1.5e6;
+  const bool tc_resp = resp_mf && mixed &&
+                       ((c.opts.flags & STD2G_FLAG_TENSOR_ALWAYS) ||
+                        (double)N * nci >= kTcResponseMinWork);
   double *K = nullptr, *J = nullptr, *Kx = nullptr;
   if (!use_mf && !resp_mf) {
     K = c.w_K.ensure(n2);
@@ -964,7 +974,7 @@ static void solve(Ctx &c, const std2g_params &p_in, std2g_result *res, const Res
     }
     if (resp_mf) {
       mf_setup_ops<double>(mf, mf.d, s, Clow, c.d_slot_ao.get(), Poo, Pia, Qs, Ps, true);
-      if (mixed) mftc_setup(c.mftc, s, Clow, nao, c.d_slot_ao.get(), Poo, Pia);
+      if (tc_resp) mftc_setup(c.mftc, s, Clow, nao, c.d_slot_ao.get(), Poo, Pia);
     } else if (tc_dav) {
       // tensor-core products for the first Davidson stage (and the velocity
       // correction's exchange products)
@@ -1072,7 +1082,7 @@ static void solve(Ctx &c, const std2g_params &p_in, std2g_result *res, const Res
                  nv, d_ci, d_ca, nci);
       if (resp_mf) {
         std::vector<int> fb;
-        response_matfree(c, nci, musel, *resp, fb, d_edall, ekd, uci, ak, p.ax, mixed);
+        response_matfree(c, nci, musel, *resp, fb, d_edall, ekd, uci, ak, p.ax, tc_resp);
         if (!fb.empty())
           throw Error{STD2G_ENOCONV,
                       "alpha(w): a frequency above the first excitation needs the dense form, "
