@@ -4,12 +4,14 @@ This module is the checker for the CUDA engine.  Only ``tests/``,
 ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline leg may import
 it; the engine itself never calls it.  It restates, in double precision and
 numpy, what ``SUBROUTINE stda`` (``stda.f:53-1606``) does between the AO
-integrals and ``tda.dat``, plus the sTD-DFT (``srpapack.f``) and the dynamic
-polarizability (``linear_response.f:23-192``) branches.  The reference keeps
+integrals and ``tda.dat``, plus the sTD-DFT (``srpapack.f``), the dynamic
+polarizability (``linear_response.f:23-192``) and the SHG hyperpolarizability
+(``linear_response.f:196-700``) branches.  The reference keeps
 charges, gamma matrices and A in ``real*4``; this oracle keeps everything in
 ``real*8`` so that it can serve as the FP64 yardstick.  It is pinned against
-the reference's golden files (``tests/expected_results/EXCI_TEST*.dat`` and the
-excitation energies of ``2PA_TEST*.txt``) by ``tests/test_oracle_golden.py``.
+the reference's golden files (``tests/expected_results/EXCI_TEST*.dat``, the
+beta_HRS values of ``BETA_TEST*.txt`` and the excitation energies of
+``2PA_TEST*.txt``) by ``tests/test_oracle_golden.py``.
 
 Conscious deviations (also applied by the engine, so both agree bit-for-bit
 on the CSF set):
@@ -237,6 +239,10 @@ def stda(xyz4, C, eps, occ, iaoat, S, Lao, Vao, Mao, p: Params, want_A=True):
     for name, mat in (("L", Lao), ("V", Vao), ("M", Mao)):
         mu[name] = np.stack([mo_ov(mat[d], Co, Cv) for d in range(3)])  # (3,no,nv)
     res.mu_ia = mu
+    # occupied-occupied and virtual-virtual length dipoles (the same packed
+    # moci x moci transform, stda.f:351-412) for the quadratic response
+    res.extras["mu_oo"] = np.stack([Co.T @ Lao[d] @ Co for d in range(3)])
+    res.extras["mu_vv"] = np.stack([Cv.T @ Lao[d] @ Cv for d in range(3)])
 
     Clow = lowdin_orthogonal_mos(S, Cact)
     ak = 0.0 if p.triplet else 2.0
@@ -449,6 +455,99 @@ def dynamic_polarizability(res: Result, omegas_eh) -> np.ndarray:
         XpY = np.linalg.solve(Mw, rhs)
         out.append(-2.0 * mL @ XpY)
     return np.array(out)
+
+
+def _xy_vectors(res: Result, w: float, inv_amb, rhs):
+    """X and Y of the linear response at frequency w (Eh, may be negative):
+    X+Y from [(A+B) - w^2 (A-B)^-1](X+Y) = rhs, X-Y = w (A-B)^-1 (X+Y)
+    (linear_response.f:312-327, 371-396)."""
+    XpY = np.linalg.solve(res.Apb - (w * w) * inv_amb, rhs)
+    XmY = w * (inv_amb @ XpY)
+    return 0.5 * (XpY + XmY), 0.5 * (XpY - XmY)
+
+
+def _hrs_invariants(b):
+    """<beta^2_ZZZ>, <beta^2_XZZ> of the hyper-Rayleigh orientational average
+    (HRS, linear_response.f:1489-1662); i, j, k run over distinct axes."""
+    ax3 = range(3)
+    pairs = [(i, j) for i in ax3 for j in ax3 if i != j]
+    trip = [(i, j, k) for i in ax3 for j in ax3 for k in ax3 if len({i, j, k}) == 3]
+    s_iii = sum(b[i, i, i] ** 2 for i in ax3)
+    s_iij = sum(b[i, i, j] ** 2 for i, j in pairs)
+    s_jii = sum(b[j, i, i] ** 2 for i, j in pairs)
+    s_ijj = sum(b[i, j, j] ** 2 for i, j in pairs)
+    s_ijk = sum(b[i, j, k] ** 2 for i, j, k in trip)
+    iii_ijj = sum(b[i, i, i] * b[i, j, j] for i, j in pairs)
+    jii_iij = sum(b[j, i, i] * b[i, i, j] for i, j in pairs)
+    iii_jji = sum(b[i, i, i] * b[j, j, i] for i, j in pairs)
+    iij_jii = sum(b[i, i, j] * b[j, i, i] for i, j in pairs)
+    iij_jkk = sum(b[i, i, j] * b[j, k, k] for i, j, k in trip)
+    jii_jkk = sum(b[j, i, i] * b[j, k, k] for i, j, k in trip)
+    iij_kkj = sum(b[i, i, j] * b[k, k, j] for i, j, k in trip)
+    ijk_jik = sum(b[i, j, k] * b[j, i, k] for i, j, k in trip)
+    ijj_ikk = sum(b[i, j, j] * b[i, k, k] for i, j, k in trip)
+    iik_jjk = sum(b[i, i, k] * b[j, j, k] for i, j, k in trip)
+    zzz = (s_iii / 7 + 4 * s_iij / 35 + s_jii / 35 + 2 * s_ijk / 105 + 2 * iii_ijj / 35
+           + 4 * jii_iij / 35 + 4 * iii_jji / 35 + 4 * iij_jkk / 105 + jii_jkk / 105
+           + 4 * iij_kkj / 105 + 4 * ijk_jik / 105)
+    xzz = (s_iii / 35 + 4 * iii_ijj / 105 - 2 * iii_jji / 35 + 8 * s_iij / 105
+           - 2 * iij_jkk / 105 + 2 * s_ijk / 35 - 2 * ijk_jik / 105 + 3 * s_ijj / 35
+           - 2 * iij_jii / 35 + ijj_ikk / 35 - 2 * iik_jjk / 105)
+    return zzz, xzz
+
+
+def shg_hyperpolarizability(res: Result, wavelengths_nm):
+    """lresp1 (linear_response.f:196-700; beta_resp_fast :911-1087, List_A /
+    List_B :1089-1167, A_beta_fast / B_beta_fast :1170-1226, HRS :1489-1662):
+    the second-harmonic first hyperpolarizability beta(-2w; w, w) of sTD-DFT
+    and its hyper-Rayleigh value beta_HRS, at w = 0 and w = 45.56335 / lambda.
+
+    The linear responses to -2 mu at +w and at -2w give X, Y per axis.  With
+    the CSF pairs (i a), (j a) that share their virtual (coupled through
+    mu_ij) and (i a), (i b) that share their occupied (coupled through mu_ab),
+    beta = A - B (no derivative of the XC kernel), each of A and B summed over
+    the six assignments of (x, y, z) to the -2w X vector, the dipole and the
+    w Y vector that lresp1 lists.  Every component is computed directly (the
+    reference copies the permutation-equivalent ones, which the sum makes
+    equal).  Returns (w in eV as printed, beta[nw, 3, 3, 3], beta_HRS[nw]).
+    """
+    if res.Apb is None:
+        raise OracleError("the hyperpolarizability needs A+B / A-B (rpa=True)")
+    nv = res.nv
+    allk = res.extras["allk"]
+    io, iv = allk // nv, allk % nv
+    rhs = -2.0 * res.mu_ia["L"][:, io, iv].T                   # (nci, 3)
+    inv_amb = np.linalg.inv(res.Amb)
+    # -mu coupling of CSF p to CSF q: -mu_ij for a shared virtual, +mu_ab for a
+    # shared occupied (the B term enters with a minus sign)
+    same_v = iv[:, None] == iv[None, :]
+    same_o = io[:, None] == io[None, :]
+    M = []
+    for d in range(3):
+        moo = res.extras["mu_oo"][d][io[:, None], io[None, :]]
+        mvv = res.extras["mu_vv"][d][iv[:, None], iv[None, :]]
+        M.append(np.where(same_v, -moo, 0.0) - np.where(same_o, -mvv, 0.0))
+    freqs = [0.0] + [NM_FAC / float(lam) for lam in wavelengths_nm]
+    betas, hrs = [], []
+    for f in freqs:
+        X1, Y1 = _xy_vectors(res, f, inv_amb, rhs)           # +w
+        X2, Y2 = _xy_vectors(res, -2.0 * f, inv_amb, rhs)    # -2w
+        Xs, Ys = {1: X1, 2: X2}, {1: Y1, 2: Y2}
+
+        def term(x, wx, y, z, wz):
+            return Xs[wx][:, x] @ M[y] @ Ys[wz][:, z]
+
+        b = np.zeros((3, 3, 3))
+        for i in range(3):
+            for j in range(3):
+                for k in range(3):
+                    b[i, j, k] = (term(i, 2, j, k, 1) + term(i, 2, k, j, 1)
+                                  + term(j, 1, k, i, 2) + term(j, 1, i, k, 1)
+                                  + term(k, 1, i, j, 1) + term(k, 1, j, i, 2))
+        zzz, xzz = _hrs_invariants(b)
+        betas.append(b)
+        hrs.append(math.sqrt(zzz + xzz))
+    return np.array(freqs) * EH2EV_OUT, np.array(betas), np.array(hrs)
 
 
 def read_tda_dat(text: str):

@@ -1,10 +1,14 @@
 """The FP64 oracle against the reference's own regression goldens.
 
 Cases and tolerances are those of the reference test driver
-(``tests/run_tests.sh``, ``tests/compare.py:163-215``): excitation energies
-(eV, 4 decimals) and f_L within 1e-3; for the 2PA cases only the sTD-DFT
+(``tests/run_tests.sh``, ``check_equal`` in ``tests/compare.py:77-97`` as
+dispatched at ``:110-127``): excitation energies (eV, 4 decimals) and f_L
+within 1e-3, beta_HRS within 1e-3; for the 2PA cases only the sTD-DFT
 excitation energies are compared (the 2PA cross sections are out of scope).
-Unlike ``compare.py`` the number of roots is checked exactly.
+Unlike ``compare.py`` the number of roots is checked exactly.  The beta_HRS
+cases (``-resp 2`` with ``tests/wavelength``: 1907 and 1064 nm) run the same
+A+B, A-B and ``[(A+B) - w^2 (A-B)^-1]`` solves as the dynamic polarizability,
+so they pin that path too.
 """
 import json
 import os
@@ -12,7 +16,7 @@ import os
 import numpy as np
 import pytest
 
-from oracle.stda_fp64 import Params, read_tda_dat, stda, tda_dat_text
+from oracle.stda_fp64 import Params, read_tda_dat, shg_hyperpolarizability, stda, tda_dat_text
 from tests.conftest import GOLDEN
 
 EXPECTED = json.load(open(os.path.join(GOLDEN, "reference_expected.json")))
@@ -70,3 +74,23 @@ def test_oracle_polarizability_static_limit(water):
     t = np.sqrt(2.0) * (mL @ (res.X + res.Y))
     sos = 2.0 * (t / res.omega) @ t.T
     assert np.allclose(a0, sos, rtol=1e-8, atol=1e-10)
+
+
+@pytest.mark.parametrize("name", ["BETA_TEST1", "BETA_TEST2", "BETA_TEST3"])
+def test_beta_hrs_golden(water, name):
+    case = EXPECTED[name]
+    p, res = run(water, rpa=True, **case["args"])
+    with open(os.path.join(GOLDEN, "wavelength")) as fh:
+        wavelengths = [float(t) for t in fh.read().split()]
+    ev, beta, hrs = shg_hyperpolarizability(res, wavelengths)
+    exp = np.array(case["rows"])
+    assert hrs.shape == (len(exp),)
+    assert np.all(np.abs(ev - exp[:, 0]) <= 1e-6)              # w (eV) as printed
+    assert np.all(np.abs(hrs - exp[:, 1]) <= 1e-3)             # the reference's rule
+    # FP64 against the reference's real*4 solves: measured agreement ~1e-6
+    assert np.all(np.abs(hrs - exp[:, 1]) <= 1e-5)
+    # SHG symmetry beta(i,j,k) = beta(i,k,j); Kleinman symmetry in the static limit
+    assert np.allclose(beta, beta.transpose(0, 1, 3, 2), rtol=1e-10, atol=1e-10)
+    b0 = beta[0]
+    for perm in [(1, 0, 2), (2, 1, 0), (1, 2, 0), (2, 0, 1)]:
+        assert np.allclose(b0, b0.transpose(perm), rtol=1e-8, atol=1e-8)
