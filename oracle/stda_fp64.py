@@ -5,13 +5,14 @@ This module is the checker for the CUDA engine.  Only ``tests/``,
 it; the engine itself never calls it.  It restates, in double precision and
 numpy, what ``SUBROUTINE stda`` (``stda.f:53-1606``) does between the AO
 integrals and ``tda.dat``, plus the sTD-DFT (``srpapack.f``), the dynamic
-polarizability (``linear_response.f:23-192``) and the SHG hyperpolarizability
-(``linear_response.f:196-700``) branches.  The reference keeps
+polarizability (``linear_response.f:23-192``), the SHG hyperpolarizability
+(``linear_response.f:196-700``) and the two-photon absorption
+(``linear_response.f:4604-5153``) branches.  The reference keeps
 charges, gamma matrices and A in ``real*4``; this oracle keeps everything in
 ``real*8`` so that it can serve as the FP64 yardstick.  It is pinned against
 the reference's golden files (``tests/expected_results/EXCI_TEST*.dat``, the
-beta_HRS values of ``BETA_TEST*.txt`` and the excitation energies of
-``2PA_TEST*.txt``) by ``tests/test_oracle_golden.py``.
+beta_HRS values of ``BETA_TEST*.txt`` and the excitation energies and 2PA
+strengths of ``2PA_TEST*.txt``) by ``tests/test_oracle_golden.py``.
 
 Conscious deviations (also applied by the engine, so both agree bit-for-bit
 on the CSF set):
@@ -372,6 +373,7 @@ def stda(xyz4, C, eps, occ, iaoat, S, Lao, Vao, Mao, p: Params, want_A=True):
         X = 0.5 * (XpY + XmY)
         Y = XpY - X
         res.omega, res.X, res.Y = om, X, Y
+        res.extras["Ambh"], res.extras["Z_rpa"] = Ambh, Zv
         uu, pp = XpY, XmY
     else:
         res.A = A
@@ -496,6 +498,29 @@ def _hrs_invariants(b):
     return zzz, xzz
 
 
+def _mu_csf(res: Result):
+    """Length dipoles of the selected CSFs, (3, nci)."""
+    allk = res.extras["allk"]
+    return res.mu_ia["L"][:, allk // res.nv, allk % res.nv]
+
+
+def _dipole_couplings(res: Result):
+    """Per axis d the nci x nci matrix that couples CSF p to CSF q in the
+    quadratic-response sums (List_A / List_B, linear_response.f:1089-1167):
+    -mu_ij when p = (i a), q = (j a) share their virtual, minus -mu_ab when
+    p = (i a), q = (i b) share their occupied, so that X M Y = A - B."""
+    allk = res.extras["allk"]
+    io, iv = allk // res.nv, allk % res.nv
+    same_v = iv[:, None] == iv[None, :]
+    same_o = io[:, None] == io[None, :]
+    M = []
+    for d in range(3):
+        moo = res.extras["mu_oo"][d][io[:, None], io[None, :]]
+        mvv = res.extras["mu_vv"][d][iv[:, None], iv[None, :]]
+        M.append(np.where(same_v, -moo, 0.0) - np.where(same_o, -mvv, 0.0))
+    return M
+
+
 def shg_hyperpolarizability(res: Result, wavelengths_nm):
     """lresp1 (linear_response.f:196-700; beta_resp_fast :911-1087, List_A /
     List_B :1089-1167, A_beta_fast / B_beta_fast :1170-1226, HRS :1489-1662):
@@ -513,20 +538,9 @@ def shg_hyperpolarizability(res: Result, wavelengths_nm):
     """
     if res.Apb is None:
         raise OracleError("the hyperpolarizability needs A+B / A-B (rpa=True)")
-    nv = res.nv
-    allk = res.extras["allk"]
-    io, iv = allk // nv, allk % nv
-    rhs = -2.0 * res.mu_ia["L"][:, io, iv].T                   # (nci, 3)
+    rhs = -2.0 * _mu_csf(res).T                                # (nci, 3)
     inv_amb = np.linalg.inv(res.Amb)
-    # -mu coupling of CSF p to CSF q: -mu_ij for a shared virtual, +mu_ab for a
-    # shared occupied (the B term enters with a minus sign)
-    same_v = iv[:, None] == iv[None, :]
-    same_o = io[:, None] == io[None, :]
-    M = []
-    for d in range(3):
-        moo = res.extras["mu_oo"][d][io[:, None], io[None, :]]
-        mvv = res.extras["mu_vv"][d][iv[:, None], iv[None, :]]
-        M.append(np.where(same_v, -moo, 0.0) - np.where(same_o, -mvv, 0.0))
+    M = _dipole_couplings(res)
     freqs = [0.0] + [NM_FAC / float(lam) for lam in wavelengths_nm]
     betas, hrs = [], []
     for f in freqs:
@@ -548,6 +562,57 @@ def shg_hyperpolarizability(res: Result, wavelengths_nm):
         betas.append(b)
         hrs.append(math.sqrt(zzz + xzz))
     return np.array(freqs) * EH2EV_OUT, np.array(betas), np.array(hrs)
+
+
+def two_photon_absorption(res: Result, ntrans: int):
+    """lresp_2PA_SP (linear_response.f:4604-4938; TPA_resp_fast_SP :4940-5025,
+    A/B_2PA_*_fast_SP :5027-5153): two-photon absorption of the lowest
+    ``ntrans`` sTD-DFT states in the single-photon-resonance form.
+
+    For state n (energy w_n) the response to -mu at w = -w_n / 2 gives X, Y per
+    axis; the two-photon tensor is
+      sigma_xy = -1/2 [X_x M_y Yn + X_y M_x Yn + Xn M_x Y_y + Xn M_y Y_x]
+    with the CSF couplings M of the quadratic response, and F, G, H (each / 30)
+    give delta_par = 2F+2G+2H, delta_perp = -F+4G-H, delta_circ = -2F+3G+3H
+    and rho = delta_par / delta_perp.
+
+    Under -2PA the reference's srpapack skips the halving of the packed
+    diagonals of (A-B)^1/2 and A+B before its packed products
+    (srpapack.f:99-106, 116-133), so its state vectors Xn, Yn carry each
+    diagonal twice; this restatement does the same so that it reproduces the
+    2PA goldens.  (The excitation energies, and every other consumer of the
+    state vectors, use the regular vectors.)  Returns rows
+    (n, w_n in eV, delta_par, delta_perp, delta_circ, rho) as in ``2PA-abs``.
+    """
+    if res.Apb is None or "Z_rpa" not in res.extras:
+        raise OracleError("two-photon absorption needs the sTD-DFT states (rpa=True)")
+    om = res.omega
+    if ntrans > len(om):
+        raise OracleError("number of 2PA excitations too large!")
+    Sh, Z = res.extras["Ambh"], res.extras["Z_rpa"]
+    Sq = Sh + np.diag(np.diag(Sh))
+    Pq = res.Apb + np.diag(np.diag(res.Apb))
+    XpYn = (Sq @ Z) / np.sqrt(om)
+    XmYn = (Pq @ XpYn) / om
+    Xn = 0.5 * (XpYn + XmYn)
+    Yn = XpYn - Xn
+    inv_amb = np.linalg.inv(res.Amb)
+    rhs = -_mu_csf(res).T
+    M = _dipole_couplings(res)
+    rows = []
+    for n in range(ntrans):
+        X, Y = _xy_vectors(res, -0.5 * om[n], inv_amb, rhs)
+        sg = np.empty((3, 3))
+        for x in range(3):
+            for y in range(3):
+                sg[x, y] = -0.5 * (X[:, x] @ M[y] @ Yn[:, n] + X[:, y] @ M[x] @ Yn[:, n]
+                                   + Xn[:, n] @ M[x] @ Y[:, y] + Xn[:, n] @ M[y] @ Y[:, x])
+        F = np.trace(sg) ** 2 / 30.0
+        G = float(np.sum(sg * sg)) / 30.0
+        H = float(np.sum(sg * sg.T)) / 30.0
+        par, perp = 2 * F + 2 * G + 2 * H, -F + 4 * G - H
+        rows.append([n + 1, om[n] * EH2EV_OUT, par, perp, -2 * F + 3 * G + 3 * H, par / perp])
+    return np.array(rows)
 
 
 def read_tda_dat(text: str):

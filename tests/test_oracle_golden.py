@@ -3,12 +3,12 @@
 Cases and tolerances are those of the reference test driver
 (``tests/run_tests.sh``, ``check_equal`` in ``tests/compare.py:77-97`` as
 dispatched at ``:110-127``): excitation energies (eV, 4 decimals) and f_L
-within 1e-3, beta_HRS within 1e-3; for the 2PA cases only the sTD-DFT
-excitation energies are compared (the 2PA cross sections are out of scope).
-Unlike ``compare.py`` the number of roots is checked exactly.  The beta_HRS
-cases (``-resp 2`` with ``tests/wavelength``: 1907 and 1064 nm) run the same
-A+B, A-B and ``[(A+B) - w^2 (A-B)^-1]`` solves as the dynamic polarizability,
-so they pin that path too.
+within 1e-3, beta_HRS within 1e-3; for the 2PA cases the sTD-DFT excitation
+energies within 1e-3 and the 2PA strengths and rho within 1e-2.  Unlike
+``compare.py`` the number of roots is checked exactly.  The beta_HRS cases
+(``-resp 2`` with ``tests/wavelength``: 1907 and 1064 nm) run the same A+B,
+A-B and ``[(A+B) - w^2 (A-B)^-1]`` solves as the dynamic polarizability, so
+they pin that path too; the 2PA cases pin the sTD-DFT state vectors.
 """
 import json
 import os
@@ -16,7 +16,8 @@ import os
 import numpy as np
 import pytest
 
-from oracle.stda_fp64 import Params, read_tda_dat, shg_hyperpolarizability, stda, tda_dat_text
+from oracle.stda_fp64 import (Params, read_tda_dat, shg_hyperpolarizability, stda, tda_dat_text,
+                               two_photon_absorption)
 from tests.conftest import GOLDEN
 
 EXPECTED = json.load(open(os.path.join(GOLDEN, "reference_expected.json")))
@@ -52,6 +53,21 @@ def test_std_dft_energies_golden(water, name):
     ev = res.omega * 27.21139
     assert len(ev) >= len(exp)
     assert np.all(np.abs(ev[:len(exp)] - exp[:, 1]) <= 1e-3)
+
+
+@pytest.mark.parametrize("name", ["2PA_TEST1", "2PA_TEST2", "2PA_TEST3"])
+def test_two_photon_golden(water, name):
+    """``-2PA 3``: energies within 1e-3 eV, delta_par, delta_perp, delta_circ and
+    rho within 1e-2 (the reference's rules); the goldens carry 3 decimals."""
+    case = EXPECTED[name]
+    p, res = run(water, rpa=True, **case["args"])
+    exp = np.array(case["rows"])
+    got = two_photon_absorption(res, len(exp))
+    assert got.shape == exp.shape
+    assert np.array_equal(got[:, 0], exp[:, 0])
+    assert np.all(np.abs(got[:, 1] - exp[:, 1]) <= 1e-3)
+    assert np.all(np.abs(got[:, 2:] - exp[:, 2:]) <= 1e-2)
+    assert np.all(np.abs(got[:, 2:] - exp[:, 2:]) <= 1e-3 + 1e-3 * np.abs(exp[:, 2:]))
 
 
 def test_oracle_csf_counts(water):
