@@ -89,6 +89,10 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def workload_name(n):
+    return WORKLOAD if n == 8 else f"flake n={n} (profiling case)"
+
+
 def build_workload(n=8):
     """Flake C_{6n^2}H_{6n}; n = 8 is the benchmark workload (C384H48)."""
     from stda_b200 import synth
@@ -295,7 +299,7 @@ def run_reference(args):
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": per * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD},
+        "config": {"workload": workload_name(args.flake)},
         "cpu_baseline": {"value": v, "unit": "solves/s", "cores": info["threads"], "kind": "port",
                          "sample": info["sample"]},
         "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -395,7 +399,7 @@ def main():
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
            "dtype": "bf16x3->f32 contractions, f64 screen/RR" if prec else "f64",
            "data": "synthetic",
-           "config": {"workload": WORKLOAD if args.flake == 8 else f"flake n={args.flake} (profiling case)",
+           "config": {"workload": workload_name(args.flake),
                       "nci": sol.nci, "nex": sol.nex, "nexpt": sol.nexpt,
                       "new_pt": sol.new, "no": sol.no, "nv": sol.nv, "nroots": len(sol.omega),
                       "parallelism": f"replicas x{world}",
