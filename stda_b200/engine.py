@@ -260,11 +260,21 @@ class Engine:
             _dp(b.muM)))
 
     def solve(self, kw: Keywords, cap: int = 4096) -> Solution:
-        bufs = [np.zeros(cap) for _ in range(6)]
-        res = Result()
-        res.cap = cap
-        res.omega, res.fL, res.fV, res.RL, res.RV, res.resid = (_dp(b) for b in bufs)
-        _check(self.lib.std2g_solve(self.ctx, C.byref(kw.to_c()), C.byref(res)))
+        """One solve; ``cap`` is the initial room for roots.  When the window
+        holds more roots (``nroots = 0`` on a large CSF space) the library
+        reports STD2G_ECAP with the count, and the solve is repeated once with
+        that much room."""
+        while True:
+            bufs = [np.zeros(cap) for _ in range(6)]
+            res = Result()
+            res.cap = cap
+            res.omega, res.fL, res.fV, res.RL, res.RV, res.resid = (_dp(b) for b in bufs)
+            code = self.lib.std2g_solve(self.ctx, C.byref(kw.to_c()), C.byref(res))
+            if code == 11 and res.nroot > cap:
+                cap = res.nroot
+                continue
+            _check(code)
+            break
         n = res.nroot
         return Solution(omega=bufs[0][:n].copy(), fL=bufs[1][:n].copy(), fV=bufs[2][:n].copy(),
                         RL=bufs[3][:n].copy(), RV=bufs[4][:n].copy(),
