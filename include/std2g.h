@@ -232,14 +232,18 @@ typedef struct {
 } std2g_request;
 
 int std2g_server_create(void **srv, const std2g_server_opts *opts);
-/* Queue one request; *ticket identifies it for poll / wait. */
+/* Queue one request; *ticket identifies it for poll / wait.  If every slot
+   has lost its context (a replacement context could not be created), queued
+   requests finish with that status and submit returns it. */
 int std2g_server_submit(void *srv, const std2g_request *rq, int64_t *ticket);
 /* *done = 1 once the request has finished (successfully or not). */
 int std2g_server_poll(void *srv, int64_t ticket, int *done);
 /* Block until the request has finished; returns its status and, on success,
    fills res (caller arrays of res->cap), alpha [nomega*9], alpha_resid
    [nomega] and timing_ms [3] = queued, running, total (submit to finish).
-   The ticket is released. */
+   The ticket is released, except on STD2G_ECAP (res->cap below the number of
+   roots): then res->nroot holds that number and the caller waits again on
+   the same ticket with more room. */
 int std2g_server_wait(void *srv, int64_t ticket, std2g_result *res, double *alpha,
                       double *alpha_resid, double *timing_ms);
 /* stats[7]: submitted, completed, in flight, peak in flight, bytes in flight

@@ -66,6 +66,8 @@ struct Server {
   int64_t next_ticket = 1;
   int64_t inflight_bytes = 0;
   int inflight = 0;
+  int alive_workers = 0;     // workers that still hold a context
+  int dead_status = STD2G_OK;  // why the last worker stopped (0 while any is alive)
   bool stop = false;
   int64_t submitted = 0, completed = 0, peak_bytes = 0;
   int peak_inflight = 0;
@@ -114,6 +116,21 @@ void run_job(void *ctx, Job &j) {
     j.res.RV = j.RV.data();
     j.res.resid = j.resid.data();
     st = std2g_solve(ctx, &j.par, &j.res);
+    if (st == STD2G_ECAP && j.res.nroot > cap) {
+      // every root of the window was asked for and there are more than cap:
+      // the solve reported the count; run it once more with that much room
+      const int need = j.res.nroot;
+      for (auto *v : {&j.om, &j.fL, &j.fV, &j.RL, &j.RV, &j.resid}) v->assign(need, 0.0);
+      j.res = std2g_result{};
+      j.res.cap = need;
+      j.res.omega = j.om.data();
+      j.res.fL = j.fL.data();
+      j.res.fV = j.fV.data();
+      j.res.RL = j.RL.data();
+      j.res.RV = j.RV.data();
+      j.res.resid = j.resid.data();
+      st = std2g_solve(ctx, &j.par, &j.res);
+    }
   }
   if (st == STD2G_OK && !j.omega.empty()) {
     j.alpha.assign(9 * j.omega.size(), 0.0);
@@ -140,17 +157,18 @@ int sm_share(const Server &s) {
   return std::max(1, dev_sms / (int)s.ctxs.size());
 }
 
-bool renew_context(Server *s, int slot) {
+int renew_context(Server *s, int slot) {
   std2g_destroy(s->ctxs[slot]);
   s->ctxs[slot] = nullptr;
   std2g_opts eo{};
   eo.device = s->opts.device;
   eo.precision = s->opts.precision;
   void *ctx = nullptr;
-  if (std2g_create(&ctx, &eo) != STD2G_OK) return false;
+  const int st = std2g_create(&ctx, &eo);
+  if (st != STD2G_OK) return st;
   std2g_set_sm_limit(ctx, sm_share(*s));
   s->ctxs[slot] = ctx;
-  return true;
+  return STD2G_OK;
 }
 
 void worker(Server *s, int slot) {
@@ -173,8 +191,9 @@ void worker(Server *s, int slot) {
     // memory the admission rule no longer counts.
     const bool out_of_memory = job->status == STD2G_ENOMEM;
     const bool large = job->footprint > s->budget / (int64_t)s->ctxs.size();
-    bool alive = true;
-    if (out_of_memory || large) alive = renew_context(s, slot);
+    int renew = STD2G_OK;
+    if (out_of_memory || large) renew = renew_context(s, slot);
+    const bool alive = renew == STD2G_OK;
     bool retry = out_of_memory && !job->exclusive && alive;
     {
       std::lock_guard<std::mutex> lk(s->mu);
@@ -189,9 +208,24 @@ void worker(Server *s, int slot) {
         job->done = true;
       }
     }
+    if (!alive) {
+      // this slot could not get a new context; when it was the last one,
+      // nothing can run what is queued, so those requests fail with the
+      // reason (and later submits are refused) instead of waiting forever
+      std::lock_guard<std::mutex> lk(s->mu);
+      if (--s->alive_workers == 0) {
+        s->dead_status = renew;
+        for (auto &q : s->queue) {
+          q->status = renew;
+          q->done = true;
+          ++s->completed;
+        }
+        s->queue.clear();
+      }
+    }
     s->cv_done.notify_all();
     s->cv_queue.notify_all();
-    if (!alive) return;   // this slot could not get a new context
+    if (!alive) return;
   }
 }
 
@@ -227,6 +261,7 @@ int std2g_server_create(void **srv, const std2g_server_opts *o) {
   }
   const int share = sm_share(*s);
   for (void *c : s->ctxs) std2g_set_sm_limit(c, share);
+  s->alive_workers = o->slots;
   for (int k = 0; k < o->slots; ++k) s->workers.emplace_back(worker, s.get(), k);
   *srv = s.release();
   return STD2G_OK;
@@ -258,6 +293,7 @@ int std2g_server_submit(void *srv, const std2g_request *rq, int64_t *ticket) {
   j->t_submit = Clock::now();
   {
     std::lock_guard<std::mutex> lk(s->mu);
+    if (s->alive_workers == 0) return s->dead_status;   // no slot left to run it
     j->ticket = s->next_ticket++;
     s->jobs[j->ticket] = j;
     s->queue.push_back(j);
@@ -289,6 +325,11 @@ int std2g_server_wait(void *srv, int64_t ticket, std2g_result *res, double *alph
     if (it == s->jobs.end()) return STD2G_EINVAL;
     j = it->second;
     s->cv_done.wait(lk, [&] { return j->done; });
+    if (res && j->status == STD2G_OK && res->cap < j->res.nroot) {
+      // keep the ticket so that the caller can wait again with more room
+      res->nroot = j->res.nroot;
+      return STD2G_ECAP;
+    }
     s->jobs.erase(ticket);
   }
   if (timing_ms) {
@@ -302,7 +343,6 @@ int std2g_server_wait(void *srv, int64_t ticket, std2g_result *res, double *alph
   if (j->status != STD2G_OK) return j->status;
   if (res) {
     const int n = j->res.nroot;
-    if (res->cap < n) return STD2G_ECAP;
     double *dst[6] = {res->omega, res->fL, res->fV, res->RL, res->RV, res->resid};
     const std::vector<double> *src[6] = {&j->om, &j->fL, &j->fV, &j->RL, &j->RV, &j->resid};
     for (int q = 0; q < 6; ++q)

@@ -384,16 +384,25 @@ class Server:
         return bool(d.value)
 
     def wait(self, ticket: int, cap: int = 4096):
+        """Block until the request has finished.  A result with more roots
+        than ``cap`` keeps its ticket (STD2G_ECAP with the count), and the wait
+        is repeated with that much room."""
         nom, kw = self._nomega.pop(ticket)
-        bufs = [np.zeros(cap) for _ in range(6)]
-        res = Result()
-        res.cap = cap
-        res.omega, res.fL, res.fV, res.RL, res.RV, res.resid = (_dp(x) for x in bufs)
         alpha = np.zeros(max(1, nom) * 9)
         ares = np.zeros(max(1, nom))
         timing = np.zeros(3)
-        _check(self.lib.std2g_server_wait(self.srv, ticket, C.byref(res), _dp(alpha), _dp(ares),
-                                          _dp(timing)))
+        while True:
+            bufs = [np.zeros(cap) for _ in range(6)]
+            res = Result()
+            res.cap = cap
+            res.omega, res.fL, res.fV, res.RL, res.RV, res.resid = (_dp(x) for x in bufs)
+            code = self.lib.std2g_server_wait(self.srv, ticket, C.byref(res), _dp(alpha),
+                                              _dp(ares), _dp(timing))
+            if code == 11 and res.nroot > cap:
+                cap = res.nroot
+                continue
+            _check(code)
+            break
         n = res.nroot
         sol = Solution(omega=bufs[0][:n].copy(), fL=bufs[1][:n].copy(), fV=bufs[2][:n].copy(),
                        RL=bufs[3][:n].copy(), RV=bufs[4][:n].copy(),
