@@ -40,6 +40,12 @@ def test_exci_golden(water, name):
     assert np.all(np.abs(got[:, 1] - exp[:, 1]) <= 1e-3)      # eV
     assert np.all(np.abs(got[:, 2] - exp[:, 2]) <= 1e-3)      # f_L
     assert np.all(np.abs(got[:, 3] - exp[:, 3]) <= 1e-3)      # f_V (not compared upstream)
+    # tighter than the reference's rule: the FP64 restatement reproduces the
+    # printed energies exactly and f to the last digits of the real*4 run
+    # (measured: eV 0, f_L / f_V <= 2e-6, R_L / R_V <= 2.5e-5 for |R| ~ 1e-5)
+    assert np.all(np.abs(got[:, 1] - exp[:, 1]) <= 1e-4)
+    assert np.all(np.abs(got[:, 2:4] - exp[:, 2:4]) <= 5e-6)
+    assert np.all(np.abs(got[:, 4:6] - exp[:, 4:6]) <= 5e-5)
     # the header of the velocity-corrected tda.dat, including MMASS
     hdr = [ln.strip() for ln in text.splitlines()[:13]]
     assert hdr == case["header"]
