@@ -207,8 +207,15 @@ def mo_ov(mat_ao, C_occ, C_virt):
 
 # ------------------------------------------------------------- pipeline ---
 
-def stda(xyz4, C, eps, occ, iaoat, S, Lao, Vao, Mao, p: Params, want_A=True):
+def stda(xyz4, C, eps, occ, iaoat, S, Lao, Vao, Mao, p: Params, want_A=True, real4=False):
     """Run the sTDA / sTD-DFT excitation path in FP64.
+
+    ``real4=True`` stores what the reference stores in ``real*4`` in single
+    precision instead -- charges and gamma matrices (``stda.f:465-532``), the
+    gamma.q products (``ssymm``), the couplings, A / A+B / A-B and the
+    eigensolves (``ssyevr``, ``sspevd``) -- with the PT sums, the diagonal and
+    the properties in double precision as there; it measures how far the
+    reference's own arithmetic sits from the FP64 yardstick.
 
     Inputs follow the boundary: ``xyz4`` (4, ncent) Bohr + Z, ``C`` (nao, nmo),
     ``eps``/``occ`` (nmo), ``iaoat`` (nao) 0-based, dense AO matrices ``S``
@@ -249,13 +256,15 @@ def stda(xyz4, C, eps, occ, iaoat, S, Lao, Vao, Mao, p: Params, want_A=True):
     ak = 0.0 if p.triplet else 2.0
     alpha_k, beta_j = default_alpha_beta(p)
     gj, gk = gamma_matrices(xyz4, p.ax, alpha_k, beta_j)
+    fdt = np.float32 if real4 else np.float64
+    gj, gk = gj.astype(fdt), gk.astype(fdt)
 
     io_all, ia_all = np.meshgrid(np.arange(no), np.arange(nv), indexing="ij")
     io_all, ia_all = io_all.ravel(), ia_all.ravel()          # k = i*nv + a
-    qii = charges(Clow, iaoat, ncent, np.arange(no), np.arange(no))
-    qaa = charges(Clow, iaoat, ncent, no + np.arange(nv), no + np.arange(nv))
+    qii = charges(Clow, iaoat, ncent, np.arange(no), np.arange(no)).astype(fdt)
+    qaa = charges(Clow, iaoat, ncent, no + np.arange(nv), no + np.arange(nv)).astype(fdt)
     uci = qaa.T @ (gj @ qii)                                  # (nv, no): (ii|aa)
-    qia = charges_block(Clow, iaoat, ncent, np.arange(no), no + np.arange(nv))    # (N, no*nv)
+    qia = charges_block(Clow, iaoat, ncent, np.arange(no), no + np.arange(nv)).astype(fdt)
     pia = gk @ qia
     ek_all = np.einsum("Ak,Ak->k", pia, qia)                  # (ia|ia)
     de_all = (epsi[no + ia_all] - epsi[io_all]) - uci[ia_all, io_all] + ak * ek_all
@@ -276,9 +285,11 @@ def stda(xyz4, C, eps, occ, iaoat, S, Lao, Vao, Mao, p: Params, want_A=True):
 
     # J-type charges for all occ pairs and virt pairs (stda.f:728-763)
     ii, jj = np.meshgrid(np.arange(no), np.arange(no), indexing="ij")
-    qoo = charges_block(Clow, iaoat, ncent, np.arange(no), np.arange(no)).reshape(ncent, no, no)
+    qoo = charges_block(Clow, iaoat, ncent, np.arange(no), np.arange(no)).reshape(
+        ncent, no, no).astype(fdt)
     aa, bb = np.meshgrid(np.arange(nv), np.arange(nv), indexing="ij")
-    qvv = charges_block(Clow, iaoat, ncent, no + np.arange(nv), no + np.arange(nv)).reshape(ncent, nv, nv)
+    qvv = charges_block(Clow, iaoat, ncent, no + np.arange(nv), no + np.arange(nv)).reshape(
+        ncent, nv, nv).astype(fdt)
     poo = (gj @ qoo.reshape(ncent, -1)).reshape(qoo.shape)
 
     def coupling(krow, kcol):
@@ -301,7 +312,7 @@ def stda(xyz4, C, eps, occ, iaoat, S, Lao, Vao, Mao, p: Params, want_A=True):
         """(ib|ja) with gamma^K for CSF pairs u=(i,a), v=(j,b) (rrpamat stda.f:1943-1946)."""
         i1, a1 = io_all[ks], ia_all[ks]
         n = len(ks)
-        out = np.empty((n, n))
+        out = np.empty((n, n), dtype=fdt)
         rb = max(1, int(3e7 // max(1, n * ncent)))
         for r0 in range(0, n, rb):
             r1 = min(n, r0 + rb)
@@ -340,7 +351,7 @@ def stda(xyz4, C, eps, occ, iaoat, S, Lao, Vao, Mao, p: Params, want_A=True):
         return res
 
     # A matrix (rtdamat stda.f:2010-2056), built in row blocks to bound memory
-    A = np.empty((nci, nci))
+    A = np.empty((nci, nci), dtype=fdt)
     rb = max(1, int(2e7 // max(1, nci)))
     for r0 in range(0, nci, rb):
         A[r0:r0 + rb] = coupling(allk[r0:r0 + rb], allk)
@@ -356,7 +367,7 @@ def stda(xyz4, C, eps, occ, iaoat, S, Lao, Vao, Mao, p: Params, want_A=True):
         np.fill_diagonal(Apb, ed - p.ax * Kd + ak * Kd)
         np.fill_diagonal(Amb, ed - ak * Kd + p.ax * Kd)
         if abs(p.ax) < 1e-6:
-            Amb = np.diag(ed - ak * Kd)
+            Amb = np.diag(ed - ak * Kd).astype(fdt)
         res.Apb, res.Amb = Apb, Amb
         # srpapack (srpapack.f:32-197): M = (A-B)^1/2 (A+B) (A-B)^1/2
         e, U = np.linalg.eigh(Amb)
@@ -675,9 +686,11 @@ def stda_timed(xyz4, C, eps, occ, iaoat, S, Lao, Vao, Mao, p: Params, budget_s=1
     pk = pk[np.argsort(de_all[pk], kind="stable")]
     ed = de_all[pk]
     ii, jj = np.meshgrid(np.arange(no), np.arange(no), indexing="ij")
-    qoo = charges_block(Clow, iaoat, ncent, np.arange(no), np.arange(no)).reshape(ncent, no, no)
+    qoo = charges_block(Clow, iaoat, ncent, np.arange(no), np.arange(no)).reshape(
+        ncent, no, no).astype(fdt)
     aa, bb = np.meshgrid(np.arange(nv), np.arange(nv), indexing="ij")
-    qvv = charges_block(Clow, iaoat, ncent, no + np.arange(nv), no + np.arange(nv)).reshape(ncent, nv, nv)
+    qvv = charges_block(Clow, iaoat, ncent, no + np.arange(nv), no + np.arange(nv)).reshape(
+        ncent, nv, nv).astype(fdt)
     poo = (gj @ qoo.reshape(ncent, -1)).reshape(qoo.shape)
     t_setup = time.perf_counter() - t_all
 

@@ -116,3 +116,23 @@ def test_beta_hrs_golden(water, name):
     b0 = beta[0]
     for perm in [(1, 0, 2), (2, 1, 0), (1, 2, 0), (2, 0, 1)]:
         assert np.allclose(b0, b0.transpose(perm), rtol=1e-8, atol=1e-8)
+
+
+def test_real4_mode_against_goldens_and_fp64(water):
+    """The oracle's real*4 storage mode (the reference's own precision) still
+    meets the reference's golden rule, selects the same CSFs as FP64 on
+    benzene, and differs from FP64 by far less than the 1e-4 eV root bar."""
+    mol, (S, L, V, M) = water
+    case = EXPECTED["EXCI_TEST1"]
+    p = Params(**case["args"])
+    res = stda(mol.xyz4(), mol.C, mol.eps, mol.occ, mol.iaoat(), S, L, V, M, p, real4=True)
+    got = read_tda_dat(tda_dat_text(res, p))
+    exp = np.array(case["rows"])
+    assert got.shape == exp.shape and np.all(np.abs(got[:, 1:3] - exp[:, 1:3]) <= 1e-3)
+    from stda_b200 import synth
+    bz, (S, L, V, M) = synth.benzene(with_ints=True)
+    p = Params(ax=0.5, e_thr_ev=10.0)
+    args = (bz.xyz4(), bz.C, bz.eps, bz.occ, bz.iaoat(), S, L, V, M, p)
+    a, b = stda(*args), stda(*args, real4=True)
+    assert np.array_equal(a.iconf, b.iconf)
+    assert np.abs(a.omega - b.omega).max() * 27.211385050 < 1e-4
