@@ -686,11 +686,9 @@ def stda_timed(xyz4, C, eps, occ, iaoat, S, Lao, Vao, Mao, p: Params, budget_s=1
     pk = pk[np.argsort(de_all[pk], kind="stable")]
     ed = de_all[pk]
     ii, jj = np.meshgrid(np.arange(no), np.arange(no), indexing="ij")
-    qoo = charges_block(Clow, iaoat, ncent, np.arange(no), np.arange(no)).reshape(
-        ncent, no, no).astype(fdt)
+    qoo = charges_block(Clow, iaoat, ncent, np.arange(no), np.arange(no)).reshape(ncent, no, no)
     aa, bb = np.meshgrid(np.arange(nv), np.arange(nv), indexing="ij")
-    qvv = charges_block(Clow, iaoat, ncent, no + np.arange(nv), no + np.arange(nv)).reshape(
-        ncent, nv, nv).astype(fdt)
+    qvv = charges_block(Clow, iaoat, ncent, no + np.arange(nv), no + np.arange(nv)).reshape(ncent, nv, nv)
     poo = (gj @ qoo.reshape(ncent, -1)).reshape(qoo.shape)
     t_setup = time.perf_counter() - t_all
 
