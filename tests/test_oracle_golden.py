@@ -136,3 +136,23 @@ def test_real4_mode_against_goldens_and_fp64(water):
     a, b = stda(*args), stda(*args, real4=True)
     assert np.array_equal(a.iconf, b.iconf)
     assert np.abs(a.omega - b.omega).max() * 27.211385050 < 1e-4
+
+
+def test_oracle_stops_like_the_reference(water):
+    """The reference's ``stop`` conditions on this path, as oracle errors:
+    no CSF below the threshold (``stda.f:644``), an MO norm off by more than
+    1e-2 after the Loewdin transform (``stda.f:436-452``), a 2PA request for
+    more states than found, and response consumers without A+B / A-B."""
+    from oracle.stda_fp64 import OracleError
+    mol, (S, L, V, M) = water
+    with pytest.raises(OracleError, match="no CSF"):
+        stda(mol.xyz4(), mol.C, mol.eps, mol.occ, mol.iaoat(), S, L, V, M, Params(e_thr_ev=0.1))
+    with pytest.raises(OracleError, match="norm"):
+        stda(mol.xyz4(), 1.1 * mol.C, mol.eps, mol.occ, mol.iaoat(), S, L, V, M,
+             Params(e_thr_ev=20.0))
+    p, res = run(water, rpa=True, ax=1.0, e_thr_ev=20.0)
+    with pytest.raises(OracleError, match="too large"):
+        two_photon_absorption(res, len(res.omega) + 1)
+    p, res = run(water, ax=1.0, e_thr_ev=20.0)
+    with pytest.raises(OracleError, match="rpa=True"):
+        shg_hyperpolarizability(res, [1064.0])
