@@ -27,6 +27,7 @@ on the CSF set):
 from __future__ import annotations
 
 import math
+import os
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -341,7 +342,8 @@ def stda(xyz4, C, eps, occ, iaoat, S, Lao, Vao, Mao, p: Params, want_A=True, rea
     nci = len(allk)
     res.iconf = np.stack([io_all[allk], ia_all[allk]], axis=1)
     res.ed = ed
-    res.extras.update(de_all=de_all, ek_all=ek_all, pk=pk, ck=ck, allk=allk)
+    res.extras.update(de_all=de_all, ek_all=ek_all, pk=pk, ck=ck, allk=allk,
+                      pair_tensors=(pia, qia, poo, qvv))
 
     mL = mu["L"][:, io_all[allk], ia_all[allk]]              # (3, nci)
     mV = mu["V"][:, io_all[allk], ia_all[allk]]
@@ -639,19 +641,109 @@ def read_tda_dat(text: str):
     return np.array(rows)
 
 
+_HERE = os.path.dirname(os.path.abspath(__file__))
+PAIRLOOPS_SRC = os.path.join(_HERE, "pairloops.c")
+PAIRLOOPS_LIB = os.path.join(_HERE, "libpairloops.so")
+_pairloops_lib = None
+
+
+def build_pairloops(force: bool = False) -> str:
+    """Compile ``pairloops.c`` (the reference's PT-selection and A-build loops
+    in C with OpenMP) next to it with gcc; returns the library path."""
+    import subprocess
+    stale = (not os.path.exists(PAIRLOOPS_LIB)
+             or os.path.getmtime(PAIRLOOPS_SRC) > os.path.getmtime(PAIRLOOPS_LIB))
+    if force or stale:
+        tmp = PAIRLOOPS_LIB + ".tmp"
+        subprocess.run(["gcc", "-O3", "-fopenmp", "-fPIC", "-shared", "-o", tmp, PAIRLOOPS_SRC],
+                       check=True, capture_output=True)
+        os.replace(tmp, PAIRLOOPS_LIB)
+    return PAIRLOOPS_LIB
+
+
+def pairloops():
+    """ctypes handle of the C pair loops, built on first use when missing."""
+    global _pairloops_lib
+    if _pairloops_lib is None:
+        import ctypes as C
+        lib = C.CDLL(build_pairloops())
+        fp, ip, dp = C.POINTER(C.c_float), C.POINTER(C.c_int), C.POINTER(C.c_double)
+        lib.pairloops_ptselect.argtypes = [C.c_int, C.c_int, fp, fp, fp, fp, C.c_int, ip, ip, dp,
+                                           C.c_int, ip, ip, dp, C.c_double, C.c_double,
+                                           C.POINTER(C.c_ubyte), dp]
+        lib.pairloops_ptselect.restype = C.c_int
+        lib.pairloops_rtdamat_rows.argtypes = [C.c_int, C.c_int, fp, fp, fp, fp, C.c_int, ip, ip,
+                                               dp, C.c_double, C.c_int, C.c_int, fp]
+        lib.pairloops_rtdamat_rows.restype = None
+        _pairloops_lib = lib
+    return _pairloops_lib
+
+
+class PairTensors32:
+    """The reference's real*4 pair tensors in the layout of ``pairloops.c``:
+    one contiguous column of N atoms per ia pair (p_ia, q_ia) and per packed
+    occupied / virtual pair (p_ij, q_ab, ``lin`` order)."""
+
+    def __init__(self, pia, qia, poo, qvv):
+        no, nv = poo.shape[1], qvv.shape[1]
+        f4 = np.float32
+        self.N, self.nv = pia.shape[0], nv
+        self.pia = np.ascontiguousarray(pia.T, dtype=f4)
+        self.qia = np.ascontiguousarray(qia.T, dtype=f4)
+        hi, lo = np.tril_indices(no)
+        self.pij = np.ascontiguousarray(poo[:, hi, lo].T, dtype=f4)
+        hi, lo = np.tril_indices(nv)
+        self.qab = np.ascontiguousarray(qvv[:, hi, lo].T, dtype=f4)
+
+    def _ptrs(self):
+        import ctypes as C
+        fp = C.POINTER(C.c_float)
+        return [a.ctypes.data_as(fp) for a in (self.pia, self.qia, self.pij, self.qab)]
+
+    def ptselect(self, kio, kiv, edpt, jo, jv, ed, ak, thrp):
+        """ptselect's loop (stda.f:1773-1863) for the given candidates and
+        primaries: (selected flags, pt2 of the unselected)."""
+        import ctypes as C
+        ip, dp = C.POINTER(C.c_int), C.POINTER(C.c_double)
+        kio, kiv, jo, jv = (np.ascontiguousarray(x, dtype=np.int32) for x in (kio, kiv, jo, jv))
+        edpt, ed = (np.ascontiguousarray(x, dtype=np.float64) for x in (edpt, ed))
+        incl = np.zeros(len(kio), dtype=np.uint8)
+        pt2 = np.zeros(len(jo))
+        pairloops().pairloops_ptselect(
+            self.N, self.nv, *self._ptrs(), len(kio), kio.ctypes.data_as(ip),
+            kiv.ctypes.data_as(ip), edpt.ctypes.data_as(dp), len(jo), jo.ctypes.data_as(ip),
+            jv.ctypes.data_as(ip), ed.ctypes.data_as(dp), float(ak), float(thrp),
+            incl.ctypes.data_as(C.POINTER(C.c_ubyte)), pt2.ctypes.data_as(dp))
+        return incl.astype(bool), pt2
+
+    def rtdamat_rows(self, io, iv, ed, ak, r0, r1):
+        """Rows r0..r1-1 of rtdamat's lower triangle (stda.f:2010-2056)."""
+        import ctypes as C
+        ip, dp = C.POINTER(C.c_int), C.POINTER(C.c_double)
+        io, iv = (np.ascontiguousarray(x, dtype=np.int32) for x in (io, iv))
+        ed = np.ascontiguousarray(ed, dtype=np.float64)
+        rows = np.zeros((r1 - r0, len(io)), dtype=np.float32)
+        pairloops().pairloops_rtdamat_rows(
+            self.N, self.nv, *self._ptrs(), len(io), io.ctypes.data_as(ip), iv.ctypes.data_as(ip),
+            ed.ctypes.data_as(dp), float(ak), r0, r1, rows.ctypes.data_as(C.POINTER(C.c_float)))
+        return rows
+
+
 def stda_timed(xyz4, C, eps, occ, iaoat, S, Lao, Vao, Mao, p: Params, budget_s=15.0):
     """Wall-clock estimate of one full FP64 CPU solve from a bounded sample.
 
     Phases that are cheap run in full (window, MO integrals, S^1/2, charges,
-    gamma, screen).  The PT selection runs on blocks of 64 consecutive
+    gamma, screen).  The PT selection and the A build run the reference's own
+    loops (``pairloops.c``: two real*4 dots of length N per CSF pair, OpenMP
+    over candidates / rows).  The PT selection runs on blocks of 64 consecutive
     candidates spread evenly over the candidate list until about half the
     budget is used and is scaled linearly to all candidates (also the estimate
     of the selected count: the selection rate varies along the list, and
     blocks of 288 gave a 9x undercount on the C384H48 flake where blocks of 64
-    came within 7 %); the A build is timed on a row block of the primary space
-    and scaled to nci^2; the dense diagonalisation (ssyevr('V','V') in real*4
+    came within 7 %); the A build is timed on the last rows of the primary
+    block and scaled by CSF pairs to nci (nci-1) / 2; the dense diagonalisation (ssyevr('V','V') in real*4
     in the reference) is timed as the same call, scipy's ``evr`` driver in
-    single precision for the lowest nex/nci fraction of a min(nci, 1500)-sized
+    single precision for the lowest nex/nci fraction of a min(nci, 4000)-sized
     matrix, and scaled as n^3.  Used only as the reported CPU baseline, never
     as a result.
     """
@@ -705,30 +797,57 @@ def stda_timed(xyz4, C, eps, occ, iaoat, S, Lao, Vao, Mao, p: Params, budget_s=1
         J4 = (P.T @ Q).reshape(len(ou1), len(ou2), len(vu1), len(vu2))
         return ak * K - J4[oinv1[:, None], oinv2[None, :], vinv1[:, None], vinv2[None, :]]
 
+    # The reference's own loops (ptselect, rtdamat: two real*4 dots of length
+    # N per CSF pair, OpenMP) in C when gcc can build them; otherwise the
+    # numpy form above, which the sample text then names
+    try:
+        pt32 = PairTensors32(pia, qia, poo, qvv)
+        pairloops()
+        loops = "C restatement of ptselect / rtdamat (real*4 dots, OpenMP)"
+    except Exception:   # no compiler: the GEMM-based numpy form
+        pt32 = None
+        loops = "numpy GEMM form of ptselect / rtdamat"
+
     # PT selection on a sample of candidate blocks spread evenly over the
     # candidate list (the selection rate varies along it), scaled linearly
     t0 = time.perf_counter()
     done, nsel = 0, 0
-    blk = 64
+    blk, group = 64, 8
     nblk_all = max(1, -(-len(ck) // blk))
     order = np.argsort((np.arange(nblk_all) * 0.6180339887) % 1.0, kind="stable")
-    for b in order:
+    for g0 in range(0, len(order), group):
         if time.perf_counter() - t0 >= 0.5 * budget_s:
             break
-        kk = ck[b * blk:(b + 1) * blk]
-        amat = coupling(kk, pk)
-        pert = (amat ** 2 / (de_all[kk][:, None] - ed[None, :] + 1e-10)).sum(axis=1)
-        nsel += int((pert > p.thrp).sum())
+        kk = np.concatenate([ck[b * blk:(b + 1) * blk] for b in order[g0:g0 + group]])
+        if pt32 is not None:
+            incl, _ = pt32.ptselect(io_all[kk], ia_all[kk], de_all[kk], io_all[pk], ia_all[pk],
+                                    ed, ak, p.thrp)
+            nsel += int(incl.sum())
+        else:
+            amat = coupling(kk, pk)
+            pert = (amat ** 2 / (de_all[kk][:, None] - ed[None, :] + 1e-10)).sum(axis=1)
+            nsel += int((pert > p.thrp).sum())
         done += len(kk)
     t_pt = (time.perf_counter() - t0) * len(ck) / max(1, done)
     nci = len(pk) + int(round(nsel * len(ck) / max(1, done)))
-    # A build on a row block of the primaries, scaled to nci^2
+    # A build: rtdamat fills the lower triangle, nci (nci-1) / 2 pairs; time the
+    # last rows of the primary block and scale by pairs
     t0 = time.perf_counter()
-    rows = pk[:min(len(pk), 256)]
-    coupling(rows, pk)
-    t_a = (time.perf_counter() - t0) * (nci / max(1, len(rows))) * (nci / max(1, len(pk)))
+    r1 = len(pk)
+    r0 = max(0, r1 - 256)
+    if pt32 is not None:
+        pt32.rtdamat_rows(io_all[pk], ia_all[pk], ed, ak, r0, r1)
+        pairs = (r0 + r1 - 1) * (r1 - r0) / 2.0
+    else:
+        coupling(pk[r0:r1], pk)
+        pairs = float(r1 - r0) * r1
+    rows = pk[r0:r1]
+    t_a = (time.perf_counter() - t0) * (nci * (nci - 1) / 2.0) / max(1.0, pairs)
     # dense diagonalisation, the roots below E_thr (about nex of them), scaled as n^3
-    n_s = min(nci, 1500)
+    # (sizes below ~3000 run at poor parallel efficiency and overstate the
+    # n^3 extrapolation by ~2x: 6467 s from 1500 against 2864 s from 4500 for
+    # the C384H48 flake on 8 cores)
+    n_s = min(nci, 4000)
     k_s = max(1, min(n_s, int(round(n_s * len(pk) / max(1, nci)))))
     rng = np.random.default_rng(0)
     Mx = rng.standard_normal((n_s, n_s)).astype(np.float32)
@@ -738,7 +857,7 @@ def stda_timed(xyz4, C, eps, occ, iaoat, S, Lao, Vao, Mao, p: Params, budget_s=1
     t_eig = (time.perf_counter() - t0) * (nci / n_s) ** 3
     est = t_setup + t_pt + t_a + t_eig
     threads = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
-    sample = (f"full window/S^1/2/charges/screen ({t_setup:.1f}s); PT on {done} of {len(ck)} "
+    sample = (f"{loops}; full window/S^1/2/charges/screen ({t_setup:.1f}s); PT on {done} of {len(ck)} "
               f"candidates (blocks of {blk} spread evenly) x {len(pk)} primaries scaled "
               f"linearly ({t_pt:.1f}s est.); A build "
               f"{len(rows)} rows scaled to nci={nci} ({t_a:.1f}s est.); real*4 evr eigh, "

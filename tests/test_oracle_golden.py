@@ -156,3 +156,26 @@ def test_oracle_stops_like_the_reference(water):
     p, res = run(water, ax=1.0, e_thr_ev=20.0)
     with pytest.raises(OracleError, match="rpa=True"):
         shg_hyperpolarizability(res, [1064.0])
+
+
+@pytest.mark.parametrize("natoms", [0, 30])
+def test_c_pair_loops_match_the_oracle(natoms):
+    """The CPU baseline's C restatement of ptselect and rtdamat (real*4 dots,
+    oracle/pairloops.c) selects the same PT candidates as the FP64 oracle and
+    reproduces its pt2 lowering and A to single precision."""
+    from oracle.stda_fp64 import PairTensors32
+    from stda_b200 import synth
+    mol, (S, L, V, M) = (synth.benzene(with_ints=True) if natoms == 0
+                         else synth.random_molecule(natoms, seed=3, with_ints=True))
+    p = Params(ax=0.5, e_thr_ev=10.0 if natoms == 0 else 7.0)
+    res = stda(mol.xyz4(), mol.C, mol.eps, mol.occ, mol.iaoat(), S, L, V, M, p)
+    x, nv = res.extras, res.nv
+    pt = PairTensors32(*x["pair_tensors"])
+    ck, pk, de = x["ck"], x["pk"], x["de_all"]
+    incl, pt2 = pt.ptselect(ck // nv, ck % nv, de[ck], pk // nv, pk % nv, de[pk], 2.0, p.thrp)
+    assert set(ck[incl]) == set(res.iconf[res.nex:, 0] * nv + res.iconf[res.nex:, 1])
+    assert np.abs(pt2 - res.pt2).max() <= 1e-5 * np.abs(res.pt2).max()
+    allk = x["allk"]
+    rows = pt.rtdamat_rows(allk // nv, allk % nv, res.ed, 2.0, 0, len(allk))
+    lt = np.tril_indices(len(allk))
+    assert np.abs(rows[lt] - res.A[lt]).max() <= 1e-6 * np.abs(res.A).max()
