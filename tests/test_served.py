@@ -78,3 +78,29 @@ def test_admission_by_footprint():
     mixed, st = _mix(reqs, 1, slots=4, budget=1)   # nothing fits beside another request
     _same(alone, mixed)
     assert st["peak_in_flight"] == 1
+
+
+def test_result_room_grows_on_demand():
+    """A full-window request (nroots = 0) with more roots than the caller's
+    room: std2g_solve reports the count with STD2G_ECAP and the binding solves
+    again with enough room; the server keeps the ticket on STD2G_ECAP and the
+    binding waits again.  Both return every root."""
+    from stda_b200 import synth
+    from stda_b200.engine import Engine, Keywords, Server, boundary_inputs
+    mol, ints = synth.benzene(seed=0, with_ints=True)
+    b = boundary_inputs(mol, ints)
+    kw = Keywords(ax=0.5, e_thr_ev=10.0)           # every root in (0, E_thr]
+    eng = Engine(0, 0)
+    eng.load(b)
+    ref = eng.solve(kw)
+    small = eng.solve(kw, cap=4)
+    eng.close()
+    assert len(ref.omega) > 4 and len(small.omega) == len(ref.omega)
+    assert np.abs(small.omega - ref.omega).max() < 1e-12
+    srv = Server(0, 0, slots=1)
+    ticket = srv.submit(b, kw, None)
+    sol = srv.wait(ticket, cap=4)[0]
+    srv.close()
+    assert len(sol.omega) == len(ref.omega)
+    assert np.abs(sol.omega - ref.omega).max() < 1e-12
+    assert np.allclose(sol.fL, ref.fL, rtol=1e-10, atol=1e-14)
