@@ -248,3 +248,19 @@ def test_mixed_form_clusters(natoms, seed):
     assert _same_csf(ref, iconf)
     n = min(10, len(ref.omega))
     assert np.abs(sol.omega[:n] - ref.omega[:n]).max() * 27.21139 < 1e-4
+
+
+def test_mixed_small_alpha_runs_the_fp64_solve(benzene):
+    """Below the tensor-core gate of the matrix-free alpha(w) solve (atoms x
+    CSFs < 1.5e6) the mixed form runs the FP64 form's solve, so the two
+    agree to rounding."""
+    from stda_b200.engine import Engine, Keywords, boundary_inputs
+    mol, ints = benzene
+    kw = Keywords(ax=0.5, e_thr_ev=10.0, solver=2)
+    out = []
+    for precision in (0, 1):
+        eng = Engine(0, precision)          # no flag: the size gates apply
+        eng.load(boundary_inputs(mol, ints))
+        out.append(eng.polarizability(kw, [0.0, 0.05])[0])
+        eng.close()
+    assert np.abs(out[0] - out[1]).max() <= 1e-12 * np.abs(out[0]).max()
