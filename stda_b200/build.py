@@ -19,7 +19,7 @@ def _stale():
     if not os.path.exists(OUT):
         return True
     t = os.path.getmtime(OUT)
-    deps = [os.path.join(CSRC, f) for f in os.listdir(CSRC)]
+    deps = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cu", ".cuh"))]
     deps.append(os.path.join(HERE, "..", "include", "std2g.h"))
     return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
 

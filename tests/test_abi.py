@@ -72,3 +72,49 @@ def test_server_arguments_checked_before_any_device_call():
     assert lib.std2g_server_wait(None, 1, None, None, None, None) == 1
     assert lib.std2g_set_sm_limit(None, 4) == 1
     lib.std2g_server_destroy(None)       # a null server is ignored
+
+
+C_HOST = r"""
+#include <stdio.h>
+#include <string.h>
+#include "std2g.h"
+int main(void) {
+  std2g_opts o;
+  std2g_params p;
+  std2g_result r;
+  void *ctx = 0;
+  int st;
+  memset(&o, 0, sizeof o);
+  memset(&p, 0, sizeof p);
+  memset(&r, 0, sizeof r);
+  st = std2g_create(&ctx, &o);
+  if (st == STD2G_OK) std2g_destroy(ctx);
+  (void)p; (void)r;
+  printf("%d %s\n", st, std2g_error_string(st));
+  return 0;
+}
+"""
+
+
+@pytest.mark.parametrize("compiler,std", [("gcc", "-std=c99"), ("g++", "-std=c++11")])
+def test_header_serves_plain_c_and_cpp_hosts(tmp_path, compiler, std):
+    """A C (or C++) host compiles against include/std2g.h without warnings,
+    links libstd2g.so and gets a status code with its message back."""
+    import shutil
+    import subprocess
+    from stda_b200.build import build
+    if shutil.which(compiler) is None:
+        pytest.skip(f"{compiler} not available")
+    lib = build()
+    src = tmp_path / ("host.c" if compiler == "gcc" else "host.cpp")
+    src.write_text(C_HOST)
+    exe = tmp_path / "host"
+    libdir = os.path.dirname(lib)
+    r = subprocess.run([compiler, std, "-Wall", "-Wextra", "-pedantic", "-Werror",
+                        "-I" + os.path.join(ROOT, "include"), str(src), "-L" + libdir, "-lstd2g",
+                        "-Wl,-rpath," + libdir, "-o", str(exe)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    out = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120)
+    assert out.returncode == 0, out.stderr
+    code, msg = out.stdout.split(" ", 1)
+    assert int(code) in (0, 12) and msg.strip()
