@@ -462,12 +462,16 @@ def dynamic_polarizability(res: Result, omegas_eh) -> np.ndarray:
     allk = res.extras["allk"]
     i1, a1 = allk // nv, allk % nv
     mL = res.mu_ia["L"][:, i1, a1]                    # (3, nci)
-    rhs = -2.0 * mL.T
+    # the solves run in the matrices' precision (real*4 ssptrf / ssptrs in the
+    # reference, FP64 here unless the result came from the real*4 mode); the
+    # sums over CSFs are real*8 in both
+    dt = res.Apb.dtype
+    rhs = (-2.0 * mL.T).astype(dt)
     inv_amb = np.linalg.inv(res.Amb)
     out = []
     for w in omegas_eh:
-        Mw = res.Apb - (w * w) * inv_amb
-        XpY = np.linalg.solve(Mw, rhs)
+        Mw = res.Apb - dt.type(w * w) * inv_amb
+        XpY = np.linalg.solve(Mw, rhs).astype(np.float64)
         out.append(-2.0 * mL @ XpY)
     return np.array(out)
 
