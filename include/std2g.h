@@ -261,7 +261,7 @@ int std2g_set_sm_limit(void *ctx, int max_sms);
 
 /* Diagnostic: lowest k eigenpairs of the symmetric n x n matrix A (host,
    column-major, lower triangle used) by the engine's single-block eigensolver
-   of the Davidson Rayleigh-Ritz step (n <= 224), and all eigenvalues by
+   of the Davidson Rayleigh-Ritz step (n <= 235), and all eigenvalues by
    cuSOLVER syevd for comparison.  w [k], Z [n*k], w_ref [n] (host).  No
    reference counterpart (the reference diagonalises with LAPACK ssyevr). */
 int std2g_symeig_check(int device, int n, int k, const double *A, double *w, double *Z,

@@ -208,7 +208,8 @@ def mo_ov(mat_ao, C_occ, C_virt):
 
 # ------------------------------------------------------------- pipeline ---
 
-def stda(xyz4, C, eps, occ, iaoat, S, Lao, Vao, Mao, p: Params, want_A=True, real4=False):
+def stda(xyz4, C, eps, occ, iaoat, S, Lao, Vao, Mao, p: Params, want_A=True, real4=False,
+         want_roots=True):
     """Run the sTDA / sTD-DFT excitation path in FP64.
 
     ``real4=True`` stores what the reference stores in ``real*4`` in single
@@ -217,6 +218,10 @@ def stda(xyz4, C, eps, occ, iaoat, S, Lao, Vao, Mao, p: Params, want_A=True, rea
     eigensolves (``ssyevr``, ``sspevd``) -- with the PT sums, the diagonal and
     the properties in double precision as there; it measures how far the
     reference's own arithmetic sits from the FP64 yardstick.
+
+    ``want_A=False`` stops after the PT selection (CSF list and lowered
+    diagonal); ``want_roots=False`` with ``rpa`` stops once A+B and A-B are
+    built (enough for :func:`dynamic_polarizability`).
 
     Inputs follow the boundary: ``xyz4`` (4, ncent) Bohr + Z, ``C`` (nao, nmo),
     ``eps``/``occ`` (nmo), ``iaoat`` (nao) 0-based, dense AO matrices ``S``
@@ -371,6 +376,9 @@ def stda(xyz4, C, eps, occ, iaoat, S, Lao, Vao, Mao, p: Params, want_A=True, rea
         if abs(p.ax) < 1e-6:
             Amb = np.diag(ed - ak * Kd).astype(fdt)
         res.Apb, res.Amb = Apb, Amb
+        if not want_roots:
+            # A+B, A-B only (what lresp needs, linear_response.f:23-192)
+            return res
         # srpapack (srpapack.f:32-197): M = (A-B)^1/2 (A+B) (A-B)^1/2
         e, U = np.linalg.eigh(Amb)
         if e[0] < 0:

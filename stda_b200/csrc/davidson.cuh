@@ -174,6 +174,11 @@ struct SectionClock {
 
 using MatVec = std::function<void(const double *V, int nb, double *W)>;
 
+// Rayleigh-Ritz problems up to this size go to symeig_small.cuh (measured
+// 0.39 / 0.94 ms at m = 64 / 128 against 0.88 / 2.1 ms for syevd); larger ones
+// to cuSOLVER syevd.
+constexpr int kRRSmallMax = 128;
+
 // Returns the number of converged wanted roots (== k on success).  `mv` forms
 // W = A V for nb column vectors (n x nb, column-major); `diag` is diag(A).
 // With `warm`, the first block is the k Ritz vectors left in dw.X by a
@@ -237,11 +242,10 @@ inline int davidson(DavidsonWork &dw, cublasHandle_t blas, cusolverDnHandle_t so
       S2G_LAUNCH(k_mirror_cols, (int)div_up((int64_t)m * nb, 256), 256, 0, s, H, mmax, m, nb);
     m += nb;
     clk.tick(1);
-    if (m <= 128 && k <= 40) {
-      // lowest k eigenpairs in one thread block, eigenvectors into Hs (ld m);
-      // measured faster than syevd for these sizes (0.5 vs 1.0 ms at m = 60,
-      // 1.1 vs 2.2 ms at m = 120, k = 30), slower for larger k
-      symeig_small(s, H, mmax, m, k, theta, Hs, m, dw.eigwork.ensure((size_t)k * 6 * m), einfo);
+    if (m <= kRRSmallMax) {
+      // lowest k eigenpairs, eigenvectors into Hs (ld m), no host synchronisation
+      symeig_small(s, H, mmax, m, std::min(k, m), theta, Hs, m,
+                   dw.eigwork.ensure(symeig_work_doubles(m, std::min(k, m))), einfo);
     } else {
       S2G_CUDA(cudaMemcpy2DAsync(Hs, sizeof(double) * m, H, sizeof(double) * mmax,
                                  sizeof(double) * m, m, cudaMemcpyDeviceToDevice, s));

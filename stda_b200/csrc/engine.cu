@@ -21,7 +21,7 @@
 #include "davidson.cuh"
 #include "matfree.cuh"
 #include "matfree_tc.cuh"
-#include "mixed.cuh"
+#include "pt_tc.cuh"
 #include "response_mixed.cuh"
 #include "symeig_small.cuh"
 
@@ -559,6 +559,7 @@ static void solve(Ctx &c, const std2g_params &p_in, std2g_result *res, const Res
   c.tc_ms = 0;
   c.tc_flop = 0;
   c.tc_launches = 0;
+  c.mixed.rechecked = 0;
   c.dav_iters = 0;
   c.dav_matvecs = 0;
   c.dav_fp64_matvecs = 0;
@@ -722,96 +723,107 @@ static void solve(Ctx &c, const std2g_params &p_in, std2g_result *res, const Res
   std::vector<int> newk;
   std::vector<double> ed_lowered(ed);
   if (nexpt > 0) {
-    // The PT kernels see the primaries in (j,b) enumeration order so that
-    // their couplings are read contiguously; pt2 is mapped back to the
-    // energy order afterwards.
-    const std::vector<int> &pko = pk_unsorted;
-    std::vector<int> kpos(nov, -1);
-    for (int q = 0; q < nex; ++q) kpos[pk[q]] = q;
-    std::vector<double> edo(nex);
-    for (int q = 0; q < nex; ++q) edo[q] = ed[kpos[pko[q]]];
-    // occupied / virtual sets spanned by the primaries
-    std::vector<int> omap(no, -1), vmap(nv, -1), OP, VP, pj(nex), pb(nex);
-    for (int q = 0; q < nex; ++q) {
-      pj[q] = pko[q] / nv;
-      pb[q] = pko[q] % nv;
-      omap[pj[q]] = 1;
-      vmap[pb[q]] = 1;
-    }
-    for (int i = 0; i < no; ++i)
-      if (omap[i] >= 0) { omap[i] = (int)OP.size(); OP.push_back(i); }
-    for (int a = 0; a < nv; ++a)
-      if (vmap[a] >= 0) { vmap[a] = (int)VP.size(); VP.push_back(a); }
-    const int nop = (int)OP.size(), nvp = (int)VP.size();
-    auto up = [&](DBuf<int> &b, const std::vector<int> &v) {
-      int *d = b.ensure(v.size());
-      S2G_CUDA(cudaMemcpyAsync(d, v.data(), sizeof(int) * v.size(), cudaMemcpyHostToDevice, s));
-      return d;
-    };
-    int *d_pk = up(c.w_pk, pko), *d_ck = up(c.w_ck, ck), *d_pj = up(c.w_pj, pj),
-        *d_pb = up(c.w_pb, pb), *d_omap = up(c.w_omap, omap), *d_vmap = up(c.w_vmap, vmap),
-        *d_OP = up(c.w_OP, OP), *d_VP = up(c.w_VP, VP);
-    double *d_ed = c.w_edsorted.ensure(nex);
-    S2G_CUDA(cudaMemcpyAsync(d_ed, edo.data(), sizeof(double) * nex, cudaMemcpyHostToDevice, s));
-    // primaries' charges and the virtual-pair factor
-    double *Qp = c.w_Qp.ensure((size_t)N * nex);
-    S2G_LAUNCH(k_gather_cols, grid_for((int64_t)N * nex), 256, 0, s, Qp, Qia, (int64_t)N, d_pk,
-               (int64_t)nex, (int64_t)N);
-    double *QvvP = c.w_QvvP.ensure((size_t)N * nv * nvp);
-    S2G_LAUNCH(k_gather_virt_pairs, grid_for((int64_t)N * nv * nvp), 256, 0, s, QvvP, Qvv, N, nv,
-               d_VP, nvp);
-    // chunk candidates by occupied index (candidates are in (i,a) order)
-    const int64_t ldj = (int64_t)nv * nvp;
-    const double budget = 6.0e9;   // bytes of K/J buffers per chunk
     // Mixed form: the couplings go to the tensor cores once there are enough
     // of them (candidates x primaries); smaller problems are latency-bound and
     // use the FP64 GEMMs, which give the FP64 selection directly.
     const bool tc_pt = mixed && ((c.opts.flags & STD2G_FLAG_TENSOR_ALWAYS) ||
                                  (double)nexpt * (double)nex >= 2.5e8);
-    const double per_occ = (tc_pt ? 4.0 : 8.0) * ((double)nex * nv + (double)ldj * nop) +
-                           8.0 * (double)N * (nv + nop) + (tc_pt ? 4.0 * 64 * (nv + nop) : 0.0);
-    int occ_chunk = std::max(1, (int)std::min<double>(no, budget / per_occ));
-    std::vector<int> first_of_occ(no + 1, nexpt);
-    {
-      int q = 0;
-      for (int i = 0; i <= no; ++i) {
-        while (q < nexpt && ck[q] / nv < i) ++q;
-        first_of_occ[i] = q;
-      }
-    }
-    bool mixed_ready = false;
-    if (mixed) {
-      c.mixed.tc.ms = 0;
-      c.mixed.tc.flop = 0;
-      c.mixed.tc.launches = 0;
-      c.mixed.rechecked = 0;
-    }
-    int nchunk = (int)div_up(no, occ_chunk);
-    // column sums of the PT terms by segments of candidate rows (deterministic order)
-    const int kSeg = 2048;
-    std::vector<int> seg_off(nchunk + 1, 0);
-    for (int q = 0; q < nchunk; ++q) {
-      int a0 = q * occ_chunk, a1 = std::min(no, a0 + occ_chunk);
-      int nrq = first_of_occ[a1] - first_of_occ[a0];
-      seg_off[q + 1] = seg_off[q] + (int)div_up(nrq, kSeg);
-    }
-    const int nseg_total = std::max(1, seg_off[nchunk]);
-    double *colpart = c.w_colpart.ensure((size_t)nseg_total * nex);
+    std::vector<int> kpos(nov, -1);
+    for (int q = 0; q < nex; ++q) kpos[pk[q]] = q;
     unsigned char *sel = c.w_sel.ensure(nexpt);
     double *pert = c.w_pert.ensure(nexpt);
-    for (int q = 0; q < nchunk; ++q) {
-      int i0 = q * occ_chunk, i1 = std::min(no, i0 + occ_chunk), ni = i1 - i0;
-      int r0 = first_of_occ[i0], r1 = first_of_occ[i1], nr = r1 - r0;
-      if (nr == 0) continue;
-      const dim3 cgrid((unsigned)div_up(nex, 128), (unsigned)(seg_off[q + 1] - seg_off[q]));
-      double *cpart = colpart + (size_t)seg_off[q] * nex;
-      double *Pc = c.w_Pc.ensure((size_t)N * nr);
-      S2G_LAUNCH(k_gather_cols, grid_for((int64_t)N * nr), 256, 0, s, Pc, Pia, (int64_t)N,
-                 d_ck + r0, (int64_t)nr, (int64_t)N);
-      double *W = c.w_W.ensure((size_t)N * ni * nop);
-      S2G_LAUNCH(k_gather_occ_pairs, grid_for((int64_t)N * ni * nop), 256, 0, s, W, Poo, N, no,
-                 i0, ni, d_OP, nop);
-      if (!tc_pt) {
+    double *pt2 = c.w_pt2.ensure(nex), *edp = c.w_edp.ensure(nex);
+    // The PT kernels see the primaries in (j,b) enumeration order (FP64 form:
+    // contiguous coupling reads) or (b,j) order (mixed form: the J
+    // contraction grouped by virtual index); pt2 is mapped back to the energy
+    // order afterwards.
+    std::vector<int> pko = pk_unsorted;
+    if (tc_pt)
+      std::stable_sort(pko.begin(), pko.end(),
+                       [&](int x, int y) { return x % nv < y % nv; });   // (b, j)
+    std::vector<double> edo(nex);
+    for (int q = 0; q < nex; ++q) edo[q] = ed[kpos[pko[q]]];
+    if (tc_pt) {
+      PtProblem pb{N, no, nv, Pia, Qia, Poo, Qvv, de, ak, p.thrp, 6.0e9};
+      c.mixed.profile = c.opts.verbose >= 2;
+      mixed_pt_select(c.mixed, s, pb, pko, edo, ck, pert, sel, pt2, edp);
+      if (c.mixed.profile)
+        std::fprintf(stderr,
+                     "pt select (mixed): operands %.2f, (ia|jb) %.2f, (ij|ab) %.2f, rows %.2f, "
+                     "recheck %.2f (%lld rows), columns %.2f ms\n",
+                     c.mixed.sec_ms[0], c.mixed.sec_ms[1], c.mixed.sec_ms[2], c.mixed.sec_ms[3],
+                     c.mixed.sec_ms[4], (long long)c.mixed.rechecked, c.mixed.sec_ms[5]);
+      c.tc_ms = c.mixed.ms;
+      c.tc_flop = c.mixed.flop;
+      c.tc_launches = c.mixed.launches;
+    } else {
+      // FP64 form: explicit K (candidates x primaries) and the (i,j) x (a,b)
+      // box of J per chunk of candidate occupied indices, FP64 GEMMs
+      std::vector<int> omap(no, -1), vmap(nv, -1), OP, VP, pj(nex), pb(nex);
+      for (int q = 0; q < nex; ++q) {
+        pj[q] = pko[q] / nv;
+        pb[q] = pko[q] % nv;
+        omap[pj[q]] = 1;
+        vmap[pb[q]] = 1;
+      }
+      for (int i = 0; i < no; ++i)
+        if (omap[i] >= 0) { omap[i] = (int)OP.size(); OP.push_back(i); }
+      for (int a = 0; a < nv; ++a)
+        if (vmap[a] >= 0) { vmap[a] = (int)VP.size(); VP.push_back(a); }
+      const int nop = (int)OP.size(), nvp = (int)VP.size();
+      auto up = [&](DBuf<int> &b, const std::vector<int> &v) {
+        int *d = b.ensure(v.size());
+        S2G_CUDA(cudaMemcpyAsync(d, v.data(), sizeof(int) * v.size(), cudaMemcpyHostToDevice, s));
+        return d;
+      };
+      int *d_pk = up(c.w_pk, pko), *d_ck = up(c.w_ck, ck), *d_pj = up(c.w_pj, pj),
+          *d_pb = up(c.w_pb, pb), *d_omap = up(c.w_omap, omap), *d_vmap = up(c.w_vmap, vmap),
+          *d_OP = up(c.w_OP, OP), *d_VP = up(c.w_VP, VP);
+      double *d_ed = c.w_edsorted.ensure(nex);
+      S2G_CUDA(cudaMemcpyAsync(d_ed, edo.data(), sizeof(double) * nex, cudaMemcpyHostToDevice, s));
+      // primaries' charges and the virtual-pair factor
+      double *Qp = c.w_Qp.ensure((size_t)N * nex);
+      S2G_LAUNCH(k_gather_cols, grid_for((int64_t)N * nex), 256, 0, s, Qp, Qia, (int64_t)N, d_pk,
+                 (int64_t)nex, (int64_t)N);
+      double *QvvP = c.w_QvvP.ensure((size_t)N * nv * nvp);
+      S2G_LAUNCH(k_gather_virt_pairs, grid_for((int64_t)N * nv * nvp), 256, 0, s, QvvP, Qvv, N, nv,
+                 d_VP, nvp);
+      // chunk candidates by occupied index (candidates are in (i,a) order)
+      const int64_t ldj = (int64_t)nv * nvp;
+      const double budget = 6.0e9;   // bytes of K/J buffers per chunk
+      const double per_occ = 8.0 * ((double)nex * nv + (double)ldj * nop) + 8.0 * (double)N * (nv + nop);
+      int occ_chunk = std::max(1, (int)std::min<double>(no, budget / per_occ));
+      std::vector<int> first_of_occ(no + 1, nexpt);
+      {
+        int q = 0;
+        for (int i = 0; i <= no; ++i) {
+          while (q < nexpt && ck[q] / nv < i) ++q;
+          first_of_occ[i] = q;
+        }
+      }
+      int nchunk = (int)div_up(no, occ_chunk);
+      // column sums of the PT terms by segments of candidate rows (deterministic order)
+      const int kSeg = 2048;
+      std::vector<int> seg_off(nchunk + 1, 0);
+      for (int q = 0; q < nchunk; ++q) {
+        int a0 = q * occ_chunk, a1 = std::min(no, a0 + occ_chunk);
+        int nrq = first_of_occ[a1] - first_of_occ[a0];
+        seg_off[q + 1] = seg_off[q] + (int)div_up(nrq, kSeg);
+      }
+      const int nseg_total = std::max(1, seg_off[nchunk]);
+      double *colpart = c.w_colpart.ensure((size_t)nseg_total * nex);
+      for (int q = 0; q < nchunk; ++q) {
+        int i0 = q * occ_chunk, i1 = std::min(no, i0 + occ_chunk), ni = i1 - i0;
+        int r0 = first_of_occ[i0], r1 = first_of_occ[i1], nr = r1 - r0;
+        if (nr == 0) continue;
+        const dim3 cgrid((unsigned)div_up(nex, 128), (unsigned)(seg_off[q + 1] - seg_off[q]));
+        double *cpart = colpart + (size_t)seg_off[q] * nex;
+        double *Pc = c.w_Pc.ensure((size_t)N * nr);
+        S2G_LAUNCH(k_gather_cols, grid_for((int64_t)N * nr), 256, 0, s, Pc, Pia, (int64_t)N,
+                   d_ck + r0, (int64_t)nr, (int64_t)N);
+        double *W = c.w_W.ensure((size_t)N * ni * nop);
+        S2G_LAUNCH(k_gather_occ_pairs, grid_for((int64_t)N * ni * nop), 256, 0, s, W, Poo, N, no,
+                   i0, ni, d_OP, nop);
         double *Kb = c.w_Kbuf.ensure((size_t)nex * nr);
         double *Jb = c.w_Jbuf.ensure((size_t)ldj * ni * nop);
         gemm(c, CUBLAS_OP_T, CUBLAS_OP_N, nex, nr, N, 1.0, Qp, N, Pc, N, 0.0, Kb, nex);
@@ -823,45 +835,17 @@ static void solve(Ctx &c, const std2g_params &p_in, std2g_result *res, const Res
         S2G_LAUNCH((k_pt_cols<double, double>), cgrid, 128, 0, s, Kb, Jb, ldj, (int64_t)nex, nex,
                    nvp, nop, nr, d_ck + r0, nv, i0, de, d_pj, d_pb, d_omap, d_vmap, d_ed, ak,
                    sel + r0, cpart, kSeg);
-      } else {
-        MixedWork &mw = c.mixed;
-        if (!mixed_ready) {
-          mixed_pt_prepare(mw, s, Qp, QvvP, N, nex, ldj);
-          const int ncol4 = (int)round_up4(nex);
-          S2G_LAUNCH(k_pt_colinfo, (int)div_up(ncol4, 128), 128, 0, s, nex, ncol4, d_pj, d_pb,
-                     d_omap, d_vmap, mw.ldJ, d_ed, mw.jcol.ensure(ncol4), mw.eh.ensure(ncol4),
-                     mw.el.ensure(ncol4));
-          mixed_ready = true;
-        }
-        mixed_pt_chunk(mw, s, Pc, W, N, nex, nr, ldj, ni * nop);
-        const float *Kf = mw.K.get(), *Jf = mw.J.get();
-        int64_t *roff = mw.roff.ensure(nr);
-        float *rhl = mw.rhl.ensure((size_t)2 * nr);
-        S2G_LAUNCH(k_pt_rows32, (int)div_up(nr, kRowWarps), 256, 0, s, Kf, Jf, mw.ldJ, mw.ldK,
-                   nex, nvp, nop, nr, d_ck + r0, nv, i0, de, mw.jcol.get(), mw.eh.get(),
-                   mw.el.get(), (float)ak, p.thrp, pert + r0, sel + r0, roff, rhl);
-        // candidates whose PT sum lies near the threshold are decided in FP64
-        mixed_pt_recheck(mw, s, pert + r0, sel + r0, nr, p.thrp, d_ck + r0, d_pk, nex, Pia, Qia,
-                         Poo, Qvv, N, no, nv, de, d_ed, ak);
-        S2G_LAUNCH(k_pt_cols32, cgrid, 128, 0, s, Kf, Jf, mw.ldK, nex, nr, mw.jcol.get(),
-                   mw.eh.get(), mw.el.get(), (float)ak, sel + r0, roff, rhl, cpart, kSeg);
       }
+      if (seg_off[nchunk] == 0) S2G_CUDA(cudaMemsetAsync(colpart, 0, sizeof(double) * nex, s));
+      S2G_LAUNCH(k_pt2_finish, (int)div_up(nex, 128), 128, 0, s, colpart, nseg_total, nex, d_ed,
+                 pt2, edp);
     }
-    double *pt2 = c.w_pt2.ensure(nex), *edp = c.w_edp.ensure(nex);
-    if (seg_off[nchunk] == 0) S2G_CUDA(cudaMemsetAsync(colpart, 0, sizeof(double) * nex, s));
-    S2G_LAUNCH(k_pt2_finish, (int)div_up(nex, 128), 128, 0, s, colpart, nseg_total, nex, d_ed, pt2,
-               edp);
     std::vector<unsigned char> h_sel(nexpt);
     std::vector<double> h_edp(nex);
     S2G_CUDA(cudaMemcpyAsync(h_sel.data(), sel, nexpt, cudaMemcpyDeviceToHost, s));
     S2G_CUDA(cudaMemcpyAsync(h_edp.data(), edp, sizeof(double) * nex, cudaMemcpyDeviceToHost, s));
     S2G_CUDA(cudaStreamSynchronize(s));
     for (int q = 0; q < nex; ++q) ed_lowered[kpos[pko[q]]] = h_edp[q];
-    if (mixed) {
-      c.tc_ms = c.mixed.tc.ms;
-      c.tc_flop = c.mixed.tc.flop;
-      c.tc_launches = c.mixed.tc.launches;
-    }
     for (int q = 0; q < nexpt; ++q)
       if (h_sel[q]) newk.push_back(ck[q]);
   }
@@ -1428,7 +1412,7 @@ int std2g_symeig_check(int device, int n, int k, const double *A, double *w, dou
     S2G_CUDA(cudaMemcpyAsync(dA.ensure(n2), A, sizeof(double) * n2, cudaMemcpyHostToDevice, s));
     S2G_CUDA(cudaMemsetAsync(dinfo.ensure(2), 0, 2 * sizeof(int), s));
     symeig_small(s, dA.get(), n, n, k, dw.ensure(k), dZ.ensure((size_t)n * k), n,
-                 dwork.ensure((size_t)k * 6 * n), dinfo.get());
+                 dwork.ensure(symeig_work_doubles(n, k)), dinfo.get());
     // cuSOLVER on a copy
     cusolverDnHandle_t h;
     S2G_CUSOLVER(cusolverDnCreate(&h));

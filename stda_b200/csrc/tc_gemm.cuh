@@ -116,18 +116,21 @@ __device__ __forceinline__ uint64_t umma_desc(uint32_t saddr) {
   return d;
 }
 
-// instruction descriptor: BF16 x BF16 -> FP32, both K-major, M=128, N=BN
+// instruction descriptors: BF16 x BF16 (or FP16 x FP16) -> FP32, both
+// K-major, M=128, N=BN (A and B always of the same type)
 constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) |
                             ((uint32_t)(BM >> 4) << 24);
+constexpr uint32_t kIdescF16 = (1u << 4) | ((uint32_t)(BN >> 3) << 17) |
+                               ((uint32_t)(BM >> 4) << 24);
 
-__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t da, uint64_t db,
-                                          uint32_t accumulate) {
+__device__ __forceinline__ void umma_f16(uint32_t tmem_d, uint64_t da, uint64_t db,
+                                         uint32_t accumulate, uint32_t idesc) {
   asm volatile(
       "{\n\t.reg .pred p;\n\t"
       "setp.ne.b32 p, %4, 0;\n\t"
       "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(
           tmem_d),
-      "l"(da), "l"(db), "r"(kIdesc), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0));
+      "l"(da), "l"(db), "r"(idesc), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0));
 }
 
 __device__ __forceinline__ void umma_commit(uint64_t *bar) {
@@ -193,16 +196,53 @@ __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(tc::smem_u32(bar)) : "memory");
 }
 
-// Persistent kernel: CTA b handles tiles b, b + gridDim.x, ... of the
-// (batch, M/128, N/128) tile space.  The TMEM accumulator is double-buffered
-// (2 x BN columns) so that the epilogue of one tile overlaps the MMAs of the
-// next; the TMA producer runs ahead across tile boundaries through the
-// 3-stage shared-memory ring.
+// One tile of the persistent loop: where its operands are and where its
+// output goes.
+struct TcTile {
+  int a_y, a_z, b_y, b_z;        // TMA row / batch coordinates of the A and B tiles
+  int m0, n0, z;                 // TMA-store epilogue: origin of the output tile
+  int m_valid, n_valid;          // direct-store epilogue: rows / columns kept
+  int64_t out_base, col_stride;  // direct-store epilogue: D[out_base + n*col_stride + m]
+  const float *rs, *cs;          // direct-store epilogue: D *= rs[m] * cs[n] (when set)
+};
+
+// Dense (batch, M/128, N/128) tiles; D row-major, stored through TMA.
+struct GridTiles {
+  int M, N, batch, b_batched;
+  __device__ __forceinline__ int64_t count() const {
+    return (int64_t)((N + tc::BN - 1) / tc::BN) * ((M + tc::BM - 1) / tc::BM) * batch;
+  }
+  __device__ __forceinline__ TcTile at(int64_t t) const {
+    const int tiles_n = (N + tc::BN - 1) / tc::BN, tiles_m = (M + tc::BM - 1) / tc::BM;
+    const int tn = (int)(t % tiles_n);
+    const int64_t rest = t / tiles_n;
+    const int tm = (int)(rest % tiles_m), z = (int)(rest / tiles_m);
+    TcTile x{};
+    x.a_y = tm * tc::BM;
+    x.a_z = z;
+    x.b_y = tn * tc::BN;
+    x.b_z = b_batched ? z : 0;
+    x.m0 = tm * tc::BM;
+    x.n0 = tn * tc::BN;
+    x.z = z;
+    return x;
+  }
+};
+
+// Persistent kernel: CTA b handles tiles b, b + gridDim.x, ... of `tiles`.
+// The TMEM accumulator is double-buffered (2 x BN columns) so that the
+// epilogue of one tile overlaps the MMAs of the next; the TMA producer runs
+// ahead across tile boundaries through the 3-stage shared-memory ring.
+// Epilogue: kDirect = false stores D[m][n] through 128B-swizzled shared
+// memory and TMA (map mD); kDirect = true writes D[out_base + n*col_stride + m]
+// from registers (the transposed layout of the PT couplings; a warp's 32 rows
+// are 128 contiguous bytes per column).
+template <class Tiles, bool kDirect, bool kF16 = false>
 __global__ void __launch_bounds__(256, 1)
 k_tc_gemm_bf16x3(const __grid_constant__ CUtensorMap mAh, const __grid_constant__ CUtensorMap mAl,
                  const __grid_constant__ CUtensorMap mBh, const __grid_constant__ CUtensorMap mBl,
-                 const __grid_constant__ CUtensorMap mD, int M, int N, int Kpad, int b_batched,
-                 int batch, int *err) {
+                 const __grid_constant__ CUtensorMap mD, const Tiles tiles, float *D, int Kpad,
+                 int *err) {
   using namespace tc;
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char *base = (unsigned char *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
@@ -215,8 +255,7 @@ k_tc_gemm_bf16x3(const __grid_constant__ CUtensorMap mAh, const __grid_constant_
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int nk = Kpad / BK;
-  const int tiles_n = (N + BN - 1) / BN, tiles_m = (M + BM - 1) / BM;
-  const int64_t ntiles = (int64_t)tiles_n * tiles_m * batch;
+  const int64_t ntiles = tiles.count();
 
   if (threadIdx.x == 0) {
     for (int q = 0; q < STAGES; ++q) {
@@ -246,10 +285,7 @@ k_tc_gemm_bf16x3(const __grid_constant__ CUtensorMap mAh, const __grid_constant_
     int64_t it = 0;
     bool ok = true;
     for (int64_t t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
-      const int tn = (int)(t % tiles_n);
-      const int64_t rest = t / tiles_n;
-      const int tm = (int)(rest % tiles_m), z = (int)(rest / tiles_m);
-      const int zb = b_batched ? z : 0;
+      const TcTile tl = tiles.at(t);
       for (int kb = 0; kb < nk; ++kb, ++it) {
         const int s = (int)(it % STAGES);
         if (it >= STAGES && !mbar_wait(&empty[s], (uint32_t)(((it / STAGES) - 1) & 1), err, 1)) {
@@ -258,10 +294,10 @@ k_tc_gemm_bf16x3(const __grid_constant__ CUtensorMap mAh, const __grid_constant_
         }
         unsigned char *st = base + s * STAGE_BYTES;
         mbar_expect_tx(&full[s], STAGE_BYTES);
-        tma_load_3d(st, &mAh, &full[s], kb * BK, tm * BM, z);
-        tma_load_3d(st + TILE_A, &mAl, &full[s], kb * BK, tm * BM, z);
-        tma_load_3d(st + 2 * TILE_A, &mBh, &full[s], kb * BK, tn * BN, zb);
-        tma_load_3d(st + 2 * TILE_A + TILE_B, &mBl, &full[s], kb * BK, tn * BN, zb);
+        tma_load_3d(st, &mAh, &full[s], kb * BK, tl.a_y, tl.a_z);
+        tma_load_3d(st + TILE_A, &mAl, &full[s], kb * BK, tl.a_y, tl.a_z);
+        tma_load_3d(st + 2 * TILE_A, &mBh, &full[s], kb * BK, tl.b_y, tl.b_z);
+        tma_load_3d(st + 2 * TILE_A + TILE_B, &mBl, &full[s], kb * BK, tl.b_y, tl.b_z);
       }
     }
   } else if (warp == 1 && lane == 0) {
@@ -287,19 +323,19 @@ k_tc_gemm_bf16x3(const __grid_constant__ CUtensorMap mAh, const __grid_constant_
         for (int kk = 0; kk < BK / 16; ++kk) {
           const uint32_t off = kk * 32;   // 16 BF16 = 32 bytes along K
           const uint32_t acc0 = (kb > 0 || kk > 0) ? 1u : 0u;
-          umma_bf16(dacc, tc::umma_desc(ah + off), tc::umma_desc(bh + off), acc0);
-          umma_bf16(dacc, tc::umma_desc(ah + off), tc::umma_desc(bl + off), 1u);
-          umma_bf16(dacc, tc::umma_desc(al + off), tc::umma_desc(bh + off), 1u);
+          constexpr uint32_t id = kF16 ? kIdescF16 : kIdesc;
+          umma_f16(dacc, tc::umma_desc(ah + off), tc::umma_desc(bh + off), acc0, id);
+          umma_f16(dacc, tc::umma_desc(ah + off), tc::umma_desc(bl + off), 1u, id);
+          umma_f16(dacc, tc::umma_desc(al + off), tc::umma_desc(bh + off), 1u, id);
         }
         umma_commit(&empty[s]);   // stage reusable once these MMAs have read it
       }
       if (ok) umma_commit(&acc_full[ab]);   // accumulator complete
     }
   } else if (warp >= 4) {
-    // ---- epilogue: TMEM -> registers -> swizzled smem -> TMA store ----
-    // Warp wq owns TMEM lanes (tile rows) 32*wq .. 32*wq+31 and writes them in
-    // 32-column blocks through two staging buffers; the store unit clips rows
-    // >= M and columns >= N.
+    // ---- epilogue ----
+    // Warp wq owns TMEM lanes (tile rows) 32*wq .. 32*wq+31 and drains them in
+    // 32-column blocks.
     const int wq = warp - 4;
     unsigned char *stage0 = epi + (wq * 2) * EPI_BUF;
     int64_t lt = 0;
@@ -308,37 +344,62 @@ k_tc_gemm_bf16x3(const __grid_constant__ CUtensorMap mAh, const __grid_constant_
       const int ab = (int)(lt & 1);
       if (!mbar_wait(&acc_full[ab], (uint32_t)((lt >> 1) & 1), err, 3)) break;
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      const int tn = (int)(t % tiles_n);
-      const int64_t rest = t / tiles_n;
-      const int tm = (int)(rest % tiles_m), z = (int)(rest / tiles_m);
-      const int m0 = tm * BM, n0 = tn * BN;
+      const TcTile tl = tiles.at(t);
+      if (kDirect) {
+        // rows >= m_valid / columns >= n_valid are not stored; a warp whose
+        // rows are all out of range skips its loads (the instruction is
+        // warp-collective, so the test is warp-uniform)
+        if (wq * 32 < tl.m_valid) {
+          const int m = wq * 32 + lane;
+          float *dst = D + tl.out_base + m;
 #pragma unroll 1
-      for (int c = 0; c < BN; c += EPI_COLS, ++nblk) {
-        unsigned char *buf = stage0 + (nblk & 1) * EPI_BUF;
-        // the store that last used this buffer has finished reading it
-        if (lane == 0) tc::bulk_wait_read1();
-        __syncwarp();
-        uint32_t v[32];
-        tc::tmem_ld32(tmem + ((uint32_t)(wq * 32) << 16) + (uint32_t)(ab * BN + c), v);
-        // row `lane`: 16-byte chunk q goes to chunk q ^ (lane % 8) (128B swizzle)
-        unsigned char *rowp = buf + lane * 128;
+          for (int c = 0; c < BN && c < tl.n_valid; c += EPI_COLS) {
+            uint32_t v[32];
+            tc::tmem_ld32(tmem + ((uint32_t)(wq * 32) << 16) + (uint32_t)(ab * BN + c), v);
+            const int nend = min(EPI_COLS, tl.n_valid - c);
+            // column scales: lane q holds cs[c + q], broadcast by shuffles
+            const float csl = (tl.cs && lane < nend) ? tl.cs[c + lane] : 1.f;
+            const bool row_ok = m < tl.m_valid;
+            const float r = (tl.rs && row_ok) ? tl.rs[m] : 1.f;
 #pragma unroll
-        for (int q = 0; q < 8; ++q) {
-          uint4 w = make_uint4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
-          *reinterpret_cast<uint4 *>(rowp + ((q ^ (lane & 7)) << 4)) = w;
+            for (int q = 0; q < EPI_COLS; ++q) {
+              const float cq = __shfl_sync(0xffffffffu, csl, q);
+              if (row_ok && q < nend)
+                dst[(int64_t)(c + q) * tl.col_stride] = __uint_as_float(v[q]) * r * cq;
+            }
+          }
         }
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        __syncwarp();
-        if (lane == 0) {
-          tc::tma_store_3d(&mD, buf, n0 + c, m0 + wq * 32, z);
-          tc::bulk_commit();
+      } else {
+        // TMEM -> registers -> 128B-swizzled smem -> TMA store; the store
+        // unit clips rows >= M and columns >= N
+#pragma unroll 1
+        for (int c = 0; c < BN; c += EPI_COLS, ++nblk) {
+          unsigned char *buf = stage0 + (nblk & 1) * EPI_BUF;
+          // the store that last used this buffer has finished reading it
+          if (lane == 0) tc::bulk_wait_read1();
+          __syncwarp();
+          uint32_t v[32];
+          tc::tmem_ld32(tmem + ((uint32_t)(wq * 32) << 16) + (uint32_t)(ab * BN + c), v);
+          // row `lane`: 16-byte chunk q goes to chunk q ^ (lane % 8) (128B swizzle)
+          unsigned char *rowp = buf + lane * 128;
+#pragma unroll
+          for (int q = 0; q < 8; ++q) {
+            uint4 w = make_uint4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+            *reinterpret_cast<uint4 *>(rowp + ((q ^ (lane & 7)) << 4)) = w;
+          }
+          asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+          __syncwarp();
+          if (lane == 0) {
+            tc::tma_store_3d(&mD, buf, tl.n0 + c, tl.m0 + wq * 32, tl.z);
+            tc::bulk_commit();
+          }
         }
       }
       // this thread's reads of the accumulator are complete
       asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
       mbar_arrive(&acc_empty[ab]);
     }
-    if (lane == 0) tc::bulk_wait_all();
+    if (!kDirect && lane == 0) tc::bulk_wait_all();
     __syncwarp();
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -388,8 +449,8 @@ struct TcGemm {
     if (!fn || q != cudaDriverEntryPointSuccess)
       throw Error{STD2G_ECUDA, "cuTensorMapEncodeTiled unavailable"};
     encode = (PFN_cuTensorMapEncodeTiled_v12000)fn;
-    S2G_CUDA(cudaFuncSetAttribute(k_tc_gemm_bf16x3, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  tc::SMEM_BYTES));
+    S2G_CUDA(cudaFuncSetAttribute(k_tc_gemm_bf16x3<GridTiles, false>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, tc::SMEM_BYTES));
     S2G_CUDA(cudaEventCreate(&e0));
     S2G_CUDA(cudaEventCreate(&e1));
     int dev = 0;
@@ -399,13 +460,14 @@ struct TcGemm {
   }
 
   // rows x Kpad BF16 matrices, `batch` of them `rows*Kpad` elements apart
-  CUtensorMap map(const __nv_bfloat16 *p, int64_t rows, int Kpad, int box_rows, int batch = 1) {
+  CUtensorMap map(const void *p, int64_t rows, int Kpad, int box_rows, int batch = 1,
+                  CUtensorMapDataType dt = CU_TENSOR_MAP_DATA_TYPE_BFLOAT16) {
     CUtensorMap m;
     cuuint64_t dims[3] = {(cuuint64_t)Kpad, (cuuint64_t)rows, (cuuint64_t)batch};
     cuuint64_t strides[2] = {(cuuint64_t)Kpad * 2, (cuuint64_t)rows * Kpad * 2};
     cuuint32_t box[3] = {(cuuint32_t)tc::BK, (cuuint32_t)box_rows, 1};
     cuuint32_t estr[3] = {1, 1, 1};
-    CUresult r = encode(&m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, (void *)p, dims, strides, box,
+    CUresult r = encode(&m, dt, 3, (void *)p, dims, strides, box,
                         estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
                         CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS)
@@ -459,8 +521,9 @@ struct TcGemm {
     const int cap = max_ctas > 0 ? std::min(max_ctas, nsm) : nsm;
     const int grid = (int)std::min<int64_t>(ntiles, cap);
     if (sync) S2G_CUDA(cudaEventRecord(e0, s));
-    S2G_LAUNCH(k_tc_gemm_bf16x3, grid, 256, tc::SMEM_BYTES, s, ah, al, bh, bl, dm, M, N, Kpad,
-               b_batched ? 1 : 0, batch, e);
+    const GridTiles tiles{M, N, batch, b_batched ? 1 : 0};
+    S2G_LAUNCH((k_tc_gemm_bf16x3<GridTiles, false>), grid, 256, tc::SMEM_BYTES, s, ah, al, bh, bl,
+               dm, tiles, (float *)nullptr, Kpad, e);
     ++launches;
     flop += nflop * batch;
     if (sync) {
@@ -470,6 +533,43 @@ struct TcGemm {
       S2G_CUDA(cudaEventElapsedTime(&t, e0, e1));
       ms += t;
     }
+  }
+
+  // D[tile.out_base + n*tile.col_stride + m] for the tiles of `tiles` (a
+  // schedule type with count() / at(), see TcTile): A (a_rows x Kpad) and B
+  // (b_rows x Kpad) split-BF16 operands read at the tiles' row coordinates;
+  // rows past the end of an operand read as zeros.  No synchronisation: the
+  // wait status is read by the next check().
+  // kF16: FP16 operands (scaled by the caller; the tiles' rs / cs undo it).
+  template <class Tiles, bool kF16 = false>
+  void run_direct(cudaStream_t s, const void *Ah, const void *Al, int64_t a_rows,
+                  const void *Bh, const void *Bl, int64_t b_rows, int Kpad, const Tiles &tiles,
+                  int64_t ntiles, float *D, double nflop) {
+    init();
+    if (ntiles <= 0) return;
+    if (Kpad % tc::BK != 0) throw Error{STD2G_EINVAL, "tc_gemm: K not padded to 64"};
+    if (((uintptr_t)Ah | (uintptr_t)Al | (uintptr_t)Bh | (uintptr_t)Bl) & 15)
+      throw Error{STD2G_EINVAL, "tc_gemm: operands not 16-byte aligned"};
+    if (a_rows >= (int64_t)1 << 31 || b_rows >= (int64_t)1 << 31)
+      throw Error{STD2G_EINVAL, "tc_gemm: operand rows beyond the TMA coordinate range"};
+    // per device and instantiation; a cheap host call, made every time
+    S2G_CUDA(cudaFuncSetAttribute(k_tc_gemm_bf16x3<Tiles, true, kF16>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, tc::SMEM_BYTES));
+    const CUtensorMapDataType dt =
+        kF16 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
+    CUtensorMap ah = map(Ah, a_rows, Kpad, tc::BM, 1, dt), al = map(Al, a_rows, Kpad, tc::BM, 1, dt);
+    CUtensorMap bh = map(Bh, b_rows, Kpad, tc::BN, 1, dt), bl = map(Bl, b_rows, Kpad, tc::BN, 1, dt);
+    int *e = err.ensure(1);
+    if (!armed) {
+      S2G_CUDA(cudaMemsetAsync(e, 0, sizeof(int), s));
+      armed = true;
+    }
+    const int cap = max_ctas > 0 ? std::min(max_ctas, nsm) : nsm;
+    const int grid = (int)std::min<int64_t>(ntiles, cap);
+    S2G_LAUNCH((k_tc_gemm_bf16x3<Tiles, true, kF16>), grid, 256, tc::SMEM_BYTES, s, ah, al, bh,
+               bl, ah, tiles, D, Kpad, e);
+    ++launches;
+    flop += nflop;
   }
 
   // read the error flag of the launches since the last check (synchronises)

@@ -15,8 +15,8 @@ LOG = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))),
 # = 64 registers); the tensor-core kernel runs one 256-thread CTA per SM.
 HOT = {
     "k_tc_gemm_bf16x3": 255,
-    "k_pt_rows32": 64,
-    "k_pt_cols32": 64,
+    "k_ptq_rows": 64,
+    "k_ptq_cols": 64,
     "k_charges_tiled": 64,
     "k_diag_screen": 64,
 }
