@@ -197,8 +197,12 @@ int std2g_solver_stats(void *ctx, int *iters, int64_t *matvecs, int64_t *matvecs
    this library keeps until the process exits; sizes with
    2N^2 + N(2no + nv) + 2 N no nv > 8 Mi doubles return STD2G_ECAP.  The first
    call on a device looks up that array's address (make it before any stream
-   capture).  All calls share the array, so calls whose kernels overlap on the
-   GPU race.  Kernels are queued on `stream` (a cudaStream_t, NULL = default). */
+   capture; several host threads may make it at once).  All calls share the
+   array, so calls whose kernels overlap on the GPU race.  Kernels are queued
+   on `stream` (a cudaStream_t, NULL = default).  The caller's current device
+   is restored on return; an error the caller left pending in the CUDA context
+   makes the call return STD2G_ECUDA without launching anything (the error is
+   left in place).  Not supported after a cudaDeviceReset by the host. */
 int std2g_screen_noalloc(int device, int ncent, int nao, int no, int nv, const double *d_xyz,
                          const int *d_iaoat, const double *d_clow, const double *d_eps,
                          const std2g_params *par, double *d_de, int *d_flag, void *stream);
@@ -261,7 +265,7 @@ int std2g_set_sm_limit(void *ctx, int max_sms);
 
 /* Diagnostic: lowest k eigenpairs of the symmetric n x n matrix A (host,
    column-major, lower triangle used) by the engine's single-block eigensolver
-   of the Davidson Rayleigh-Ritz step (n <= 235), and all eigenvalues by
+   of the Davidson Rayleigh-Ritz step (n <= 320), and all eigenvalues by
    cuSOLVER syevd for comparison.  w [k], Z [n*k], w_ref [n] (host).  No
    reference counterpart (the reference diagonalises with LAPACK ssyevr). */
 int std2g_symeig_check(int device, int n, int k, const double *A, double *w, double *Z,

@@ -132,14 +132,90 @@ __global__ void k_diag_matrix(double *__restrict__ H, int ld, int k, const doubl
   H[r + (int64_t)ld * c] = r == c ? th[r] : 0.0;
 }
 
-// d[j] = A[j + lda*j]
-__global__ void k_diag_of(const double *__restrict__ A, int lda, int n, double *__restrict__ d) {
-  int j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j < n) d[j] = A[j + (int64_t)lda * j];
+// Cholesky QR factor of a small Gram matrix, in one CTA: G = L L^T (nc x nc,
+// lower triangle read, nc <= kCholMax), then out = L^-T (upper triangular,
+// column-major nc x nc, zero below the diagonal) so that T L^-T has
+// orthonormal columns.  stat[0] = 1 when a pivot is not positive or its
+// square root falls below sqrt(tol) (the block is numerically dependent),
+// else 0; stat[1] = the smallest pivot (the diagonal of L).  Right-looking
+// factorisation, then one forward substitution per column of L^-1 (thread j
+// solves L x = e_j); deterministic.
+constexpr int kCholMax = 112;   // 2 nc^2 doubles of shared memory
+__global__ void __launch_bounds__(256)
+k_chol_inv(const double *__restrict__ G, int nc, double tol, double *__restrict__ out,
+           double *__restrict__ stat) {
+  extern __shared__ double sm[];
+  double *L = sm;               // column-major nc x nc
+  double *X = sm + nc * nc;     // X[j*nc + i] = (L^-1)[i][j]
+  __shared__ int fail;
+  __shared__ double dmin;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  for (int q = tid; q < nc * nc; q += nt) {
+    const int i = q % nc, j = q / nc;
+    L[q] = i >= j ? G[q] : 0.0;
+  }
+  if (tid == 0) {
+    fail = 0;
+    dmin = 1e300;
+  }
+  __syncthreads();
+  for (int j = 0; j < nc; ++j) {
+    if (tid == 0) {
+      const double d = L[j + nc * j];
+      if (!(d > 0.0) || !(d * d > 0.0) || !isfinite(d)) {
+        fail = 1;
+      } else {
+        const double r = sqrt(d);
+        L[j + nc * j] = r;
+        dmin = fmin(dmin, r);
+        if (!(r * r > tol)) fail = 1;
+      }
+    }
+    __syncthreads();
+    if (fail) break;
+    const double r = L[j + nc * j];
+    for (int i = j + 1 + tid; i < nc; i += nt) L[i + nc * j] /= r;
+    __syncthreads();
+    // trailing update of the lower triangle: columns l > j, rows i >= l
+    const int m = nc - j - 1;
+    for (int q = tid; q < m * m; q += nt) {
+      const int l = j + 1 + q / m, i = j + 1 + q % m;
+      if (i >= l) L[i + nc * l] -= L[i + nc * j] * L[l + nc * j];
+    }
+    __syncthreads();
+  }
+  if (fail) {
+    if (tid == 0) {
+      stat[0] = 1.0;
+      stat[1] = dmin;
+    }
+    return;
+  }
+  for (int j = tid; j < nc; j += nt) {
+    double *x = X + (size_t)j * nc;
+    for (int i = 0; i < j; ++i) x[i] = 0.0;
+    x[j] = 1.0 / L[j + nc * j];
+    for (int i = j + 1; i < nc; ++i) {
+      double acc = 0.0;
+      for (int k = j; k < i; ++k) acc += L[i + nc * k] * x[k];
+      x[i] = -acc / L[i + nc * i];
+    }
+  }
+  __syncthreads();
+  // out[r + nc*c] = (L^-1)[c][r] = X[r*nc + c]  (upper: r <= c)
+  for (int q = tid; q < nc * nc; q += nt) {
+    const int r = q % nc, c = q / nc;
+    out[q] = r <= c ? X[(size_t)r * nc + c] : 0.0;
+  }
+  if (tid == 0) {
+    stat[0] = 0.0;
+    stat[1] = dmin;
+  }
 }
 
 struct DavidsonWork {
-  DBuf<double> V, W, H, Hs, theta, X, R, T, tmp, rn, proj, G, Gc, lam, work2, part, eigwork;
+  DBuf<double> V, W, H, Hs, theta, X, R, T, tmp, rn, proj, G, Gc, Gz, lam, work2, part, eigwork,
+      stat;
   DBuf<int> cols, idx, info, einfo;
   DBuf<double> work;
   int iters = 0;
@@ -174,9 +250,9 @@ struct SectionClock {
 
 using MatVec = std::function<void(const double *V, int nb, double *W)>;
 
-// Rayleigh-Ritz problems up to this size go to symeig_small.cuh (measured
-// 0.39 / 0.94 ms at m = 64 / 128 against 0.88 / 2.1 ms for syevd); larger ones
-// to cuSOLVER syevd.
+// Rayleigh-Ritz problems up to this size go to the engine's own eigensolver
+// (symeig_small.cuh: 0.43 / 1.09 ms at m = 64 / 128 against 0.88 / 2.1 ms for
+// syevd); larger ones to cuSOLVER syevd.
 constexpr int kRRSmallMax = 128;
 
 // Returns the number of converged wanted roots (== k on success).  `mv` forms
@@ -317,44 +393,46 @@ inline int davidson(DavidsonWork &dw, cublasHandle_t blas, cusolverDnHandle_t so
         // G = Tb^T Tb; Cholesky QR when G is safely positive definite
         S2G_CUBLAS(cublasDgemm(blas, CUBLAS_OP_T, CUBLAS_OP_N, ncur, ncur, n, &one, Tb, n, Tb, n,
                                &zero, G, ncur));
-        {
-          double *Gc = dw.Gc.ensure((size_t)k * k);
-          S2G_CUDA(cudaMemcpyAsync(Gc, G, sizeof(double) * ncur * ncur, cudaMemcpyDeviceToDevice,
-                                   s));
-          int lwp = 0;
-          S2G_CUSOLVER(cusolverDnDpotrf_bufferSize(sol, CUBLAS_FILL_MODE_LOWER, ncur, Gc, ncur,
-                                                   &lwp));
-          double *wp = dw.work2.ensure((size_t)lwp + 1);
-          S2G_CUSOLVER(cusolverDnDpotrf(sol, CUBLAS_FILL_MODE_LOWER, ncur, Gc, ncur, wp, lwp,
-                                        info));
-          S2G_LAUNCH(k_diag_of, (int)div_up(ncur, 128), 128, 0, s, Gc, ncur, ncur, lam);
-          int h_info = 0;
-          std::vector<double> h_d(ncur);
-          S2G_CUDA(cudaMemcpyAsync(&h_info, info, sizeof(int), cudaMemcpyDeviceToHost, s));
-          S2G_CUDA(cudaMemcpyAsync(h_d.data(), lam, sizeof(double) * ncur, cudaMemcpyDeviceToHost,
-                                   s));
+        if (ncur <= kCholMax) {
+          // Cholesky QR: L^-T from the engine's small factorisation kernel
+          double *Li = dw.Gc.ensure((size_t)k * k), *st = dw.stat.ensure(2);
+          S2G_CUDA(cudaFuncSetAttribute(k_chol_inv, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)(2 * sizeof(double) * kCholMax * kCholMax)));
+          S2G_LAUNCH(k_chol_inv, 1, 256, 2 * sizeof(double) * ncur * ncur, s, G, ncur, 1e-8, Li,
+                     st);
+          double h_st[2];
+          S2G_CUDA(cudaMemcpyAsync(h_st, st, sizeof(h_st), cudaMemcpyDeviceToHost, s));
           S2G_CUDA(cudaStreamSynchronize(s));
-          double dmin = 1e300;
-          for (double v : h_d) dmin = std::min(dmin, v);
-          if (h_info == 0 && dmin * dmin > 1e-8) {
+          if (h_st[0] == 0.0) {
+            // dst <- Tb L^-T (through tmp when Tb already is dst)
             double *dst = V + (size_t)n * m;
-            if (Tb != dst)
-              S2G_CUDA(cudaMemcpyAsync(dst, Tb, sizeof(double) * n * ncur,
+            double *o = Tb == dst ? tmp : dst;
+            S2G_CUBLAS(cublasDgemm(blas, CUBLAS_OP_N, CUBLAS_OP_N, n, ncur, ncur, &one, Tb, n, Li,
+                                   ncur, &zero, o, n));
+            if (o != dst)
+              S2G_CUDA(cudaMemcpyAsync(dst, o, sizeof(double) * n * ncur,
                                        cudaMemcpyDeviceToDevice, s));
-            // dst <- dst L^-T
-            S2G_CUBLAS(cublasDtrsm(blas, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_T,
-                                   CUBLAS_DIAG_NON_UNIT, n, ncur, &one, Gc, ncur, dst, n));
             Tb = dst;
             continue;
           }
         }
         // eigenpairs of G ascending: drop dependent directions
-        int lw2 = 0;
-        S2G_CUSOLVER(cusolverDnDsyevd_bufferSize(sol, CUSOLVER_EIG_MODE_VECTOR,
-                                                 CUBLAS_FILL_MODE_LOWER, ncur, G, ncur, lam, &lw2));
-        double *work2 = dw.work2.ensure((size_t)lw2 + 1);
-        S2G_CUSOLVER(cusolverDnDsyevd(sol, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, ncur,
-                                      G, ncur, lam, work2, lw2, info));
+        if (ncur <= kRRSmallMax) {
+          double *Z = dw.Gz.ensure((size_t)k * k);
+          S2G_CUDA(cudaMemsetAsync(info, 0, sizeof(int), s));
+          symeig_small(s, G, ncur, ncur, ncur, lam, Z, ncur,
+                       dw.eigwork.ensure(symeig_work_doubles(ncur, ncur)), info);
+          S2G_CUDA(cudaMemcpyAsync(G, Z, sizeof(double) * ncur * ncur, cudaMemcpyDeviceToDevice,
+                                   s));
+        } else {
+          int lw2 = 0;
+          S2G_CUSOLVER(cusolverDnDsyevd_bufferSize(sol, CUSOLVER_EIG_MODE_VECTOR,
+                                                   CUBLAS_FILL_MODE_LOWER, ncur, G, ncur, lam,
+                                                   &lw2));
+          double *work2 = dw.work2.ensure((size_t)lw2 + 1);
+          S2G_CUSOLVER(cusolverDnDsyevd(sol, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER,
+                                        ncur, G, ncur, lam, work2, lw2, info));
+        }
         std::vector<double> h_lam(ncur);
         S2G_CUDA(cudaMemcpyAsync(h_lam.data(), lam, sizeof(double) * ncur, cudaMemcpyDeviceToHost,
                                  s));

@@ -17,6 +17,7 @@
 #include <cub/cub.cuh>
 
 #include "common.cuh"
+#include "eta_table.cuh"
 #include "kernels_fp64.cuh"
 #include "davidson.cuh"
 #include "matfree.cuh"
@@ -29,21 +30,6 @@ namespace std2g {
 
 std::atomic<int64_t> g_launches{0};
 
-static const double kEta[94] = {
-    0.472592880, 0.922033910, 0.174528880, 0.257007330, 0.339490860, 0.421954120, 0.504381930,
-    0.586918630, 0.669313510, 0.751916070, 0.179641050, 0.221572760, 0.263485780, 0.305396450,
-    0.347340140, 0.389247250, 0.431156700, 0.473082690, 0.171054690, 0.202762440, 0.210073220,
-    0.217396470, 0.224710390, 0.232015010, 0.239339690, 0.246656380, 0.253982550, 0.261288630,
-    0.268594760, 0.275925650, 0.307629990, 0.339315800, 0.372359850, 0.402735490, 0.434457760,
-    0.466117080, 0.155850790, 0.186493240, 0.193562100, 0.200633110, 0.207705220, 0.214772540,
-    0.221846140, 0.228918720, 0.235986210, 0.243056120, 0.250130180, 0.257199370, 0.287847800,
-    0.318486730, 0.349124310, 0.379765930, 0.410408080, 0.441057770, 0.050193320, 0.067625700,
-    0.085044450, 0.102477360, 0.119911050, 0.137327720, 0.154762970, 0.172182650, 0.189612880,
-    0.207047600, 0.224467520, 0.241896450, 0.259325030, 0.276760940, 0.294182310, 0.311595870,
-    0.329022740, 0.345922980, 0.363880480, 0.381305860, 0.398774760, 0.416142980, 0.433645100,
-    0.451040140, 0.468489860, 0.485845500, 0.125267300, 0.142686770, 0.160116150, 0.177558890,
-    0.194975570, 0.212407780, 0.072635250, 0.094221580, 0.099202950, 0.104186210, 0.142356330,
-    0.163942940, 0.185519410, 0.223701390};   // setrep, stda.f:2060-2167
 
 enum Phase {
   PH_SETUP = 0, PH_SQRTS, PH_MOINT, PH_CHARGES, PH_SCREEN, PH_PT, PH_BUILD, PH_EIGEN, PH_PROPS,

@@ -5,47 +5,49 @@
 // quantities std2g_solve forms internally before the PT selection (charges
 // q_ia, gamma^J / gamma^K, (ii|aa), (ia|ia)).  Unlike std2g_solve it calls no
 // cudaMalloc, cudaFree or library routine that allocates: its working arrays
-// live in one file-scope __device__ array of fixed size (kScratchBytes) that
-// every GPU loading this library keeps until the process exits.  It is meant
-// for hosts whose device memory is owned by another allocator (a framework
-// that has reserved the GPU's memory for its own pool) or that must not call
-// cudaMalloc at this point (it synchronises the device), and who hand in
-// device buffers they already own.
+// live in one file-scope __device__ array of fixed size (kScratchDoubles,
+// 64 MiB) that every GPU loading this library keeps until the process exits.
+// It is meant for hosts whose device memory is owned by another allocator (a
+// framework that has reserved the GPU's memory for its own pool) or that must
+// not call cudaMalloc at this point (it synchronises the device), and who hand
+// in device buffers they already own.  The array's device address is looked
+// up once per device and kept; a cudaDeviceReset by the host invalidates it,
+// so the entry point does not support hosts that reset the device.
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <mutex>
 
 #include "../../include/std2g.h"
+#include "eta_table.cuh"
 
 namespace {
 
 constexpr size_t kScratchDoubles = 8u << 20;   // 64 MiB
-constexpr size_t kScratchBytes = kScratchDoubles * sizeof(double);
 constexpr int kMaxDevices = 64;
 
 // Shared by every call on a device; it keeps the last call's contents.
 static __device__ __align__(256) double g_noalloc_scratch[kScratchDoubles];
 
-// Device address of g_noalloc_scratch per device (set-up on first use).
+// Device address of g_noalloc_scratch per device, looked up once per device
+// (std::call_once: several host threads may make the first call at once).
 static double *g_scratch_ptr[kMaxDevices] = {nullptr};
+static cudaError_t g_setup_status[kMaxDevices];
+static std::once_flag g_setup_once[kMaxDevices];
 
-const double kEta[94] = {
-    0.472592880, 0.922033910, 0.174528880, 0.257007330, 0.339490860, 0.421954120, 0.504381930,
-    0.586918630, 0.669313510, 0.751916070, 0.179641050, 0.221572760, 0.263485780, 0.305396450,
-    0.347340140, 0.389247250, 0.431156700, 0.473082690, 0.171054690, 0.202762440, 0.210073220,
-    0.217396470, 0.224710390, 0.232015010, 0.239339690, 0.246656380, 0.253982550, 0.261288630,
-    0.268594760, 0.275925650, 0.307629990, 0.339315800, 0.372359850, 0.402735490, 0.434457760,
-    0.466117080, 0.155850790, 0.186493240, 0.193562100, 0.200633110, 0.207705220, 0.214772540,
-    0.221846140, 0.228918720, 0.235986210, 0.243056120, 0.250130180, 0.257199370, 0.287847800,
-    0.318486730, 0.349124310, 0.379765930, 0.410408080, 0.441057770, 0.050193320, 0.067625700,
-    0.085044450, 0.102477360, 0.119911050, 0.137327720, 0.154762970, 0.172182650, 0.189612880,
-    0.207047600, 0.224467520, 0.241896450, 0.259325030, 0.276760940, 0.294182310, 0.311595870,
-    0.329022740, 0.345922980, 0.363880480, 0.381305860, 0.398774760, 0.416142980, 0.433645100,
-    0.451040140, 0.468489860, 0.485845500, 0.125267300, 0.142686770, 0.160116150, 0.177558890,
-    0.194975570, 0.212407780, 0.072635250, 0.094221580, 0.099202950, 0.104186210, 0.142356330,
-    0.163942940, 0.185519410, 0.223701390};
+// hardness table in constant memory, initialised with the module
+__constant__ double c_eta[std2g::kEtaElements] = {STD2G_ETA_VALUES};
 
-__constant__ double c_eta[94];
+// Restores the caller's current device when the entry point returns.
+struct DeviceGuard {
+  int prev = -1;
+  DeviceGuard() {
+    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+  }
+  ~DeviceGuard() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+};
 
 // gamma^J and gamma^K (stda.f:509-532) from xyz(4,ncent)
 __global__ void na_gamma(const double *__restrict__ xyz, int n, double ax, double alpha,
@@ -58,8 +60,8 @@ __global__ void na_gamma(const double *__restrict__ xyz, int n, double ax, doubl
            dz = xyz[4 * i + 2] - xyz[4 * j + 2];
     double r = sqrt(dx * dx + dy * dy + dz * dz);
     int zi = (int)llrint(xyz[4 * i + 3]), zj = (int)llrint(xyz[4 * j + 3]);
-    zi = zi < 1 ? 1 : (zi > 94 ? 94 : zi);   // table range; callers pass Z in 1..94
-    zj = zj < 1 ? 1 : (zj > 94 ? 94 : zj);
+    zi = zi < 1 ? 1 : (zi > std2g::kEtaElements ? std2g::kEtaElements : zi);   // table range
+    zj = zj < 1 ? 1 : (zj > std2g::kEtaElements ? std2g::kEtaElements : zj);
     double eb = 0.5 * (c_eta[zi - 1] + c_eta[zj - 1]);
     double xj = eb * ax;
     gj[t] = xj > 0.0 ? 1.0 / pow(pow(r, beta) + 1.0 / pow(xj, beta), 1.0 / beta) : 0.0;
@@ -160,17 +162,22 @@ extern "C" int std2g_screen_noalloc(int device, int ncent, int nao, int no, int 
   // scratch layout (doubles): gj, gk (N^2 each), Qii, Pii (N*no), Qaa (N*nv), Qia, Pia (N*nov)
   const int64_t need = 2 * (int64_t)N * N + 2 * (int64_t)N * no + (int64_t)N * nv + 2 * N * nov;
   if (need > (int64_t)kScratchDoubles) return STD2G_ECAP;   // larger than the fixed scratch
+  DeviceGuard guard;   // the caller's current device is restored on every return
   if (cudaSetDevice(device) != cudaSuccess) return STD2G_ENODEV;
-  cudaStream_t s = (cudaStream_t)stream;
-  if (!g_scratch_ptr[device]) {
-    // one-time set-up on this device: device address of the scratch array and
-    // the hardness table (first call on a device; make it before any capture)
+  // an error the caller left pending is not ours to report or to clear
+  if (cudaPeekAtLastError() != cudaSuccess) return STD2G_ECUDA;
+  std::call_once(g_setup_once[device], [device] {
+    // one-time set-up on this device, with the device current: the device
+    // address of the scratch array (the first call on a device does it; make
+    // that call before any stream capture)
     double *p = nullptr;
-    if (cudaGetSymbolAddress((void **)&p, g_noalloc_scratch) != cudaSuccess || !p)
-      return STD2G_ECUDA;
-    if (cudaMemcpyToSymbol(c_eta, kEta, sizeof(kEta)) != cudaSuccess) return STD2G_ECUDA;
-    g_scratch_ptr[device] = p;
-  }
+    cudaError_t e = cudaGetSymbolAddress((void **)&p, g_noalloc_scratch);
+    if (e == cudaSuccess && !p) e = cudaErrorInvalidSymbol;
+    g_setup_status[device] = e;
+    if (e == cudaSuccess) g_scratch_ptr[device] = p;
+  });
+  if (g_setup_status[device] != cudaSuccess) return STD2G_ECUDA;
+  cudaStream_t s = (cudaStream_t)stream;
   double *base = g_scratch_ptr[device];
   double *gj = base, *gk = gj + (int64_t)N * N, *Qii = gk + (int64_t)N * N;
   double *Pii = Qii + (int64_t)N * no, *Qaa = Pii + (int64_t)N * no, *Qia = Qaa + (int64_t)N * nv;
@@ -183,16 +190,29 @@ extern "C" int std2g_screen_noalloc(int device, int ncent, int nao, int no, int 
   const double ak = par->triplet ? 0.0 : 2.0;
   const double thr = par->e_thr_ev / 27.211385050;
   const double fthr = par->fthr_ev < 1.79e308 ? par->fthr_ev / 27.211385050 : INFINITY;
+  // each launch's configuration error is checked where it happens
+#define NA_CHECK()                                                               \
+  do {                                                                           \
+    if (cudaGetLastError() != cudaSuccess) return STD2G_ECUDA;                   \
+  } while (0)
   na_gamma<<<grid_of((int64_t)N * N), 256, 0, s>>>(d_xyz, N, ax, alpha, beta, gj, gk);
+  NA_CHECK();
   na_charges<<<grid_of((int64_t)N * no), 256, 0, s>>>(Qii, d_clow, nao, N, d_iaoat, 0, no, 0, no, 1);
+  NA_CHECK();
   na_charges<<<grid_of((int64_t)N * nv), 256, 0, s>>>(Qaa, d_clow, nao, N, d_iaoat, no, nv, no, nv,
                                                       1);
+  NA_CHECK();
   na_charges<<<grid_of(N * nov), 256, 0, s>>>(Qia, d_clow, nao, N, d_iaoat, 0, no, no, nv, 0);
+  NA_CHECK();
   na_gamma_apply<<<grid_of((int64_t)N * no), 256, 0, s>>>(Pii, gj, Qii, N, no);
+  NA_CHECK();
   na_gamma_apply<<<grid_of(N * nov), 256, 0, s>>>(Pia, gk, Qia, N, nov);
+  NA_CHECK();
   na_screen<<<grid_of(nov * 32), 256, 0, s>>>(Pia, Qia, Pii, Qaa, N, no, nv, d_eps, ak, par->kshift,
                                               par->shftmax * 0.036749320,
                                               par->shftwidth * 0.036749320, par->shftsteep, thr,
                                               fthr, d_de, d_flag);
-  return cudaGetLastError() == cudaSuccess ? STD2G_OK : STD2G_ECUDA;
+  NA_CHECK();
+#undef NA_CHECK
+  return STD2G_OK;
 }

@@ -14,12 +14,13 @@
 // scales (exact).  The couplings are written for one chunk of candidate occupied
 // indices i in [i0, i0 + ni) into two FP32 buffers of the same layout
 //
-//     X[(q * ni + (i - i0)) * nva + a]          (nva = nv rounded up to 32)
+//     X[((i - i0) * nex + q) * nva + a]          (nva = nv rounded up to 32)
 //
-// so that both passes over them read 128 contiguous bytes per warp:
+// so that both passes over them sweep contiguous memory (rows of nva values
+// for consecutive q):
 //   (ia|jb): for each i, rows a (p_ia) times columns q (q_jb);
 //   (ij|ab): grouped by the primaries' virtual index b -- rows a of the slab
-//            q_ab (b fixed) times columns (q, i) with j = j_q (p_ij) -- so
+//            q_ab (b fixed) times columns (i, q) with j = j_q (p_ij) -- so
 //            only the (i, a, q) combinations the sums need are formed.
 // The primaries are taken in (b, j) order so that each group's columns are
 // contiguous.
@@ -66,7 +67,8 @@ inline float coupling_error_bound(int Kpad) {
 //     chunk's p_ia, B rows qb*128 of the primaries' q.
 //   mode 1, (ij|ab): group g (virtual b of the primaries qs[g] .. qs[g]+nq[g]),
 //     tile (ab, nb), nb fastest; A rows g*nv + ab*128 of the q_ab slabs, B rows
-//     qs[g]*ni + nb*128 of p_{i j_q} laid out as (q * ni + ii).
+//     qs[g]*ni + nb*128 of p_{i j_q}, whose rows are grouped the same way and
+//     ordered (ii, q) within a group: row qs[g]*ni + ii*nq[g] + (q - qs[g]).
 // Rows of a tile past nv (or past the end of a group's columns) read the next
 // rows of the operand or zeros; they are not stored.
 struct PairTiles {
@@ -86,8 +88,8 @@ struct PairTiles {
       x.b_y = qb * tc::BN;
       x.m_valid = min(tc::BM, nv - ab * tc::BM);
       x.n_valid = min(tc::BN, nex - qb * tc::BN);
-      x.out_base = ((int64_t)qb * tc::BN * ni + ii) * nva + ab * tc::BM;
-      x.col_stride = (int64_t)ni * nva;
+      x.out_base = ((int64_t)ii * nex + qb * tc::BN) * nva + ab * tc::BM;
+      x.col_stride = nva;
       x.rs = a_inv + x.a_y;
       x.cs = b_inv + x.b_y;
     } else {
@@ -105,8 +107,13 @@ struct PairTiles {
       x.b_y = qs * ni + nb * tc::BN;
       x.m_valid = min(tc::BM, nv - ab * tc::BM);
       x.n_valid = min(tc::BN, ncol - nb * tc::BN);
-      x.out_base = ((int64_t)qs * ni + nb * tc::BN) * nva + ab * tc::BM;
+      // column n = ii * nq + (q - qs) of the group
+      const int nq = g_nq[g], n0 = nb * tc::BN, ii0 = n0 / nq, qq0 = n0 - ii0 * nq;
+      x.out_base = ((int64_t)ii0 * nex + qs + qq0) * nva + ab * tc::BM;
       x.col_stride = nva;
+      x.run_len = nq;
+      x.run_pos = qq0;
+      x.run_skip = ((int64_t)nex - (nq - 1)) * nva;
       x.rs = a_inv + x.a_y;
       x.cs = b_inv + x.b_y;
     }
@@ -123,40 +130,73 @@ __device__ __forceinline__ void split_f16(double x, double sc, __half &hi, __hal
 }
 
 // Operand rows c = 0..ncols-1: column idx[c] (or c) of an Nk-row FP64 matrix
-// (ld), scaled by 1 / inv[c], as FP16 hi / lo rows of Kpad (zero padded)
-__global__ void k_split_f16s(__half *__restrict__ hi, __half *__restrict__ lo,
-                             const double *__restrict__ src, int64_t ld, const int *__restrict__ idx,
-                             const float *__restrict__ inv, int64_t ncols, int Nk, int Kpad) {
-  const int64_t total = ncols * Kpad;
-  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
-       t += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t c = t / Kpad;
-    const int k = (int)(t - c * Kpad);
-    double x = 0.0;
-    if (k < Nk) x = src[(idx ? (int64_t)idx[c] : c) * ld + k];
-    split_f16(x, (double)__frcp_rn(inv[c]), hi[t], lo[t]);   // exact: inv is a power of 2
+// (ld), scaled by 1 / inv[c], as FP16 hi / lo rows of Kpad (zero padded).
+// One block of 64 threads per row (grid.x = rows, grid.y covers the rest), two
+// consecutive elements per thread and step.
+constexpr int kSplitThreads = 64;
+__global__ void __launch_bounds__(kSplitThreads)
+k_split_f16s(__half *__restrict__ hi, __half *__restrict__ lo, const double *__restrict__ src,
+             int64_t ld, const int *__restrict__ idx, const float *__restrict__ inv,
+             int64_t ncols, int Nk, int Kpad) {
+  for (int64_t c = blockIdx.x + (int64_t)blockIdx.y * gridDim.x; c < ncols;
+       c += (int64_t)gridDim.x * gridDim.y) {
+    const double *x = src + (idx ? (int64_t)idx[c] : c) * ld;
+    const double sc = (double)__frcp_rn(inv[c]);   // exact: inv is a power of 2
+    __half2 *h2 = reinterpret_cast<__half2 *>(hi + c * Kpad);
+    __half2 *l2 = reinterpret_cast<__half2 *>(lo + c * Kpad);
+    for (int k2 = threadIdx.x; 2 * k2 < Kpad; k2 += kSplitThreads) {
+      const int k = 2 * k2;
+      __half a0, a1, b0, b1;
+      split_f16(k < Nk ? x[k] : 0.0, sc, a0, b0);
+      split_f16(k + 1 < Nk ? x[k + 1] : 0.0, sc, a1, b1);
+      h2[k2] = __halves2half2(a0, a1);
+      l2[k2] = __halves2half2(b0, b1);
+    }
   }
 }
 
-// p_{i j_q} for the chunk, row t = q * ni + ii (source: column (i0 + ii) * no
-// + j_q of Poo, N values), scaled; wsc[t] = 1 / scale of that row
-__global__ void k_split_wexp(__half *__restrict__ hi, __half *__restrict__ lo,
-                             const double *__restrict__ Poo, int N, const int *__restrict__ jq,
-                             const float *__restrict__ winv, int nex, int ni, int i0, int no,
-                             int Kpad, float *__restrict__ wsc) {
-  const int64_t total = (int64_t)nex * ni * Kpad;
-  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
-       t += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t row = t / Kpad;
-    const int k = (int)(t - row * Kpad);
-    const int q = (int)(row / ni), ii = (int)(row - (int64_t)q * ni);
+// p_{i j_q} for the chunk, scaled, in the row order of the (ij|ab) tiles:
+// row qs[g]*ni + ii*nq[g] + (q - qs[g]) for the primaries q of group g
+// (source: column (i0 + ii) * no + j_q of Poo, N values); wsc[row] = 1 / scale
+__global__ void __launch_bounds__(kSplitThreads)
+k_split_wexp(__half *__restrict__ hi, __half *__restrict__ lo, const double *__restrict__ Poo,
+             int N, const int *__restrict__ jq, const float *__restrict__ winv, int nex, int ni,
+             int i0, int no, int Kpad, const int *__restrict__ g_qs,
+             const int *__restrict__ g_nq, int ngroups, float *__restrict__ wsc) {
+  const int64_t rows = (int64_t)nex * ni;
+  for (int64_t row = blockIdx.x + (int64_t)blockIdx.y * gridDim.x; row < rows;
+       row += (int64_t)gridDim.x * gridDim.y) {
+    int lo_g = 0, hi_g = ngroups;   // g_qs[lo_g] * ni <= row < g_qs[hi_g] * ni
+    while (hi_g - lo_g > 1) {
+      const int mid = (lo_g + hi_g) >> 1;
+      if ((int64_t)g_qs[mid] * ni <= row) lo_g = mid;
+      else hi_g = mid;
+    }
+    const int qs = g_qs[lo_g], nq = g_nq[lo_g];
+    const int rel = (int)(row - (int64_t)qs * ni), ii = rel / nq, q = qs + (rel - ii * nq);
     const int64_t col = (int64_t)(i0 + ii) * no + jq[q];
     const float iv = winv[col];
-    double x = 0.0;
-    if (k < N) x = Poo[col * N + k];
-    split_f16(x, (double)__frcp_rn(iv), hi[t], lo[t]);   // exact: iv is a power of 2
-    if (k == 0) wsc[row] = iv;
+    const double sc = (double)__frcp_rn(iv);   // exact: iv is a power of 2
+    const double *x = Poo + col * N;
+    __half2 *h2 = reinterpret_cast<__half2 *>(hi + row * Kpad);
+    __half2 *l2 = reinterpret_cast<__half2 *>(lo + row * Kpad);
+    for (int k2 = threadIdx.x; 2 * k2 < Kpad; k2 += kSplitThreads) {
+      const int k = 2 * k2;
+      __half a0, a1, b0, b1;
+      split_f16(k < N ? x[k] : 0.0, sc, a0, b0);
+      split_f16(k + 1 < N ? x[k + 1] : 0.0, sc, a1, b1);
+      h2[k2] = __halves2half2(a0, a1);
+      l2[k2] = __halves2half2(b0, b1);
+    }
+    if (threadIdx.x == 0) wsc[row] = iv;
   }
+}
+
+// grid of the split kernels for `rows` operand rows
+inline dim3 split_grid(int64_t rows) {
+  const int64_t gx = std::min<int64_t>(rows, 65535);
+  const int64_t gy = std::min<int64_t>(div_up(rows, gx), 64);
+  return dim3((unsigned)gx, (unsigned)gy);
 }
 
 // For column x_c = column idx[c] (or c) of an N-row FP64 matrix (one warp per
@@ -223,9 +263,9 @@ k_ptq_rows(const float *__restrict__ K, const float *__restrict__ J, int ni, int
   if (z == 0 && live) rhl[ii * nv + a] = make_float2(rh, rl);
   const float pr = pn[k];
   double acc_t = 0.0, acc_b = 0.0;
-  const int64_t cstride = (int64_t)ni * nva;
-  const float *Kp = K + ((int64_t)q0 * ni + ii) * nva + (live ? a : 0);
-  const float *Jp = J + ((int64_t)q0 * ni + ii) * nva + (live ? a : 0);
+  const int64_t cstride = nva;   // next primary
+  const float *Kp = K + ((int64_t)ii * nex + q0) * nva + (live ? a : 0);
+  const float *Jp = J + ((int64_t)ii * nex + q0) * nva + (live ? a : 0);
   for (int s0 = q0; s0 < q1; s0 += kRowStage) {
     const int ns = min(kRowStage, q1 - s0);
     __syncthreads();
@@ -249,14 +289,16 @@ k_ptq_rows(const float *__restrict__ K, const float *__restrict__ J, int ni, int
           const float vv = vn[(int64_t)s_g[t] * nv + a];
           const float am = akf * kv - jv;
           const float den = (rh - s_eh[t]) + (rl - s_el[t]);
-          const float tt = am * am / den;
+          const float rden = __frcp_rn(den);   // correctly rounded
+          const float tt = am * am * rden;
           // coupling error (Cauchy-Schwarz) plus the FP32 rounding of am
           const float da = ecoup * (akf * pr * s_qn[t] + s_wn[t] * vv) +
                            2.f * kU32 * (akf * fabsf(kv) + fabsf(jv));
-          // denominator: FP32 rounding and the hi/lo representation of both energies
-          const float ed = 4.f * kU32 + 3e-14f / den;
+          // denominator: FP32 rounding and the hi/lo representation of both
+          // energies; term: reciprocal and two products (4 roundings)
+          const float ed = 4.f * kU32 + 3e-14f * rden;
           const float bt = den > 0.f && ed < 0.25f
-                               ? (2.f * fabsf(am) * da + da * da) / den + tt * (2.f * ed + 4.f * kU32)
+                               ? (2.f * fabsf(am) * da + da * da) * rden + tt * (2.f * ed + 6.f * kU32)
                                : INFINITY;
           gt += tt;
           gb += bt;
@@ -334,17 +376,17 @@ k_ptq_cols(const float *__restrict__ K, const float *__restrict__ J, int ni, int
     elq[u] = el[q];
     acc[u] = 0.0;
   }
-  const int64_t cstride = (int64_t)ni * nva;
+  const int64_t cstride = nva;   // next primary
   for (int ii = warp; ii < ni; ii += 8) {
     for (int a = lane; a < nv; a += 32) {
       if (!use[ii * nv + a]) continue;
       const float2 r = rhl[ii * nv + a];
-      const int64_t o = ((int64_t)q0 * ni + ii) * nva + a;
+      const int64_t o = ((int64_t)ii * nex + q0) * nva + a;
 #pragma unroll
       for (int u = 0; u < kColQ; ++u) {
         if (q0 + u < nex) {
           const float am = akf * K[o + u * cstride] - J[o + u * cstride];
-          acc[u] += (double)(am * am / ((r.x - ehq[u]) + (r.y - elq[u])));
+          acc[u] += (double)(am * am * __frcp_rn((r.x - ehq[u]) + (r.y - elq[u])));
         }
       }
     }
@@ -541,8 +583,8 @@ inline void mixed_pt_select(MixedWork &mw, cudaStream_t s, const PtProblem &pb,
   auto split = [&](DBuf<__half> &h, DBuf<__half> &l, const double *src, const int *idx,
                    const float *inv, int64_t ncols) {
     __half *ph = h.ensure((size_t)ncols * Kpad + 64), *pl = l.ensure((size_t)ncols * Kpad + 64);
-    const int g = (int)std::min<int64_t>(div_up(ncols * Kpad, 256), 148 * 32);
-    S2G_LAUNCH(k_split_f16s, g, 256, 0, s, ph, pl, src, (int64_t)N, idx, inv, ncols, N, Kpad);
+    S2G_LAUNCH(k_split_f16s, split_grid(ncols), kSplitThreads, 0, s, ph, pl, src, (int64_t)N, idx,
+               inv, ncols, N, Kpad);
   };
   split(mw.q_hi, mw.q_lo, pb.Qia, d_pk, mw.qinv.get(), nex);
   split(mw.v_hi, mw.v_lo, pb.Qvv, d_vidx, mw.vinv.get(), (int64_t)ng * nv);
@@ -573,9 +615,8 @@ inline void mixed_pt_select(MixedWork &mw, cudaStream_t s, const PtProblem &pb,
     {
       __half *h = mw.w_hi.ensure((size_t)rows_w * Kpad + 64),
              *l = mw.w_lo.ensure((size_t)rows_w * Kpad + 64);
-      const int g = (int)std::min<int64_t>(div_up(rows_w * Kpad, 256), 148 * 32);
-      S2G_LAUNCH(k_split_wexp, g, 256, 0, s, h, l, pb.Poo, N, d_jq, mw.winv.get(), nex, ni, i0,
-                 no, Kpad, wsc);
+      S2G_LAUNCH(k_split_wexp, split_grid(rows_w), kSplitThreads, 0, s, h, l, pb.Poo, N, d_jq,
+                 mw.winv.get(), nex, ni, i0, no, Kpad, d_qs, d_nq, ng, wsc);
     }
     std::vector<int> tile0(ng + 1, 0);
     for (int g = 0; g < ng; ++g)

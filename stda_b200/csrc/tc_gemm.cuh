@@ -202,7 +202,13 @@ struct TcTile {
   int a_y, a_z, b_y, b_z;        // TMA row / batch coordinates of the A and B tiles
   int m0, n0, z;                 // TMA-store epilogue: origin of the output tile
   int m_valid, n_valid;          // direct-store epilogue: rows / columns kept
-  int64_t out_base, col_stride;  // direct-store epilogue: D[out_base + n*col_stride + m]
+  // direct-store epilogue: column n of the tile goes to D + out_base + m plus
+  // n * col_stride, except that the columns form runs of run_len (0: one run):
+  // the step from the last column of a run to the first of the next is
+  // run_skip instead of col_stride; the tile's first column is run_pos within
+  // its run
+  int64_t out_base, col_stride, run_skip;
+  int run_len, run_pos;
   const float *rs, *cs;          // direct-store epilogue: D *= rs[m] * cs[n] (when set)
 };
 
@@ -351,7 +357,8 @@ k_tc_gemm_bf16x3(const __grid_constant__ CUtensorMap mAh, const __grid_constant_
         // warp-collective, so the test is warp-uniform)
         if (wq * 32 < tl.m_valid) {
           const int m = wq * 32 + lane;
-          float *dst = D + tl.out_base + m;
+          float *dst = D + tl.out_base + m;   // column c of the tile (advanced below)
+          int rpos = tl.run_pos;
 #pragma unroll 1
           for (int c = 0; c < BN && c < tl.n_valid; c += EPI_COLS) {
             uint32_t v[32];
@@ -364,8 +371,13 @@ k_tc_gemm_bf16x3(const __grid_constant__ CUtensorMap mAh, const __grid_constant_
 #pragma unroll
             for (int q = 0; q < EPI_COLS; ++q) {
               const float cq = __shfl_sync(0xffffffffu, csl, q);
-              if (row_ok && q < nend)
-                dst[(int64_t)(c + q) * tl.col_stride] = __uint_as_float(v[q]) * r * cq;
+              if (row_ok && q < nend) *dst = __uint_as_float(v[q]) * r * cq;
+              if (tl.run_len > 0 && ++rpos == tl.run_len) {
+                rpos = 0;
+                dst += tl.run_skip;
+              } else {
+                dst += tl.col_stride;
+              }
             }
           }
         }
