@@ -240,11 +240,13 @@ struct PtCols {
 
 constexpr int kRowThreads = 128;
 constexpr int kRowStage = 256;   // primaries staged in shared memory at a time
+constexpr int kRowBatch = 8;     // primaries whose loads are issued together
 
 // Partial PT sums of the candidate rows (ii, a) over primaries
 // [z * qlen, (z + 1) * qlen): part_t[z][ii * nv + a] = sum of the terms,
 // part_b[z][...] = bound on the error of that sum.  Terms are formed in FP32
-// and summed in groups of eight before the FP64 accumulation.
+// and summed in groups of kRowBatch before the FP64 accumulation; each group's
+// loads are issued before any of its arithmetic (memory-level parallelism).
 __global__ void __launch_bounds__(kRowThreads)
 k_ptq_rows(const float *__restrict__ K, const float *__restrict__ J, int ni, int nv, int nva,
            int nex, int qlen, int no, int i0, const double *__restrict__ de_all,
@@ -257,15 +259,15 @@ k_ptq_rows(const float *__restrict__ K, const float *__restrict__ J, int ni, int
   const int ii = blockIdx.y, z = blockIdx.z;
   const int q0 = z * qlen, q1 = min(nex, q0 + qlen);
   const bool live = a < nv;
-  const int64_t k = (int64_t)(i0 + ii) * nv + (live ? a : 0);
+  const int al = live ? a : 0;
+  const int64_t k = (int64_t)(i0 + ii) * nv + al;
   const double d = de_all[k] + 1e-10;
   const float rh = (float)d, rl = (float)(d - (double)rh);
   if (z == 0 && live) rhl[ii * nv + a] = make_float2(rh, rl);
   const float pr = pn[k];
   double acc_t = 0.0, acc_b = 0.0;
-  const int64_t cstride = nva;   // next primary
-  const float *Kp = K + ((int64_t)ii * nex + q0) * nva + (live ? a : 0);
-  const float *Jp = J + ((int64_t)ii * nex + q0) * nva + (live ? a : 0);
+  const float *Kp = K + ((int64_t)ii * nex + q0) * nva + al;
+  const float *Jp = J + ((int64_t)ii * nex + q0) * nva + al;
   for (int s0 = q0; s0 < q1; s0 += kRowStage) {
     const int ns = min(kRowStage, q1 - s0);
     __syncthreads();
@@ -278,28 +280,34 @@ k_ptq_rows(const float *__restrict__ K, const float *__restrict__ J, int ni, int
       s_g[t] = cols.gq[q];
     }
     __syncthreads();
-    if (!live) continue;
-    for (int t0 = 0; t0 < ns; t0 += 8) {
+    for (int t0 = 0; t0 < ns; t0 += kRowBatch) {
+      const int nb = min(kRowBatch, ns - t0);
+      float kv[kRowBatch], jv[kRowBatch], vv[kRowBatch];
+#pragma unroll
+      for (int u = 0; u < kRowBatch; ++u) {   // all loads of the batch first
+        const int t = t0 + (u < nb ? u : 0);
+        kv[u] = Kp[(int64_t)t * nva];
+        jv[u] = Jp[(int64_t)t * nva];
+        vv[u] = vn[(int64_t)s_g[t] * nv + al];
+      }
       float gt = 0.f, gb = 0.f;
 #pragma unroll
-      for (int u = 0; u < 8; ++u) {
+      for (int u = 0; u < kRowBatch; ++u) {
         const int t = t0 + u;
-        if (t < ns) {
-          const float kv = Kp[(int64_t)t * cstride], jv = Jp[(int64_t)t * cstride];
-          const float vv = vn[(int64_t)s_g[t] * nv + a];
-          const float am = akf * kv - jv;
-          const float den = (rh - s_eh[t]) + (rl - s_el[t]);
-          const float rden = __frcp_rn(den);   // correctly rounded
-          const float tt = am * am * rden;
-          // coupling error (Cauchy-Schwarz) plus the FP32 rounding of am
-          const float da = ecoup * (akf * pr * s_qn[t] + s_wn[t] * vv) +
-                           2.f * kU32 * (akf * fabsf(kv) + fabsf(jv));
-          // denominator: FP32 rounding and the hi/lo representation of both
-          // energies; term: reciprocal and two products (4 roundings)
-          const float ed = 4.f * kU32 + 3e-14f * rden;
-          const float bt = den > 0.f && ed < 0.25f
-                               ? (2.f * fabsf(am) * da + da * da) * rden + tt * (2.f * ed + 6.f * kU32)
-                               : INFINITY;
+        const float am = akf * kv[u] - jv[u];
+        const float den = (rh - s_eh[t < ns ? t : t0]) + (rl - s_el[t < ns ? t : t0]);
+        const float rden = __frcp_rn(den);   // correctly rounded
+        const float tt = am * am * rden;
+        // coupling error (Cauchy-Schwarz) plus the FP32 rounding of am
+        const float da = ecoup * (akf * pr * s_qn[t < ns ? t : t0] + s_wn[t < ns ? t : t0] * vv[u]) +
+                         2.f * kU32 * (akf * fabsf(kv[u]) + fabsf(jv[u]));
+        // denominator: FP32 rounding and the hi/lo representation of both
+        // energies; term: reciprocal and two products (4 roundings)
+        const float ed = 4.f * kU32 + 3e-14f * rden;
+        const float bt = den > 0.f && ed < 0.25f
+                             ? (2.f * fabsf(am) * da + da * da) * rden + tt * (2.f * ed + 6.f * kU32)
+                             : INFINITY;
+        if (u < nb) {
           gt += tt;
           gb += bt;
         }
@@ -307,8 +315,8 @@ k_ptq_rows(const float *__restrict__ K, const float *__restrict__ J, int ni, int
       acc_t += (double)gt;
       acc_b += (double)gb;
     }
-    Kp += (int64_t)ns * cstride;
-    Jp += (int64_t)ns * cstride;
+    Kp += (int64_t)ns * nva;
+    Jp += (int64_t)ns * nva;
   }
   if (live) {
     part_t[(int64_t)z * ni * nv + ii * nv + a] = acc_t;
@@ -354,13 +362,16 @@ __global__ void k_ptq_use(int ni, int nv, int i0, const int *__restrict__ cand_p
 }
 
 // ---------------------------------------------------------------- column pass
-constexpr int kColQ = 4;   // primaries per block
+constexpr int kColQ = 4;     // primaries per block
+constexpr int kColRows = 4;  // candidate rows per thread and step (loads issued together)
 
 // colpart[q] = sum over the non-selected candidates (ii, a) of the chunk of
-// the terms t_(ii,a),q, for kColQ primaries per block: warp w takes rows
-// ii = w, w + 8, ..., lanes take a; per-thread FP64 sums, then a fixed-order
-// warp and block reduction (deterministic).
-__global__ void __launch_bounds__(256)
+// the terms t_(ii,a),q, for kColQ primaries per block: the block's threads
+// walk the chunk's (ii, a) rows (a fastest), kColRows at a time with all their
+// loads issued first, terms of rows that are not summed multiplied by zero;
+// per-thread FP64 sums, then a fixed-order warp and block reduction
+// (deterministic).
+__global__ void __launch_bounds__(256, 3)
 k_ptq_cols(const float *__restrict__ K, const float *__restrict__ J, int ni, int nv, int nva,
            int nex, const unsigned char *__restrict__ use, const float2 *__restrict__ rhl,
            const float *__restrict__ eh, const float *__restrict__ el, float akf,
@@ -376,19 +387,34 @@ k_ptq_cols(const float *__restrict__ K, const float *__restrict__ J, int ni, int
     elq[u] = el[q];
     acc[u] = 0.0;
   }
-  const int64_t cstride = nva;   // next primary
-  for (int ii = warp; ii < ni; ii += 8) {
-    for (int a = lane; a < nv; a += 32) {
-      if (!use[ii * nv + a]) continue;
-      const float2 r = rhl[ii * nv + a];
+  const int64_t nrow = (int64_t)ni * nv;
+  for (int64_t e0 = threadIdx.x; e0 < nrow; e0 += (int64_t)blockDim.x * kColRows) {
+    float kv[kColRows][kColQ], jv[kColRows][kColQ], w[kColRows];
+    float2 r[kColRows];
+#pragma unroll
+    for (int v = 0; v < kColRows; ++v) {   // rows e0, e0 + blockDim, ...: coalesced
+      const int64_t ev = e0 + (int64_t)v * blockDim.x;
+      const int64_t e = min(ev, nrow - 1);
+      const int ii = (int)(e / nv), a = (int)(e - (int64_t)ii * nv);
+      w[v] = (ev < nrow && use[e]) ? 1.f : 0.f;
+      r[v] = rhl[e];
       const int64_t o = ((int64_t)ii * nex + q0) * nva + a;
 #pragma unroll
       for (int u = 0; u < kColQ; ++u) {
-        if (q0 + u < nex) {
-          const float am = akf * K[o + u * cstride] - J[o + u * cstride];
-          acc[u] += (double)(am * am * __frcp_rn((r.x - ehq[u]) + (r.y - elq[u])));
-        }
+        const int64_t ou = q0 + u < nex ? o + (int64_t)u * nva : o;
+        kv[v][u] = K[ou];
+        jv[v][u] = J[ou];
       }
+    }
+#pragma unroll
+    for (int u = 0; u < kColQ; ++u) {
+      float t = 0.f;
+#pragma unroll
+      for (int v = 0; v < kColRows; ++v) {
+        const float am = akf * kv[v][u] - jv[v][u];
+        t += w[v] * (am * am * __frcp_rn((r[v].x - ehq[u]) + (r[v].y - elq[u])));
+      }
+      acc[u] += (double)t;
     }
   }
   __shared__ double red[8][kColQ];
@@ -401,7 +427,7 @@ k_ptq_cols(const float *__restrict__ K, const float *__restrict__ J, int ni, int
   __syncthreads();
   if (threadIdx.x < kColQ && q0 + (int)threadIdx.x < nex) {
     double v = 0.0;
-    for (int w = 0; w < 8; ++w) v += red[w][threadIdx.x];
+    for (int ww = 0; ww < 8; ++ww) v += red[ww][threadIdx.x];
     colpart[q0 + threadIdx.x] = v;
   }
 }
