@@ -3,9 +3,11 @@
 Workload (single large sTDA, mixed precision): a synthetic graphene flake
 C384H48 with a minimal valence basis (1584 AOs, 780 occupied MOs, seeded
 MOs/energies), ax = 0.5, E_thr = 7 eV, PT threshold 1e-4, lowest 50 roots.
-One step = one full solve through the engine (orbital window -> S^1/2 ->
+One step = one solve through the engine (orbital window -> Loewdin MOs ->
 charges -> screen -> PT selection -> blocked Davidson -> properties with the
-velocity correction).
+velocity correction).  S^1/2 belongs to the wavefunction: std2g_load forms it
+once (the reference forms it once per run, stda.f:1615), so the device-resident
+steps of ``value`` reuse it and the ``e2e`` steps, which reload, include it.
 
 * ``value``: solves/s with inputs already resident on the device, timed with
   CUDA events on the engine's stream (max over ranks).
@@ -14,11 +16,13 @@ velocity correction).
   results back.
 * ``fp64_form``: the plain FP64 GPU form of the same solve (the denominator
   of the mixed-vs-FP64 comparison) and the mixed form's deviation from it.
-* ``roofline``: the tensor-core contraction of the PT selection, algorithmic
-  FLOPs (2 M N K with K = atoms) over its device time, against the measured
-  bf16 peak.
-* ``cpu_baseline``: the FP64 CPU restatement of the reference algorithm
-  (numpy, all host threads) on a bounded sample of the same solve.
+* ``roofline``: the tensor-core contractions of the PT selection, algorithmic
+  FLOPs (2 M N K with K = atoms) over their device time, against the measured
+  dense 16-bit tensor peak.
+* ``cpu_baseline``: the CPU restatement of the reference algorithm (the
+  reference's pair loops in C with real*4 dots, numpy for the rest, all host
+  threads) on a bounded sample of the same solve, and the same estimator
+  checked against a complete timed CPU solve of the C54H18 flake.
 
 ``--impl reference`` times that CPU restatement alone (the reference std2 is
 Fortran and cannot be built on this image).
@@ -39,6 +43,9 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 KW = dict(ax=0.5, e_thr_ev=7.0, thrp=1e-4, nroots=50)
+# DRAM bytes (read + write) per FP32 coupling of the PT contractions, from one
+# ncu capture of both coupling launches on the C216H36 flake
+TC_BYTES_PER_COUPLING = 4.6
 WORKLOAD = ("graphene flake C384H48, valence minimal basis (1584 AOs), ax=0.5, E_thr=7 eV, "
             "thrp=1e-4, lowest 50 roots")
 
@@ -108,6 +115,25 @@ def cpu_sample(mol, ints, budget_s=15.0):
     p = Params(**{k: v for k, v in KW.items() if k != "nroots"})
     return stda_timed(mol.xyz4(), mol.C, mol.eps, mol.occ, mol.iaoat(), S, L, V, M, p,
                       budget_s=budget_s)
+
+
+def cpu_validation():
+    """The CPU estimator against a complete timed CPU solve of the C54H18
+    flake (same keywords): every phase the estimate samples and scales (PT
+    selection, A build, dense real*4 eigensolve) run in full there."""
+    from oracle.stda_fp64 import Params, stda_full_timed, stda_timed
+    from stda_b200 import synth
+    mol, ints = synth.graphene_flake(3, with_ints=True)
+    S, L, V, M = ints
+    p = Params(**{k: v for k, v in KW.items() if k != "nroots"})
+    args = (mol.xyz4(), mol.C, mol.eps, mol.occ, mol.iaoat(), S, L, V, M, p)
+    est = stda_timed(*args, budget_s=4.0)
+    full = stda_full_timed(*args)
+    return {"molecule": "graphene flake C54H18", "nci": full["nci"],
+            "estimate_s": est["est_total_s"], "measured_s": full["total_s"],
+            "estimate_over_measured": est["est_total_s"] / full["total_s"],
+            "phases_estimate_s": {k: round(est[k + "_s"], 3) for k in ("setup", "pt", "a", "eig")},
+            "phases_measured_s": {k: round(full[k + "_s"], 3) for k in ("setup", "pt", "a", "eig")}}
 
 
 def molecule_pool(kind, count, seed):
@@ -298,10 +324,12 @@ def run_reference(args):
         "impl": "reference", "metric": "sTDA solves/s", "value": v, "unit": "solves/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": per * 1e3, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "vs_baseline": None,
+        "dtype": "f32 pair dots and eigensolve (the reference's real*4), f64 sums and screen",
+        "data": "synthetic",
         "config": {"workload": workload_name(args.flake)},
         "cpu_baseline": {"value": v, "unit": "solves/s", "cores": info["threads"], "kind": "port",
-                         "sample": info["sample"]},
+                         "sample": info["sample"], "validation": cpu_validation()},
         "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }))
 
@@ -403,7 +431,8 @@ def main():
                       "nci": sol.nci, "nex": sol.nex, "nexpt": sol.nexpt,
                       "new_pt": sol.new, "no": sol.no, "nv": sol.nv, "nroots": len(sol.omega),
                       "parallelism": f"replicas x{world}",
-                      "l2": "inputs > L2: per-solve charge/PT buffers are GBs"},
+                      "l2": "inputs > L2: per-solve charge/PT buffers are GBs",
+                      "sqrt_S": "once per std2g_load (reused by value steps, included in e2e)"},
            "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
            "phases_ms": {k: round(v, 3) for k, v in phases.items()}, "solver": solver,
            "gpu_launches": int(launches), "clocks": clocks, "e2e": e2e}
@@ -411,19 +440,20 @@ def main():
     if tc_launch > 0:
         pk, src = peaks()
         ach = tc_flop / (tc_ms / 1e3) / 1e12
-        # DRAM traffic per launch from the ncu capture of the same kernel on the
-        # flake-6 case (profiles/tc_gemm_bf16x3_pt_flake6.md): 4.27 B per FP32
-        # output element (output written once + operands read once), scaled by
-        # the output elements of an average launch here (FLOP / (2 N_atoms))
-        traffic = 4.27 * (tc_flop / tc_launch) / (2.0 * b.ncent)
+        # DRAM bytes per FP32 coupling written, measured by ncu on the two
+        # coupling launches of the C216H36 flake (the same kernel and tile
+        # schedule on a workload small enough to capture), times the couplings
+        # of an average launch here (algorithmic FLOP / (2 N_atoms))
+        traffic = TC_BYTES_PER_COUPLING * (tc_flop / tc_launch) / (2.0 * b.ncent)
         out["roofline"] = {"bound": "tensor", "achieved": ach, "peak": pk["bf16_tflops"],
                            "unit": "TFLOP/s", "frac": ach / pk["bf16_tflops"],
                            "traffic": traffic,
-                           "traffic_source": "ncu dram bytes per output element (flake-6 "
-                                             "capture) x output elements per launch",
-                           "kernel": "k_tc_gemm_bf16x3 (PT-selection contractions)",
-                           "flop_count": "algorithmic 2*M*N*N_atoms; the bf16 hi/lo split "
-                                         "executes 3x as many tensor-core FLOPs",
+                           "traffic_source": f"ncu dram bytes per coupling ({TC_BYTES_PER_COUPLING} B, "
+                                             "C216H36 flake capture) x couplings per launch",
+                           "kernel": "k_tc_gemm_bf16x3<PairTiles> (PT-selection couplings "
+                                     "(ia|jb) and (ij|ab))",
+                           "flop_count": "algorithmic 2*M*N*N_atoms; the split-FP16 operands "
+                                         "execute 3x as many tensor-core FLOPs",
                            "peak_source": src, "avg_launch_ms": tc_ms / tc_launch}
 
     if rank == 0 and not args.no_fp64 and prec == 1:
@@ -453,7 +483,8 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu:
         info = cpu_sample(mol, ints, budget_s=args.cpu_budget)
         out["cpu_baseline"] = {"value": 1.0 / info["est_total_s"], "unit": "solves/s",
-                               "cores": info["threads"], "kind": "port", "sample": info["sample"]}
+                               "cores": info["threads"], "kind": "port", "sample": info["sample"],
+                               "validation": cpu_validation()}
     if rank == 0:
         print(json.dumps(out))
     eng.close()

@@ -759,7 +759,14 @@ def stda_timed(xyz4, C, eps, occ, iaoat, S, Lao, Vao, Mao, p: Params, budget_s=1
     matrix, and scaled as n^3.  Used only as the reported CPU baseline, never
     as a result.
     """
-    import os
+    st = _cpu_setup(xyz4, C, eps, occ, iaoat, S, Lao, Vao, Mao, p)
+    return _timed_sample(st, p, budget_s)
+
+
+def _cpu_setup(xyz4, C, eps, occ, iaoat, S, Lao, Vao, Mao, p: Params):
+    """The phases of the CPU restatement that run in full in both the sampled
+    estimate and the complete timed solve: window, MO integrals, S^1/2,
+    charges, gamma, gamma.q and the diagonal screen (numpy, FP64)."""
     import time
     t_all = time.perf_counter()
     thr = p.e_thr_ev / EH2EV_IN
@@ -795,6 +802,60 @@ def stda_timed(xyz4, C, eps, occ, iaoat, S, Lao, Vao, Mao, p: Params, budget_s=1
     qvv = charges_block(Clow, iaoat, ncent, no + np.arange(nv), no + np.arange(nv)).reshape(ncent, nv, nv)
     poo = (gj @ qoo.reshape(ncent, -1)).reshape(qoo.shape)
     t_setup = time.perf_counter() - t_all
+    return dict(thr=thr, ak=ak, ncent=ncent, io_all=io_all, ia_all=ia_all, pia=pia, qia=qia,
+                poo=poo, qvv=qvv, de_all=de_all, pk=pk, ck=ck, ed=ed, t_setup=t_setup)
+
+
+def _pair_loops(st):
+    """The reference's own pair loops (ptselect, rtdamat: two real*4 dots of
+    length N per CSF pair, OpenMP) in C when gcc can build them, else None."""
+    try:
+        pt32 = PairTensors32(st["pia"], st["qia"], st["poo"], st["qvv"])
+        pairloops()
+        return pt32
+    except Exception:
+        return None
+
+
+def stda_full_timed(xyz4, C, eps, occ, iaoat, S, Lao, Vao, Mao, p: Params):
+    """One complete CPU solve with the pieces stda_timed samples, timed phase
+    by phase: the full PT selection and the full A build with the reference's
+    pair loops (pairloops.c), and the real*4 evr eigensolve of the roots in
+    (0, E_thr] of that A.  Used to check the sampled estimate at a size where
+    the complete solve finishes in seconds; never a result."""
+    import time
+    st = _cpu_setup(xyz4, C, eps, occ, iaoat, S, Lao, Vao, Mao, p)
+    pt32 = _pair_loops(st)
+    if pt32 is None:
+        raise OracleError("the complete timed solve needs the C pair loops (gcc)")
+    io_all, ia_all, de_all = st["io_all"], st["ia_all"], st["de_all"]
+    pk, ck, ed, ak = st["pk"], st["ck"], st["ed"], st["ak"]
+    t0 = time.perf_counter()
+    incl, pt2 = pt32.ptselect(io_all[ck], ia_all[ck], de_all[ck], io_all[pk], ia_all[pk], ed, ak,
+                              p.thrp)
+    t_pt = time.perf_counter() - t0
+    allk = np.concatenate([pk, ck[incl]])
+    ed_all = np.concatenate([ed - pt2, de_all[ck[incl]]])
+    nci = len(allk)
+    t0 = time.perf_counter()
+    A = pt32.rtdamat_rows(io_all[allk], ia_all[allk], ed_all, ak, 0, nci)
+    t_a = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    sla.eigh(A, lower=True, subset_by_value=(0.0, st["thr"]), driver="evr",
+             overwrite_a=True, check_finite=False)
+    t_eig = time.perf_counter() - t0
+    return dict(total_s=st["t_setup"] + t_pt + t_a + t_eig, setup_s=st["t_setup"], pt_s=t_pt,
+                a_s=t_a, eig_s=t_eig, nci=nci)
+
+
+def _timed_sample(st, p: Params, budget_s):
+    """The sampled phases of stda_timed (see there)."""
+    import os
+    import time
+    thr, ak, ncent = st["thr"], st["ak"], st["ncent"]
+    io_all, ia_all, pia, qia, poo, qvv = (st[k] for k in ("io_all", "ia_all", "pia", "qia",
+                                                          "poo", "qvv"))
+    de_all, pk, ck, ed, t_setup = st["de_all"], st["pk"], st["ck"], st["ed"], st["t_setup"]
 
     def coupling(krow, kcol):
         i1, a1 = io_all[krow], ia_all[krow]
@@ -812,13 +873,9 @@ def stda_timed(xyz4, C, eps, occ, iaoat, S, Lao, Vao, Mao, p: Params, budget_s=1
     # The reference's own loops (ptselect, rtdamat: two real*4 dots of length
     # N per CSF pair, OpenMP) in C when gcc can build them; otherwise the
     # numpy form above, which the sample text then names
-    try:
-        pt32 = PairTensors32(pia, qia, poo, qvv)
-        pairloops()
-        loops = "C restatement of ptselect / rtdamat (real*4 dots, OpenMP)"
-    except Exception:   # no compiler: the GEMM-based numpy form
-        pt32 = None
-        loops = "numpy GEMM form of ptselect / rtdamat"
+    pt32 = _pair_loops(st)
+    loops = ("C restatement of ptselect / rtdamat (real*4 dots, OpenMP)" if pt32 is not None
+             else "numpy GEMM form of ptselect / rtdamat")
 
     # PT selection on a sample of candidate blocks spread evenly over the
     # candidate list (the selection rate varies along it), scaled linearly
