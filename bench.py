@@ -187,6 +187,49 @@ def run_server(precision, pool, reqs, arrivals, slots, device):
                  "peak_in_flight": st["peak_in_flight"], "slots": slots}
 
 
+def served_saturation(precision, pool, reqs, slots, device, rates=(8, 16, 32, 64, 128),
+                      nreq=40, repeats=3, slo_ms=1000.0, seed=7):
+    """Saturation throughput of the served form: the request mix at stepped
+    Poisson rates through one server (warmed once); at each rate nreq requests
+    arrive and complete, and stepping stops at the first rate whose p99
+    latency exceeds the SLO.  The saturation throughput of a repeat is the
+    completed solves/s at the highest rate that met the SLO."""
+    from stda_b200.engine import Server
+    srv = Server(device, precision, slots=slots)
+    big = max(range(len(pool)), key=lambda i: pool[i].nao)
+    for om in (None, [0.0, 0.03, 0.06]):
+        for t in [srv.submit(pool[big], reqs[0][1], om) for _ in range(slots)]:
+            srv.wait(t)
+    rng = np.random.default_rng(seed)
+    runs, sat = [], []
+    for rep in range(repeats):
+        best = 0.0
+        for rate in rates:
+            pick = rng.integers(len(reqs), size=nreq)
+            arrivals = np.cumsum(rng.exponential(1.0 / rate, nreq))
+            t0 = time.perf_counter()
+            tickets = []
+            for k, q in enumerate(pick):
+                dt = arrivals[k] - (time.perf_counter() - t0)
+                if dt > 0:
+                    time.sleep(dt)
+                i, kw, om = reqs[q]
+                tickets.append(srv.submit(pool[i], kw, om))
+            res = [srv.wait(t) for t in tickets]
+            span = time.perf_counter() - t0
+            lat = [r[3]["latency_ms"] for r in res]
+            p99 = float(np.percentile(lat, 99))
+            runs.append({"repeat": rep, "rate": rate, "solves_per_s": nreq / span,
+                         "p50_ms": float(np.percentile(lat, 50)), "p99_ms": p99})
+            if p99 > slo_ms:
+                break
+            best = nreq / span
+        sat.append(best)
+    srv.close()
+    return {"slo_p99_ms": slo_ms, "requests_per_rate": nreq, "rates_per_s": list(rates),
+            "saturation_solves_per_s": sat, "median": float(np.median(sat)), "runs": runs}
+
+
 def plain_fp64(pool, reqs, device):
     """The plain FP64 GPU form: one engine, one molecule at a time."""
     from stda_b200.engine import Engine
@@ -281,12 +324,17 @@ def served_and_batched(device, args):
     arrivals = np.cumsum(rng.exponential(1.0 / args.serve_rate, len(reqs)))
     rm, sm = run_server(1, pool, reqs, arrivals, args.slots, device)
     rd, sd = run_server(0, pool, reqs, arrivals, args.slots, device)
+    sat_m = served_saturation(1, pool, reqs, args.slots, device)
+    sat_d = served_saturation(0, pool, reqs, args.slots, device)
     out["served"] = {"workload": f"{len(reqs)} requests, Poisson {args.serve_rate}/s, "
                                  f"{len(pool)} molecules of {int(atoms.min())}-{int(atoms.max())} "
                                  "atoms (lognormal, median 60), E_thr 6.5 eV, 32 roots (residual 1e-7), "
                                  "20 % with alpha(w) at 3 w",
                      "mixed": sm, "fp64": sd,
                      "p99_ratio_fp64_over_mixed": sd["latency_ms"]["p99"] / sm["latency_ms"]["p99"],
+                     "saturation": {"mixed": sat_m, "fp64": sat_d,
+                                    "ratio_mixed_over_fp64":
+                                        sat_m["median"] / sat_d["median"] if sat_d["median"] else None},
                      "accuracy": compare_forms(rm, rd),
                      "nci_range": [int(min(r[0].nci for r in rm)), int(max(r[0].nci for r in rm))]}
     # config 3: a batch submitted at once, 20 roots

@@ -151,6 +151,30 @@ int std2g_solve(void *ctx, const std2g_params *par, std2g_result *res);
 int std2g_polarizability(void *ctx, const std2g_params *par, const double *omega,
                          int nomega, double *alpha, double *resid);
 
+/* First hyperpolarizability beta(-2w; w, w) of sTD-DFT, the second-harmonic
+   tensor that lresp1 prints (linear_response.f:196-700; the -resp keyword),
+   at the frequencies omega [nomega] (Eh; the reference reads wavelengths and
+   prepends w = 0, linear_response.f:283-287).  The linear responses at +w and
+   -2w come from the same solver as std2g_polarizability (FP64 residuals below
+   1e-10 in both forms) and are contracted with the occupied-occupied and
+   virtual-virtual dipole couplings (List_A / List_B, :1089-1167).
+   beta [nomega*27]: row-major beta[w][x][y][z] (atomic units); beta_hrs
+   [nomega] (may be NULL): the hyper-Rayleigh value sqrt(<beta^2_ZZZ> +
+   <beta^2_XZZ>) (:1489-1662). */
+int std2g_hyperpolarizability(void *ctx, const std2g_params *par, const double *omega,
+                              int nomega, double *beta, double *beta_hrs);
+
+/* Two-photon absorption of the lowest ntrans sTD-DFT states in the
+   single-photon-resonance form (lresp_2PA_SP, linear_response.f:4604-4938;
+   the -2PA keyword): rows [ntrans*6] = (n, w_n in eV, delta_par, delta_perp,
+   delta_circ, rho = delta_par / delta_perp) as in the reference's 2PA-abs
+   file.  The states are those of the dense sTD-DFT solve of par's window, with
+   the reference's -2PA state vectors (srpapack.f:99-106 skips the halving of
+   the packed diagonals under that keyword, so each diagonal enters twice);
+   the responses at -w_n / 2 are the FP64 form's dense solves.  STD2G_EINVAL
+   when ntrans exceeds the roots below E_thr. */
+int std2g_two_photon(void *ctx, const std2g_params *par, int ntrans, double *rows);
+
 /* Selected CSF list of the last solve: iconf [2*cap] as (i,a) pairs, 1-based
    MO indices within the active window (occupied 1..no, virtual no+1..no+nv,
    as iconf(:,1:2) in stda.f), and the diagonal ed [cap] after PT lowering. */

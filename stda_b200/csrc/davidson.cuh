@@ -255,6 +255,106 @@ using MatVec = std::function<void(const double *V, int nb, double *W)>;
 // syevd); larger ones to cuSOLVER syevd.
 constexpr int kRRSmallMax = 128;
 
+// Orthonormalises the nc columns of T (n x nc) against the m orthonormal
+// columns of V and among themselves, and appends the result to V after column
+// m (BCGS2: normalise, then two rounds of one block classical Gram-Schmidt
+// projection against V followed by Cholesky QR of the block, or, when its Gram
+// matrix is not safely positive definite, orthonormalisation through the Gram
+// matrix's eigen-decomposition that drops dependent directions).  Returns the
+// number of columns appended.  kcap: capacity of the k x k work arrays.
+inline int dav_orthonormalize(DavidsonWork &dw, cublasHandle_t blas, cusolverDnHandle_t sol,
+                              cudaStream_t s, double *V, int n, int m, double *T, int nc,
+                              int kcap) {
+  const int k = kcap;
+  const int grid = 148 * 4;
+  const double one = 1.0, zero = 0.0, mone = -1.0;
+  double *tmp = dw.tmp.ensure((size_t)n * k);
+  double *proj = dw.proj.ensure((size_t)(m + k) * k + 4);
+  int *info = dw.info.ensure(1);
+  int nb = 0;
+  {
+    double *G = dw.G.ensure((size_t)k * k), *lam = dw.lam.ensure(k);
+    double *part = dw.part.ensure((size_t)k * kColSplit);
+    S2G_LAUNCH(k_colnorm_part, dim3(kColSplit, (unsigned)nc), 256, 0, s, T, n, part);
+    S2G_LAUNCH(k_colnorm_finish, (int)div_up(nc, 128), 128, 0, s, part, kColSplit, nc, lam);
+    S2G_LAUNCH(k_scale_by, grid, 256, 0, s, T, n, nc, lam, 0);
+    double *Tb = T;
+    int ncur = nc;
+    for (int round = 0; round < 2 && ncur > 0; ++round) {
+      S2G_CUBLAS(cublasDgemm(blas, CUBLAS_OP_T, CUBLAS_OP_N, m, ncur, n, &one, V, n, Tb, n,
+                             &zero, proj, m));
+      S2G_CUBLAS(cublasDgemm(blas, CUBLAS_OP_N, CUBLAS_OP_N, n, ncur, m, &mone, V, n, proj, m,
+                             &one, Tb, n));
+      // G = Tb^T Tb; Cholesky QR when G is safely positive definite
+      S2G_CUBLAS(cublasDgemm(blas, CUBLAS_OP_T, CUBLAS_OP_N, ncur, ncur, n, &one, Tb, n, Tb, n,
+                             &zero, G, ncur));
+      if (ncur <= kCholMax) {
+        // Cholesky QR: L^-T from the engine's small factorisation kernel
+        double *Li = dw.Gc.ensure((size_t)k * k), *st = dw.stat.ensure(2);
+        S2G_CUDA(cudaFuncSetAttribute(k_chol_inv, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)(2 * sizeof(double) * kCholMax * kCholMax)));
+        S2G_LAUNCH(k_chol_inv, 1, 256, 2 * sizeof(double) * ncur * ncur, s, G, ncur, 1e-8, Li,
+                   st);
+        double h_st[2];
+        S2G_CUDA(cudaMemcpyAsync(h_st, st, sizeof(h_st), cudaMemcpyDeviceToHost, s));
+        S2G_CUDA(cudaStreamSynchronize(s));
+        if (h_st[0] == 0.0) {
+          // dst <- Tb L^-T (through tmp when Tb already is dst)
+          double *dst = V + (size_t)n * m;
+          double *o = Tb == dst ? tmp : dst;
+          S2G_CUBLAS(cublasDgemm(blas, CUBLAS_OP_N, CUBLAS_OP_N, n, ncur, ncur, &one, Tb, n, Li,
+                                 ncur, &zero, o, n));
+          if (o != dst)
+            S2G_CUDA(cudaMemcpyAsync(dst, o, sizeof(double) * n * ncur,
+                                     cudaMemcpyDeviceToDevice, s));
+          Tb = dst;
+          continue;
+        }
+      }
+      // eigenpairs of G ascending: drop dependent directions
+      if (ncur <= kRRSmallMax) {
+        double *Z = dw.Gz.ensure((size_t)k * k);
+        S2G_CUDA(cudaMemsetAsync(info, 0, sizeof(int), s));
+        symeig_small(s, G, ncur, ncur, ncur, lam, Z, ncur,
+                     dw.eigwork.ensure(symeig_work_doubles(ncur, ncur)), info);
+        S2G_CUDA(cudaMemcpyAsync(G, Z, sizeof(double) * ncur * ncur, cudaMemcpyDeviceToDevice,
+                                 s));
+      } else {
+        int lw2 = 0;
+        S2G_CUSOLVER(cusolverDnDsyevd_bufferSize(sol, CUSOLVER_EIG_MODE_VECTOR,
+                                                 CUBLAS_FILL_MODE_LOWER, ncur, G, ncur, lam,
+                                                 &lw2));
+        double *work2 = dw.work2.ensure((size_t)lw2 + 1);
+        S2G_CUSOLVER(cusolverDnDsyevd(sol, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER,
+                                      ncur, G, ncur, lam, work2, lw2, info));
+      }
+      std::vector<double> h_lam(ncur);
+      S2G_CUDA(cudaMemcpyAsync(h_lam.data(), lam, sizeof(double) * ncur, cudaMemcpyDeviceToHost,
+                               s));
+      S2G_CUDA(cudaStreamSynchronize(s));
+      int first = 0;   // keep eigenvalues above the dependence threshold
+      const double cut = round == 0 ? 1e-10 : 1e-14;
+      while (first < ncur && !(h_lam[first] > cut)) ++first;
+      int nkeep = ncur - first;
+      if (nkeep == 0) {
+        ncur = 0;
+        break;
+      }
+      // new block = Tb U_keep diag(lam_keep)^-1/2, written into V after column m
+      double *dst = V + (size_t)n * m;
+      S2G_CUBLAS(cublasDgemm(blas, CUBLAS_OP_N, CUBLAS_OP_N, n, nkeep, ncur, &one, Tb, n,
+                             G + (size_t)ncur * first, ncur, &zero, tmp, n));
+      S2G_LAUNCH(k_scale_by, grid, 256, 0, s, tmp, n, nkeep, lam + first, 1);
+      S2G_CUDA(cudaMemcpyAsync(dst, tmp, sizeof(double) * n * nkeep, cudaMemcpyDeviceToDevice,
+                               s));
+      Tb = dst;   // second round re-orthogonalises the appended block in place
+      ncur = nkeep;
+    }
+    nb = ncur;
+  }
+  return nb;
+}
+
 // Returns the number of converged wanted roots (== k on success).  `mv` forms
 // W = A V for nb column vectors (n x nb, column-major); `diag` is diag(A).
 // With `warm`, the first block is the k Ritz vectors left in dw.X by a
@@ -371,92 +471,8 @@ inline int davidson(DavidsonWork &dw, cublasHandle_t blas, cusolverDnHandle_t so
       // H restricted to the Ritz vectors is diag(theta)
       S2G_LAUNCH(k_diag_matrix, (int)div_up((int64_t)k * k, 256), 256, 0, s, H, mmax, k, theta);
     }
-    // block orthogonalisation of the corrections (BCGS2): normalise, then two
-    // rounds of one block classical Gram-Schmidt projection against V (GEMMs)
-    // followed by Cholesky QR of the block, or, when its Gram matrix is not
-    // safely positive definite, orthonormalisation through the Gram matrix's
-    // eigen-decomposition that drops dependent directions
-    nb = 0;
-    {
-      double *G = dw.G.ensure((size_t)k * k), *lam = dw.lam.ensure(k);
-      double *part = dw.part.ensure((size_t)k * kColSplit);
-      S2G_LAUNCH(k_colnorm_part, dim3(kColSplit, (unsigned)nc), 256, 0, s, T, n, part);
-      S2G_LAUNCH(k_colnorm_finish, (int)div_up(nc, 128), 128, 0, s, part, kColSplit, nc, lam);
-      S2G_LAUNCH(k_scale_by, grid, 256, 0, s, T, n, nc, lam, 0);
-      double *Tb = T;
-      int ncur = nc;
-      for (int round = 0; round < 2 && ncur > 0; ++round) {
-        S2G_CUBLAS(cublasDgemm(blas, CUBLAS_OP_T, CUBLAS_OP_N, m, ncur, n, &one, V, n, Tb, n,
-                               &zero, proj, m));
-        S2G_CUBLAS(cublasDgemm(blas, CUBLAS_OP_N, CUBLAS_OP_N, n, ncur, m, &mone, V, n, proj, m,
-                               &one, Tb, n));
-        // G = Tb^T Tb; Cholesky QR when G is safely positive definite
-        S2G_CUBLAS(cublasDgemm(blas, CUBLAS_OP_T, CUBLAS_OP_N, ncur, ncur, n, &one, Tb, n, Tb, n,
-                               &zero, G, ncur));
-        if (ncur <= kCholMax) {
-          // Cholesky QR: L^-T from the engine's small factorisation kernel
-          double *Li = dw.Gc.ensure((size_t)k * k), *st = dw.stat.ensure(2);
-          S2G_CUDA(cudaFuncSetAttribute(k_chol_inv, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)(2 * sizeof(double) * kCholMax * kCholMax)));
-          S2G_LAUNCH(k_chol_inv, 1, 256, 2 * sizeof(double) * ncur * ncur, s, G, ncur, 1e-8, Li,
-                     st);
-          double h_st[2];
-          S2G_CUDA(cudaMemcpyAsync(h_st, st, sizeof(h_st), cudaMemcpyDeviceToHost, s));
-          S2G_CUDA(cudaStreamSynchronize(s));
-          if (h_st[0] == 0.0) {
-            // dst <- Tb L^-T (through tmp when Tb already is dst)
-            double *dst = V + (size_t)n * m;
-            double *o = Tb == dst ? tmp : dst;
-            S2G_CUBLAS(cublasDgemm(blas, CUBLAS_OP_N, CUBLAS_OP_N, n, ncur, ncur, &one, Tb, n, Li,
-                                   ncur, &zero, o, n));
-            if (o != dst)
-              S2G_CUDA(cudaMemcpyAsync(dst, o, sizeof(double) * n * ncur,
-                                       cudaMemcpyDeviceToDevice, s));
-            Tb = dst;
-            continue;
-          }
-        }
-        // eigenpairs of G ascending: drop dependent directions
-        if (ncur <= kRRSmallMax) {
-          double *Z = dw.Gz.ensure((size_t)k * k);
-          S2G_CUDA(cudaMemsetAsync(info, 0, sizeof(int), s));
-          symeig_small(s, G, ncur, ncur, ncur, lam, Z, ncur,
-                       dw.eigwork.ensure(symeig_work_doubles(ncur, ncur)), info);
-          S2G_CUDA(cudaMemcpyAsync(G, Z, sizeof(double) * ncur * ncur, cudaMemcpyDeviceToDevice,
-                                   s));
-        } else {
-          int lw2 = 0;
-          S2G_CUSOLVER(cusolverDnDsyevd_bufferSize(sol, CUSOLVER_EIG_MODE_VECTOR,
-                                                   CUBLAS_FILL_MODE_LOWER, ncur, G, ncur, lam,
-                                                   &lw2));
-          double *work2 = dw.work2.ensure((size_t)lw2 + 1);
-          S2G_CUSOLVER(cusolverDnDsyevd(sol, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER,
-                                        ncur, G, ncur, lam, work2, lw2, info));
-        }
-        std::vector<double> h_lam(ncur);
-        S2G_CUDA(cudaMemcpyAsync(h_lam.data(), lam, sizeof(double) * ncur, cudaMemcpyDeviceToHost,
-                                 s));
-        S2G_CUDA(cudaStreamSynchronize(s));
-        int first = 0;   // keep eigenvalues above the dependence threshold
-        const double cut = round == 0 ? 1e-10 : 1e-14;
-        while (first < ncur && !(h_lam[first] > cut)) ++first;
-        int nkeep = ncur - first;
-        if (nkeep == 0) {
-          ncur = 0;
-          break;
-        }
-        // new block = Tb U_keep diag(lam_keep)^-1/2, written into V after column m
-        double *dst = V + (size_t)n * m;
-        S2G_CUBLAS(cublasDgemm(blas, CUBLAS_OP_N, CUBLAS_OP_N, n, nkeep, ncur, &one, Tb, n,
-                               G + (size_t)ncur * first, ncur, &zero, tmp, n));
-        S2G_LAUNCH(k_scale_by, grid, 256, 0, s, tmp, n, nkeep, lam + first, 1);
-        S2G_CUDA(cudaMemcpyAsync(dst, tmp, sizeof(double) * n * nkeep, cudaMemcpyDeviceToDevice,
-                                 s));
-        Tb = dst;   // second round re-orthogonalises the appended block in place
-        ncur = nkeep;
-      }
-      nb = ncur;
-    }
+    // block orthogonalisation of the corrections, appended to V after column m
+    nb = dav_orthonormalize(dw, blas, sol, s, V, n, m, T, nc, k);
     clk.tick(4);
     if (nb == 0) break;
   }

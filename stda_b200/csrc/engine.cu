@@ -20,6 +20,7 @@
 #include "eta_table.cuh"
 #include "kernels_fp64.cuh"
 #include "davidson.cuh"
+#include "davidson_rpa.cuh"
 #include "matfree.cuh"
 #include "matfree_tc.cuh"
 #include "pt_tc.cuh"
@@ -65,6 +66,10 @@ struct Ctx {
   DBuf<unsigned char> w_sel;
   DBuf<double> w_Qs, w_Ps, w_K, w_J, w_Kx, w_A, w_Apb, w_Amb, w_Bh, w_Ambh, w_M, w_eval, w_X,
       w_Y, w_tmp, w_musel, w_TL, w_TVM, w_T2, w_props, w_work;
+  // quadratic response: length dipoles in the occupied and virtual blocks,
+  // response vectors, and the work arrays of the M Y products
+  DBuf<double> w_To, w_moo, w_mvv, w_Uall, w_Vall, w_qx, w_qy, w_qbox, w_qmy, w_qsel, w_qg,
+      w_tpx, w_tpy;
   DBuf<int> w_info;
   DBuf<char> w_cub;
   MixedWork mixed;
@@ -77,6 +82,7 @@ struct Ctx {
     int outer = 0, inner = 0;
   } rw;
   DavidsonWork dav;
+  DavidsonRpaWork davr;
   MatFree mf;
   MatFreeTc mftc;
   // tensor-core contraction statistics of the last solve
@@ -243,12 +249,30 @@ static void load(Ctx &c, int ncent, int nmo, int nao, const double *xyz, const d
   c.loaded = true;
 }
 
-// A dynamic-polarizability request (lresp, linear_response.f:23-192).
+// Quadratic-response consumers of the linear-response vectors (lresp1,
+// linear_response.f:196-908; lresp_2PA_SP, :4604-4938).
+struct QuadReq {
+  // beta(-2w; w, w): the response frequencies are (w_k, -2 w_k) pairs
+  double *beta = nullptr;       // [nbeta*27] row-major beta[k][x][y][z]
+  double *beta_hrs = nullptr;   // [nbeta]
+  int nbeta = 0;
+  // two-photon absorption of the lowest ntpa sTD-DFT states
+  double *tpa = nullptr;        // [ntpa*6] rows (n, w_n eV, delta_par, delta_perp, delta_circ, rho)
+  int ntpa = 0;
+};
+
+// A dynamic-polarizability request (lresp, linear_response.f:23-192).  With U
+// and V set (device, n x 3 per frequency slot), the solvers also leave the
+// vectors X+Y (U) and X-Y (V) of every frequency there; slot[w] (NULL: w)
+// names the slot of frequency w.
 struct RespReq {
   const double *omega;
   int n;
   double *alpha;   // [n*9]
   double *resid;   // [n] or NULL
+  double *U = nullptr, *V = nullptr;
+  const int *slot = nullptr;
+  const QuadReq *quad = nullptr;
 };
 
 // (A-B)^-1 by Cholesky (ssptrf/ssptri, linear_response.f:89-95), then per omega
@@ -318,6 +342,13 @@ static void response(Ctx &c, double *Apb, double *Amb, int nci, const double *mu
     for (int x = 0; x < 3; ++x)
       for (int y = 0; y < 3; ++y) rq.alpha[(size_t)w * 9 + 3 * x + y] = h[x + 3 * y];
     if (rq.resid) rq.resid[w] = h[9];
+    if (rq.U) {
+      // X+Y and X-Y = w (A-B)^-1 (X+Y) (linear_response.f:312-327)
+      const size_t off = (size_t)nci * 3 * (rq.slot ? rq.slot[w] : w);
+      S2G_CUDA(cudaMemcpyAsync(rq.U + off, Xs, sizeof(double) * nci * 3, cudaMemcpyDeviceToDevice,
+                               s));
+      gemm(c, CUBLAS_OP_N, CUBLAS_OP_N, nci, 3, nci, om, Ainv, nci, Xs, nci, 0.0, rq.V + off, nci);
+    }
   }
 }
 
@@ -449,6 +480,13 @@ static void response_ir(Ctx &c, int n, const double *musel, const RespReq &rq,
   double *a9 = c.w_props.ensure(16);
   for (int fw = 0; fw < nw; ++fw) {
     if (std::find(fallback.begin(), fallback.end(), fw) != fallback.end()) continue;
+    if (rq.U) {
+      const size_t off = (size_t)n * 3 * (rq.slot ? rq.slot[fw] : fw);
+      S2G_CUDA(cudaMemcpyAsync(rq.U + off, U + (size_t)n * 3 * fw, sizeof(double) * n * 3,
+                               cudaMemcpyDeviceToDevice, s));
+      S2G_CUDA(cudaMemcpyAsync(rq.V + off, V + (size_t)n * 3 * fw, sizeof(double) * n * 3,
+                               cudaMemcpyDeviceToDevice, s));
+    }
     gemm(c, CUBLAS_OP_T, CUBLAS_OP_N, 3, 3, n, -2.0, musel, n, U + (size_t)n * 3 * fw, n, 0.0,
          a9, 3);
     double ha[9];
@@ -531,7 +569,176 @@ static void response_matfree(Ctx &c, int n, const double *musel, const RespReq &
 }
 
 // --------------------------------------------------------------------------
-static void solve(Ctx &c, const std2g_params &p_in, std2g_result *res, const RespReq *resp) {
+// Quadratic-response dot products G[x + nx*(y*ny + v)] = X_x . (M_y Y_v) for
+// the sums of lresp1 / lresp_2PA_SP (List_A / List_B, linear_response.f:
+// 1089-1167), where M_y couples CSFs that share their virtual (through
+// -mu^y_ij) or their occupied MO (through mu^y_ab):
+//   (M_y Y)_(i,a) = -sum_j mu^y_ij Y_(j,a) + sum_b mu^y_ab Y_(i,b)
+// over the selected CSFs.  Y is scattered into (no x nv) boxes, M_y applied as
+// two GEMMs with the occupied / virtual dipole blocks, gathered back at the
+// CSFs and dotted with X.  X: nci x nx, Y: nci x ny (device, column-major).
+static std::vector<double> quad_dots(Ctx &c, int nci, int no, int nv, const int *ci,
+                                     const int *ca, const double *X, int nx, const double *Y,
+                                     int ny) {
+  cudaStream_t s = c.stream;
+  const int64_t box = (int64_t)no * nv;
+  double *bx = c.w_qbox.ensure((size_t)box * ny);
+  S2G_CUDA(cudaMemsetAsync(bx, 0, sizeof(double) * box * ny, s));
+  S2G_LAUNCH(k_box_scatter, grid_for((int64_t)nci * ny), 256, 0, s, bx, Y, ci, ca, nci, no, nv,
+             ny);
+  double *my = c.w_qmy.ensure((size_t)box * ny * 3);
+  const double one = 1.0, mone = -1.0, zero = 0.0;
+  for (int y = 0; y < 3; ++y) {
+    double *out = my + (size_t)box * ny * y;
+    S2G_CUBLAS(cublasDgemm(c.blas, CUBLAS_OP_N, CUBLAS_OP_N, no, nv * ny, no, &mone,
+                           c.w_moo.get() + (size_t)no * no * y, no, bx, no, &zero, out, no));
+    S2G_CUBLAS(cublasDgemmStridedBatched(c.blas, CUBLAS_OP_N, CUBLAS_OP_N, no, nv, nv, &one, bx,
+                                         no, box, c.w_mvv.get() + (size_t)nv * nv * y, nv, 0,
+                                         &one, out, no, box, ny));
+  }
+  double *sel = c.w_qsel.ensure((size_t)nci * 3 * ny);
+  S2G_LAUNCH(k_box_gather, grid_for((int64_t)nci * 3 * ny), 256, 0, s, sel, my, ci, ca, nci, no,
+             nv, 3 * ny);
+  double *G = c.w_qg.ensure((size_t)nx * 3 * ny);
+  gemm(c, CUBLAS_OP_T, CUBLAS_OP_N, nx, 3 * ny, nci, 1.0, X, nci, sel, nci, 0.0, G, nx);
+  std::vector<double> h((size_t)nx * 3 * ny);
+  S2G_CUDA(cudaMemcpyAsync(h.data(), G, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, s));
+  S2G_CUDA(cudaStreamSynchronize(s));
+  return h;
+}
+
+// <beta^2_ZZZ> + <beta^2_XZZ> of the hyper-Rayleigh orientational average
+// (linear_response.f:1489-1662); i, j, k run over distinct axes
+static double beta_hrs_value(const double b[3][3][3]) {
+  double s_iii = 0, s_iij = 0, s_jii = 0, s_ijj = 0, s_ijk = 0, iii_ijj = 0, jii_iij = 0,
+         iii_jji = 0, iij_jii = 0, iij_jkk = 0, jii_jkk = 0, iij_kkj = 0, ijk_jik = 0,
+         ijj_ikk = 0, iik_jjk = 0;
+  for (int i = 0; i < 3; ++i) {
+    s_iii += b[i][i][i] * b[i][i][i];
+    for (int j = 0; j < 3; ++j) {
+      if (j == i) continue;
+      s_iij += b[i][i][j] * b[i][i][j];
+      s_jii += b[j][i][i] * b[j][i][i];
+      s_ijj += b[i][j][j] * b[i][j][j];
+      iii_ijj += b[i][i][i] * b[i][j][j];
+      jii_iij += b[j][i][i] * b[i][i][j];
+      iii_jji += b[i][i][i] * b[j][j][i];
+      iij_jii += b[i][i][j] * b[j][i][i];
+      for (int k = 0; k < 3; ++k) {
+        if (k == i || k == j) continue;
+        s_ijk += b[i][j][k] * b[i][j][k];
+        iij_jkk += b[i][i][j] * b[j][k][k];
+        jii_jkk += b[j][i][i] * b[j][k][k];
+        iij_kkj += b[i][i][j] * b[k][k][j];
+        ijk_jik += b[i][j][k] * b[j][i][k];
+        ijj_ikk += b[i][j][j] * b[i][k][k];
+        iik_jjk += b[i][i][k] * b[j][j][k];
+      }
+    }
+  }
+  const double zzz = s_iii / 7 + 4 * s_iij / 35 + s_jii / 35 + 2 * s_ijk / 105 + 2 * iii_ijj / 35 +
+                     4 * jii_iij / 35 + 4 * iii_jji / 35 + 4 * iij_jkk / 105 + jii_jkk / 105 +
+                     4 * iij_kkj / 105 + 4 * ijk_jik / 105;
+  const double xzz = s_iii / 35 + 4 * iii_ijj / 105 - 2 * iii_jji / 35 + 8 * s_iij / 105 -
+                     2 * iij_jkk / 105 + 2 * s_ijk / 35 - 2 * ijk_jik / 105 + 3 * s_ijj / 35 -
+                     2 * iij_jii / 35 + ijj_ikk / 35 - 2 * iik_jjk / 105;
+  return std::sqrt(zzz + xzz);
+}
+
+// beta(-2w; w, w) from the response vectors of the frequency pairs
+// (w_k, -2 w_k) in slots (2k, 2k+1) of U = X+Y, V = X-Y (lresp1,
+// linear_response.f:196-700: beta = A - B summed over the six assignments of
+// the axes to the -2w X vector, the dipole and the w Y vector).
+static void hyperpolarizability(Ctx &c, int nci, int no, int nv, const int *ci, const int *ca,
+                                const double *U, const double *V, const QuadReq &q) {
+  cudaStream_t s = c.stream;
+  double *Xa = c.w_qx.ensure((size_t)nci * 6), *Ya = c.w_qy.ensure((size_t)nci * 6);
+  for (int kk = 0; kk < q.nbeta; ++kk) {
+    // columns (w-1)*3 + x of X and Y: w = 1 the +w vectors, w = 2 the -2w ones
+    for (int w = 0; w < 2; ++w) {
+      const size_t off = (size_t)nci * 3 * (2 * kk + w);
+      S2G_LAUNCH(k_xy_from_uv, grid_for((int64_t)nci * 3), 256, 0, s, Xa + (size_t)nci * 3 * w,
+                 Ya + (size_t)nci * 3 * w, U + off, V + off, (int64_t)nci * 3, 0.5);
+    }
+    const std::vector<double> G = quad_dots(c, nci, no, nv, ci, ca, Xa, 6, Ya, 6);
+    // T(x, wx, y, z, wz) = X_wx[:, x] . M_y . Y_wz[:, z]
+    auto T = [&](int x, int wx, int y, int z, int wz) {
+      return G[(size_t)((wx - 1) * 3 + x) + 6 * (size_t)(y * 6 + (wz - 1) * 3 + z)];
+    };
+    double b[3][3][3];
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j)
+        for (int k = 0; k < 3; ++k) {
+          b[i][j][k] = T(i, 2, j, k, 1) + T(i, 2, k, j, 1) + T(j, 1, k, i, 2) + T(j, 1, i, k, 1) +
+                       T(k, 1, i, j, 1) + T(k, 1, j, i, 2);
+          q.beta[(size_t)kk * 27 + 9 * i + 3 * j + k] = b[i][j][k];
+        }
+    if (q.beta_hrs) q.beta_hrs[kk] = beta_hrs_value(b);
+  }
+}
+
+static void response(Ctx &c, double *Apb, double *Amb, int nci, const double *musel,
+                     const RespReq &rq);
+
+// Two-photon absorption of the lowest q.ntpa sTD-DFT states (lresp_2PA_SP,
+// linear_response.f:4604-4938; TPA_resp_fast_SP :4940-5025): for state n the
+// response to -mu at w = -w_n / 2 gives X, Y per axis, and
+//   sigma_xy = -1/2 [X_x M_y Yn + X_y M_x Yn + Xn M_x Y_y + Xn M_y Y_x]
+// with the state vectors Xn, Yn (w_tpx, w_tpy); F, G, H (each / 30) give
+// delta_par = 2F+2G+2H, delta_perp = -F+4G-H, delta_circ = -2F+3G+3H and
+// rho = delta_par / delta_perp.  The responses are the FP64 form's dense
+// solves of the A+B, A-B built for the states.
+static void two_photon(Ctx &c, int nci, int no, int nv, const int *ci, const int *ca,
+                       const double *musel, const std::vector<double> &w, const QuadReq &q) {
+  cudaStream_t s = c.stream;
+  const int nt = q.ntpa;
+  double *Xq = c.w_qx.ensure((size_t)nci * 4), *Yq = c.w_qy.ensure((size_t)nci * 4);
+  for (int n0 = 0; n0 < nt; n0 += 10) {
+    const int ng = std::min(10, nt - n0);
+    std::vector<double> om(ng), al((size_t)ng * 9), rs(ng);
+    for (int k = 0; k < ng; ++k) om[k] = -0.5 * w[n0 + k];
+    RespReq sub{om.data(), ng, al.data(), rs.data()};
+    sub.U = c.w_Uall.ensure((size_t)nci * 3 * ng);
+    sub.V = c.w_Vall.ensure((size_t)nci * 3 * ng);
+    response(c, c.w_Apb.get(), c.w_Amb.get(), nci, musel, sub);
+    for (int k = 0; k < ng; ++k) {
+      const int n = n0 + k;
+      const size_t off = (size_t)nci * 3 * k;
+      // the solver answers -2 mu: a quarter of U +- V is X, Y for -mu
+      S2G_LAUNCH(k_xy_from_uv, grid_for((int64_t)nci * 3), 256, 0, s, Xq, Yq, sub.U + off,
+                 sub.V + off, (int64_t)nci * 3, 0.25);
+      S2G_CUDA(cudaMemcpyAsync(Xq + (size_t)nci * 3, c.w_tpx.get() + (size_t)nci * n,
+                               sizeof(double) * nci, cudaMemcpyDeviceToDevice, s));
+      S2G_CUDA(cudaMemcpyAsync(Yq + (size_t)nci * 3, c.w_tpy.get() + (size_t)nci * n,
+                               sizeof(double) * nci, cudaMemcpyDeviceToDevice, s));
+      const std::vector<double> G = quad_dots(c, nci, no, nv, ci, ca, Xq, 4, Yq, 4);
+      auto T = [&](int a, int y, int v) { return G[(size_t)a + 4 * (size_t)(y * 4 + v)]; };
+      double sg[3][3], tr = 0.0, g2 = 0.0, h2 = 0.0;
+      for (int x = 0; x < 3; ++x)
+        for (int y = 0; y < 3; ++y)
+          sg[x][y] = -0.5 * (T(x, y, 3) + T(y, x, 3) + T(3, x, y) + T(3, y, x));
+      for (int x = 0; x < 3; ++x) {
+        tr += sg[x][x];
+        for (int y = 0; y < 3; ++y) {
+          g2 += sg[x][y] * sg[x][y];
+          h2 += sg[x][y] * sg[y][x];
+        }
+      }
+      const double F = tr * tr / 30.0, Gs = g2 / 30.0, H = h2 / 30.0;
+      const double par = 2 * F + 2 * Gs + 2 * H, perp = -F + 4 * Gs - H;
+      double *row = q.tpa + (size_t)6 * n;
+      row[0] = n + 1;
+      row[1] = w[n] * 27.21139;
+      row[2] = par;
+      row[3] = perp;
+      row[4] = -2 * F + 3 * Gs + 3 * H;
+      row[5] = par / perp;
+    }
+  }
+}
+
+static void solve(Ctx &c, const std2g_params &p_in, std2g_result *res, const RespReq *resp,
+                  const QuadReq *tpa = nullptr) {
   if (!c.loaded) throw Error{STD2G_ESTATE, "solve before load"};
   std2g_params p = p_in;
   if (resp) {
@@ -555,6 +762,7 @@ static void solve(Ctx &c, const std2g_params &p_in, std2g_result *res, const Res
   const double ak = p.triplet ? 0.0 : 2.0;
   const double beta_j = p.beta_j >= -99.0 ? p.beta_j : 0.20 + 1.830 * p.ax;
   const double alpha_k = p.alpha_k >= -99.0 ? p.alpha_k : 1.420 + 0.480 * p.ax;
+  const bool want_quad = (resp && resp->quad) || (tpa && tpa->ntpa > 0);
 
   // ---- orbital window and energy sort (stda.f:145-192, 261-308, 333) ----
   const double deps = 2.0 * (1.0 + 0.8 * p.ax) * thr;
@@ -620,6 +828,23 @@ static void solve(Ctx &c, const std2g_params &p_in, std2g_result *res, const Res
     S2G_CUBLAS(cublasDgemmStridedBatched(c.blas, CUBLAS_OP_T, CUBLAS_OP_N, no, nv, nao, &one,
                                          Cact, nao, 0, T, nao, (long long)nao * nv, &zero, mu, no,
                                          (long long)no * nv, 9));
+    if (want_quad) {
+      // length dipoles of the occupied-occupied and virtual-virtual blocks
+      // (the same packed moci x moci transform, stda.f:351-412; lresp1 reads them)
+      double *To = c.w_To.ensure((size_t)nao * no * 3);
+      S2G_CUBLAS(cublasDgemmStridedBatched(c.blas, CUBLAS_OP_N, CUBLAS_OP_N, nao, no, nao, &one,
+                                           c.d_ao9.get(), nao, (long long)nn, Cact, nao, 0, &zero,
+                                           To, nao, (long long)nao * no, 3));
+      S2G_CUBLAS(cublasDgemmStridedBatched(c.blas, CUBLAS_OP_T, CUBLAS_OP_N, no, no, nao, &one,
+                                           Cact, nao, 0, To, nao, (long long)nao * no, &zero,
+                                           c.w_moo.ensure((size_t)no * no * 3), no,
+                                           (long long)no * no, 3));
+      S2G_CUBLAS(cublasDgemmStridedBatched(c.blas, CUBLAS_OP_T, CUBLAS_OP_N, nv, nv, nao, &one,
+                                           Cact + (size_t)nao * no, nao, 0, T, nao,
+                                           (long long)nao * nv, &zero,
+                                           c.w_mvv.ensure((size_t)nv * nv * 3), nv,
+                                           (long long)nv * nv, 3));
+    }
   }
 
   // ---- gamma and charges (stda.f:465-479, 509-532, 558-590, 728-763) ----
@@ -878,7 +1103,9 @@ static void solve(Ctx &c, const std2g_params &p_in, std2g_result *res, const Res
              (int64_t)1);
   // Large TDA problems with a root count use the matrix-free operators and the
   // blocked Davidson solver; everything else builds the matrices explicitly.
-  const bool use_mf = !p.rpa && p.nroots > 0 && (p.solver == 2 || (p.solver == 0 && nci > 1024));
+  // (sTD-DFT roots: the matrix-free A+B, A-B products and the Davidson of
+  // davidson_rpa.cuh, FP64 products in both forms)
+  const bool use_mf = !resp && p.nroots > 0 && (p.solver == 2 || (p.solver == 0 && nci > 1024));
   // Mixed form: the tensor-core first Davidson stage pays off once the
   // products dominate; below kTcDavidsonMin CSFs (solver auto) the solve is
   // latency-bound and runs the single FP64 stage.  The tensor-core stage
@@ -887,7 +1114,7 @@ static void solve(Ctx &c, const std2g_params &p_in, std2g_result *res, const Res
   // also run the single FP64 stage.
   constexpr int kTcDavidsonMin = 16384;
   const bool tc_dav =
-      mixed && ((c.opts.flags & STD2G_FLAG_TENSOR_ALWAYS) ||
+      mixed && !p.rpa && ((c.opts.flags & STD2G_FLAG_TENSOR_ALWAYS) ||
                 ((p.solver == 2 || nci >= kTcDavidsonMin) && !(p.conv_tol > 0 && p.conv_tol < 1e-6)));
   // alpha(w) through the matrix-free operators and the refined iterative solve:
   // when requested (solver == 2), when the dense A+B, A-B and their work copies
@@ -950,7 +1177,8 @@ static void solve(Ctx &c, const std2g_params &p_in, std2g_result *res, const Res
       // correction's exchange products)
       mftc_setup(c.mftc, s, Clow, nao, c.d_slot_ao.get(), Poo, p.velcorr ? Pia : nullptr);
     } else {
-      mf_setup_ops<double>(mf, mf.d, s, Clow, c.d_slot_ao.get(), Poo, Pia, Qs, Ps, p.velcorr);
+      mf_setup_ops<double>(mf, mf.d, s, Clow, c.d_slot_ao.get(), Poo, Pia, Qs, Ps,
+                           p.velcorr || p.rpa);
     }
     mf.ci = d_ci;
     mf.ca = d_ca;
@@ -960,7 +1188,36 @@ static void solve(Ctx &c, const std2g_params &p_in, std2g_result *res, const Res
   int nroot = 0;
   double *X = nullptr, *Yv = nullptr, *om = nullptr;
   double *Bh = nullptr;
-  if (!p.rpa && use_mf) {
+  if (p.rpa && use_mf) {
+    // sTD-DFT roots by the subspace form of srpapack (davidson_rpa.cuh)
+    record(c, PH_EIGEN);
+    om = c.w_eval.ensure(std::max(nci, nao));
+    const double tol = p.conv_tol > 0 ? p.conv_tol : 1e-6;
+    double *d = c.rw.dmf.ensure(nci), *dpd = c.rw.dpd.ensure(nci), *dmd = c.rw.dmd.ensure(nci);
+    S2G_LAUNCH(k_rpa_mf_diag, (int)div_up(nci, 128), 128, 0, s, d, dpd, dmd, d_edall, ekd, uci,
+               d_ci, d_ca, nci, nv, ak, p.ax);
+    const bool amb_diag = std::fabs(p.ax) < 1e-6;
+    MatVec mv_p = [&](const double *V, int nb, double *W) {
+      mf_apply(c.mf, c.blas, s, V, nb, W, 2.0 * ak, -1.0, -p.ax, d);
+    };
+    MatVec mv_m = [&](const double *V, int nb, double *W) {
+      if (amb_diag)   // ax = 0: A-B is its diagonal ed - ak (ia|ia)
+        S2G_LAUNCH(k_diag_mul, grid_for((int64_t)nci * nb), 256, 0, s, W, dmd, V, nci, nb);
+      else
+        mf_apply(c.mf, c.blas, s, V, nb, W, 0.0, -1.0, p.ax, d);
+    };
+    nroot = std::min(p.nroots, nci);
+    X = c.w_X.ensure((size_t)nci * nroot);
+    Yv = c.w_Y.ensure((size_t)nci * nroot);
+    const int conv = davidson_rpa(c.dav, c.davr, c.blas, c.solver, s, mv_p, mv_m, dpd, dmd, nci,
+                                  p.nroots, tol, 300, om, X, Yv);
+    c.dav_iters = c.davr.iters;
+    c.dav_matvecs = 0;
+    c.dav_fp64_matvecs = c.davr.matvecs;
+    if (conv < nroot)
+      throw Error{STD2G_ENOCONV, "sTD-DFT Davidson: " + std::to_string(conv) + " of " +
+                                     std::to_string(nroot) + " roots converged"};
+  } else if (!p.rpa && use_mf) {
     record(c, PH_EIGEN);
     om = c.w_eval.ensure(std::max(nci, nao));
     // residual norm tolerance of the final (FP64) stage; the tensor-core stage
@@ -1050,21 +1307,32 @@ static void solve(Ctx &c, const std2g_params &p_in, std2g_result *res, const Res
       double *musel = c.w_musel.ensure((size_t)nci * 9);
       S2G_LAUNCH(k_gather_mu, grid_for((int64_t)nci * 9), 256, 0, s, musel, c.w_mu_ov.get(), no,
                  nv, d_ci, d_ca, nci);
+      RespReq rq = *resp;
+      if (want_quad && rq.quad->nbeta > 0) {
+        rq.U = c.w_Uall.ensure((size_t)nci * 3 * rq.n);
+        rq.V = c.w_Vall.ensure((size_t)nci * 3 * rq.n);
+      }
       if (resp_mf) {
         std::vector<int> fb;
-        response_matfree(c, nci, musel, *resp, fb, d_edall, ekd, uci, ak, p.ax, tc_resp);
+        response_matfree(c, nci, musel, rq, fb, d_edall, ekd, uci, ak, p.ax, tc_resp);
         if (!fb.empty())
           throw Error{STD2G_ENOCONV,
                       "alpha(w): a frequency above the first excitation needs the dense form, "
                       "which does not fit for this CSF space"};
       } else if (mixed) {
         std::vector<int> fb;
-        response_mixed(c, Apb, Amb, nci, musel, *resp, fb);
+        response_mixed(c, Apb, Amb, nci, musel, rq, fb);
         if (!fb.empty()) {
           // frequencies above the first excitation: the FP64 form's factorisations
           std::vector<double> om(fb.size()), al(fb.size() * 9), rs(fb.size());
           for (size_t q = 0; q < fb.size(); ++q) om[q] = resp->omega[fb[q]];
           RespReq sub{om.data(), (int)fb.size(), al.data(), rs.data()};
+          std::vector<int> slots(fb.begin(), fb.end());
+          if (rq.U) {
+            sub.U = rq.U;
+            sub.V = rq.V;
+            sub.slot = slots.data();
+          }
           response(c, Apb, Amb, nci, musel, sub);
           for (size_t q = 0; q < fb.size(); ++q) {
             std::copy(al.begin() + 9 * q, al.begin() + 9 * q + 9, resp->alpha + 9 * fb[q]);
@@ -1072,8 +1340,10 @@ static void solve(Ctx &c, const std2g_params &p_in, std2g_result *res, const Res
           }
         }
       } else {
-        response(c, Apb, Amb, nci, musel, *resp);
+        response(c, Apb, Amb, nci, musel, rq);
       }
+      if (want_quad && rq.quad->nbeta > 0)
+        hyperpolarizability(c, nci, no, nv, d_ci, d_ca, rq.U, rq.V, *rq.quad);
       record(c, PH_COUNT);
       S2G_CUDA(cudaStreamSynchronize(s));
       for (int q = 0; q < PH_COUNT; ++q) {
@@ -1132,6 +1402,29 @@ static void solve(Ctx &c, const std2g_params &p_in, std2g_result *res, const Res
     gemm(c, CUBLAS_OP_N, CUBLAS_OP_N, nci, nroot, nci, 1.0, Apb, nci, X, nci, 0.0, Yv, nci);
     S2G_LAUNCH(k_scale_columns, grid_for((int64_t)nci * nroot), 256, 0, s, Yv, (int64_t)nci,
                nroot, om, 1);
+    if (tpa && tpa->ntpa > 0) {
+      // The state vectors lresp_2PA_SP contracts: under its keyword srpapack
+      // skips the halving of the packed diagonals of (A-B)^1/2 and A+B before
+      // its packed products (srpapack.f:99-106, 116-133), so each diagonal
+      // enters twice: X+Y = (S + diag S) Z / sqrt(w), X-Y = (P + diag P)(X+Y) / w
+      // with S = (A-B)^1/2, P = A+B.  Only the two-photon sums use them.
+      if (tpa->ntpa > nroot)
+        throw Error{STD2G_EINVAL, "number of 2PA excitations too large (more than the roots "
+                                  "below the energy threshold)"};
+      const int nt = tpa->ntpa;
+      double *U2 = c.w_Uall.ensure((size_t)nci * nt), *V2 = c.w_Vall.ensure((size_t)nci * nt);
+      S2G_CUDA(cudaMemcpyAsync(U2, X, sizeof(double) * nci * nt, cudaMemcpyDeviceToDevice, s));
+      S2G_LAUNCH(k_add_diag_cols, grid_for((int64_t)nci * nt), 256, 0, s, U2, Ambh, Mm,
+                 (int64_t)nci, nt, om, 0);
+      gemm(c, CUBLAS_OP_N, CUBLAS_OP_N, nci, nt, nci, 1.0, Apb, nci, U2, nci, 0.0, V2, nci);
+      S2G_LAUNCH(k_add_diag_cols, grid_for((int64_t)nci * nt), 256, 0, s, V2, Apb, U2,
+                 (int64_t)nci, nt, om, 1);
+      S2G_LAUNCH(k_scale_columns, grid_for((int64_t)nci * nt), 256, 0, s, V2, (int64_t)nci, nt,
+                 om, 1);
+      S2G_LAUNCH(k_xy_from_uv, grid_for((int64_t)nci * nt), 256, 0, s,
+                 c.w_tpx.ensure((size_t)nci * nt), c.w_tpy.ensure((size_t)nci * nt), U2, V2,
+                 (int64_t)nci * nt, 0.5);
+    }
   }
 
   // ---- properties (stda.f:1207-1289, apbtrafo.f:23-243) ----
@@ -1213,6 +1506,10 @@ static void solve(Ctx &c, const std2g_params &p_in, std2g_result *res, const Res
     }
     for (int q = 0; q < 6; ++q) res->alpha0[q] = h_props[4 * nroot + q];
     if (nroot > res->cap) throw Error{STD2G_ECAP, "result capacity too small"};
+  }
+  if (tpa && tpa->ntpa > 0) {
+    if (!p.rpa) throw Error{STD2G_EINVAL, "two-photon absorption needs the sTD-DFT states"};
+    two_photon(c, nci, no, nv, d_ci, d_ca, musel, h_om, *tpa);
   }
 }
 
@@ -1301,6 +1598,48 @@ int std2g_polarizability(void *ctx, const std2g_params *par, const double *omega
     S2G_CUDA(cudaSetDevice(c->opts.device));
     std2g::RespReq rq{omega, nomega, alpha, resid};
     std2g::solve(*c, *par, nullptr, &rq);
+  });
+}
+
+int std2g_hyperpolarizability(void *ctx, const std2g_params *par, const double *omega,
+                              int nomega, double *beta, double *beta_hrs) {
+  if (!ctx || !par || !omega || nomega <= 0 || !beta) return STD2G_EINVAL;
+  auto *c = (Ctx *)ctx;
+  return guard([&] {
+    S2G_CUDA(cudaSetDevice(c->opts.device));
+    // at most 5 (w, -2w) pairs per refined solve: its CG runs 3 columns per frequency
+    for (int k0 = 0; k0 < nomega; k0 += 5) {
+      const int nk = std::min(5, nomega - k0);
+      std::vector<double> om(2 * nk), al(2 * nk * 9), rs(2 * nk);
+      for (int k = 0; k < nk; ++k) {
+        om[2 * k] = omega[k0 + k];
+        om[2 * k + 1] = -2.0 * omega[k0 + k];
+      }
+      std2g::QuadReq q;
+      q.beta = beta + (size_t)27 * k0;
+      q.beta_hrs = beta_hrs ? beta_hrs + k0 : nullptr;
+      q.nbeta = nk;
+      std2g::RespReq rq{om.data(), 2 * nk, al.data(), rs.data()};
+      rq.quad = &q;
+      std2g::solve(*c, *par, nullptr, &rq);
+    }
+  });
+}
+
+int std2g_two_photon(void *ctx, const std2g_params *par, int ntrans, double *rows) {
+  if (!ctx || !par || ntrans <= 0 || !rows) return STD2G_EINVAL;
+  auto *c = (Ctx *)ctx;
+  return guard([&] {
+    S2G_CUDA(cudaSetDevice(c->opts.device));
+    std2g_params p = *par;
+    p.rpa = 1;
+    p.velcorr = 0;
+    p.nroots = 0;      // the states come from the dense sRPA window (srpapack)
+    p.solver = 1;
+    std2g::QuadReq q;
+    q.tpa = rows;
+    q.ntpa = ntrans;
+    std2g::solve(*c, p, nullptr, nullptr, &q);
   });
 }
 

@@ -586,4 +586,54 @@ __global__ void k_resid_ratio(const double *__restrict__ R, const double *__rest
   if (threadIdx.x == 0) *out = worst;
 }
 
+// box[v*no*nv + i + no*a] = Y[u + nci*v] for the CSF u = (i, a) (box zeroed first)
+__global__ void k_box_scatter(double *__restrict__ box, const double *__restrict__ Y,
+                              const int *__restrict__ ci, const int *__restrict__ ca, int nci,
+                              int no, int nv, int nvec) {
+  const int64_t total = (int64_t)nci * nvec;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int v = (int)(t / nci), u = (int)(t - (int64_t)v * nci);
+    box[(int64_t)v * no * nv + ci[u] + (int64_t)no * ca[u]] = Y[t];
+  }
+}
+
+// sel[u + nci*col] = box[col*no*nv + i + no*a] for the CSF u = (i, a)
+__global__ void k_box_gather(double *__restrict__ sel, const double *__restrict__ box,
+                             const int *__restrict__ ci, const int *__restrict__ ca, int nci,
+                             int no, int nv, int ncol) {
+  const int64_t total = (int64_t)nci * ncol;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int col = (int)(t / nci), u = (int)(t - (int64_t)col * nci);
+    sel[t] = box[(int64_t)col * no * nv + ci[u] + (int64_t)no * ca[u]];
+  }
+}
+
+// X = f (U + V), Y = f (U - V) from U = X+Y, V = X-Y (f = 1/2; 1/4 also halves
+// a response to -2 mu into the response to -mu)
+__global__ void k_xy_from_uv(double *__restrict__ X, double *__restrict__ Y,
+                             const double *__restrict__ U, const double *__restrict__ V,
+                             int64_t n, double f) {
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    X[t] = f * (U[t] + V[t]);
+    Y[t] = f * (U[t] - V[t]);
+  }
+}
+
+// out[i + n*c] += M[i + n*i] * src[i + n*c] * g_c, g_c = 1/sqrt(w_c) (mode 0) or
+// 1 (mode 1): the diagonal of M counted once more in a product with src
+__global__ void k_add_diag_cols(double *__restrict__ out, const double *__restrict__ M,
+                                const double *__restrict__ src, int64_t n, int ncol,
+                                const double *__restrict__ w, int mode) {
+  const int64_t total = n * ncol;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t c = t / n, i = t - c * n;
+    const double g = mode == 0 ? 1.0 / sqrt(w[c]) : 1.0;
+    out[t] += M[i + n * i] * src[t] * g;
+  }
+}
+
 }  // namespace std2g

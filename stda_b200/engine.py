@@ -32,7 +32,7 @@ EXPORTS = [
     "std2g_kernel_launches", "std2g_kernel_stats", "std2g_solver_stats", "std2g_error_string",
     "std2g_destroy", "std2g_screen_noalloc", "std2g_server_create", "std2g_server_submit",
     "std2g_server_poll", "std2g_server_wait", "std2g_server_stats", "std2g_server_destroy",
-    "std2g_symeig_check", "std2g_set_sm_limit",
+    "std2g_symeig_check", "std2g_set_sm_limit", "std2g_hyperpolarizability", "std2g_two_photon",
 ]
 
 
@@ -100,6 +100,9 @@ def library():
                                    dp, dp, dp, dp]
         lib.std2g_solve.argtypes = [C.c_void_p, C.POINTER(Params), C.POINTER(Result)]
         lib.std2g_polarizability.argtypes = [C.c_void_p, C.POINTER(Params), dp, C.c_int, dp, dp]
+        lib.std2g_hyperpolarizability.argtypes = [C.c_void_p, C.POINTER(Params), dp, C.c_int, dp,
+                                                  dp]
+        lib.std2g_two_photon.argtypes = [C.c_void_p, C.POINTER(Params), C.c_int, dp]
         lib.std2g_get_csf.argtypes = [C.c_void_p, ip, dp, C.c_int, ip]
         lib.std2g_get_vectors.argtypes = [C.c_void_p, dp, dp, C.c_int, ip, ip]
         lib.std2g_phase_times.argtypes = [C.c_void_p, dp, C.c_int]
@@ -290,6 +293,25 @@ class Engine:
         _check(self.lib.std2g_polarizability(self.ctx, C.byref(kw.to_c()), _dp(om), len(om),
                                              _dp(out), _dp(resid)))
         return out.reshape(len(om), 3, 3), resid
+
+    def hyperpolarizability(self, kw: Keywords, wavelengths_nm):
+        """beta(-2w; w, w) as lresp1 prints it (linear_response.f:196-700): at
+        w = 0 and at w = 45.56335 / lambda for each wavelength (nm).  Returns
+        (w in eV as printed, beta [nw, 3, 3, 3], beta_HRS [nw])."""
+        om = np.ascontiguousarray([0.0] + [45.56335 / float(w) for w in wavelengths_nm])
+        beta = np.zeros((len(om), 3, 3, 3))
+        hrs = np.zeros(len(om))
+        _check(self.lib.std2g_hyperpolarizability(self.ctx, C.byref(kw.to_c()), _dp(om), len(om),
+                                                  _dp(beta), _dp(hrs)))
+        return om * 27.21139, beta, hrs
+
+    def two_photon(self, kw: Keywords, ntrans: int):
+        """Two-photon absorption of the lowest ``ntrans`` sTD-DFT states as
+        lresp_2PA_SP writes its 2PA-abs rows (linear_response.f:4604-4938):
+        (n, w_n eV, delta_par, delta_perp, delta_circ, rho) per state."""
+        rows = np.zeros((ntrans, 6))
+        _check(self.lib.std2g_two_photon(self.ctx, C.byref(kw.to_c()), int(ntrans), _dp(rows)))
+        return rows
 
     def csf(self):
         n = C.c_int()

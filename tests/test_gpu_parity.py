@@ -264,3 +264,33 @@ def test_mixed_small_alpha_runs_the_fp64_solve(benzene):
         out.append(eng.polarizability(kw, [0.0, 0.05])[0])
         eng.close()
     assert np.abs(out[0] - out[1]).max() <= 1e-12 * np.abs(out[0]).max()
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_std_dft_iterative_vs_dense_oracle(precision):
+    """sTD-DFT roots by the matrix-free subspace solver (solver 2) against the
+    oracle's dense srpapack restatement: roots to 1e-9 Eh, f_L and f_V to 1e-5
+    relative (FP64 products in both forms)."""
+    from stda_b200 import synth
+    mol, ints = synth.random_molecule(40, seed=4, with_ints=True)
+    kw = dict(ax=0.5, e_thr_ev=8.0)
+    eng, sol, iconf, ed = _run(mol, ints, precision=precision, rpa=True, nroots=10, solver=2,
+                               conv_tol=1e-8, **kw)
+    ref = _oracle(mol, ints, rpa=True, **kw)
+    assert _same_csf(ref, iconf)
+    n = min(10, len(ref.omega))
+    assert len(sol.omega) == n
+    assert np.abs(sol.omega - ref.omega[:n]).max() < 1e-9
+    assert np.allclose(sol.fL, ref.fL[:n], rtol=1e-5, atol=1e-8)
+    assert np.allclose(sol.fV, ref.fV[:n], rtol=1e-5, atol=1e-8)
+    assert np.allclose(sol.RL, ref.RL[:n], rtol=1e-4, atol=1e-6)
+
+
+def test_std_dft_iterative_pure_functional(benzene):
+    """ax = 0: A-B is diagonal (rrpamat stda.f:1893-1928)."""
+    mol, ints = benzene
+    kw = dict(ax=0.0, e_thr_ev=10.0)
+    eng, sol, iconf, ed = _run(mol, ints, rpa=True, nroots=8, solver=2, conv_tol=1e-8, **kw)
+    ref = _oracle(mol, ints, rpa=True, **kw)
+    assert np.abs(sol.omega - ref.omega[:8]).max() < 1e-9
+    assert np.allclose(sol.fL, ref.fL[:8], rtol=1e-5, atol=1e-8)
