@@ -2,7 +2,7 @@
  * std2g -- B200 (sm_100a) engine for the sTDA / sTD-DFT excited-state path of
  * std2.  Plain C ABI: plain pointers and sizes, integer status codes, no
  * C++ or framework types, so that the Fortran host can bind it with
- * iso_c_binding (see INTEGRATION.md) and any other host through its FFI.
+ * iso_c_binding and any other host through its FFI.
  *
  * The boundary replaces one Fortran call of the reference,
  *
@@ -245,7 +245,8 @@ typedef struct {
   int device;
   int precision;        /* as std2g_opts.precision, for every slot */
   int slots;            /* concurrent solves (1..64) */
-  int reserved;
+  int trace;            /* > 0: one line per finished request on stderr (slot,
+                           times, phase times of its solve and alpha(omega)) */
   int64_t hbm_budget;   /* bytes the admitted requests may use (0: 80 % of free memory) */
 } std2g_server_opts;
 

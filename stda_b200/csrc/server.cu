@@ -12,9 +12,10 @@
 //     requests already in flight (or nothing else is in flight), in FIFO
 //     order, so requests that arrive while others run start as soon as slots
 //     and memory free up and their kernels overlap on the device;
-//   * each slot's persistent tensor-core kernels use an equal share of the SMs
-//     (std2g_set_sm_limit), so a large request does not hold every SM while
-//     small ones wait;
+//   * a request's persistent tensor-core kernels use an equal share of the
+//     SMs among the requests in flight when it starts (std2g_set_sm_limit):
+//     the whole device when it runs alone, a 1/k share when k run at once, so
+//     a large request does not hold every SM while small ones wait;
 //   * inputs are copied at submit, results are kept until std2g_server_wait;
 //   * a slot that ran a large request (estimate above budget / slots) or
 //     ran out of memory gets a fresh context; a request that ran out of
@@ -22,7 +23,9 @@
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
+#include <cstdio>
 #include <cstring>
+#include <string>
 #include <deque>
 #include <memory>
 #include <mutex>
@@ -52,6 +55,9 @@ struct Job {
   int status = STD2G_OK;
   std2g_result res{};
   std::vector<double> om, fL, fV, RL, RV, resid, alpha, alpha_resid;
+  // trace: phase times (ms) of the solve and of alpha(omega), load time
+  std::vector<double> ph_solve, ph_alpha;
+  double load_ms = 0;
 };
 
 struct Server {
@@ -71,13 +77,19 @@ struct Server {
   bool stop = false;
   int64_t submitted = 0, completed = 0, peak_bytes = 0;
   int peak_inflight = 0;
+  int dev_sms = 148;
 };
 
-// Estimated device bytes of one solve from the input sizes alone (the CSF
+// Estimated device bytes of one request from the input sizes alone (the CSF
 // count is not known before the screen): charge and gamma-product tensors
 // over the largest possible window (all occupied x all virtual MOs), AO-basis
-// work arrays, and the PT coupling buffers up to their chunk budget.
-int64_t footprint_estimate(const Job &j) {
+// work arrays, the PT coupling buffers up to their chunk budget, and either
+// the dense CSF matrices or the matrix-free solvers' subspaces, chosen by the
+// engine's own rules (std2g_solve: dense eigensolve for all roots, solver 1 or
+// up to 1024 CSFs; std2g_polarizability: matrix-free for solver 2, when the
+// dense form needs more than 24 GB, and in the mixed form (precision 1) with
+// solver 0 above 4096 CSFs).
+int64_t footprint_estimate(const Job &j, int precision) {
   int64_t nocc = 0;
   for (double o : j.occ)
     if (o > 1e-8) ++nocc;
@@ -87,18 +99,32 @@ int64_t footprint_estimate(const Job &j) {
   b += 8 * (16 * nao * nao + 12 * (int64_t)j.nmo * nao);
   b += std::min<int64_t>(6000000000LL, 8 * pairs * std::min<int64_t>(pairs, 4096));
   const int64_t nci = std::min<int64_t>(pairs, 30000);
-  if (nci <= 1024 || j.par.rpa || !j.omega.empty())
+  bool dense = j.par.nroots <= 0 || j.par.solver == 1 || nci <= 1024;
+  if (!j.omega.empty()) {
+    const bool resp_mf = j.par.solver == 2 || (double)nci * nci * 8.0 * 10.0 > 24e9 ||
+                         (precision == 1 && j.par.solver == 0 && nci > 4096);
+    dense |= !resp_mf;
+  }
+  if (dense)
     b += 12 * 8 * nci * nci;   // dense K, J, Kx, A+B, A-B and their work copies
   else
-    b += 4 * 8 * nci * 512;    // Davidson subspace and products
+    b += 4 * 8 * nci * 512;    // Davidson subspace and products, CG vectors
   return b;
 }
 
-void run_job(void *ctx, Job &j) {
+std::vector<double> phases_of(void *ctx) {
+  std::vector<double> ph(32, 0.0);
+  ph.resize(std::min(32, std2g_phase_times(ctx, ph.data(), 32)));
+  return ph;
+}
+
+void run_job(void *ctx, Job &j, bool trace) {
   j.t_start = Clock::now();
   int st = std2g_load(ctx, j.ncent, j.nmo, j.nao, j.xyz.data(), j.C.data(), j.eps.data(),
                       j.occ.data(), j.iaoat.data(), j.S.data(), j.muL.data(), j.muV.data(),
                       j.muM.data());
+  if (trace)
+    j.load_ms = std::chrono::duration<double, std::milli>(Clock::now() - j.t_start).count();
   if (st == STD2G_OK) {
     const int cap = j.par.nroots > 0 ? j.par.nroots : 20000;
     j.om.assign(cap, 0.0);
@@ -131,15 +157,40 @@ void run_job(void *ctx, Job &j) {
       j.res.resid = j.resid.data();
       st = std2g_solve(ctx, &j.par, &j.res);
     }
+    if (trace) j.ph_solve = phases_of(ctx);
   }
   if (st == STD2G_OK && !j.omega.empty()) {
     j.alpha.assign(9 * j.omega.size(), 0.0);
     j.alpha_resid.assign(j.omega.size(), 0.0);
     st = std2g_polarizability(ctx, &j.par, j.omega.data(), (int)j.omega.size(), j.alpha.data(),
                               j.alpha_resid.data());
+    if (trace) j.ph_alpha = phases_of(ctx);
   }
   j.status = st;
   j.t_end = Clock::now();
+}
+
+void print_trace(const Job &j, int slot, int inflight, int share, bool renewed) {
+  using ms = std::chrono::duration<double, std::milli>;
+  std::string line = "std2g server: ticket " + std::to_string(j.ticket) + " slot " +
+                     std::to_string(slot) + " atoms " + std::to_string(j.ncent) + " status " +
+                     std::to_string(j.status) + " inflight " + std::to_string(inflight) +
+                     " sms " + std::to_string(share) + (renewed ? " renewed" : "");
+  char buf[96];
+  std::snprintf(buf, sizeof buf, " queued %.1f run %.1f load %.1f ms",
+                ms(j.t_start - j.t_submit).count(), ms(j.t_end - j.t_start).count(), j.load_ms);
+  line += buf;
+  for (int pass = 0; pass < 2; ++pass) {
+    const auto &ph = pass ? j.ph_alpha : j.ph_solve;
+    if (ph.empty()) continue;
+    line += pass ? " | alpha" : " | solve";
+    for (size_t q = 0; q < ph.size(); ++q)
+      if (ph[q] >= 0.5) {
+        std::snprintf(buf, sizeof buf, " %s %.1f", std2g_phase_name((int)q), ph[q]);
+        line += buf;
+      }
+  }
+  std::fprintf(stderr, "%s\n", line.c_str());
 }
 
 bool can_admit(const Server &s) {
@@ -149,14 +200,14 @@ bool can_admit(const Server &s) {
   return !j.exclusive && s.inflight_bytes + j.footprint <= s.budget;
 }
 
-// Fresh context for a slot: releases every device buffer the old one held.
-// SMs for one slot's persistent tensor-core kernels: an equal share of the device
-int sm_share(const Server &s) {
-  int dev_sms = 148;
-  cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, s.opts.device);
-  return std::max(1, dev_sms / (int)s.ctxs.size());
+// SMs for the persistent tensor-core kernels of a request that starts with
+// `inflight` requests running (itself included): all of them when it runs
+// alone (0 = no cap), else an equal share.
+int sm_share(const Server &s, int inflight) {
+  return inflight <= 1 ? 0 : std::max(1, s.dev_sms / inflight);
 }
 
+// Fresh context for a slot: releases every device buffer the old one held.
 int renew_context(Server *s, int slot) {
   std2g_destroy(s->ctxs[slot]);
   s->ctxs[slot] = nullptr;
@@ -166,7 +217,6 @@ int renew_context(Server *s, int slot) {
   void *ctx = nullptr;
   const int st = std2g_create(&ctx, &eo);
   if (st != STD2G_OK) return st;
-  std2g_set_sm_limit(ctx, sm_share(*s));
   s->ctxs[slot] = ctx;
   return STD2G_OK;
 }
@@ -174,6 +224,7 @@ int renew_context(Server *s, int slot) {
 void worker(Server *s, int slot) {
   for (;;) {
     std::shared_ptr<Job> job;
+    int share = 0, inflight_at_start = 1;
     {
       std::unique_lock<std::mutex> lk(s->mu);
       s->cv_queue.wait(lk, [&] { return s->stop || can_admit(*s); });
@@ -184,8 +235,11 @@ void worker(Server *s, int slot) {
       ++s->inflight;
       s->peak_inflight = std::max(s->peak_inflight, s->inflight);
       s->peak_bytes = std::max(s->peak_bytes, s->inflight_bytes);
+      share = sm_share(*s, s->inflight);
+      inflight_at_start = s->inflight;
     }
-    run_job(s->ctxs[slot], *job);
+    std2g_set_sm_limit(s->ctxs[slot], share);
+    run_job(s->ctxs[slot], *job, s->opts.trace > 0);
     // Context buffers only grow; after a large request (or a failed one) the
     // slot starts again from a fresh context so that idle slots do not hold
     // memory the admission rule no longer counts.
@@ -193,6 +247,7 @@ void worker(Server *s, int slot) {
     const bool large = job->footprint > s->budget / (int64_t)s->ctxs.size();
     int renew = STD2G_OK;
     if (out_of_memory || large) renew = renew_context(s, slot);
+    if (s->opts.trace > 0) print_trace(*job, slot, inflight_at_start, share, out_of_memory || large);
     const bool alive = renew == STD2G_OK;
     bool retry = out_of_memory && !job->exclusive && alive;
     {
@@ -246,6 +301,7 @@ int std2g_server_create(void **srv, const std2g_server_opts *o) {
   size_t free_b = 0, total_b = 0;
   if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) return STD2G_ECUDA;
   s->budget = o->hbm_budget > 0 ? o->hbm_budget : (int64_t)(0.8 * (double)free_b);
+  cudaDeviceGetAttribute(&s->dev_sms, cudaDevAttrMultiProcessorCount, o->device);
   for (int k = 0; k < o->slots; ++k) {
     std2g_opts eo{};
     eo.device = o->device;
@@ -259,8 +315,6 @@ int std2g_server_create(void **srv, const std2g_server_opts *o) {
     }
     s->ctxs.push_back(ctx);
   }
-  const int share = sm_share(*s);
-  for (void *c : s->ctxs) std2g_set_sm_limit(c, share);
   s->alive_workers = o->slots;
   for (int k = 0; k < o->slots; ++k) s->workers.emplace_back(worker, s.get(), k);
   *srv = s.release();
@@ -289,7 +343,7 @@ int std2g_server_submit(void *srv, const std2g_request *rq, int64_t *ticket) {
   j->muM = copy_of(rq->mu_M, 3 * npk);
   if (rq->nomega > 0) j->omega = copy_of(rq->omega, (size_t)rq->nomega);
   j->par = rq->params;
-  j->footprint = footprint_estimate(*j);
+  j->footprint = footprint_estimate(*j, s->opts.precision);
   j->t_submit = Clock::now();
   {
     std::lock_guard<std::mutex> lk(s->mu);

@@ -61,7 +61,7 @@ class Params(C.Structure):
 
 class ServerOpts(C.Structure):
     _fields_ = [("device", C.c_int), ("precision", C.c_int), ("slots", C.c_int),
-                ("reserved", C.c_int), ("hbm_budget", C.c_int64)]
+                ("trace", C.c_int), ("hbm_budget", C.c_int64)]
 
 
 class Request(C.Structure):
@@ -378,14 +378,17 @@ class Server:
     ``submit`` copies the inputs and returns a ticket at once; ``wait`` blocks
     until that request has finished and returns its roots and properties,
     alpha(omega) when requested, and its queued / running / total times (ms).
+    ``trace=True`` prints one line per finished request on stderr (slot,
+    requests in flight at its start, SM share, times, phase times).
     """
 
     def __init__(self, device: int = 0, precision: int = 1, slots: int = 4,
-                 hbm_budget: int = 0):
+                 hbm_budget: int = 0, trace: bool = False):
         self.lib = library()
         self.srv = C.c_void_p()
         _check(self.lib.std2g_server_create(C.byref(self.srv),
-                                            C.byref(ServerOpts(device, precision, slots, 0,
+                                            C.byref(ServerOpts(device, precision, slots,
+                                                               int(bool(trace)),
                                                                int(hbm_budget)))))
         self._nomega = {}
 
