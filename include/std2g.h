@@ -136,6 +136,29 @@ int std2g_load(void *ctx, int ncent, int nmo, int nao,
                const double *occ, const int *iaoat, const double *S,
                const double *mu_L, const double *mu_V, const double *mu_M);
 
+/* AO one-electron integrals on the device from the primitive list the
+   reference's readers fill (readbasmold.f:330-517, readxtb.f:150-160) and its
+   integral step consumes (intslvm.f:21-210; libcint.f:19-352, 653-756):
+     ipty [nprims]  Cartesian type 1..20: s; px py pz; xx yy zz xy xz yz;
+                    xxx yyy zzz xxy xxz xyy yyz xzz yzz xyz (intpack.f90:1213-1218)
+     ipao [nprims]  AO of the primitive, 1-based
+     ipat [nprims]  atom of the primitive, 1-based
+     exip [nprims]  exponent;  cxip [nprims] coefficient, all normalisation folded in
+   Writes the packed S, mu_L, mu_V, mu_M of std2g_load (host arrays; any may be
+   NULL to skip it).  Replaces the host precompute of main.f:756-797. */
+int std2g_ao_integrals(void *ctx, int ncent, const double *xyz, int nao, int nprims,
+                       const int *ipty, const int *ipao, const int *ipat,
+                       const double *exip, const double *cxip, double *S,
+                       double *mu_L, double *mu_V, double *mu_M);
+
+/* std2g_load with the AO integrals formed on the device from the primitive
+   list (as std2g_ao_integrals); iaoat follows from iaoat(ipao(i)) = ipat(i)
+   (intslvm.f:71-74).  No integral array crosses the host link. */
+int std2g_load_prims(void *ctx, int ncent, int nmo, int nao, const double *xyz,
+                     const double *C, const double *eps, const double *occ,
+                     int nprims, const int *ipty, const int *ipao, const int *ipat,
+                     const double *exip, const double *cxip);
+
 /* Run the excitation path: orbital window, S^1/2, Loewdin charges, gamma,
    diagonal screen, PT selection, A (or A+B / A-B), eigen-solve, properties and
    (sTDA) the velocity correction.  Replaces stda.f:142-1471 for the RKS

@@ -21,6 +21,7 @@
 #include "kernels_fp64.cuh"
 #include "davidson.cuh"
 #include "davidson_rpa.cuh"
+#include "ao_ints.cuh"
 #include "matfree.cuh"
 #include "matfree_tc.cuh"
 #include "pt_tc.cuh"
@@ -50,6 +51,7 @@ struct Ctx {
   bool loaded = false;
   int ncent = 0, nmo = 0, nao = 0;
   std::vector<double> h_eps, h_occ, h_xyz;
+  AoIntsWork aoi;   // primitive list of the device AO integrals (ao_ints.cuh)
   // device inputs
   DBuf<double> d_xyz, d_C, d_eps_act, d_eta, d_Sfull, d_sqrtS, d_ao9;
   DBuf<int> d_ao_ptr, d_ao_list, d_iaoat, d_slot_ao;
@@ -181,11 +183,15 @@ static uint64_t fnv1a(const std::vector<int> &a, const std::vector<int> &b) {
 }
 
 // --------------------------------------------------------------------------
+// Inputs of one molecule.  The packed integrals come either from the host
+// (S, muL, muV, muM) or, with pk_dev, already on the device in the layout of
+// k_ao_ints (10 x npk: S, L, V, M).
 static void load(Ctx &c, int ncent, int nmo, int nao, const double *xyz, const double *C,
                  const double *eps, const double *occ, const int *iaoat, const double *S,
-                 const double *muL, const double *muV, const double *muM) {
-  if (ncent <= 0 || nmo <= 0 || nao <= 0 || !xyz || !C || !eps || !occ || !iaoat || !S || !muL ||
-      !muV || !muM)
+                 const double *muL, const double *muV, const double *muM,
+                 const double *pk_dev = nullptr) {
+  if (ncent <= 0 || nmo <= 0 || nao <= 0 || !xyz || !C || !eps || !occ || !iaoat ||
+      (!pk_dev && (!S || !muL || !muV || !muM)))
     throw Error{STD2G_EINVAL, "load: bad arguments"};
   c.ncent = ncent;
   c.nmo = nmo;
@@ -232,11 +238,17 @@ static void load(Ctx &c, int ncent, int nmo, int nao, const double *xyz, const d
   S2G_CUDA(cudaMemcpyAsync(c.d_ao_list.ensure(nao), list.data(), sizeof(int) * nao,
                            cudaMemcpyHostToDevice, s));
   // packed integrals -> full AO matrices (BLOWSY, onetri.f:62-80)
-  double *pk = c.w_work.ensure(npk * 10);
-  S2G_CUDA(cudaMemcpyAsync(pk, S, sizeof(double) * npk, cudaMemcpyHostToDevice, s));
-  S2G_CUDA(cudaMemcpyAsync(pk + npk, muL, sizeof(double) * npk * 3, cudaMemcpyHostToDevice, s));
-  S2G_CUDA(cudaMemcpyAsync(pk + 4 * npk, muV, sizeof(double) * npk * 3, cudaMemcpyHostToDevice, s));
-  S2G_CUDA(cudaMemcpyAsync(pk + 7 * npk, muM, sizeof(double) * npk * 3, cudaMemcpyHostToDevice, s));
+  const double *pk = pk_dev;
+  if (!pk) {
+    double *h2d = c.w_work.ensure(npk * 10);
+    S2G_CUDA(cudaMemcpyAsync(h2d, S, sizeof(double) * npk, cudaMemcpyHostToDevice, s));
+    S2G_CUDA(cudaMemcpyAsync(h2d + npk, muL, sizeof(double) * npk * 3, cudaMemcpyHostToDevice, s));
+    S2G_CUDA(cudaMemcpyAsync(h2d + 4 * npk, muV, sizeof(double) * npk * 3, cudaMemcpyHostToDevice,
+                             s));
+    S2G_CUDA(cudaMemcpyAsync(h2d + 7 * npk, muM, sizeof(double) * npk * 3, cudaMemcpyHostToDevice,
+                             s));
+    pk = h2d;
+  }
   size_t nn = (size_t)nao * nao;
   double *Sf = c.d_Sfull.ensure(nn);
   double *ao9 = c.d_ao9.ensure(nn * 9);
@@ -1577,6 +1589,43 @@ int std2g_load(void *ctx, int ncent, int nmo, int nao, const double *xyz, const 
   return guard([&] {
     S2G_CUDA(cudaSetDevice(c->opts.device));
     std2g::load(*c, ncent, nmo, nao, xyz, C, eps, occ, iaoat, S, mu_L, mu_V, mu_M);
+  });
+}
+
+int std2g_ao_integrals(void *ctx, int ncent, const double *xyz, int nao, int nprims,
+                       const int *ipty, const int *ipao, const int *ipat, const double *exip,
+                       const double *cxip, double *S, double *mu_L, double *mu_V, double *mu_M) {
+  if (!ctx) return STD2G_EINVAL;
+  auto *c = (Ctx *)ctx;
+  return guard([&] {
+    S2G_CUDA(cudaSetDevice(c->opts.device));
+    cudaStream_t s = c->stream;
+    const size_t npk = (size_t)nao * (nao + 1) / 2;
+    double *pk = c->w_work.ensure(npk * 10);
+    std2g::ao_ints(c->aoi, s, ncent, xyz, nao, nprims, ipty, ipao, ipat, exip, cxip, pk);
+    double *dst[4] = {S, mu_L, mu_V, mu_M};
+    const size_t off[4] = {0, npk, 4 * npk, 7 * npk}, cnt[4] = {npk, 3 * npk, 3 * npk, 3 * npk};
+    for (int q = 0; q < 4; ++q)
+      if (dst[q])
+        S2G_CUDA(cudaMemcpyAsync(dst[q], pk + off[q], sizeof(double) * cnt[q],
+                                 cudaMemcpyDeviceToHost, s));
+    S2G_CUDA(cudaStreamSynchronize(s));
+  });
+}
+
+int std2g_load_prims(void *ctx, int ncent, int nmo, int nao, const double *xyz, const double *C,
+                     const double *eps, const double *occ, int nprims, const int *ipty,
+                     const int *ipao, const int *ipat, const double *exip, const double *cxip) {
+  if (!ctx) return STD2G_EINVAL;
+  auto *c = (Ctx *)ctx;
+  return guard([&] {
+    S2G_CUDA(cudaSetDevice(c->opts.device));
+    const size_t npk = (size_t)nao * (nao + 1) / 2;
+    double *pk = c->w_work.ensure(npk * 10);
+    const std::vector<int> iaoat = std2g::ao_ints(c->aoi, c->stream, ncent, xyz, nao, nprims,
+                                                  ipty, ipao, ipat, exip, cxip, pk);
+    std2g::load(*c, ncent, nmo, nao, xyz, C, eps, occ, iaoat.data(), nullptr, nullptr, nullptr,
+                nullptr, pk);
   });
 }
 

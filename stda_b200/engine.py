@@ -33,6 +33,7 @@ EXPORTS = [
     "std2g_destroy", "std2g_screen_noalloc", "std2g_server_create", "std2g_server_submit",
     "std2g_server_poll", "std2g_server_wait", "std2g_server_stats", "std2g_server_destroy",
     "std2g_symeig_check", "std2g_set_sm_limit", "std2g_hyperpolarizability", "std2g_two_photon",
+    "std2g_ao_integrals", "std2g_load_prims",
 ]
 
 
@@ -98,6 +99,10 @@ def library():
         lib.std2g_create.argtypes = [C.POINTER(C.c_void_p), C.POINTER(Opts)]
         lib.std2g_load.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, dp, dp, dp, dp, ip,
                                    dp, dp, dp, dp]
+        lib.std2g_ao_integrals.argtypes = [C.c_void_p, C.c_int, dp, C.c_int, C.c_int, ip, ip, ip,
+                                           dp, dp, dp, dp, dp, dp]
+        lib.std2g_load_prims.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, dp, dp, dp, dp,
+                                         C.c_int, ip, ip, ip, dp, dp]
         lib.std2g_solve.argtypes = [C.c_void_p, C.POINTER(Params), C.POINTER(Result)]
         lib.std2g_polarizability.argtypes = [C.c_void_p, C.POINTER(Params), dp, C.c_int, dp, dp]
         lib.std2g_hyperpolarizability.argtypes = [C.c_void_p, C.POINTER(Params), dp, C.c_int, dp,
@@ -230,6 +235,45 @@ def boundary_inputs(mol, ints=None) -> BoundaryInputs:
         muV=np.ascontiguousarray(pack_lower(V)), muM=np.ascontiguousarray(pack_lower(M)))
 
 
+@dataclass
+class Primitives:
+    """The primitive list of std2's readers (readbasmold.f:330-517,
+    readxtb.f:150-160): per primitive its Cartesian type (1..20), AO and atom
+    (1-based), exponent and coefficient with every normalisation folded in."""
+    ipty: np.ndarray
+    ipao: np.ndarray
+    ipat: np.ndarray
+    exip: np.ndarray
+    cxip: np.ndarray
+
+    @property
+    def nprims(self):
+        return len(self.ipty)
+
+
+# Cartesian exponents -> the reference's primitive type (intpack.f90:1213-1218)
+_CART_TYPE = {(0, 0, 0): 1, (1, 0, 0): 2, (0, 1, 0): 3, (0, 0, 1): 4, (2, 0, 0): 5,
+              (0, 2, 0): 6, (0, 0, 2): 7, (1, 1, 0): 8, (1, 0, 1): 9, (0, 1, 1): 10,
+              (3, 0, 0): 11, (0, 3, 0): 12, (0, 0, 3): 13, (2, 1, 0): 14, (2, 0, 1): 15,
+              (1, 2, 0): 16, (0, 2, 1): 17, (1, 0, 2): 18, (0, 1, 2): 19, (1, 1, 1): 20}
+
+
+def primitives(mol) -> Primitives:
+    """The primitive list of a molecule's contracted Cartesian basis (AO order
+    and normalisation of :meth:`~stda_b200.molden.Molecule.ao_functions`)."""
+    ipty, ipao, ipat, exip, cxip = [], [], [], [], []
+    for k, (atom, lmn, exps, c) in enumerate(mol.ao_functions()):
+        for a, cc in zip(exps, c):
+            ipty.append(_CART_TYPE[tuple(lmn)])
+            ipao.append(k + 1)
+            ipat.append(atom + 1)
+            exip.append(float(a))
+            cxip.append(float(cc))
+    i32 = lambda v: np.ascontiguousarray(v, dtype=np.int32)  # noqa: E731
+    f64 = lambda v: np.ascontiguousarray(v, dtype=np.float64)  # noqa: E731
+    return Primitives(i32(ipty), i32(ipao), i32(ipat), f64(exip), f64(cxip))
+
+
 class Engine:
     """One std2g context on one device (``precision`` 0: FP64, 1: mixed)."""
 
@@ -261,6 +305,32 @@ class Engine:
             self.ctx, b.ncent, b.nmo, b.nao, _dp(b.xyz4), _dp(b.C), _dp(b.eps), _dp(b.occ),
             b.iaoat1.ctypes.data_as(C.POINTER(C.c_int)), _dp(b.S), _dp(b.muL), _dp(b.muV),
             _dp(b.muM)))
+
+    def ao_integrals(self, xyz4, nao: int, pr: Primitives):
+        """Packed S, mu_L, mu_V, mu_M (std2g_load layout) formed on the device."""
+        npk = nao * (nao + 1) // 2
+        S, L, V, M = np.zeros(npk), np.zeros(3 * npk), np.zeros(3 * npk), np.zeros(3 * npk)
+        ip = lambda a: a.ctypes.data_as(C.POINTER(C.c_int))  # noqa: E731
+        xyz4 = np.ascontiguousarray(xyz4, dtype=np.float64)
+        _check(self.lib.std2g_ao_integrals(self.ctx, xyz4.shape[0], _dp(xyz4), nao, pr.nprims,
+                                           ip(pr.ipty), ip(pr.ipao), ip(pr.ipat), _dp(pr.exip),
+                                           _dp(pr.cxip), _dp(S), _dp(L), _dp(V), _dp(M)))
+        return S, L.reshape(3, npk), V.reshape(3, npk), M.reshape(3, npk)
+
+    def load_prims(self, xyz4, C_mo, eps, occ, pr: Primitives):
+        """std2g_load_prims: MOs plus the primitive list; integrals on the device."""
+        xyz4 = np.ascontiguousarray(xyz4, dtype=np.float64)
+        Cf = np.asfortranarray(C_mo, dtype=np.float64)
+        eps = np.ascontiguousarray(eps, dtype=np.float64)
+        occ = np.ascontiguousarray(occ, dtype=np.float64)
+        from .tdadat import molecular_mass
+        self.xmolw = molecular_mass(xyz4[:, 3])
+        self.inputs = None
+        ip = lambda a: a.ctypes.data_as(C.POINTER(C.c_int))  # noqa: E731
+        _check(self.lib.std2g_load_prims(self.ctx, xyz4.shape[0], Cf.shape[1], Cf.shape[0],
+                                         _dp(xyz4), _dp(Cf), _dp(eps), _dp(occ), pr.nprims,
+                                         ip(pr.ipty), ip(pr.ipao), ip(pr.ipat), _dp(pr.exip),
+                                         _dp(pr.cxip)))
 
     def solve(self, kw: Keywords, cap: int = 4096) -> Solution:
         """One solve; ``cap`` is the initial room for roots.  When the window
