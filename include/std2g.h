@@ -281,6 +281,12 @@ typedef struct {
   std2g_params params;  /* the excitation solve (std2g_solve) */
   int nomega;           /* > 0: also alpha(omega) (std2g_polarizability) */
   const double *omega;  /* [nomega] Eh */
+  /* optional primitive list (as std2g_load_prims): with nprims > 0 the AO
+     integrals are formed on the device and iaoat, S, mu_L, mu_V, mu_M may be
+     NULL */
+  int nprims;
+  const int *ipty, *ipao, *ipat;
+  const double *exip, *cxip;
 } std2g_request;
 
 int std2g_server_create(void **srv, const std2g_server_opts *opts);

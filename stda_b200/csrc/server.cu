@@ -46,6 +46,9 @@ struct Job {
   int ncent = 0, nmo = 0, nao = 0;
   std::vector<double> xyz, C, eps, occ, S, muL, muV, muM, omega;
   std::vector<int> iaoat;
+  // primitive list: AO integrals formed on the device (std2g_load_prims)
+  std::vector<int> ipty, ipao, ipat;
+  std::vector<double> exip, cxip;
   std2g_params par{};
   int64_t footprint = 0;
   bool exclusive = false;   // admitted only when nothing else is in flight
@@ -120,9 +123,13 @@ std::vector<double> phases_of(void *ctx) {
 
 void run_job(void *ctx, Job &j, bool trace) {
   j.t_start = Clock::now();
-  int st = std2g_load(ctx, j.ncent, j.nmo, j.nao, j.xyz.data(), j.C.data(), j.eps.data(),
-                      j.occ.data(), j.iaoat.data(), j.S.data(), j.muL.data(), j.muV.data(),
-                      j.muM.data());
+  int st = j.ipty.empty()
+               ? std2g_load(ctx, j.ncent, j.nmo, j.nao, j.xyz.data(), j.C.data(), j.eps.data(),
+                            j.occ.data(), j.iaoat.data(), j.S.data(), j.muL.data(),
+                            j.muV.data(), j.muM.data())
+               : std2g_load_prims(ctx, j.ncent, j.nmo, j.nao, j.xyz.data(), j.C.data(),
+                                  j.eps.data(), j.occ.data(), (int)j.ipty.size(), j.ipty.data(),
+                                  j.ipao.data(), j.ipat.data(), j.exip.data(), j.cxip.data());
   if (trace)
     j.load_ms = std::chrono::duration<double, std::milli>(Clock::now() - j.t_start).count();
   if (st == STD2G_OK) {
@@ -323,8 +330,12 @@ int std2g_server_create(void **srv, const std2g_server_opts *o) {
 
 int std2g_server_submit(void *srv, const std2g_request *rq, int64_t *ticket) {
   if (!srv || !rq || !ticket || rq->ncent <= 0 || rq->nmo <= 0 || rq->nao <= 0 || !rq->xyz ||
-      !rq->C || !rq->eps || !rq->occ || !rq->iaoat || !rq->S || !rq->mu_L || !rq->mu_V ||
-      !rq->mu_M || rq->nomega < 0 || (rq->nomega > 0 && !rq->omega))
+      !rq->C || !rq->eps || !rq->occ || rq->nomega < 0 || (rq->nomega > 0 && !rq->omega) ||
+      rq->nprims < 0)
+    return STD2G_EINVAL;
+  const bool prims = rq->nprims > 0;
+  if (prims ? (!rq->ipty || !rq->ipao || !rq->ipat || !rq->exip || !rq->cxip)
+            : (!rq->iaoat || !rq->S || !rq->mu_L || !rq->mu_V || !rq->mu_M))
     return STD2G_EINVAL;
   auto *s = (Server *)srv;
   auto j = std::make_shared<Job>();
@@ -336,11 +347,20 @@ int std2g_server_submit(void *srv, const std2g_request *rq, int64_t *ticket) {
   j->C = copy_of(rq->C, (size_t)rq->nao * rq->nmo);
   j->eps = copy_of(rq->eps, (size_t)rq->nmo);
   j->occ = copy_of(rq->occ, (size_t)rq->nmo);
-  j->iaoat = copy_of(rq->iaoat, (size_t)rq->nao);
-  j->S = copy_of(rq->S, npk);
-  j->muL = copy_of(rq->mu_L, 3 * npk);
-  j->muV = copy_of(rq->mu_V, 3 * npk);
-  j->muM = copy_of(rq->mu_M, 3 * npk);
+  if (prims) {
+    const size_t np = (size_t)rq->nprims;
+    j->ipty = copy_of(rq->ipty, np);
+    j->ipao = copy_of(rq->ipao, np);
+    j->ipat = copy_of(rq->ipat, np);
+    j->exip = copy_of(rq->exip, np);
+    j->cxip = copy_of(rq->cxip, np);
+  } else {
+    j->iaoat = copy_of(rq->iaoat, (size_t)rq->nao);
+    j->S = copy_of(rq->S, npk);
+    j->muL = copy_of(rq->mu_L, 3 * npk);
+    j->muV = copy_of(rq->mu_V, 3 * npk);
+    j->muM = copy_of(rq->mu_M, 3 * npk);
+  }
   if (rq->nomega > 0) j->omega = copy_of(rq->omega, (size_t)rq->nomega);
   j->par = rq->params;
   j->footprint = footprint_estimate(*j, s->opts.precision);

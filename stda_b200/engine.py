@@ -72,7 +72,10 @@ class Request(C.Structure):
                 ("iaoat", C.POINTER(C.c_int)), ("S", C.POINTER(C.c_double)),
                 ("mu_L", C.POINTER(C.c_double)), ("mu_V", C.POINTER(C.c_double)),
                 ("mu_M", C.POINTER(C.c_double)), ("params", Params), ("nomega", C.c_int),
-                ("omega", C.POINTER(C.c_double))]
+                ("omega", C.POINTER(C.c_double)), ("nprims", C.c_int),
+                ("ipty", C.POINTER(C.c_int)), ("ipao", C.POINTER(C.c_int)),
+                ("ipat", C.POINTER(C.c_int)), ("exip", C.POINTER(C.c_double)),
+                ("cxip", C.POINTER(C.c_double))]
 
 
 class Result(C.Structure):
@@ -274,6 +277,37 @@ def primitives(mol) -> Primitives:
     return Primitives(i32(ipty), i32(ipao), i32(ipat), f64(exip), f64(cxip))
 
 
+@dataclass
+class PrimInputs:
+    """A wavefunction with its primitive list instead of AO integrals (the
+    served form's std2g_load_prims requests)."""
+    xyz4: np.ndarray
+    C: np.ndarray
+    eps: np.ndarray
+    occ: np.ndarray
+    prims: Primitives
+
+    @property
+    def ncent(self):
+        return self.xyz4.shape[0]
+
+    @property
+    def nao(self):
+        return self.C.shape[0]
+
+    @property
+    def nmo(self):
+        return self.C.shape[1]
+
+
+def prim_inputs(mol) -> PrimInputs:
+    """Pack a molecule with MOs and its primitive list (no host integrals)."""
+    xyz4 = np.ascontiguousarray(np.hstack([mol.xyz, mol.Z[:, None].astype(np.float64)]))
+    return PrimInputs(xyz4, np.asfortranarray(mol.C, dtype=np.float64),
+                      np.ascontiguousarray(mol.eps, dtype=np.float64),
+                      np.ascontiguousarray(mol.occ, dtype=np.float64), primitives(mol))
+
+
 class Engine:
     """One std2g context on one device (``precision`` 0: FP64, 1: mixed)."""
 
@@ -462,12 +496,23 @@ class Server:
                                                                int(hbm_budget)))))
         self._nomega = {}
 
-    def submit(self, b: BoundaryInputs, kw: Keywords, omegas=None) -> int:
+    def submit(self, b, kw: Keywords, omegas=None) -> int:
+        """Queue one request: ``b`` is a :class:`BoundaryInputs` (packed AO
+        integrals from the host) or a :class:`PrimInputs` (primitive list; the
+        integrals are formed on the device)."""
         om = None if omegas is None else np.ascontiguousarray(omegas, dtype=np.float64)
-        rq = Request(b.ncent, b.nmo, b.nao, _dp(b.xyz4), _dp(b.C), _dp(b.eps), _dp(b.occ),
-                     b.iaoat1.ctypes.data_as(C.POINTER(C.c_int)), _dp(b.S), _dp(b.muL),
-                     _dp(b.muV), _dp(b.muM), kw.to_c(), 0 if om is None else len(om),
-                     None if om is None else _dp(om))
+        ip = lambda a: a.ctypes.data_as(C.POINTER(C.c_int))  # noqa: E731
+        nom = 0 if om is None else len(om)
+        omp = None if om is None else _dp(om)
+        if isinstance(b, PrimInputs):
+            pr = b.prims
+            rq = Request(b.ncent, b.nmo, b.nao, _dp(b.xyz4), _dp(b.C), _dp(b.eps), _dp(b.occ),
+                         None, None, None, None, None, kw.to_c(), nom, omp, pr.nprims,
+                         ip(pr.ipty), ip(pr.ipao), ip(pr.ipat), _dp(pr.exip), _dp(pr.cxip))
+        else:
+            rq = Request(b.ncent, b.nmo, b.nao, _dp(b.xyz4), _dp(b.C), _dp(b.eps), _dp(b.occ),
+                         ip(b.iaoat1), _dp(b.S), _dp(b.muL), _dp(b.muV), _dp(b.muM), kw.to_c(),
+                         nom, omp, 0, None, None, None, None, None)
         t = C.c_int64()
         _check(self.lib.std2g_server_submit(self.srv, C.byref(rq), C.byref(t)))
         self._nomega[t.value] = (0 if om is None else len(om), kw)

@@ -104,3 +104,22 @@ def test_result_room_grows_on_demand():
     assert len(sol.omega) == len(ref.omega)
     assert np.abs(sol.omega - ref.omega).max() < 1e-12
     assert np.allclose(sol.fL, ref.fL, rtol=1e-10, atol=1e-14)
+
+
+def test_primitive_list_requests_in_the_mix():
+    """Requests that carry the primitive list instead of packed integrals
+    (std2g_request.nprims > 0: the worker forms S and mu on the device with
+    std2g_load_prims) give the results of the host-integral requests, also
+    when both kinds share the server."""
+    from stda_b200 import synth
+    from stda_b200.engine import Keywords, boundary_inputs, prim_inputs
+    reqs, reqs_p = [], []
+    for natoms, seed, om in ((20, 31, None), (34, 32, [0.0, 0.05]), (26, 33, None)):
+        mol, ints = synth.random_molecule(natoms, seed=seed, with_ints=True)
+        kw = Keywords(ax=0.5, e_thr_ev=8.5, nroots=6)
+        reqs.append((boundary_inputs(mol, ints), kw, om))
+        reqs_p.append((prim_inputs(mol), kw, om))
+    alone = _alone(reqs, 0)
+    mixed, st = _mix(reqs_p + reqs, 0, slots=3)
+    _same(alone + alone, mixed)
+    assert st["completed"] == 2 * len(reqs)
