@@ -43,9 +43,14 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 KW = dict(ax=0.5, e_thr_ev=7.0, thrp=1e-4, nroots=50)
+# the plain FP64 GPU form that the mixed form is compared with runs its FP64
+# matrix products on cuBLAS (the library baseline, STD2G_FLAG_LIBRARY_FP64);
+# the engine's own DMMA products are reported beside it
+LIB64 = 2
 # DRAM bytes (read + write) per FP32 coupling of the PT contractions, from one
-# ncu capture of both coupling launches on the C216H36 flake
-TC_BYTES_PER_COUPLING = 4.6
+# ncu capture of both coupling launches on the C216H36 flake: (ia|jb) 1.60 GB
+# for 354 M couplings, (ij|ab) 2.72 GB for 360 M couplings
+TC_BYTES_PER_COUPLING = 6.05
 WORKLOAD = ("graphene flake C384H48, valence minimal basis (1584 AOs), ax=0.5, E_thr=7 eV, "
             "thrp=1e-4, lowest 50 roots")
 
@@ -158,7 +163,7 @@ def run_server(precision, pool, reqs, arrivals, slots, device):
     (s, None = all at once) to a request server; return per-request results
     and the throughput / latency summary."""
     from stda_b200.engine import Server
-    srv = Server(device, precision, slots=slots)
+    srv = Server(device, precision, slots=slots, flags=LIB64 if precision == 0 else 0)
     # warm-up (untimed): every context sizes its device buffers for the largest
     # molecule of the pool, with and without alpha(w)
     big = max(range(len(pool)), key=lambda i: pool[i].nao)
@@ -194,7 +199,7 @@ def served_saturation(precision, pool, reqs, slots, device, rates=(8, 16, 32, 64
     arrive and complete.  The saturation throughput of a repeat is the highest
     completed solves/s among the rates whose p99 latency met the SLO."""
     from stda_b200.engine import Server
-    srv = Server(device, precision, slots=slots)
+    srv = Server(device, precision, slots=slots, flags=LIB64 if precision == 0 else 0)
     big = max(range(len(pool)), key=lambda i: pool[i].nao)
     for om in (None, [0.0, 0.03, 0.06]):
         for t in [srv.submit(pool[big], reqs[0][1], om) for _ in range(slots)]:
@@ -231,7 +236,7 @@ def served_saturation(precision, pool, reqs, slots, device, rates=(8, 16, 32, 64
 def plain_fp64(pool, reqs, device):
     """The plain FP64 GPU form: one engine, one molecule at a time."""
     from stda_b200.engine import Engine
-    eng = Engine(device, 0)
+    eng = Engine(device, 0, flags=LIB64)
     i, kw, _ = reqs[0]
     eng.load(pool[i])
     eng.solve(kw)
@@ -274,7 +279,7 @@ def response_cfg2(device):
     out, ref = {}, None
     for name, prec, solver in (("fp64", 0, 0), ("mixed", 1, 0), ("fp64_matrix_free", 0, 2),
                                ("mixed_dense", 1, 1)):
-        eng = Engine(device, prec)
+        eng = Engine(device, prec, flags=LIB64 if prec == 0 else 0)
         eng.load(b)
         kw = Keywords(ax=0.5, e_thr_ev=7.0, solver=solver)
         eng.polarizability(kw, om)
@@ -524,10 +529,15 @@ def main():
                            "peak_source": src, "avg_launch_ms": tc_ms / tc_launch}
 
     if rank == 0 and not args.no_fp64 and prec == 1:
-        e64 = Engine(local, 0)
+        e64 = Engine(local, 0, flags=LIB64)
         e64.load(b)
         s64 = e64.solve(kw)
         l64 = [e64.solve(kw).ms for _ in range(2)]
+        own = Engine(local, 0)
+        own.load(b)
+        own.solve(kw)
+        l64_own = [own.solve(kw).ms for _ in range(2)]
+        own.close()
         iconf_m, _ = eng.csf()
         iconf_d, _ = e64.csf()
         n = min(len(s64.omega), len(sol.omega))
@@ -540,7 +550,9 @@ def main():
                                                       s64.fL[:n][big])) if big.any() else None,
             "max_fL_abs_err": float(np.abs(sol.fL[:n] - s64.fL[:n]).max()),
             "csf_identical": bool(np.array_equal(iconf_m, iconf_d)),
-            "phases_ms": {k: round(v, 3) for k, v in e64.phase_times().items()}}
+            "phases_ms": {k: round(v, 3) for k, v in e64.phase_times().items()},
+            "fp64_products": "cuBLAS DGEMM (library baseline)",
+            "own_dmma_products_ms": statistics.median(l64_own)}
         e64.close()
 
     if rank == 0 and world == 1 and not args.no_serve:

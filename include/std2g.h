@@ -61,6 +61,9 @@ enum {
    size (by default they are used from ~2.5e8 PT couplings and 16384 CSFs, below
    which the solve is latency-bound and the FP64 GEMMs serve it). */
 #define STD2G_FLAG_TENSOR_ALWAYS 1
+/* FP64 matrix products through cuBLAS instead of the engine's own DMMA kernel
+   (the library baseline that the plain FP64 form is compared with). */
+#define STD2G_FLAG_LIBRARY_FP64 2
 
 typedef struct {
   int device;            /* CUDA device ordinal */
@@ -271,6 +274,7 @@ typedef struct {
   int trace;            /* > 0: one line per finished request on stderr (slot,
                            times, phase times of its solve and alpha(omega)) */
   int64_t hbm_budget;   /* bytes the admitted requests may use (0: 80 % of free memory) */
+  int flags;            /* STD2G_FLAG_* of every slot's context */
 } std2g_server_opts;
 
 typedef struct {
@@ -316,6 +320,16 @@ void std2g_server_destroy(void *srv);
    request server's slots) leave SMs to each other's kernels.  No reference
    counterpart. */
 int std2g_set_sm_limit(void *ctx, int max_sms);
+
+/* Diagnostic: the engine's FP64 matrix product (DMMA kernel with split-K,
+   used for ONETRI, the Loewdin transform, gamma.q and the property
+   contractions): C = alpha op(A) op(B) + beta C on host arrays, column-major,
+   op = transpose when ta / tb; batch members follow one another at sizes
+   lda*cols(A), ldb*cols(B), ldc*n.  *ms (may be NULL): device time of the
+   product alone.  No reference counterpart (the reference calls BLAS). */
+int std2g_dgemm_check(int device, int ta, int tb, int m, int n, int k, double alpha,
+                      const double *A, int64_t lda, const double *B, int64_t ldb,
+                      double beta, double *C, int64_t ldc, int batch, double *ms);
 
 /* Diagnostic: lowest k eigenpairs of the symmetric n x n matrix A (host,
    column-major, lower triangle used) by the engine's single-block eigensolver

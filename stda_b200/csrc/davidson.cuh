@@ -18,6 +18,7 @@
 #include <vector>
 
 #include "common.cuh"
+#include "dgemm.cuh"
 #include "symeig_small.cuh"
 
 namespace std2g {
@@ -226,6 +227,7 @@ struct DavidsonWork {
   // [3] Ritz vectors + residuals, [4] orthogonalisation
   bool profile = false;
   double sec_ms[5] = {0, 0, 0, 0, 0};
+  Dgemm *dg = nullptr;   // the context's FP64 products (dgemm.cuh)
 };
 
 // host wall-clock section timer used when DavidsonWork::profile is set
@@ -281,12 +283,12 @@ inline int dav_orthonormalize(DavidsonWork &dw, cublasHandle_t blas, cusolverDnH
     double *Tb = T;
     int ncur = nc;
     for (int round = 0; round < 2 && ncur > 0; ++round) {
-      S2G_CUBLAS(cublasDgemm(blas, CUBLAS_OP_T, CUBLAS_OP_N, m, ncur, n, &one, V, n, Tb, n,
+      (dw.dg->gemm(s, CUBLAS_OP_T, CUBLAS_OP_N, m, ncur, n, &one, V, n, Tb, n,
                              &zero, proj, m));
-      S2G_CUBLAS(cublasDgemm(blas, CUBLAS_OP_N, CUBLAS_OP_N, n, ncur, m, &mone, V, n, proj, m,
+      (dw.dg->gemm(s, CUBLAS_OP_N, CUBLAS_OP_N, n, ncur, m, &mone, V, n, proj, m,
                              &one, Tb, n));
       // G = Tb^T Tb; Cholesky QR when G is safely positive definite
-      S2G_CUBLAS(cublasDgemm(blas, CUBLAS_OP_T, CUBLAS_OP_N, ncur, ncur, n, &one, Tb, n, Tb, n,
+      (dw.dg->gemm(s, CUBLAS_OP_T, CUBLAS_OP_N, ncur, ncur, n, &one, Tb, n, Tb, n,
                              &zero, G, ncur));
       if (ncur <= kCholMax) {
         // Cholesky QR: L^-T from the engine's small factorisation kernel
@@ -302,7 +304,7 @@ inline int dav_orthonormalize(DavidsonWork &dw, cublasHandle_t blas, cusolverDnH
           // dst <- Tb L^-T (through tmp when Tb already is dst)
           double *dst = V + (size_t)n * m;
           double *o = Tb == dst ? tmp : dst;
-          S2G_CUBLAS(cublasDgemm(blas, CUBLAS_OP_N, CUBLAS_OP_N, n, ncur, ncur, &one, Tb, n, Li,
+          (dw.dg->gemm(s, CUBLAS_OP_N, CUBLAS_OP_N, n, ncur, ncur, &one, Tb, n, Li,
                                  ncur, &zero, o, n));
           if (o != dst)
             S2G_CUDA(cudaMemcpyAsync(dst, o, sizeof(double) * n * ncur,
@@ -342,7 +344,7 @@ inline int dav_orthonormalize(DavidsonWork &dw, cublasHandle_t blas, cusolverDnH
       }
       // new block = Tb U_keep diag(lam_keep)^-1/2, written into V after column m
       double *dst = V + (size_t)n * m;
-      S2G_CUBLAS(cublasDgemm(blas, CUBLAS_OP_N, CUBLAS_OP_N, n, nkeep, ncur, &one, Tb, n,
+      (dw.dg->gemm(s, CUBLAS_OP_N, CUBLAS_OP_N, n, nkeep, ncur, &one, Tb, n,
                              G + (size_t)ncur * first, ncur, &zero, tmp, n));
       S2G_LAUNCH(k_scale_by, grid, 256, 0, s, tmp, n, nkeep, lam + first, 1);
       S2G_CUDA(cudaMemcpyAsync(dst, tmp, sizeof(double) * n * nkeep, cudaMemcpyDeviceToDevice,
@@ -412,7 +414,7 @@ inline int davidson(DavidsonWork &dw, cublasHandle_t blas, cusolverDnHandle_t so
     clk.tick(0);
     // H = V^T W (ld mmax): only the new columns are formed; the new rows
     // follow from the symmetry of A
-    S2G_CUBLAS(cublasDgemm(blas, CUBLAS_OP_T, CUBLAS_OP_N, m + nb, nb, n, &one, V, n,
+    (dw.dg->gemm(s, CUBLAS_OP_T, CUBLAS_OP_N, m + nb, nb, n, &one, V, n,
                            W + (size_t)n * m, n, &zero, H + (size_t)mmax * m, mmax));
     if (m > 0)
       S2G_LAUNCH(k_mirror_cols, (int)div_up((int64_t)m * nb, 256), 256, 0, s, H, mmax, m, nb);
@@ -430,8 +432,8 @@ inline int davidson(DavidsonWork &dw, cublasHandle_t blas, cusolverDnHandle_t so
     }
     clk.tick(2);
     // Ritz vectors X = V Y_k, residuals R = W Y_k - X theta
-    S2G_CUBLAS(cublasDgemm(blas, CUBLAS_OP_N, CUBLAS_OP_N, n, k, m, &one, V, n, Hs, m, &zero, X, n));
-    S2G_CUBLAS(cublasDgemm(blas, CUBLAS_OP_N, CUBLAS_OP_N, n, k, m, &one, W, n, Hs, m, &zero, R, n));
+    (dw.dg->gemm(s, CUBLAS_OP_N, CUBLAS_OP_N, n, k, m, &one, V, n, Hs, m, &zero, X, n));
+    (dw.dg->gemm(s, CUBLAS_OP_N, CUBLAS_OP_N, n, k, m, &one, W, n, Hs, m, &zero, R, n));
     {
       double *part = dw.part.ensure((size_t)k * kColSplit);
       S2G_LAUNCH(k_dav_resid, dim3(kColSplit, (unsigned)k), 256, 0, s, R, X, theta, n, part);
@@ -463,7 +465,7 @@ inline int davidson(DavidsonWork &dw, cublasHandle_t blas, cusolverDnHandle_t so
     S2G_LAUNCH(k_dav_precond, grid, 256, 0, s, T, R, diag, theta, cols, n, nc);
     if (m + nc > mmax) {
       // restart with the current Ritz vectors: V <- X, W <- W Y_k
-      S2G_CUBLAS(cublasDgemm(blas, CUBLAS_OP_N, CUBLAS_OP_N, n, k, m, &one, W, n, Hs, m, &zero,
+      (dw.dg->gemm(s, CUBLAS_OP_N, CUBLAS_OP_N, n, k, m, &one, W, n, Hs, m, &zero,
                              tmp, n));
       S2G_CUDA(cudaMemcpyAsync(W, tmp, sizeof(double) * n * k, cudaMemcpyDeviceToDevice, s));
       S2G_CUDA(cudaMemcpyAsync(V, X, sizeof(double) * n * k, cudaMemcpyDeviceToDevice, s));

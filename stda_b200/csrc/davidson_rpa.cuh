@@ -168,7 +168,7 @@ inline int davidson_rpa(DavidsonWork &dw, DavidsonRpaWork &rw, cublasHandle_t bl
   rw.iters = 0;
   rw.matvecs = 0;
   auto add_columns = [&](double *H, const double *W, int mnew, int nbn) {
-    S2G_CUBLAS(cublasDgemm(blas, CUBLAS_OP_T, CUBLAS_OP_N, mnew + nbn, nbn, n, &one, B, n,
+    (dw.dg->gemm(s, CUBLAS_OP_T, CUBLAS_OP_N, mnew + nbn, nbn, n, &one, B, n,
                            W + (size_t)n * mnew, n, &zero, H + (size_t)mmax * mnew, mmax));
     if (mnew > 0)
       S2G_LAUNCH(k_mirror_cols, (int)div_up((int64_t)mnew * nbn, 256), 256, 0, s, H, mmax, mnew,
@@ -187,32 +187,32 @@ inline int davidson_rpa(DavidsonWork &dw, DavidsonRpaWork &rw, cublasHandle_t bl
     S2G_CUDA(cudaMemcpyAsync(h_lam.data(), lam, sizeof(double), cudaMemcpyDeviceToHost, s));
     S2G_CUDA(cudaMemcpyAsync(T1, U, sizeof(double) * m * m, cudaMemcpyDeviceToDevice, s));
     S2G_LAUNCH(k_cols_times_sqrt, grid, 256, 0, s, T1, lam, m);
-    S2G_CUBLAS(cublasDgemm(blas, CUBLAS_OP_N, CUBLAS_OP_T, m, m, m, &one, T1, m, U, m, &zero, S,
+    (dw.dg->gemm(s, CUBLAS_OP_N, CUBLAS_OP_T, m, m, m, &one, T1, m, U, m, &zero, S,
                            m));
     // M_r = S Ap S, its lowest k pairs
-    S2G_CUBLAS(cublasDgemm(blas, CUBLAS_OP_N, CUBLAS_OP_N, m, m, m, &one, Ap, mmax, S, m, &zero,
+    (dw.dg->gemm(s, CUBLAS_OP_N, CUBLAS_OP_N, m, m, m, &one, Ap, mmax, S, m, &zero,
                            T1, m));
-    S2G_CUBLAS(cublasDgemm(blas, CUBLAS_OP_N, CUBLAS_OP_N, m, m, m, &one, S, m, T1, m, &zero, Mr,
+    (dw.dg->gemm(s, CUBLAS_OP_N, CUBLAS_OP_N, m, m, m, &one, S, m, T1, m, &zero, Mr,
                            m));
     const int kk = std::min(k, m);
     rpa_small_eig(dw, rw, sol, s, Mr, m, m, kk, ev, Z, Zf, einfo);
     S2G_LAUNCH(k_sqrt_inplace, (int)div_up(kk, 128), 128, 0, s, ev, kk);
     S2G_CUDA(cudaMemcpyAsync(om, ev, sizeof(double) * kk, cudaMemcpyDeviceToDevice, s));
     // (X+Y)_r = S z / sqrt(w), (X-Y)_r = Ap (X+Y)_r / w
-    S2G_CUBLAS(cublasDgemm(blas, CUBLAS_OP_N, CUBLAS_OP_N, m, kk, m, &one, S, m, Z, m, &zero, Xp,
+    (dw.dg->gemm(s, CUBLAS_OP_N, CUBLAS_OP_N, m, kk, m, &one, S, m, Z, m, &zero, Xp,
                            m));
     S2G_LAUNCH(k_cols_scale_w, grid, 256, 0, s, Xp, m, m, kk, om, 0);
-    S2G_CUBLAS(cublasDgemm(blas, CUBLAS_OP_N, CUBLAS_OP_N, m, kk, m, &one, Ap, mmax, Xp, m, &zero,
+    (dw.dg->gemm(s, CUBLAS_OP_N, CUBLAS_OP_N, m, kk, m, &one, Ap, mmax, Xp, m, &zero,
                            Xm, m));
     S2G_LAUNCH(k_cols_scale_w, grid, 256, 0, s, Xm, m, m, kk, om, 1);
     // full-space vectors and residuals
-    S2G_CUBLAS(cublasDgemm(blas, CUBLAS_OP_N, CUBLAS_OP_N, n, kk, m, &one, B, n, Xp, m, &zero,
+    (dw.dg->gemm(s, CUBLAS_OP_N, CUBLAS_OP_N, n, kk, m, &one, B, n, Xp, m, &zero,
                            XpY, n));
-    S2G_CUBLAS(cublasDgemm(blas, CUBLAS_OP_N, CUBLAS_OP_N, n, kk, m, &one, B, n, Xm, m, &zero,
+    (dw.dg->gemm(s, CUBLAS_OP_N, CUBLAS_OP_N, n, kk, m, &one, B, n, Xm, m, &zero,
                            XmY, n));
-    S2G_CUBLAS(cublasDgemm(blas, CUBLAS_OP_N, CUBLAS_OP_N, n, kk, m, &one, P, n, Xp, m, &zero, Rp,
+    (dw.dg->gemm(s, CUBLAS_OP_N, CUBLAS_OP_N, n, kk, m, &one, P, n, Xp, m, &zero, Rp,
                            n));
-    S2G_CUBLAS(cublasDgemm(blas, CUBLAS_OP_N, CUBLAS_OP_N, n, kk, m, &one, Q, n, Xm, m, &zero, Rm,
+    (dw.dg->gemm(s, CUBLAS_OP_N, CUBLAS_OP_N, n, kk, m, &one, Q, n, Xm, m, &zero, Rm,
                            n));
     S2G_LAUNCH(k_rpa_resid, dim3(kColSplit, (unsigned)kk), 256, 0, s, Rp, Rm, XpY, XmY, om, n,
                part);
@@ -246,7 +246,7 @@ inline int davidson_rpa(DavidsonWork &dw, DavidsonRpaWork &rw, cublasHandle_t bl
       S2G_CUDA(cudaMemcpyAsync(C + (size_t)m * kk, Xm, sizeof(double) * m * kk,
                                cudaMemcpyDeviceToDevice, s));
       double *G = dw.G.ensure((size_t)4 * k * k), *gl = dw.lam.ensure(2 * k);
-      S2G_CUBLAS(cublasDgemm(blas, CUBLAS_OP_T, CUBLAS_OP_N, nc2, nc2, m, &one, C, m, C, m, &zero,
+      (dw.dg->gemm(s, CUBLAS_OP_T, CUBLAS_OP_N, nc2, nc2, m, &one, C, m, C, m, &zero,
                              G, nc2));
       double *Gz = dw.Gz.ensure((size_t)4 * k * k);
       rpa_small_eig(dw, rw, sol, s, G, nc2, nc2, nc2, gl, Gz, Zf, einfo);
@@ -257,20 +257,20 @@ inline int davidson_rpa(DavidsonWork &dw, DavidsonRpaWork &rw, cublasHandle_t bl
       while (first < nc2 && !(h_gl[first] > 1e-10 * h_gl[nc2 - 1])) ++first;
       const int nkeep = nc2 - first;
       double *Qc = rw.Qc.ensure((size_t)mmax * 2 * k);
-      S2G_CUBLAS(cublasDgemm(blas, CUBLAS_OP_N, CUBLAS_OP_N, m, nkeep, nc2, &one, C, m,
+      (dw.dg->gemm(s, CUBLAS_OP_N, CUBLAS_OP_N, m, nkeep, nc2, &one, C, m,
                              Gz + (size_t)nc2 * first, nc2, &zero, Qc, m));
       S2G_LAUNCH(k_scale_by, grid, 256, 0, s, Qc, m, nkeep, gl + first, 1);
       // b <- b Qc, P <- P Qc, Q <- Q Qc; Ap, Am <- Qc^T (.) Qc
       double *tn = rw.tmpn.ensure((size_t)n * 2 * k);
       for (double *X : {B, P, Q}) {
-        S2G_CUBLAS(cublasDgemm(blas, CUBLAS_OP_N, CUBLAS_OP_N, n, nkeep, m, &one, X, n, Qc, m,
+        (dw.dg->gemm(s, CUBLAS_OP_N, CUBLAS_OP_N, n, nkeep, m, &one, X, n, Qc, m,
                                &zero, tn, n));
         S2G_CUDA(cudaMemcpyAsync(X, tn, sizeof(double) * n * nkeep, cudaMemcpyDeviceToDevice, s));
       }
       for (double *H : {Ap, Am}) {
-        S2G_CUBLAS(cublasDgemm(blas, CUBLAS_OP_N, CUBLAS_OP_N, m, nkeep, m, &one, H, mmax, Qc, m,
+        (dw.dg->gemm(s, CUBLAS_OP_N, CUBLAS_OP_N, m, nkeep, m, &one, H, mmax, Qc, m,
                                &zero, T1, m));
-        S2G_CUBLAS(cublasDgemm(blas, CUBLAS_OP_T, CUBLAS_OP_N, nkeep, nkeep, m, &one, Qc, m, T1, m,
+        (dw.dg->gemm(s, CUBLAS_OP_T, CUBLAS_OP_N, nkeep, nkeep, m, &one, Qc, m, T1, m,
                                &zero, H, mmax));
       }
       m = nkeep;

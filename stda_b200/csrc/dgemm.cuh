@@ -1,0 +1,284 @@
+// FP64 matrix products of the engine: C = alpha op(A) op(B) + beta C,
+// column-major, op = N or T, optionally batched with fixed strides.
+//
+// B200 has no FP64 kind of tcgen05; its FP64 tensor path is the warp-level
+// DMMA (mma.sync m8n8k4 .f64).  Each CTA (4 warps) computes a 64 x 64 tile of C
+// over a K range in steps of 16: the A (64 x 16) and B (16 x 64) tiles arrive
+// by 8-byte cp.async in a 4-stage shared-memory ring (three tiles in flight
+// while one is multiplied), kept in the global layout's fast order and
+// XOR-swizzled so that the fragment reads are conflict-free, and each warp
+// owns a 32 x 32 sub-tile = 4 x 4 DMMA tiles (32 accumulators per thread).
+//
+// Tall-skinny products (the Davidson projections V^T W: 300 x 75 outputs over
+// 5e4-long sums) split K across CTAs.  The partial tiles go to a workspace and
+// a second kernel adds them in a fixed order, so every result is bit-for-bit
+// reproducible from run to run (no atomics).  With beta = 0, C is not read.
+#pragma once
+
+#include <cublas_v2.h>
+
+#include "common.cuh"
+
+namespace std2g {
+
+namespace dg {
+constexpr int BM = 64, BN = 64, BK = 16, THREADS = 128, STAGES = 4;
+constexpr int TILE = 64 * BK;                      // doubles per operand tile (no padding)
+constexpr int SMEM_BYTES = STAGES * 2 * TILE * 8;  // 64 KB: three CTAs per SM
+// Shared-memory positions, XOR-swizzled so that the fragment reads of a half
+// warp (g = 0..3 along m or n, t = 0..3 along k) hit 16 distinct 8-byte banks:
+// operand stored with m (or n) fastest, [BK][64]:
+__device__ __forceinline__ int pos_mfast(int k, int m) { return k * 64 + (m ^ ((k & 3) << 2)); }
+// operand stored with k fastest, [64][BK]:
+__device__ __forceinline__ int pos_kfast(int m, int k) { return m * 16 + (k ^ ((m & 3) << 2)); }
+}
+
+// D (8x8) += A (8x4, row) * B (4x8, col), FP64.  Fragments: a = A[g][t],
+// b = B[t][g], d = {D[g][2t], D[g][2t+1]} with g = lane / 4, t = lane % 4.
+__device__ __forceinline__ void dmma_8x8x4(double &d0, double &d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+
+// 8-byte asynchronous global -> shared copy; ok = false fills zeros
+__device__ __forceinline__ void cp_async8(double *dst, const double *src, bool ok) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(d), "l"(src),
+               "r"(ok ? 8 : 0)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;" ::: "memory");
+}
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// blockIdx.x: tile of C (m fastest); blockIdx.y: batch * ksplit + split.
+// Each split covers K range [split * kchunk, min(K, (split + 1) * kchunk)).
+// ksplit == 1: C = alpha acc + beta C;  else work[(b * ksplit + split)][m + n M] = acc.
+// A tiles are kept in the global layout's fast order: m fastest for op(A) = A
+// ([k][m]), k fastest for op(A) = A^T ([m][k]); B tiles k fastest for
+// op(B) = B ([n][k]), n fastest for op(B) = B^T ([k][n]); swizzled (pos_*).
+template <bool TA, bool TB>
+__global__ void __launch_bounds__(dg::THREADS, 3)
+    k_dgemm(int M, int N, int K, double alpha, const double *__restrict__ A, int64_t lda,
+            int64_t sA, const double *__restrict__ B, int64_t ldb, int64_t sB, double beta,
+            double *__restrict__ C, int64_t ldc, int64_t sC, int ksplit, int kchunk,
+            double *__restrict__ work) {
+  using namespace dg;
+  extern __shared__ __align__(16) double smem_d[];
+  const int tiles_m = (M + BM - 1) / BM;
+  const int m0 = (blockIdx.x % tiles_m) * BM, n0 = (blockIdx.x / tiles_m) * BN;
+  const int batch = blockIdx.y / ksplit, split = blockIdx.y % ksplit;
+  const int kb = split * kchunk, ke = min(K, kb + kchunk);
+  A += batch * sA;
+  B += batch * sB;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  const int wm = (warp & 1) * 32, wn = (warp >> 1) * 32;
+  auto As = [&](int st) { return smem_d + (size_t)st * 2 * TILE; };
+  auto Bs = [&](int st) { return smem_d + (size_t)st * 2 * TILE + TILE; };
+
+  // issue the copies of the K tile starting at k0 into stage st
+  auto issue = [&](int st, int k0) {
+    double *a = As(st), *b = Bs(st);
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const int idx = tid + THREADS * q;
+      if (!TA) {
+        const int m = idx & 63, k = idx >> 6, gm = m0 + m, gk = k0 + k;
+        const bool ok = gm < M && gk < ke;
+        cp_async8(a + pos_mfast(k, m), ok ? A + gm + (int64_t)gk * lda : A, ok);
+      } else {
+        const int k = idx & 15, m = idx >> 4, gm = m0 + m, gk = k0 + k;
+        const bool ok = gm < M && gk < ke;
+        cp_async8(a + pos_kfast(m, k), ok ? A + gk + (int64_t)gm * lda : A, ok);
+      }
+      if (!TB) {
+        const int k = idx & 15, n = idx >> 4, gn = n0 + n, gk = k0 + k;
+        const bool ok = gn < N && gk < ke;
+        cp_async8(b + pos_kfast(n, k), ok ? B + gk + (int64_t)gn * ldb : B, ok);
+      } else {
+        const int n = idx & 63, k = idx >> 6, gn = n0 + n, gk = k0 + k;
+        const bool ok = gn < N && gk < ke;
+        cp_async8(b + pos_mfast(k, n), ok ? B + gn + (int64_t)gk * ldb : B, ok);
+      }
+    }
+  };
+
+  double acc[4][4][2];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+
+  const int nt = ke > kb ? (ke - kb + BK - 1) / BK : 0;
+#pragma unroll
+  for (int p = 0; p < STAGES - 1; ++p) {
+    if (p < nt) issue(p, kb + p * BK);
+    cp_async_commit();
+  }
+  for (int it = 0; it < nt; ++it) {
+    cp_async_wait<STAGES - 2>();
+    __syncthreads();
+    {
+      const int nx = it + STAGES - 1;
+      if (nx < nt) issue(nx % STAGES, kb + nx * BK);
+      cp_async_commit();
+    }
+    const double *a = As(it % STAGES), *b = Bs(it % STAGES);
+#pragma unroll
+    for (int ks = 0; ks < BK; ks += 4) {
+      double fa[4], fb[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const int m = wm + 8 * i + g, k = ks + t;
+        fa[i] = TA ? a[pos_kfast(m, k)] : a[pos_mfast(k, m)];
+      }
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int n = wn + 8 * j + g, k = ks + t;
+        fb[j] = TB ? b[pos_mfast(k, n)] : b[pos_kfast(n, k)];
+      }
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) dmma_8x8x4(acc[i][j][0], acc[i][j][1], fa[i], fb[j]);
+    }
+  }
+  cp_async_wait<0>();
+
+  // epilogue: element (i, j, e) of this thread is C[m0 + wm + 8 i + g][n0 + wn + 8 j + 2 t + e]
+  if (ksplit == 1) {
+    C += batch * sC;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int row = m0 + wm + 8 * i + g;
+      if (row >= M) continue;
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          const int col = n0 + wn + 8 * j + 2 * t + e;
+          if (col >= N) continue;
+          double *p = C + row + (int64_t)col * ldc;
+          const double v = alpha * acc[i][j][e];
+          *p = beta == 0.0 ? v : v + beta * *p;
+        }
+    }
+  } else {
+    double *wp = work + (int64_t)blockIdx.y * M * N;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int row = m0 + wm + 8 * i + g;
+      if (row >= M) continue;
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          const int col = n0 + wn + 8 * j + 2 * t + e;
+          if (col < N) wp[row + (int64_t)col * M] = acc[i][j][e];
+        }
+    }
+  }
+}
+
+// C = alpha sum_s work[b][s] + beta C, splits added in order 0, 1, ...
+__global__ void k_dgemm_reduce(int M, int N, int batch, int ksplit, double alpha,
+                               const double *__restrict__ work, double beta,
+                               double *__restrict__ C, int64_t ldc, int64_t sC) {
+  const int64_t mn = (int64_t)M * N, total = mn * batch;
+  for (int64_t x = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; x < total;
+       x += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t b = x / mn, r = x - b * mn;
+    const int64_t col = r / M, row = r - col * M;
+    const double *w = work + b * ksplit * mn + r;
+    double s = 0.0;
+    for (int q = 0; q < ksplit; ++q) s += w[q * mn];
+    double *p = C + b * sC + row + col * ldc;
+    *p = beta == 0.0 ? alpha * s : alpha * s + beta * *p;
+  }
+}
+
+// Launch wrapper with the split-K workspace.
+struct Dgemm {
+  DBuf<double> work;
+  int nsm = 148;
+  int64_t launches = 0;
+  // set: the products go to cuBLAS on this handle instead (the library
+  // baseline of the plain FP64 form, STD2G_FLAG_LIBRARY_FP64)
+  cublasHandle_t lib = nullptr;
+
+  // the argument order of cublasDgemm (alpha / beta by pointer, host values)
+  void gemm(cudaStream_t s, cublasOperation_t ta, cublasOperation_t tb, int m, int n, int k,
+            const double *alpha, const double *A, int64_t lda, const double *B, int64_t ldb,
+            const double *beta, double *C, int64_t ldc) {
+    run(s, ta != CUBLAS_OP_N, tb != CUBLAS_OP_N, m, n, k, *alpha, A, lda, 0, B, ldb, 0, *beta, C,
+        ldc, 0, 1);
+  }
+
+  // op(A) is m x k, op(B) is k x n; strides between batch members (0 for one).
+  void run(cudaStream_t s, bool ta, bool tb, int m, int n, int k, double alpha, const double *A,
+           int64_t lda, int64_t sA, const double *B, int64_t ldb, int64_t sB, double beta,
+           double *C, int64_t ldc, int64_t sC, int batch = 1) {
+    if (m <= 0 || n <= 0 || batch <= 0) return;
+    if (k < 0) throw Error{STD2G_EINVAL, "dgemm: negative k"};
+    if (lib) {
+      const cublasOperation_t oa = ta ? CUBLAS_OP_T : CUBLAS_OP_N, ob = tb ? CUBLAS_OP_T : CUBLAS_OP_N;
+      S2G_CUBLAS(cublasSetStream(lib, s));
+      if (batch == 1)
+        S2G_CUBLAS(cublasDgemm(lib, oa, ob, m, n, k, &alpha, A, (int)lda, B, (int)ldb, &beta, C,
+                               (int)ldc));
+      else
+        S2G_CUBLAS(cublasDgemmStridedBatched(lib, oa, ob, m, n, k, &alpha, A, (int)lda, sA, B,
+                                             (int)ldb, sB, &beta, C, (int)ldc, sC, batch));
+      return;
+    }
+    const int tiles = (int)(div_up(m, dg::BM) * div_up(n, dg::BN));
+    // split K to fill the device: CTAs run in waves of 3 per SM; pick the
+    // split count with the fewest K steps on the busiest SM (each split at
+    // least 256 long; a split adds its workspace pass, weighted 3 %)
+    const int64_t ctas = (int64_t)tiles * batch, slots = 3 * (int64_t)nsm;
+    const int kmax = (int)std::max<int64_t>(1, std::min<int64_t>(64, k / 256));
+    int ksplit = 1;
+    double best = 0.0;
+    for (int ks = 1; ks <= kmax; ++ks) {
+      const int64_t steps = div_up(ctas * ks, slots) * div_up(div_up(std::max(k, 1), ks), dg::BK);
+      const double cost = (double)steps * (ks > 1 ? 1.03 : 1.0);
+      if (ks == 1 || cost < best) {
+        best = cost;
+        ksplit = ks;
+      }
+    }
+    int kchunk = (int)div_up(div_up(std::max(k, 1), ksplit), dg::BK) * dg::BK;
+    ksplit = (int)div_up(std::max(k, 1), kchunk);
+    if (batch * ksplit > 65535) throw Error{STD2G_EINVAL, "dgemm: batch too large"};
+    double *wk = nullptr;
+    if (ksplit > 1) wk = work.ensure((size_t)ksplit * batch * m * n);
+    const dim3 grid(tiles, batch * ksplit);
+#define S2G_DGEMM(TA_, TB_)                                                                   \
+  do {                                                                                        \
+    S2G_CUDA(cudaFuncSetAttribute(k_dgemm<TA_, TB_>,                                          \
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, dg::SMEM_BYTES)); \
+    S2G_LAUNCH((k_dgemm<TA_, TB_>), grid, dg::THREADS, dg::SMEM_BYTES, s, m, n, k, alpha, A,   \
+               lda, sA, B, ldb, sB, beta, C, ldc, sC, ksplit, kchunk, wk);                    \
+  } while (0)
+    if (!ta && !tb) S2G_DGEMM(false, false);
+    else if (!ta && tb) S2G_DGEMM(false, true);
+    else if (ta && !tb) S2G_DGEMM(true, false);
+    else S2G_DGEMM(true, true);
+#undef S2G_DGEMM
+    ++launches;
+    if (ksplit > 1) {
+      const int64_t total = (int64_t)m * n * batch;
+      const int g = (int)std::min<int64_t>(div_up(total, 256), (int64_t)nsm * 8);
+      S2G_LAUNCH(k_dgemm_reduce, g, 256, 0, s, m, n, batch, ksplit, alpha, wk, beta, C, ldc, sC);
+      ++launches;
+    }
+  }
+};
+
+}  // namespace std2g

@@ -7,6 +7,7 @@
 // the charge formation, the screen, the PT selection and the A build use the
 // kernels of this library (kernels_fp64.cuh, tc_gemm.cuh).
 #include <algorithm>
+#include <dlfcn.h>
 #include <functional>
 #include <chrono>
 #include <cmath>
@@ -22,6 +23,7 @@
 #include "davidson.cuh"
 #include "davidson_rpa.cuh"
 #include "ao_ints.cuh"
+#include "dgemm.cuh"
 #include "matfree.cuh"
 #include "matfree_tc.cuh"
 #include "pt_tc.cuh"
@@ -52,6 +54,7 @@ struct Ctx {
   int ncent = 0, nmo = 0, nao = 0;
   std::vector<double> h_eps, h_occ, h_xyz;
   AoIntsWork aoi;   // primitive list of the device AO integrals (ao_ints.cuh)
+  Dgemm dg;         // the engine's FP64 matrix products (dgemm.cuh)
   // device inputs
   DBuf<double> d_xyz, d_C, d_eps_act, d_eta, d_Sfull, d_sqrtS, d_ao9;
   DBuf<int> d_ao_ptr, d_ao_list, d_iaoat, d_slot_ao;
@@ -100,11 +103,15 @@ struct Ctx {
 };
 
 // --------------------------------------------------------------------------
+// FP64 C = alpha op(A) op(B) + beta C through the engine's DMMA kernel
+// (dgemm.cuh); batch > 1: members at fixed strides sA, sB, sC.
 static void gemm(Ctx &c, cublasOperation_t ta, cublasOperation_t tb, int m, int n, int k,
-                 double alpha, const double *A, int lda, const double *B, int ldb, double beta,
-                 double *C, int ldc) {
+                 double alpha, const double *A, int64_t lda, const double *B, int64_t ldb,
+                 double beta, double *C, int64_t ldc, int batch = 1, int64_t sA = 0,
+                 int64_t sB = 0, int64_t sC = 0) {
   if (m == 0 || n == 0) return;
-  S2G_CUBLAS(cublasDgemm(c.blas, ta, tb, m, n, k, &alpha, A, lda, B, ldb, &beta, C, ldc));
+  c.dg.run(c.stream, ta != CUBLAS_OP_N, tb != CUBLAS_OP_N, m, n, k, alpha, A, lda, sA, B, ldb,
+           sB, beta, C, ldc, sC, batch);
 }
 
 static int grid_for(int64_t n, int block = 256) {
@@ -531,10 +538,8 @@ static void response_mixed(Ctx &c, const double *Apb, const double *Amb, int n,
   const float one = 1.f, zero = 0.f;
   const double done = 1.0, dzero = 0.0;
   auto fp64 = [&](const double *U, const double *V, double *PU, double *MV) {
-    S2G_CUBLAS(cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, n, ncol, n, &done, Apb, n, U, n, &dzero,
-                           PU, n));
-    S2G_CUBLAS(cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, n, ncol, n, &done, Amb, n, V, n, &dzero,
-                           MV, n));
+    c.dg.gemm(s, CUBLAS_OP_N, CUBLAS_OP_N, n, ncol, n, &done, Apb, n, U, n, &dzero, PU, n);
+    c.dg.gemm(s, CUBLAS_OP_N, CUBLAS_OP_N, n, ncol, n, &done, Amb, n, V, n, &dzero, MV, n);
   };
   auto inner = [&](const float *pu, const float *pv, float *qu, float *qv) {
     S2G_CUBLAS(cublasSgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, n, ncol, n, &one, Apb32, n, pu, n, &zero,
@@ -599,14 +604,12 @@ static std::vector<double> quad_dots(Ctx &c, int nci, int no, int nv, const int 
   S2G_LAUNCH(k_box_scatter, grid_for((int64_t)nci * ny), 256, 0, s, bx, Y, ci, ca, nci, no, nv,
              ny);
   double *my = c.w_qmy.ensure((size_t)box * ny * 3);
-  const double one = 1.0, mone = -1.0, zero = 0.0;
   for (int y = 0; y < 3; ++y) {
     double *out = my + (size_t)box * ny * y;
-    S2G_CUBLAS(cublasDgemm(c.blas, CUBLAS_OP_N, CUBLAS_OP_N, no, nv * ny, no, &mone,
-                           c.w_moo.get() + (size_t)no * no * y, no, bx, no, &zero, out, no));
-    S2G_CUBLAS(cublasDgemmStridedBatched(c.blas, CUBLAS_OP_N, CUBLAS_OP_N, no, nv, nv, &one, bx,
-                                         no, box, c.w_mvv.get() + (size_t)nv * nv * y, nv, 0,
-                                         &one, out, no, box, ny));
+    gemm(c, CUBLAS_OP_N, CUBLAS_OP_N, no, nv * ny, no, -1.0, c.w_moo.get() + (size_t)no * no * y,
+         no, bx, no, 0.0, out, no);
+    gemm(c, CUBLAS_OP_N, CUBLAS_OP_N, no, nv, nv, 1.0, bx, no, c.w_mvv.get() + (size_t)nv * nv * y,
+         nv, 1.0, out, no, ny, box, 0, box);
   }
   double *sel = c.w_qsel.ensure((size_t)nci * 3 * ny);
   S2G_LAUNCH(k_box_gather, grid_for((int64_t)nci * 3 * ny), 256, 0, s, sel, my, ci, ca, nci, no,
@@ -833,29 +836,22 @@ static void solve(Ctx &c, const std2g_params &p_in, std2g_result *res, const Res
     size_t nn = (size_t)nao * nao;
     double *T = c.w_T.ensure((size_t)nao * nv * 9);
     double *mu = c.w_mu_ov.ensure((size_t)no * nv * 9);
-    double one = 1.0, zero = 0.0;
-    S2G_CUBLAS(cublasDgemmStridedBatched(c.blas, CUBLAS_OP_N, CUBLAS_OP_N, nao, nv, nao, &one,
-                                         c.d_ao9.get(), nao, (long long)nn, Cact + (size_t)nao * no,
-                                         nao, 0, &zero, T, nao, (long long)nao * nv, 9));
-    S2G_CUBLAS(cublasDgemmStridedBatched(c.blas, CUBLAS_OP_T, CUBLAS_OP_N, no, nv, nao, &one,
-                                         Cact, nao, 0, T, nao, (long long)nao * nv, &zero, mu, no,
-                                         (long long)no * nv, 9));
+    // T_q = O_q C_v, mu_q = C_o^T T_q for the nine AO operators (batched)
+    gemm(c, CUBLAS_OP_N, CUBLAS_OP_N, nao, nv, nao, 1.0, c.d_ao9.get(), nao,
+         Cact + (size_t)nao * no, nao, 0.0, T, nao, 9, (int64_t)nn, 0, (int64_t)nao * nv);
+    gemm(c, CUBLAS_OP_T, CUBLAS_OP_N, no, nv, nao, 1.0, Cact, nao, T, nao, 0.0, mu, no, 9, 0,
+         (int64_t)nao * nv, (int64_t)no * nv);
     if (want_quad) {
       // length dipoles of the occupied-occupied and virtual-virtual blocks
       // (the same packed moci x moci transform, stda.f:351-412; lresp1 reads them)
       double *To = c.w_To.ensure((size_t)nao * no * 3);
-      S2G_CUBLAS(cublasDgemmStridedBatched(c.blas, CUBLAS_OP_N, CUBLAS_OP_N, nao, no, nao, &one,
-                                           c.d_ao9.get(), nao, (long long)nn, Cact, nao, 0, &zero,
-                                           To, nao, (long long)nao * no, 3));
-      S2G_CUBLAS(cublasDgemmStridedBatched(c.blas, CUBLAS_OP_T, CUBLAS_OP_N, no, no, nao, &one,
-                                           Cact, nao, 0, To, nao, (long long)nao * no, &zero,
-                                           c.w_moo.ensure((size_t)no * no * 3), no,
-                                           (long long)no * no, 3));
-      S2G_CUBLAS(cublasDgemmStridedBatched(c.blas, CUBLAS_OP_T, CUBLAS_OP_N, nv, nv, nao, &one,
-                                           Cact + (size_t)nao * no, nao, 0, T, nao,
-                                           (long long)nao * nv, &zero,
-                                           c.w_mvv.ensure((size_t)nv * nv * 3), nv,
-                                           (long long)nv * nv, 3));
+      gemm(c, CUBLAS_OP_N, CUBLAS_OP_N, nao, no, nao, 1.0, c.d_ao9.get(), nao, Cact, nao, 0.0, To,
+           nao, 3, (int64_t)nn, 0, (int64_t)nao * no);
+      gemm(c, CUBLAS_OP_T, CUBLAS_OP_N, no, no, nao, 1.0, Cact, nao, To, nao, 0.0,
+           c.w_moo.ensure((size_t)no * no * 3), no, 3, 0, (int64_t)nao * no, (int64_t)no * no);
+      gemm(c, CUBLAS_OP_T, CUBLAS_OP_N, nv, nv, nao, 1.0, Cact + (size_t)nao * no, nao, T, nao,
+           0.0, c.w_mvv.ensure((size_t)nv * nv * 3), nv, 3, 0, (int64_t)nao * nv,
+           (int64_t)nv * nv);
     }
   }
 
@@ -1566,16 +1562,29 @@ int std2g_create(void **ctx, const std2g_opts *opts) {
     S2G_CUDA(cudaSetDevice(o.device));
     auto *c = new Ctx();
     c->opts = o;
+    c->dg.nsm = prop.multiProcessorCount;
+    c->dav.dg = &c->dg;
+    c->mf.dg = &c->dg;
+    c->mftc.side.dg.nsm = prop.multiProcessorCount;
     S2G_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
     S2G_CUBLAS(cublasCreate(&c->blas));
     S2G_CUBLAS(cublasSetStream(c->blas, c->stream));
-    // FP32 GEMMs of this handle (the mixed form's matrix-free products) run on
-    // the tensor cores as split-BF16 products (FP32 emulation); FP64 GEMMs are
-    // unaffected
-    S2G_CUBLAS(cublasSetMathMode(c->blas, CUBLAS_FP32_EMULATED_BF16X9_MATH));
-    S2G_CUBLAS(cublasSetEmulationStrategy(c->blas, CUBLAS_EMULATION_STRATEGY_EAGER));
+    // FP32 GEMMs of this handle (the mixed form's dense response products) run
+    // on the tensor cores as split-BF16 products (FP32 emulation) where the
+    // cuBLAS in the process has that mode (12.9 and later; a host that loaded
+    // an older cuBLAS first keeps plain FP32 GEMMs, which the FP64 refinement
+    // of those solves accepts as well)
+    using SetEmulation = cublasStatus_t (*)(cublasHandle_t, cublasEmulationStrategy_t);
+    auto set_emulation = (SetEmulation)dlsym(RTLD_DEFAULT, "cublasSetEmulationStrategy");
+    if (set_emulation &&
+        cublasSetMathMode(c->blas, CUBLAS_FP32_EMULATED_BF16X9_MATH) == CUBLAS_STATUS_SUCCESS)
+      set_emulation(c->blas, CUBLAS_EMULATION_STRATEGY_EAGER);
     S2G_CUSOLVER(cusolverDnCreate(&c->solver));
     S2G_CUSOLVER(cusolverDnSetStream(c->solver, c->stream));
+    if (o.flags & STD2G_FLAG_LIBRARY_FP64) {
+      c->dg.lib = c->blas;
+      c->mftc.side.lib_fp64 = true;
+    }
     for (auto &e : c->ev) S2G_CUDA(cudaEventCreate(&e));
     *ctx = c;
   });
@@ -1808,6 +1817,54 @@ int std2g_symeig_check(int device, int n, int k, const double *A, double *w, dou
     cudaStreamDestroy(s);
     if (hinfo[0] != 0) throw Error{STD2G_ECUDA, "symeig_small: non-finite result"};
     if (hinfo[1] != 0) throw Error{STD2G_ECUDA, "syevd info " + std::to_string(hinfo[1])};
+  });
+}
+
+int std2g_dgemm_check(int device, int ta, int tb, int m, int n, int k, double alpha,
+                      const double *A, int64_t lda, const double *B, int64_t ldb, double beta,
+                      double *C, int64_t ldc, int batch, double *ms) {
+  if (m < 1 || n < 1 || k < 0 || batch < 1 || !A || !B || !C) return STD2G_EINVAL;
+  const int64_t ar = ta ? k : m, ac = ta ? m : k, br = tb ? n : k, bc = tb ? k : n;
+  if (lda < std::max<int64_t>(1, ar) || ldb < std::max<int64_t>(1, br) || ldc < m)
+    return STD2G_EINVAL;
+  return guard([&] {
+    using namespace std2g;
+    S2G_CUDA(cudaSetDevice(device));
+    cudaStream_t s;
+    S2G_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    const size_t na = (size_t)lda * ac, nb = (size_t)ldb * bc, nc = (size_t)ldc * n;
+    DBuf<double> dA, dB, dC;
+    S2G_CUDA(cudaMemcpyAsync(dA.ensure(na * batch), A, sizeof(double) * na * batch,
+                             cudaMemcpyHostToDevice, s));
+    S2G_CUDA(cudaMemcpyAsync(dB.ensure(nb * batch), B, sizeof(double) * nb * batch,
+                             cudaMemcpyHostToDevice, s));
+    S2G_CUDA(cudaMemcpyAsync(dC.ensure(nc * batch), C, sizeof(double) * nc * batch,
+                             cudaMemcpyHostToDevice, s));
+    Dgemm g;
+    cudaDeviceProp prop;
+    S2G_CUDA(cudaGetDeviceProperties(&prop, device));
+    g.nsm = prop.multiProcessorCount;
+    // an untimed run into a scratch copy of C sizes the split-K workspace
+    DBuf<double> dW;
+    S2G_CUDA(cudaMemcpyAsync(dW.ensure(nc * batch), dC.get(), sizeof(double) * nc * batch,
+                             cudaMemcpyDeviceToDevice, s));
+    g.run(s, ta != 0, tb != 0, m, n, k, alpha, dA.get(), lda, (int64_t)na, dB.get(), ldb,
+          (int64_t)nb, beta, dW.get(), ldc, (int64_t)nc, batch);
+    cudaEvent_t e0, e1;
+    S2G_CUDA(cudaEventCreate(&e0));
+    S2G_CUDA(cudaEventCreate(&e1));
+    S2G_CUDA(cudaEventRecord(e0, s));
+    g.run(s, ta != 0, tb != 0, m, n, k, alpha, dA.get(), lda, (int64_t)na, dB.get(), ldb,
+          (int64_t)nb, beta, dC.get(), ldc, (int64_t)nc, batch);
+    S2G_CUDA(cudaEventRecord(e1, s));
+    S2G_CUDA(cudaMemcpyAsync(C, dC.get(), sizeof(double) * nc * batch, cudaMemcpyDeviceToHost, s));
+    S2G_CUDA(cudaStreamSynchronize(s));
+    float t = 0;
+    S2G_CUDA(cudaEventElapsedTime(&t, e0, e1));
+    if (ms) *ms = t;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaStreamDestroy(s);
   });
 }
 

@@ -20,6 +20,7 @@
 #pragma once
 
 #include "common.cuh"
+#include "dgemm.cuh"
 
 namespace std2g {
 
@@ -220,22 +221,24 @@ struct MatFreeOps {
 struct MatFree {
   int N = 0, maxa = 0, no = 0, nv = 0, nci = 0, nao = 0;
   bool f32 = false;
+  Dgemm *dg = nullptr;   // FP64 products (dgemm.cuh); FP32 ones go to cuBLAS
   DBuf<double> dA;
   const int *ci = nullptr, *ca = nullptr;
   MatFreeOps<double> d;
   MatFreeOps<float> f;
 };
 
-inline void mf_gemm(cublasHandle_t h, cublasOperation_t ta, cublasOperation_t tb, int m, int n,
-                    int k, double alpha, const double *A, int lda, const double *B, int ldb,
-                    double beta, double *C, int ldc) {
+inline void mf_gemm(MatFree &mf, cublasHandle_t, cudaStream_t s, cublasOperation_t ta,
+                    cublasOperation_t tb, int m, int n, int k, double alpha, const double *A,
+                    int lda, const double *B, int ldb, double beta, double *C, int ldc) {
   if (m == 0 || n == 0) return;
-  S2G_CUBLAS(cublasDgemm(h, ta, tb, m, n, k, &alpha, A, lda, B, ldb, &beta, C, ldc));
+  mf.dg->run(s, ta != CUBLAS_OP_N, tb != CUBLAS_OP_N, m, n, k, alpha, A, lda, 0, B, ldb, 0, beta,
+             C, ldc, 0);
 }
 
-inline void mf_gemm(cublasHandle_t h, cublasOperation_t ta, cublasOperation_t tb, int m, int n,
-                    int k, double alpha, const float *A, int lda, const float *B, int ldb,
-                    double beta, float *C, int ldc) {
+inline void mf_gemm(MatFree &, cublasHandle_t h, cudaStream_t, cublasOperation_t ta,
+                    cublasOperation_t tb, int m, int n, int k, double alpha, const float *A,
+                    int lda, const float *B, int ldb, double beta, float *C, int ldc) {
   if (m == 0 || n == 0) return;
   float a = (float)alpha, b = (float)beta;
   S2G_CUBLAS(cublasGemmEx(h, ta, tb, m, n, k, &a, A, CUDA_R_32F, lda, B, CUDA_R_32F, ldb, &b, C,
@@ -243,17 +246,15 @@ inline void mf_gemm(cublasHandle_t h, cublasOperation_t ta, cublasOperation_t tb
                           CUBLAS_GEMM_DEFAULT));
 }
 
-inline void mf_gemm_batched(cublasHandle_t h, int m, int n, int k, const double *A, int lda,
-                            long long sa, const double *B, int ldb, long long sb, double *C,
-                            int ldc, long long sc, int batch) {
-  const double one = 1.0, zero = 0.0;
-  S2G_CUBLAS(cublasDgemmStridedBatched(h, CUBLAS_OP_N, CUBLAS_OP_N, m, n, k, &one, A, lda, sa, B,
-                                       ldb, sb, &zero, C, ldc, sc, batch));
+inline void mf_gemm_batched(MatFree &mf, cublasHandle_t, cudaStream_t s, int m, int n, int k,
+                            const double *A, int lda, long long sa, const double *B, int ldb,
+                            long long sb, double *C, int ldc, long long sc, int batch) {
+  mf.dg->run(s, false, false, m, n, k, 1.0, A, lda, sa, B, ldb, sb, 0.0, C, ldc, sc, batch);
 }
 
-inline void mf_gemm_batched(cublasHandle_t h, int m, int n, int k, const float *A, int lda,
-                            long long sa, const float *B, int ldb, long long sb, float *C,
-                            int ldc, long long sc, int batch) {
+inline void mf_gemm_batched(MatFree &, cublasHandle_t h, cudaStream_t, int m, int n, int k,
+                            const float *A, int lda, long long sa, const float *B, int ldb,
+                            long long sb, float *C, int ldc, long long sc, int batch) {
   const float one = 1.f, zero = 0.f;
   S2G_CUBLAS(cublasGemmStridedBatchedEx(h, CUBLAS_OP_N, CUBLAS_OP_N, m, n, k, &one, A, CUDA_R_32F,
                                         lda, sa, B, CUDA_R_32F, ldb, sb, &zero, C, CUDA_R_32F, ldc,
@@ -302,8 +303,8 @@ inline void mf_apply_t(MatFree &mf, MatFreeOps<T> &o, cublasHandle_t h, cudaStre
     T *Xc = o.Xc.ensure((size_t)lc * m), *Yc = o.Yc.ensure((size_t)lc * m);
     T *G = o.G.ensure((size_t)N * m);
     S2G_LAUNCH(k_mf_convert_ld<T>, grid, 256, 0, s, Xc, lc, X, nci, m);
-    mf_gemm(h, CUBLAS_OP_N, CUBLAS_OP_N, N, m, nci, 1.0, o.Qs.get(), N, Xc, lc, 0.0, G, N);
-    mf_gemm(h, CUBLAS_OP_T, CUBLAS_OP_N, nci, m, N, cK, o.Ps.get(), N, G, N, 0.0, Yc, lc);
+    mf_gemm(mf, h, s, CUBLAS_OP_N, CUBLAS_OP_N, N, m, nci, 1.0, o.Qs.get(), N, Xc, lc, 0.0, G, N);
+    mf_gemm(mf, h, s, CUBLAS_OP_T, CUBLAS_OP_N, nci, m, N, cK, o.Ps.get(), N, G, N, 0.0, Yc, lc);
     S2G_LAUNCH(k_mf_accum_ld<T>, grid, 256, 0, s, out, Yc, lc, nci, m);
   }
   if (cJ != 0.0 || cX != 0.0) {
@@ -323,12 +324,12 @@ inline void mf_apply_t(MatFree &mf, MatFreeOps<T> &o, cublasHandle_t h, cudaStre
       S2G_LAUNCH(k_mf_scatter<T>, grid, 256, 0, s, box, X, mf.ci, mf.ca, nci, lv,
                  (int64_t)lv * no, m, 1);
       // Z = CvP (rows x nv) * XbT (nv x no*m)
-      mf_gemm(h, CUBLAS_OP_N, CUBLAS_OP_N, rows, no * m, nv, 1.0, o.CvP.get(), lr, box, lv, 0.0,
+      mf_gemm(mf, h, s, CUBLAS_OP_N, CUBLAS_OP_N, rows, no * m, nv, 1.0, o.CvP.get(), lr, box, lv, 0.0,
               Z, lr);
       S2G_LAUNCH(k_mf_to_atom_major<T>, tgrid(no), dim3(32, 8), 0, s, Zt, Z, N, maxa, no, m, lr,
                  lo);
       // T_A = P^A_oo (no x no) * Zt_A (no x maxa*m), batched over atoms
-      mf_gemm_batched(h, no, maxa * m, no, o.PooA.get(), lo, (long long)lo * no, Zt, lo,
+      mf_gemm_batched(mf, h, s, no, maxa * m, no, o.PooA.get(), lo, (long long)lo * no, Zt, lo,
                       (long long)lo * maxa * m, Tm, lo, (long long)lo * maxa * m, N);
       S2G_LAUNCH(k_mf_from_atom_major<T>, tgrid(no), dim3(32, 8), 0, s, Tacc, Tm, N, maxa, no, m,
                  lr, lo, cJ, 0);
@@ -340,18 +341,18 @@ inline void mf_apply_t(MatFree &mf, MatFreeOps<T> &o, cublasHandle_t h, cudaStre
       S2G_LAUNCH(k_mf_scatter<T>, grid, 256, 0, s, box, X, mf.ci, mf.ca, nci, lo,
                  (int64_t)lo * nv, m, 0);
       // Z2 = CoP (rows x no) * Xb (no x nv*m)
-      mf_gemm(h, CUBLAS_OP_N, CUBLAS_OP_N, rows, nv * m, no, 1.0, o.CoP.get(), lr, box, lo, 0.0,
+      mf_gemm(mf, h, s, CUBLAS_OP_N, CUBLAS_OP_N, rows, nv * m, no, 1.0, o.CoP.get(), lr, box, lo, 0.0,
               Z, lr);
       S2G_LAUNCH(k_mf_to_atom_major<T>, tgrid(nv), dim3(32, 8), 0, s, Zt, Z, N, maxa, nv, m, lr,
                  lv);
       // U_A = P^A_ov (no x nv) * Z2t_A (nv x maxa*m)
-      mf_gemm_batched(h, no, maxa * m, nv, o.PovA.get(), lo, (long long)lo * nv, Zt, lv,
+      mf_gemm_batched(mf, h, s, no, maxa * m, nv, o.PovA.get(), lo, (long long)lo * nv, Zt, lv,
                       (long long)lv * maxa * m, Tm, lo, (long long)lo * maxa * m, N);
       S2G_LAUNCH(k_mf_from_atom_major<T>, tgrid(no), dim3(32, 8), 0, s, Tacc, Tm, N, maxa, no, m,
                  lr, lo, cX, have ? 1 : 0);
     }
     // box[a + lv*(i + no*r)] = CvP^T (nv x rows) * Tacc (rows x no*m)
-    mf_gemm(h, CUBLAS_OP_T, CUBLAS_OP_N, nv, no * m, rows, 1.0, o.CvP.get(), lr, Tacc, lr, 0.0,
+    mf_gemm(mf, h, s, CUBLAS_OP_T, CUBLAS_OP_N, nv, no * m, rows, 1.0, o.CvP.get(), lr, Tacc, lr, 0.0,
             box, lv);
     S2G_LAUNCH(k_mf_gather<T>, grid, 256, 0, s, out, box, mf.ci, mf.ca, nci, no, lv, m);
   }

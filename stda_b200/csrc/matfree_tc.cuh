@@ -172,12 +172,15 @@ __global__ void k_tcs_gather(double *__restrict__ out, const float *__restrict__
 struct SideStream {
   cudaStream_t s = nullptr;
   cublasHandle_t h = nullptr;
+  Dgemm dg;   // FP64 products on this stream (own split-K workspace)
+  bool lib_fp64 = false;   // those products through cuBLAS (STD2G_FLAG_LIBRARY_FP64)
   cudaEvent_t fork = nullptr, join = nullptr;
   void init() {
     if (s) return;
     S2G_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
     S2G_CUBLAS(cublasCreate(&h));
     S2G_CUBLAS(cublasSetStream(h, s));
+    if (lib_fp64) dg.lib = h;
     S2G_CUDA(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
     S2G_CUDA(cudaEventCreateWithFlags(&join, cudaEventDisableTiming));
   }
@@ -259,10 +262,10 @@ inline void mftc_apply(MatFreeTc &w, cublasHandle_t h, cudaStream_t s, const dou
     S2G_CUDA(cudaStreamWaitEvent(w.side.s, w.side.fork, 0));
     double *G = w.G.ensure((size_t)N * m);
     const double one = 1.0, zero = 0.0, ck = cK;
-    S2G_CUBLAS(cublasDgemm(w.side.h, CUBLAS_OP_N, CUBLAS_OP_N, N, m, nci, &one, w.Qs, N, X, nci,
-                           &zero, G, N));
-    S2G_CUBLAS(cublasDgemm(w.side.h, CUBLAS_OP_T, CUBLAS_OP_N, nci, m, N, &ck, w.Ps, N, G, N,
-                           &zero, out, nci));
+    w.side.dg.gemm(w.side.s, CUBLAS_OP_N, CUBLAS_OP_N, N, m, nci, &one, w.Qs, N, X, nci, &zero,
+                   G, N);
+    w.side.dg.gemm(w.side.s, CUBLAS_OP_T, CUBLAS_OP_N, nci, m, N, &ck, w.Ps, N, G, N, &zero, out,
+                   nci);
     S2G_CUDA(cudaEventRecord(w.side.join, w.side.s));
   } else {
     S2G_CUDA(cudaMemsetAsync(out, 0, sizeof(double) * nci * m, s));

@@ -221,6 +221,7 @@ int renew_context(Server *s, int slot) {
   std2g_opts eo{};
   eo.device = s->opts.device;
   eo.precision = s->opts.precision;
+  eo.flags = s->opts.flags;
   void *ctx = nullptr;
   const int st = std2g_create(&ctx, &eo);
   if (st != STD2G_OK) return st;
@@ -313,6 +314,7 @@ int std2g_server_create(void **srv, const std2g_server_opts *o) {
     std2g_opts eo{};
     eo.device = o->device;
     eo.precision = o->precision;
+    eo.flags = o->flags;
     eo.verbose = 0;
     void *ctx = nullptr;
     int st = std2g_create(&ctx, &eo);

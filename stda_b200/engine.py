@@ -33,7 +33,7 @@ EXPORTS = [
     "std2g_destroy", "std2g_screen_noalloc", "std2g_server_create", "std2g_server_submit",
     "std2g_server_poll", "std2g_server_wait", "std2g_server_stats", "std2g_server_destroy",
     "std2g_symeig_check", "std2g_set_sm_limit", "std2g_hyperpolarizability", "std2g_two_photon",
-    "std2g_ao_integrals", "std2g_load_prims",
+    "std2g_ao_integrals", "std2g_load_prims", "std2g_dgemm_check",
 ]
 
 
@@ -50,6 +50,7 @@ class Opts(C.Structure):
 
 
 FLAG_TENSOR_ALWAYS = 1
+FLAG_LIBRARY_FP64 = 2   # FP64 products through cuBLAS (library baseline)
 
 
 class Params(C.Structure):
@@ -62,7 +63,7 @@ class Params(C.Structure):
 
 class ServerOpts(C.Structure):
     _fields_ = [("device", C.c_int), ("precision", C.c_int), ("slots", C.c_int),
-                ("trace", C.c_int), ("hbm_budget", C.c_int64)]
+                ("trace", C.c_int), ("hbm_budget", C.c_int64), ("flags", C.c_int)]
 
 
 class Request(C.Structure):
@@ -128,6 +129,9 @@ def library():
         lib.std2g_server_wait.argtypes = [C.c_void_p, C.c_int64, C.POINTER(Result), dp, dp, dp]
         lib.std2g_server_stats.argtypes = [C.c_void_p, C.POINTER(C.c_int64)]
         lib.std2g_set_sm_limit.argtypes = [C.c_void_p, C.c_int]
+        lib.std2g_dgemm_check.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                          C.c_double, dp, C.c_int64, dp, C.c_int64, C.c_double,
+                                          dp, C.c_int64, C.c_int, dp]
         lib.std2g_symeig_check.argtypes = [C.c_int, C.c_int, C.c_int, dp, dp, dp, dp]
         lib.std2g_server_destroy.argtypes = [C.c_void_p]
         lib.std2g_server_destroy.restype = None
@@ -487,13 +491,13 @@ class Server:
     """
 
     def __init__(self, device: int = 0, precision: int = 1, slots: int = 4,
-                 hbm_budget: int = 0, trace: bool = False):
+                 hbm_budget: int = 0, trace: bool = False, flags: int = 0):
         self.lib = library()
         self.srv = C.c_void_p()
         _check(self.lib.std2g_server_create(C.byref(self.srv),
                                             C.byref(ServerOpts(device, precision, slots,
                                                                int(bool(trace)),
-                                                               int(hbm_budget)))))
+                                                               int(hbm_budget), int(flags)))))
         self._nomega = {}
 
     def submit(self, b, kw: Keywords, omegas=None) -> int:
@@ -571,6 +575,29 @@ class Server:
             self.close()
         except Exception:
             pass
+
+
+def dgemm_check(A, B, Cm, ta=False, tb=False, alpha=1.0, beta=0.0, device: int = 0):
+    """The engine's FP64 product on host arrays: A, B, Cm are (batch, rows,
+    cols) or 2-D; returns (alpha op(A) op(B) + beta Cm, device ms)."""
+    A3, B3, C3 = (np.asfortranarray(x if x.ndim == 3 else x[None]).astype(np.float64)
+                  for x in (A, B, Cm))
+    batch = A3.shape[0]
+    # column-major members laid out one after another
+    a = np.concatenate([np.asfortranarray(x).ravel(order="F") for x in A3])
+    b = np.concatenate([np.asfortranarray(x).ravel(order="F") for x in B3])
+    c = np.concatenate([np.asfortranarray(x).ravel(order="F") for x in C3])
+    m, n = C3.shape[1], C3.shape[2]
+    k = A3.shape[1] if ta else A3.shape[2]
+    ms = np.zeros(1)
+    lib = library()
+    a = a if a.size else np.zeros(1)
+    b = b if b.size else np.zeros(1)
+    _check(lib.std2g_dgemm_check(device, int(ta), int(tb), m, n, k, alpha, _dp(a),
+                                 max(1, A3.shape[1]), _dp(b), max(1, B3.shape[1]), beta, _dp(c), m,
+                                 batch, _dp(ms)))
+    out = c.reshape(batch, n, m).transpose(0, 2, 1)
+    return (out if Cm.ndim == 3 else out[0]), float(ms[0])
 
 
 def symeig_check(A, k, device: int = 0):
