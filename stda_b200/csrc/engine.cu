@@ -61,6 +61,8 @@ struct Ctx {
   int maxa = 1;
   int chunk_rows = 1;   // largest AO count of kChAtoms consecutive atoms
   bool sqrtS_ready = false;
+  int ns_iters = 0;            // Newton-Schulz steps of the last S^1/2
+  DBuf<double> w_ns;           // its scale / error words
   // work buffers
   DBuf<double> w_Cact, w_Clow, w_T, w_mu_ov, w_gj, w_gk, w_Qii, w_Qaa, w_Pii, w_uci;
   DBuf<double> w_Qia, w_Pia, w_Qoo, w_Poo, w_Qvv, w_de, w_ek;
@@ -174,6 +176,63 @@ static void sym_sqrt(Ctx &c, double *U, const double *w, int n, double *out, dou
   S2G_CUDA(cudaMemcpyAsync(tmp, U, sizeof(double) * n * n, cudaMemcpyDeviceToDevice, c.stream));
   S2G_LAUNCH(k_scale_cols_sqrt, grid_for((int64_t)n * n), 256, 0, c.stream, tmp, w, n);
   gemm(c, CUBLAS_OP_N, CUBLAS_OP_T, n, n, n, 1.0, tmp, n, U, n, 0.0, out, n);
+}
+
+// S^1/2 of the AO overlap (makel, stda.f:1615-1691) without an eigensolver:
+// with A = S / c (c = largest absolute row sum >= lambda_max, so the spectrum
+// of A lies in (0, 1]), the coupled Newton-Schulz iteration
+//   T_k = (3 I - Z_k A Z_k) / 2,   Z_{k+1} = T_k Z_k,   Z_0 = I
+// converges quadratically to A^-1/2 (every iterate is a polynomial in A, so
+// Y_k = A Z_k is the companion sequence that converges to A^1/2), and
+// S^1/2 = sqrt(c) A Z.  Stops when max |I - Z A Z| < 1e-14 or stagnates at the
+// rounding level below 1e-10.  A spectrum that is
+// not positive (makel's negative-eigenvalue stop, stda.f:1658-1670) makes
+// the iteration fail its final check ||Y Y - A||_max < 1e-10 ||A||_max.
+// Three FP64 products per step on the engine's DMMA kernel.
+static void sqrt_overlap(Ctx &c, const double *S, int n, double *out) {
+  cudaStream_t s = c.stream;
+  const size_t nn = (size_t)n * n;
+  double *A = c.w_tmp.ensure(nn * 4), *Z = A + nn, *P = A + 2 * nn, *T = A + 3 * nn;
+  auto *flags = (unsigned long long *)c.w_ns.ensure(2);
+  S2G_CUDA(cudaMemsetAsync(flags, 0, 2 * sizeof(unsigned long long), s));
+  S2G_LAUNCH(k_row_abs_max, (int)div_up(n, 256), 256, 0, s, S, n, flags);
+  S2G_LAUNCH(k_ns_init, grid_for((int64_t)nn), 256, 0, s, A, Z, S, n, flags);
+  unsigned long long h[2] = {0, 0};
+  double err = 1.0, prev = 2.0;
+  int it = 0;
+  // quadratic convergence ends at the rounding level of the products: stop at
+  // 1e-14, or once below 1e-10 a step no longer halves the error
+  for (; it < 100 && err >= 1e-14 && !(err < 1e-10 && err > 0.5 * prev); ++it) {
+    prev = err;
+    gemm(c, CUBLAS_OP_N, CUBLAS_OP_N, n, n, n, 1.0, A, n, Z, n, 0.0, P, n);   // P = A Z
+    gemm(c, CUBLAS_OP_N, CUBLAS_OP_N, n, n, n, 1.0, Z, n, P, n, 0.0, T, n);   // T = Z A Z
+    S2G_CUDA(cudaMemsetAsync(flags + 1, 0, sizeof(unsigned long long), s));
+    S2G_LAUNCH(k_ns_step, grid_for((int64_t)nn), 256, 0, s, T, n, flags + 1);
+    gemm(c, CUBLAS_OP_N, CUBLAS_OP_N, n, n, n, 1.0, T, n, Z, n, 0.0, P, n);   // Z <- T Z
+    std::swap(Z, P);
+    S2G_CUDA(cudaMemcpyAsync(h, flags, sizeof(h), cudaMemcpyDeviceToHost, s));
+    S2G_CUDA(cudaStreamSynchronize(s));
+    std::memcpy(&err, &h[1], sizeof(double));
+    if (!std::isfinite(err) || err > 1e6) break;
+  }
+  c.ns_iters = it;
+  double cmax;
+  std::memcpy(&cmax, &h[0], sizeof(double));
+  // Y = A Z (= A^1/2); check Y Y = A, then S^1/2 = sqrt(c) Y
+  gemm(c, CUBLAS_OP_N, CUBLAS_OP_N, n, n, n, 1.0, A, n, Z, n, 0.0, P, n);
+  S2G_CUDA(cudaMemcpyAsync(T, A, sizeof(double) * nn, cudaMemcpyDeviceToDevice, s));
+  gemm(c, CUBLAS_OP_N, CUBLAS_OP_N, n, n, n, 1.0, P, n, P, n, -1.0, T, n);   // T = Y Y - A
+  S2G_CUDA(cudaMemsetAsync(flags + 1, 0, sizeof(unsigned long long), s));
+  S2G_LAUNCH(k_abs_max, grid_for((int64_t)nn), 256, 0, s, T, (int64_t)nn, flags + 1);
+  S2G_CUDA(cudaMemcpyAsync(h, flags, sizeof(h), cudaMemcpyDeviceToHost, s));
+  S2G_CUDA(cudaStreamSynchronize(s));
+  double resid;
+  std::memcpy(&resid, &h[1], sizeof(double));
+  // ||A||_max <= 1 by the scaling
+  if (!(err < 1e-10) || !(resid < 1e-10))
+    throw Error{STD2G_ES_NOT_PD, "S^1/2: overlap matrix not positive definite (Newton-Schulz "
+                                 "did not converge)"};
+  S2G_LAUNCH(k_scale_copy, grid_for((int64_t)nn), 256, 0, s, out, P, (int64_t)nn, std::sqrt(cmax));
 }
 
 static uint64_t fnv1a(const std::vector<int> &a, const std::vector<int> &b) {
@@ -811,16 +870,7 @@ static void solve(Ctx &c, const std2g_params &p_in, std2g_result *res, const Res
   // ---- S^1/2 (makel stda.f:1615-1691), once per load ----
   record(c, PH_SQRTS);
   if (!c.sqrtS_ready) {
-    size_t nn = (size_t)nao * nao;
-    double *U = c.w_tmp.ensure(nn * 2);
-    S2G_CUDA(cudaMemcpyAsync(U, c.d_Sfull.get(), sizeof(double) * nn, cudaMemcpyDeviceToDevice, s));
-    double *w = c.w_eval.ensure(std::max(nao, 16));
-    dense_eig_full(c, U, nao, w);
-    double wmin = 0;
-    S2G_CUDA(cudaMemcpyAsync(&wmin, w, sizeof(double), cudaMemcpyDeviceToHost, s));
-    S2G_CUDA(cudaStreamSynchronize(s));
-    if (wmin < 0) throw Error{STD2G_ES_NOT_PD, "negative overlap eigenvalue (S^1/2)"};
-    sym_sqrt(c, U, w, nao, c.d_sqrtS.ensure(nn), U + nn);
+    sqrt_overlap(c, c.d_Sfull.get(), nao, c.d_sqrtS.ensure((size_t)nao * nao));
     c.sqrtS_ready = true;
   }
   double *Clow = c.w_Clow.ensure((size_t)nao * moci);

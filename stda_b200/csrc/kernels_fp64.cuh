@@ -45,6 +45,71 @@ __global__ void k_unpack(double *__restrict__ full, const double *__restrict__ p
   }
 }
 
+// ---- S^1/2 by a coupled Newton-Schulz iteration (makel, stda.f:1615-1691) ----
+// Largest absolute row sum of the symmetric n x n S (a bound on its largest
+// eigenvalue): block maxima combined with an atomic max on the bit pattern,
+// which orders non-negative doubles like their values.
+__global__ void k_row_abs_max(const double *__restrict__ S, int n,
+                              unsigned long long *__restrict__ out) {
+  double best = 0.0;
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+    double r = 0.0;
+    for (int i = 0; i < n; ++i) r += fabs(S[(int64_t)j * n + i]);   // column j = row j
+    best = fmax(best, r);
+  }
+  for (int o = 16; o > 0; o >>= 1) best = fmax(best, __shfl_xor_sync(0xffffffffu, best, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(out, (unsigned long long)__double_as_longlong(best));
+}
+
+// A = S / c (c = *cmax as stored by k_row_abs_max), Z = I
+__global__ void k_ns_init(double *__restrict__ A, double *__restrict__ Z,
+                          const double *__restrict__ S, int n,
+                          const unsigned long long *__restrict__ cmax) {
+  const double inv = 1.0 / __longlong_as_double((long long)*cmax);
+  const int64_t total = (int64_t)n * n;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t j = t / n, i = t - j * n;
+    A[t] = S[t] * inv;
+    Z[t] = i == j ? 1.0 : 0.0;
+  }
+}
+
+// in place: Q = Z A Z becomes T = (3 I - Q) / 2, and *err = max |I - Q|
+// (bit-pattern max)
+__global__ void k_ns_step(double *__restrict__ QT, int n, unsigned long long *__restrict__ err) {
+  const int64_t total = (int64_t)n * n;
+  double e = 0.0;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t j = t / n, i = t - j * n;
+    const double d = (i == j ? 1.0 : 0.0) - QT[t];
+    QT[t] = (i == j ? 1.0 : 0.0) + 0.5 * d;
+    e = fmax(e, fabs(d));
+  }
+  for (int o = 16; o > 0; o >>= 1) e = fmax(e, __shfl_xor_sync(0xffffffffu, e, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(err, (unsigned long long)__double_as_longlong(e));
+}
+
+// *out = max |x| (bit-pattern max; NaN propagates as a huge pattern)
+__global__ void k_abs_max(const double *__restrict__ x, int64_t n,
+                          unsigned long long *__restrict__ out) {
+  double e = 0.0;
+  bool nan = false;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const double v = fabs(x[t]);
+    nan |= v != v;
+    e = fmax(e, v);
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    e = fmax(e, __shfl_xor_sync(0xffffffffu, e, o));
+    nan |= __shfl_xor_sync(0xffffffffu, (int)nan, o) != 0;
+  }
+  if ((threadIdx.x & 31) == 0)
+    atomicMax(out, nan ? 0x7ff8000000000000ull : (unsigned long long)__double_as_longlong(e));
+}
+
 // U[:, c] *= sqrt(w[c])   (makel, stda.f:1672-1686)
 __global__ void k_scale_cols_sqrt(double *__restrict__ U, const double *__restrict__ w, int n) {
   int64_t total = (int64_t)n * n;

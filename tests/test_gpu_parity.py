@@ -294,3 +294,20 @@ def test_std_dft_iterative_pure_functional(benzene):
     ref = _oracle(mol, ints, rpa=True, **kw)
     assert np.abs(sol.omega - ref.omega[:8]).max() < 1e-9
     assert np.allclose(sol.fL, ref.fL[:8], rtol=1e-5, atol=1e-8)
+
+
+def test_indefinite_overlap_is_refused(water):
+    """makel stops on a negative overlap eigenvalue (stda.f:1658-1670); the
+    engine's Newton-Schulz S^1/2 reports it as STD2G_ES_NOT_PD."""
+    from stda_b200.engine import Engine, Keywords, Std2gError, boundary_inputs
+    mol, ints = water
+    b = boundary_inputs(mol, ints)
+    S = b.S.copy()
+    S[1] = 1.5            # element (2, 1): |S_21| > 1 makes S indefinite
+    b.S = S
+    eng = Engine(0, 0)
+    eng.load(b)
+    with pytest.raises(Std2gError) as e:
+        eng.solve(Keywords(ax=1.0, e_thr_ev=20.0))
+    assert e.value.name == "ES_NOT_PD"
+    eng.close()
