@@ -112,10 +112,24 @@ typedef struct {
   double *omega;     /* [cap] excitation energies (Eh) */
   double *fL, *fV;   /* [cap] oscillator strengths, length / velocity */
   double *RL, *RV;   /* [cap] rotatory strengths (R_V velocity-corrected for sTDA) */
-  double *resid;     /* [cap] residual norm ||A x - w x|| per root (may be NULL) */
+  double *resid;     /* [cap] FP64 residual norm of each returned root's vector
+                        (||A x - w x||, or the sTD-DFT pair's residual); -1
+                        where none is formed (dense sTD-DFT); may be NULL */
   double alpha0[6];  /* alpha(0) sum over states, xx xy yy xz yz zz (stda.f:1247-1252) */
   uint64_t csf_hash; /* FNV-1a hash of the selected CSF list (i,a) in order */
   double ms_total;   /* device time of the solve (ms) */
+  /* the three dominant CSFs of each root, as the reference's state table
+     prints them (stda.f:1222-1358, 1456-1462): value (TDA coefficient, or
+     X^2 - Y^2 for sTD-DFT) and the CSF's occupied / virtual MO (1-based,
+     virtual numbered after the occupied ones as in std2g_get_csf); may be NULL */
+  double *dom_coef;  /* [3*cap] */
+  int *dom_i, *dom_a;/* [3*cap] */
+  /* per-root bound on |omega - omega_FP64-exact| (Eh): from the FP64 residual
+     r of the returned vector, min(||r||, ||r||^2 / gap) with the gap to the
+     other eigenvalue estimates (Kato-Temple), plus, in the mixed form, the
+     bound on the PT-lowered diagonal's deviation from its FP64 value (Weyl);
+     -1 where no residual is formed (dense sTD-DFT); may be NULL */
+  double *err_est;   /* [cap] */
 } std2g_result;
 
 /* Create a context on opts->device.  Replaces the allocation part of stda.f

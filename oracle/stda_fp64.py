@@ -933,3 +933,41 @@ def _timed_sample(st, p: Params, budget_s):
               f"lowest {k_s} of {n_s}, scaled to nci^3 ({t_eig:.1f}s est.)")
     return dict(est_total_s=est, setup_s=t_setup, pt_s=t_pt, a_s=t_a, eig_s=t_eig, nci=nci,
                 threads=threads, sample=sample)
+
+
+def dominant_csfs(res: Result):
+    """The three dominant CSFs of each root as the reference picks them for
+    its state table (stda.f:1222-1358): over the CSFs in order, with
+    u = X + Y, p = X - Y (sTD-DFT) or u = p = X (TDA), the first is the last
+    CSF where |u p| exceeded the running value umax (which then becomes u p,
+    signed), the second and third where u p exceeded it (umax reset to -1,
+    earlier picks skipped).  Returns (value, i, a) arrays of shape (nroot, 3):
+    value = the TDA coefficient or X^2 - Y^2; i, a = the occupied and virtual
+    MO of the CSF, 1-based, virtual numbered after the no occupied MOs."""
+    X = res.X
+    Y = res.Y if res.Y is not None else None
+    nci, nroot = X.shape
+    val = np.zeros((nroot, 3))
+    oi = np.zeros((nroot, 3), dtype=int)
+    oa = np.zeros((nroot, 3), dtype=int)
+    for r in range(nroot):
+        x = X[:, r]
+        y = Y[:, r] if Y is not None else np.zeros(nci)
+        up = (x + y) * (x - y)
+        picks = []
+        umax, k = -1.0, 0
+        for j in range(nci):
+            if abs(up[j]) > umax:
+                umax, k = up[j], j
+        picks.append(k)
+        for _ in range(2):
+            umax, k = -1.0, 0
+            for j in range(nci):
+                if up[j] > umax and j not in picks:
+                    umax, k = up[j], j
+            picks.append(k)
+        for q, j in enumerate(picks):
+            val[r, q] = x[j] ** 2 - y[j] ** 2 if Y is not None else x[j]
+            oi[r, q] = res.iconf[j, 0] + 1
+            oa[r, q] = res.iconf[j, 1] + res.no + 1
+    return val, oi, oa

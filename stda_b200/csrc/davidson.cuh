@@ -228,6 +228,9 @@ struct DavidsonWork {
   bool profile = false;
   double sec_ms[5] = {0, 0, 0, 0, 0};
   Dgemm *dg = nullptr;   // the context's FP64 products (dgemm.cuh)
+  // residual norms and Ritz values of the last Rayleigh-Ritz step (every
+  // tracked pair, the buffer roots above the wanted ones included)
+  std::vector<double> final_resid, final_theta;
 };
 
 // host wall-clock section timer used when DavidsonWork::profile is set
@@ -480,7 +483,11 @@ inline int davidson(DavidsonWork &dw, cublasHandle_t blas, cusolverDnHandle_t so
   }
   S2G_CUDA(cudaMemcpyAsync(omega_out, theta, sizeof(double) * kwant, cudaMemcpyDeviceToDevice, s));
   S2G_CUDA(cudaMemcpyAsync(X_out, X, sizeof(double) * n * kwant, cudaMemcpyDeviceToDevice, s));
+  dw.final_theta.assign(k, 0.0);
+  S2G_CUDA(cudaMemcpyAsync(dw.final_theta.data(), theta, sizeof(double) * k,
+                           cudaMemcpyDeviceToHost, s));
   S2G_CUDA(cudaStreamSynchronize(s));
+  dw.final_resid = h_rn;
   return nconv;
 }
 

@@ -96,6 +96,8 @@ struct DavidsonRpaWork {
   DBuf<int> cols, einfo;
   int iters = 0;
   int64_t matvecs = 0;
+  // residual norms and roots of the last subspace step (all tracked pairs)
+  std::vector<double> final_resid, final_omega;
 };
 
 // Symmetric eigen-decomposition of the m x m matrix A (ld lda, lower read):
@@ -163,7 +165,7 @@ inline int davidson_rpa(DavidsonWork &dw, DavidsonRpaWork &rw, cublasHandle_t bl
   int *idx = dw.idx.ensure(k);
   S2G_CUDA(cudaMemcpyAsync(idx, order.data(), sizeof(int) * k, cudaMemcpyHostToDevice, s));
   S2G_LAUNCH(k_unit_vectors, grid, 256, 0, s, B, n, idx, k);
-  int m = 0, nb = k, nconv = 0;
+  int m = 0, nb = k, nconv = 0, last_kk = 0;
   std::vector<double> h_rn(k), h_lam(1);
   rw.iters = 0;
   rw.matvecs = 0;
@@ -195,6 +197,7 @@ inline int davidson_rpa(DavidsonWork &dw, DavidsonRpaWork &rw, cublasHandle_t bl
     (dw.dg->gemm(s, CUBLAS_OP_N, CUBLAS_OP_N, m, m, m, &one, S, m, T1, m, &zero, Mr,
                            m));
     const int kk = std::min(k, m);
+    last_kk = kk;
     rpa_small_eig(dw, rw, sol, s, Mr, m, m, kk, ev, Z, Zf, einfo);
     S2G_LAUNCH(k_sqrt_inplace, (int)div_up(kk, 128), 128, 0, s, ev, kk);
     S2G_CUDA(cudaMemcpyAsync(om, ev, sizeof(double) * kk, cudaMemcpyDeviceToDevice, s));
@@ -281,7 +284,11 @@ inline int davidson_rpa(DavidsonWork &dw, DavidsonRpaWork &rw, cublasHandle_t bl
   S2G_CUDA(cudaMemcpyAsync(omega_out, om, sizeof(double) * kwant, cudaMemcpyDeviceToDevice, s));
   S2G_CUDA(cudaMemcpyAsync(XpY_out, XpY, sizeof(double) * n * kwant, cudaMemcpyDeviceToDevice, s));
   S2G_CUDA(cudaMemcpyAsync(XmY_out, XmY, sizeof(double) * n * kwant, cudaMemcpyDeviceToDevice, s));
+  rw.final_omega.assign(last_kk, 0.0);
+  S2G_CUDA(cudaMemcpyAsync(rw.final_omega.data(), om, sizeof(double) * last_kk,
+                           cudaMemcpyDeviceToHost, s));
   S2G_CUDA(cudaStreamSynchronize(s));
+  rw.final_resid.assign(h_rn.begin(), h_rn.begin() + last_kk);
   return nconv;
 }
 

@@ -54,6 +54,8 @@ struct Ctx {
   int ncent = 0, nmo = 0, nao = 0;
   std::vector<double> h_eps, h_occ, h_xyz;
   AoIntsWork aoi;   // primitive list of the device AO integrals (ao_ints.cuh)
+  DBuf<double> w_Ares, w_Rres, w_part, w_rn, w_domc;   // dense residuals, dominant CSFs
+  DBuf<int> w_domi;
   Dgemm dg;         // the engine's FP64 matrix products (dgemm.cuh)
   // device inputs
   DBuf<double> d_xyz, d_C, d_eps_act, d_eta, d_Sfull, d_sqrtS, d_ao9;
@@ -827,6 +829,7 @@ static void solve(Ctx &c, const std2g_params &p_in, std2g_result *res, const Res
   c.tc_flop = 0;
   c.tc_launches = 0;
   c.mixed.rechecked = 0;
+  c.mixed.ed_bound_max = 0.0;   // the FP64 PT path lowers the diagonal in FP64
   c.dav_iters = 0;
   c.dav_matvecs = 0;
   c.dav_fp64_matvecs = 0;
@@ -1246,6 +1249,9 @@ static void solve(Ctx &c, const std2g_params &p_in, std2g_result *res, const Res
   int nroot = 0;
   double *X = nullptr, *Yv = nullptr, *om = nullptr;
   double *Bh = nullptr;
+  // FP64 residual norms of the returned roots and the eigenvalue estimates
+  // around them (the error estimates of the result); empty: not formed
+  std::vector<double> root_resid, root_ritz;
   if (p.rpa && use_mf) {
     // sTD-DFT roots by the subspace form of srpapack (davidson_rpa.cuh)
     record(c, PH_EIGEN);
@@ -1275,6 +1281,8 @@ static void solve(Ctx &c, const std2g_params &p_in, std2g_result *res, const Res
     if (conv < nroot)
       throw Error{STD2G_ENOCONV, "sTD-DFT Davidson: " + std::to_string(conv) + " of " +
                                      std::to_string(nroot) + " roots converged"};
+    root_resid = c.davr.final_resid;
+    root_ritz = c.davr.final_omega;
   } else if (!p.rpa && use_mf) {
     record(c, PH_EIGEN);
     om = c.w_eval.ensure(std::max(nci, nao));
@@ -1335,6 +1343,8 @@ static void solve(Ctx &c, const std2g_params &p_in, std2g_result *res, const Res
     nroot = std::min(p.nroots, nci);
     X = Xd;
     c.mixed.lastX = X;
+    root_resid = c.dav.final_resid;
+    root_ritz = c.dav.final_theta;
   } else if (!p.rpa) {
     double *A = c.w_A.ensure(n2);
     S2G_LAUNCH(k_combine_tda, grid_for(n2), 256, 0, s, A, K, J, (int64_t)nci, ak, d_edall);
@@ -1349,6 +1359,23 @@ static void solve(Ctx &c, const std2g_params &p_in, std2g_result *res, const Res
     X = A;
     c.mixed.lastX = X;
     if (nroot < 1) throw Error{STD2G_ENOROOT, "no root below the energy threshold"};
+    // FP64 residuals ||A x - w x|| of the returned eigenvectors: A rebuilt
+    // from K, J and the diagonal (its storage now holds the eigenvectors)
+    {
+      double *Ar = c.w_Ares.ensure(n2), *Rr = c.w_Rres.ensure((size_t)nci * nroot);
+      S2G_LAUNCH(k_combine_tda, grid_for(n2), 256, 0, s, Ar, K, J, (int64_t)nci, ak, d_edall);
+      gemm(c, CUBLAS_OP_N, CUBLAS_OP_N, nci, nroot, nci, 1.0, Ar, nci, X, nci, 0.0, Rr, nci);
+      double *part = c.w_part.ensure((size_t)nroot * kColSplit), *rn = c.w_rn.ensure(nroot);
+      S2G_LAUNCH(k_dav_resid, dim3(kColSplit, (unsigned)nroot), 256, 0, s, Rr, X, om, nci, part);
+      S2G_LAUNCH(k_colnorm_finish, (int)div_up(nroot, 128), 128, 0, s, part, kColSplit, nroot,
+                 rn);
+      root_resid.assign(nroot, 0.0);
+      root_ritz.assign(nroot, 0.0);
+      S2G_CUDA(cudaMemcpyAsync(root_resid.data(), rn, sizeof(double) * nroot,
+                               cudaMemcpyDeviceToHost, s));
+      S2G_CUDA(cudaMemcpyAsync(root_ritz.data(), om, sizeof(double) * nroot,
+                               cudaMemcpyDeviceToHost, s));
+    }
   } else {
     double *Apb = nullptr, *Amb = nullptr;
     if (!resp_mf) {
@@ -1521,13 +1548,23 @@ static void solve(Ctx &c, const std2g_params &p_in, std2g_result *res, const Res
              (!p.rpa && p.velcorr) ? 1 : 0, props, props + nroot, props + 2 * nroot,
              props + 3 * nroot);
   S2G_LAUNCH(k_alpha0, 1, 128, 0, s, TL, nroot, nroot, om, ak, props + 4 * nroot);
+  // the three dominant CSFs of each root (stda.f:1222-1358)
+  double *dom_c = c.w_domc.ensure((size_t)3 * nroot);
+  int *dom_ia = c.w_domi.ensure((size_t)6 * nroot);
+  S2G_LAUNCH(k_dominant_csfs, nroot, 256, 0, s, X, p.rpa ? Yv : (const double *)nullptr, nci,
+             d_ci, d_ca, no, dom_c, dom_ia, dom_ia + 3 * nroot);
   record(c, PH_RESPONSE);
   record(c, PH_COUNT);
 
   // ---- results ----
-  std::vector<double> h_props((size_t)nroot * 4 + 6), h_om(nroot);
+  std::vector<double> h_props((size_t)nroot * 4 + 6), h_om(nroot), h_domc((size_t)3 * nroot);
+  std::vector<int> h_domi((size_t)6 * nroot);
   S2G_CUDA(cudaMemcpyAsync(h_props.data(), props, sizeof(double) * (nroot * 4 + 6),
                            cudaMemcpyDeviceToHost, s));
+  S2G_CUDA(cudaMemcpyAsync(h_domc.data(), dom_c, sizeof(double) * 3 * nroot,
+                           cudaMemcpyDeviceToHost, s));
+  S2G_CUDA(cudaMemcpyAsync(h_domi.data(), dom_ia, sizeof(int) * 6 * nroot, cudaMemcpyDeviceToHost,
+                           s));
   S2G_CUDA(cudaMemcpyAsync(h_om.data(), om, sizeof(double) * nroot, cudaMemcpyDeviceToHost, s));
   S2G_CUDA(cudaStreamSynchronize(s));
   for (int q = 0; q < PH_COUNT; ++q) {
@@ -1560,7 +1597,28 @@ static void solve(Ctx &c, const std2g_params &p_in, std2g_result *res, const Res
       if (res->fV) res->fV[r] = h_props[nroot + r];
       if (res->RL) res->RL[r] = h_props[2 * nroot + r];
       if (res->RV) res->RV[r] = h_props[3 * nroot + r];
-      if (res->resid) res->resid[r] = 0.0;
+      const bool have = r < (int)root_resid.size();
+      const double rr = have ? root_resid[r] : -1.0;
+      if (res->resid) res->resid[r] = rr;
+      if (res->err_est) {
+        // |w - w(A)| <= min(||r||, ||r||^2 / gap) (Kato-Temple), the gap
+        // from the other eigenvalue estimates less their own residuals
+        double gap = 1e300;
+        for (size_t q = 0; q < root_ritz.size(); ++q)
+          if ((int)q != r)
+            gap = std::min(gap, std::fabs(root_ritz[q] - h_om[r]) -
+                                    (q < root_resid.size() ? root_resid[q] : 0.0));
+        // plus (Weyl) the bound on the PT-lowered diagonal's deviation from
+        // its FP64 value, nonzero where the tensor-core selection formed it
+        res->err_est[r] = !have ? -1.0
+                                : (gap > 0 ? std::min(rr, rr * rr / gap) : rr) +
+                                      c.mixed.ed_bound_max;
+      }
+      for (int q = 0; q < 3; ++q) {
+        if (res->dom_coef) res->dom_coef[3 * r + q] = h_domc[3 * r + q];
+        if (res->dom_i) res->dom_i[3 * r + q] = h_domi[3 * r + q];
+        if (res->dom_a) res->dom_a[3 * r + q] = h_domi[3 * nroot + 3 * r + q];
+      }
     }
     for (int q = 0; q < 6; ++q) res->alpha0[q] = h_props[4 * nroot + q];
     if (nroot > res->cap) throw Error{STD2G_ECAP, "result capacity too small"};

@@ -110,6 +110,93 @@ __global__ void k_abs_max(const double *__restrict__ x, int64_t n,
     atomicMax(out, nan ? 0x7ff8000000000000ull : (unsigned long long)__double_as_longlong(e));
 }
 
+// ---- the three dominant CSFs of each root (stda.f:1222-1358) ----
+// TDA (Y == nullptr): weights w_j = c_j^2; the reference keeps the first CSF
+// whose weight exceeds the running maximum, i.e. the largest weight with the
+// lowest CSF index on ties, then the next two the same way excluding the
+// ones already taken; the reported value is the coefficient c_j.  One block
+// per root, three block-wide arg-max passes.
+// sTD-DFT (Y given): u = X + Y, p = X - Y and the first pick follows the
+// reference's running comparison |u p| > umax with umax = u p (signed), the
+// second and third u p > umax; reported value X^2 - Y^2.  That comparison is
+// order dependent, so one thread of the block scans the CSFs in order.
+// out_i / out_a: occupied and virtual MO of the CSF (1-based, virtual
+// numbered after the no occupied MOs).
+__global__ void k_dominant_csfs(const double *__restrict__ X, const double *__restrict__ Y,
+                                int nci, const int *__restrict__ ci, const int *__restrict__ ca,
+                                int no, double *__restrict__ out_c, int *__restrict__ out_i,
+                                int *__restrict__ out_a) {
+  const int r = blockIdx.x;
+  const double *x = X + (int64_t)r * nci;
+  const double *y = Y ? Y + (int64_t)r * nci : nullptr;
+  __shared__ double sv[32];
+  __shared__ int si[32];
+  __shared__ int pick[3];
+  if (y) {
+    if (threadIdx.x == 0) {
+      int k0 = 0, k1 = 0, k2 = 0;
+      double um = -1.0;
+      for (int j = 0; j < nci; ++j) {
+        const double v = (x[j] + y[j]) * (x[j] - y[j]);
+        if (fabs(v) > um) { um = v; k0 = j; }
+      }
+      um = -1.0;
+      for (int j = 0; j < nci; ++j) {
+        const double v = (x[j] + y[j]) * (x[j] - y[j]);
+        if (v > um && j != k0) { um = v; k1 = j; }
+      }
+      um = -1.0;
+      for (int j = 0; j < nci; ++j) {
+        const double v = (x[j] + y[j]) * (x[j] - y[j]);
+        if (v > um && j != k0 && j != k1) { um = v; k2 = j; }
+      }
+      pick[0] = k0;
+      pick[1] = k1;
+      pick[2] = k2;
+    }
+  } else {
+    for (int q = 0; q < 3; ++q) {
+      double bv = -1.0;
+      int bi = nci;
+      for (int j = threadIdx.x; j < nci; j += blockDim.x) {
+        if ((q > 0 && j == pick[0]) || (q > 1 && j == pick[1])) continue;
+        const double v = x[j] * x[j];
+        if (v > bv) { bv = v; bi = j; }     // strided scan: the first of equal values kept
+      }
+      for (int o = 16; o > 0; o >>= 1) {
+        const double ov = __shfl_xor_sync(0xffffffffu, bv, o);
+        const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+        if (ov > bv || (ov == bv && oi < bi)) { bv = ov; bi = oi; }
+      }
+      if ((threadIdx.x & 31) == 0) {
+        sv[threadIdx.x >> 5] = bv;
+        si[threadIdx.x >> 5] = bi;
+      }
+      __syncthreads();
+      if (threadIdx.x < 32) {
+        const int nw = blockDim.x >> 5;
+        bv = threadIdx.x < nw ? sv[threadIdx.x] : -1.0;
+        bi = threadIdx.x < nw ? si[threadIdx.x] : nci;
+        for (int o = 16; o > 0; o >>= 1) {
+          const double ov = __shfl_xor_sync(0xffffffffu, bv, o);
+          const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+          if (ov > bv || (ov == bv && oi < bi)) { bv = ov; bi = oi; }
+        }
+        if (threadIdx.x == 0) pick[q] = bi < nci ? bi : 0;
+      }
+      __syncthreads();
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x < 3) {
+    const int j = pick[threadIdx.x];
+    const double v = y ? (x[j] * x[j] - y[j] * y[j]) : x[j];
+    out_c[3 * r + threadIdx.x] = nci > threadIdx.x ? v : 0.0;
+    out_i[3 * r + threadIdx.x] = nci > threadIdx.x ? ci[j] + 1 : 0;
+    out_a[3 * r + threadIdx.x] = nci > threadIdx.x ? ca[j] + no + 1 : 0;
+  }
+}
+
 // U[:, c] *= sqrt(w[c])   (makel, stda.f:1672-1686)
 __global__ void k_scale_cols_sqrt(double *__restrict__ U, const double *__restrict__ w, int n) {
   int64_t total = (int64_t)n * n;

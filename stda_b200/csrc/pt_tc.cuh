@@ -238,6 +238,19 @@ struct PtCols {
   const int *gq;          // slab (group) index of b_q
 };
 
+// inputs of the column pass's error bound: the row pass's norms, with the
+// J-side norms replaced by their maxima over the row's occupied partner j
+// (wrow) and over the primary's q_ab slab (vmax)
+struct PtColBound {
+  const float *pn;     // ||p_ia|| of every (i, a)
+  const float *qn;     // ||q_q|| of the primaries
+  const int *gq;       // slab of each primary
+  const float *wrow;   // max_j ||p_ij|| per occupied i
+  const float *vmax;   // max_a ||q_ab|| per slab
+  float ecoup;
+  int i0;
+};
+
 constexpr int kRowThreads = 128;
 constexpr int kRowStage = 256;   // primaries staged in shared memory at a time
 constexpr int kRowBatch = 8;     // primaries whose loads are issued together
@@ -371,25 +384,27 @@ constexpr int kColRows = 4;  // candidate rows per thread and step (loads issued
 // loads issued first, terms of rows that are not summed multiplied by zero;
 // per-thread FP64 sums, then a fixed-order warp and block reduction
 // (deterministic).
-__global__ void __launch_bounds__(256, 3)
+__global__ void __launch_bounds__(256, 2)
 k_ptq_cols(const float *__restrict__ K, const float *__restrict__ J, int ni, int nv, int nva,
            int nex, const unsigned char *__restrict__ use, const float2 *__restrict__ rhl,
            const float *__restrict__ eh, const float *__restrict__ el, float akf,
-           double *__restrict__ colpart) {
+           double *__restrict__ colpart, PtColBound cb, double *__restrict__ colbnd) {
   const int q0 = blockIdx.x * kColQ;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  float ehq[kColQ], elq[kColQ];
-  double acc[kColQ];
+  float ehq[kColQ], elq[kColQ], qnq[kColQ], vmq[kColQ];
+  double acc[kColQ], accb[kColQ];
 #pragma unroll
   for (int u = 0; u < kColQ; ++u) {
     const int q = min(q0 + u, nex - 1);
     ehq[u] = eh[q];
     elq[u] = el[q];
-    acc[u] = 0.0;
+    qnq[u] = cb.qn[q];
+    vmq[u] = cb.vmax[cb.gq[q]];
+    acc[u] = accb[u] = 0.0;
   }
   const int64_t nrow = (int64_t)ni * nv;
   for (int64_t e0 = threadIdx.x; e0 < nrow; e0 += (int64_t)blockDim.x * kColRows) {
-    float kv[kColRows][kColQ], jv[kColRows][kColQ], w[kColRows];
+    float kv[kColRows][kColQ], jv[kColRows][kColQ], w[kColRows], pr[kColRows], wr[kColRows];
     float2 r[kColRows];
 #pragma unroll
     for (int v = 0; v < kColRows; ++v) {   // rows e0, e0 + blockDim, ...: coalesced
@@ -398,6 +413,8 @@ k_ptq_cols(const float *__restrict__ K, const float *__restrict__ J, int ni, int
       const int ii = (int)(e / nv), a = (int)(e - (int64_t)ii * nv);
       w[v] = (ev < nrow && use[e]) ? 1.f : 0.f;
       r[v] = rhl[e];
+      pr[v] = cb.pn[(int64_t)(cb.i0 + ii) * nv + a];
+      wr[v] = cb.wrow[cb.i0 + ii];
       const int64_t o = ((int64_t)ii * nex + q0) * nva + a;
 #pragma unroll
       for (int u = 0; u < kColQ; ++u) {
@@ -408,28 +425,76 @@ k_ptq_cols(const float *__restrict__ K, const float *__restrict__ J, int ni, int
     }
 #pragma unroll
     for (int u = 0; u < kColQ; ++u) {
-      float t = 0.f;
+      float t = 0.f, b = 0.f;
 #pragma unroll
       for (int v = 0; v < kColRows; ++v) {
         const float am = akf * kv[v][u] - jv[v][u];
-        t += w[v] * (am * am * __frcp_rn((r[v].x - ehq[u]) + (r[v].y - elq[u])));
+        const float den = (r[v].x - ehq[u]) + (r[v].y - elq[u]);
+        const float rden = __frcp_rn(den);
+        const float tt = am * am * rden;
+        t += w[v] * tt;
+        // the row pass's term bound with the coupling's J norms bounded by
+        // their row / slab maxima, plus the FP32 partial sum of kColRows terms
+        const float da = cb.ecoup * (akf * pr[v] * qnq[u] + wr[v] * vmq[u]) +
+                         2.f * kU32 * (akf * fabsf(kv[v][u]) + fabsf(jv[v][u]));
+        const float ed = 4.f * kU32 + 3e-14f * rden;
+        const float bt = den > 0.f && ed < 0.25f
+                             ? (2.f * fabsf(am) * da + da * da) * rden +
+                                   fabsf(tt) * (2.f * ed + (6.f + kColRows) * kU32)
+                             : INFINITY;
+        b += w[v] * bt;
       }
       acc[u] += (double)t;
+      accb[u] += (double)b * (1.0 + 8.0 * kU32);
     }
   }
-  __shared__ double red[8][kColQ];
+  __shared__ double red[8][kColQ], redb[8][kColQ];
 #pragma unroll
   for (int u = 0; u < kColQ; ++u) {
-    double v = acc[u];
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    if (lane == 0) red[warp][u] = v;
+    double v = acc[u], vb = accb[u];
+    for (int o = 16; o > 0; o >>= 1) {
+      v += __shfl_xor_sync(0xffffffffu, v, o);
+      vb += __shfl_xor_sync(0xffffffffu, vb, o);
+    }
+    if (lane == 0) {
+      red[warp][u] = v;
+      redb[warp][u] = vb;
+    }
   }
   __syncthreads();
   if (threadIdx.x < kColQ && q0 + (int)threadIdx.x < nex) {
-    double v = 0.0;
-    for (int ww = 0; ww < 8; ++ww) v += red[ww][threadIdx.x];
+    double v = 0.0, vb = 0.0;
+    for (int ww = 0; ww < 8; ++ww) {
+      v += red[ww][threadIdx.x];
+      vb += redb[ww][threadIdx.x];
+    }
     colpart[q0 + threadIdx.x] = v;
+    colbnd[q0 + threadIdx.x] = vb;
   }
+}
+
+// largest entry of each row of a rows x cols FP32 array (row-major)
+__global__ void k_rowmax(const float *__restrict__ x, int64_t rows, int cols,
+                         float *__restrict__ out) {
+  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < rows;
+       r += (int64_t)gridDim.x * blockDim.x) {
+    float m = 0.f;
+    for (int c = 0; c < cols; ++c) m = fmaxf(m, x[r * cols + c]);
+    out[r] = m;
+  }
+}
+
+// per primary: the bound of its PT lowering summed over the chunks; *maxb =
+// the largest (bit-pattern max of non-negative doubles)
+__global__ void k_pt2_bound_finish(const double *__restrict__ colbnd, int nchunk, int nex,
+                                   unsigned long long *__restrict__ maxb) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  double s = 0.0;
+  if (c < nex)
+    for (int q = 0; q < nchunk; ++q) s += colbnd[(int64_t)q * nex + c];
+  if (!(s >= 0.0)) s = 1e300;   // INF / NaN: no usable bound
+  for (int o = 16; o > 0; o >>= 1) s = fmax(s, __shfl_xor_sync(0xffffffffu, s, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(maxb, (unsigned long long)__double_as_longlong(s));
 }
 
 // ---------------------------------------------------------------- FP64 recheck
@@ -498,7 +563,10 @@ struct MixedWork {
   DBuf<float> K, J, pn, qn, wn, vn, eh, el, pinv, qinv, winv, vinv, wsc;
   DBuf<float2> rhl;
   DBuf<int> pk, ck, cand_pos, jq, gq, vidx, g_tile0, g_qs, g_nq, recheck;
-  DBuf<double> ed, part_t, part_b, bnd, colpart, recheck_part;
+  DBuf<double> ed, part_t, part_b, bnd, colpart, colbnd, recheck_part, ed_bound;
+  DBuf<float> wrow, vmax;
+  // bound on max_q |PT-lowered diagonal - its FP64 value| of the last selection
+  double ed_bound_max = 0.0;
   DBuf<unsigned char> use;
   double *lastX = nullptr;
   int64_t rechecked = 0;
@@ -605,6 +673,10 @@ inline void mixed_pt_select(MixedWork &mw, cudaStream_t s, const PtProblem &pb,
   stats(mw.wn, mw.winv, pb.Poo, nullptr, (int64_t)no * no);
   stats(mw.vn, mw.vinv, pb.Qvv, d_vidx, (int64_t)ng * nv);
   const float *d_pn = mw.pn.get(), *d_wn = mw.wn.get(), *d_vn = mw.vn.get();
+  float *d_wrow = mw.wrow.ensure(no), *d_vmax = mw.vmax.ensure(std::max(ng, 1));
+  S2G_LAUNCH(k_rowmax, (int)div_up(no, 128), 128, 0, s, d_wn, (int64_t)no, no, d_wrow);
+  if (ng > 0)
+    S2G_LAUNCH(k_rowmax, (int)div_up(ng, 128), 128, 0, s, d_vn, (int64_t)ng, nv, d_vmax);
   // operands shared by all chunks: the primaries' q and the q_ab slabs
   auto split = [&](DBuf<__half> &h, DBuf<__half> &l, const double *src, const int *idx,
                    const float *inv, int64_t ncols) {
@@ -625,6 +697,7 @@ inline void mixed_pt_select(MixedWork &mw, cudaStream_t s, const PtProblem &pb,
   const int occ_chunk = std::max(1, (int)std::min<double>(no, pb.budget / per_occ));
   const int nchunk = (int)div_up(no, occ_chunk);
   double *colpart = mw.colpart.ensure((size_t)nchunk * nex);
+  double *colbnd = mw.colbnd.ensure((size_t)nchunk * nex);
   double *bnd = mw.bnd.ensure(std::max(nexpt, 1));
   std::vector<double> h_pert, h_bnd;
   std::vector<int> rows;
@@ -717,13 +790,21 @@ inline void mixed_pt_select(MixedWork &mw, cudaStream_t s, const PtProblem &pb,
     // column sums over the candidates that stay out
     unsigned char *use = mw.use.ensure((size_t)ni * nv);
     S2G_LAUNCH(k_ptq_use, gfin, 256, 0, s, ni, nv, i0, d_cpos, sel, use);
+    const PtColBound cb{d_pn, mw.qn.get(), d_gq, d_wrow, d_vmax, ecoup, i0};
     S2G_LAUNCH(k_ptq_cols, (int)div_up(nex, kColQ), 256, 0, s, K, J, ni, nv, nva, nex, use, rhl,
-               d_eh, d_el, akf, colpart + (size_t)ch * nex);
+               d_eh, d_el, akf, colpart + (size_t)ch * nex, cb, colbnd + (size_t)ch * nex);
     tick(5);
     r_begin = r_end;
   }
   mw.tc.check(s);
   S2G_LAUNCH(k_pt2_finish, (int)div_up(nex, 128), 128, 0, s, colpart, nchunk, nex, d_ed, pt2, edp);
+  auto *mb = (unsigned long long *)mw.ed_bound.ensure(1);
+  S2G_CUDA(cudaMemsetAsync(mb, 0, sizeof(unsigned long long), s));
+  S2G_LAUNCH(k_pt2_bound_finish, (int)div_up(nex, 128), 128, 0, s, colbnd, nchunk, nex, mb);
+  double h_mb = 0.0;
+  S2G_CUDA(cudaMemcpyAsync(&h_mb, mb, sizeof(double), cudaMemcpyDeviceToHost, s));
+  S2G_CUDA(cudaStreamSynchronize(s));
+  mw.ed_bound_max = h_mb;
 }
 
 }  // namespace std2g

@@ -57,7 +57,8 @@ struct Job {
   bool done = false;
   int status = STD2G_OK;
   std2g_result res{};
-  std::vector<double> om, fL, fV, RL, RV, resid, alpha, alpha_resid;
+  std::vector<double> om, fL, fV, RL, RV, resid, alpha, alpha_resid, err, domc;
+  std::vector<int> domi, doma;
   // trace: phase times (ms) of the solve and of alpha(omega), load time
   std::vector<double> ph_solve, ph_alpha;
   double load_ms = 0;
@@ -115,6 +116,26 @@ int64_t footprint_estimate(const Job &j, int precision) {
   return b;
 }
 
+// result arrays of a job for cap roots, bound into its std2g_result
+void room(Job &j, int cap) {
+  for (auto *v : {&j.om, &j.fL, &j.fV, &j.RL, &j.RV, &j.resid, &j.err}) v->assign(cap, 0.0);
+  j.domc.assign(3 * (size_t)cap, 0.0);
+  j.domi.assign(3 * (size_t)cap, 0);
+  j.doma.assign(3 * (size_t)cap, 0);
+  j.res = std2g_result{};
+  j.res.cap = cap;
+  j.res.omega = j.om.data();
+  j.res.fL = j.fL.data();
+  j.res.fV = j.fV.data();
+  j.res.RL = j.RL.data();
+  j.res.RV = j.RV.data();
+  j.res.resid = j.resid.data();
+  j.res.err_est = j.err.data();
+  j.res.dom_coef = j.domc.data();
+  j.res.dom_i = j.domi.data();
+  j.res.dom_a = j.doma.data();
+}
+
 std::vector<double> phases_of(void *ctx) {
   std::vector<double> ph(32, 0.0);
   ph.resize(std::min(32, std2g_phase_times(ctx, ph.data(), 32)));
@@ -134,34 +155,12 @@ void run_job(void *ctx, Job &j, bool trace) {
     j.load_ms = std::chrono::duration<double, std::milli>(Clock::now() - j.t_start).count();
   if (st == STD2G_OK) {
     const int cap = j.par.nroots > 0 ? j.par.nroots : 20000;
-    j.om.assign(cap, 0.0);
-    j.fL.assign(cap, 0.0);
-    j.fV.assign(cap, 0.0);
-    j.RL.assign(cap, 0.0);
-    j.RV.assign(cap, 0.0);
-    j.resid.assign(cap, 0.0);
-    j.res = std2g_result{};
-    j.res.cap = cap;
-    j.res.omega = j.om.data();
-    j.res.fL = j.fL.data();
-    j.res.fV = j.fV.data();
-    j.res.RL = j.RL.data();
-    j.res.RV = j.RV.data();
-    j.res.resid = j.resid.data();
+    room(j, cap);
     st = std2g_solve(ctx, &j.par, &j.res);
     if (st == STD2G_ECAP && j.res.nroot > cap) {
       // every root of the window was asked for and there are more than cap:
       // the solve reported the count; run it once more with that much room
-      const int need = j.res.nroot;
-      for (auto *v : {&j.om, &j.fL, &j.fV, &j.RL, &j.RV, &j.resid}) v->assign(need, 0.0);
-      j.res = std2g_result{};
-      j.res.cap = need;
-      j.res.omega = j.om.data();
-      j.res.fL = j.fL.data();
-      j.res.fV = j.fV.data();
-      j.res.RL = j.RL.data();
-      j.res.RV = j.RV.data();
-      j.res.resid = j.resid.data();
+      room(j, j.res.nroot);
       st = std2g_solve(ctx, &j.par, &j.res);
     }
     if (trace) j.ph_solve = phases_of(ctx);
@@ -419,10 +418,14 @@ int std2g_server_wait(void *srv, int64_t ticket, std2g_result *res, double *alph
   if (j->status != STD2G_OK) return j->status;
   if (res) {
     const int n = j->res.nroot;
-    double *dst[6] = {res->omega, res->fL, res->fV, res->RL, res->RV, res->resid};
-    const std::vector<double> *src[6] = {&j->om, &j->fL, &j->fV, &j->RL, &j->RV, &j->resid};
-    for (int q = 0; q < 6; ++q)
-      if (dst[q]) std::copy(src[q]->begin(), src[q]->begin() + n, dst[q]);
+    double *dst[8] = {res->omega, res->fL, res->fV, res->RL,
+                      res->RV,    res->resid, res->err_est, res->dom_coef};
+    const std::vector<double> *src[8] = {&j->om, &j->fL,    &j->fV,  &j->RL,
+                                         &j->RV, &j->resid, &j->err, &j->domc};
+    for (int q = 0; q < 8; ++q)
+      if (dst[q]) std::copy(src[q]->begin(), src[q]->begin() + (q == 7 ? 3 * n : n), dst[q]);
+    if (res->dom_i) std::copy(j->domi.begin(), j->domi.begin() + 3 * n, res->dom_i);
+    if (res->dom_a) std::copy(j->doma.begin(), j->doma.begin() + 3 * n, res->dom_a);
     const int cap = res->cap;
     std2g_result keep = *res;
     *res = j->res;
@@ -433,6 +436,10 @@ int std2g_server_wait(void *srv, int64_t ticket, std2g_result *res, double *alph
     res->RL = keep.RL;
     res->RV = keep.RV;
     res->resid = keep.resid;
+    res->err_est = keep.err_est;
+    res->dom_coef = keep.dom_coef;
+    res->dom_i = keep.dom_i;
+    res->dom_a = keep.dom_a;
   }
   if (alpha && !j->alpha.empty()) std::copy(j->alpha.begin(), j->alpha.end(), alpha);
   if (alpha_resid && !j->alpha_resid.empty())

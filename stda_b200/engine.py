@@ -85,7 +85,39 @@ class Result(C.Structure):
                 ("omega", C.POINTER(C.c_double)), ("fL", C.POINTER(C.c_double)),
                 ("fV", C.POINTER(C.c_double)), ("RL", C.POINTER(C.c_double)),
                 ("RV", C.POINTER(C.c_double)), ("resid", C.POINTER(C.c_double)),
-                ("alpha0", C.c_double * 6), ("csf_hash", C.c_uint64), ("ms_total", C.c_double)]
+                ("alpha0", C.c_double * 6), ("csf_hash", C.c_uint64), ("ms_total", C.c_double),
+                ("dom_coef", C.POINTER(C.c_double)), ("dom_i", C.POINTER(C.c_int)),
+                ("dom_a", C.POINTER(C.c_int)), ("err_est", C.POINTER(C.c_double))]
+
+
+class _ResultBuffers:
+    """Host arrays behind one std2g_result (cap roots)."""
+
+    def __init__(self, cap: int):
+        self.cap = cap
+        self.d = [np.zeros(cap) for _ in range(7)]      # omega fL fV RL RV resid err_est
+        self.dc = np.zeros(3 * cap)
+        self.di = np.zeros(3 * cap, dtype=np.int32)
+        self.da = np.zeros(3 * cap, dtype=np.int32)
+        self.res = Result()
+        r = self.res
+        r.cap = cap
+        r.omega, r.fL, r.fV, r.RL, r.RV, r.resid, r.err_est = (_dp(x) for x in self.d)
+        r.dom_coef = _dp(self.dc)
+        r.dom_i = self.di.ctypes.data_as(C.POINTER(C.c_int))
+        r.dom_a = self.da.ctypes.data_as(C.POINTER(C.c_int))
+
+    def solution(self, velo: bool, xmolw: float = 0.0):
+        r, n = self.res, self.res.nroot
+        return Solution(omega=self.d[0][:n].copy(), fL=self.d[1][:n].copy(),
+                        fV=self.d[2][:n].copy(), RL=self.d[3][:n].copy(), RV=self.d[4][:n].copy(),
+                        alpha0=np.array(r.alpha0[:]), no=r.no, nv=r.nv, nex=r.nex,
+                        nexpt=r.nexpt, new=r.new_pt, nci=r.nci, csf_hash=r.csf_hash,
+                        ms=r.ms_total, velo=velo, xmolw=xmolw,
+                        extras=dict(resid=self.d[5][:n].copy(), err_est=self.d[6][:n].copy(),
+                                    dominant=dict(value=self.dc[:3 * n].reshape(n, 3).copy(),
+                                                  i=self.di[:3 * n].reshape(n, 3).copy(),
+                                                  a=self.da[:3 * n].reshape(n, 3).copy())))
 
 
 _lib = None
@@ -376,23 +408,14 @@ class Engine:
         reports STD2G_ECAP with the count, and the solve is repeated once with
         that much room."""
         while True:
-            bufs = [np.zeros(cap) for _ in range(6)]
-            res = Result()
-            res.cap = cap
-            res.omega, res.fL, res.fV, res.RL, res.RV, res.resid = (_dp(b) for b in bufs)
-            code = self.lib.std2g_solve(self.ctx, C.byref(kw.to_c()), C.byref(res))
-            if code == 11 and res.nroot > cap:
-                cap = res.nroot
+            rb = _ResultBuffers(cap)
+            code = self.lib.std2g_solve(self.ctx, C.byref(kw.to_c()), C.byref(rb.res))
+            if code == 11 and rb.res.nroot > cap:
+                cap = rb.res.nroot
                 continue
             _check(code)
             break
-        n = res.nroot
-        return Solution(omega=bufs[0][:n].copy(), fL=bufs[1][:n].copy(), fV=bufs[2][:n].copy(),
-                        RL=bufs[3][:n].copy(), RV=bufs[4][:n].copy(),
-                        alpha0=np.array(res.alpha0[:]), no=res.no, nv=res.nv, nex=res.nex,
-                        nexpt=res.nexpt, new=res.new_pt, nci=res.nci, csf_hash=res.csf_hash,
-                        ms=res.ms_total, velo=(not kw.rpa) and kw.velcorr, xmolw=self.xmolw,
-                        extras=dict(resid=bufs[5][:n].copy()))
+        return rb.solution((not kw.rpa) and kw.velcorr, self.xmolw)
 
     def polarizability(self, kw: Keywords, omegas):
         om = np.ascontiguousarray(omegas, dtype=np.float64)
@@ -536,24 +559,15 @@ class Server:
         ares = np.zeros(max(1, nom))
         timing = np.zeros(3)
         while True:
-            bufs = [np.zeros(cap) for _ in range(6)]
-            res = Result()
-            res.cap = cap
-            res.omega, res.fL, res.fV, res.RL, res.RV, res.resid = (_dp(x) for x in bufs)
-            code = self.lib.std2g_server_wait(self.srv, ticket, C.byref(res), _dp(alpha),
+            rb = _ResultBuffers(cap)
+            code = self.lib.std2g_server_wait(self.srv, ticket, C.byref(rb.res), _dp(alpha),
                                               _dp(ares), _dp(timing))
-            if code == 11 and res.nroot > cap:
-                cap = res.nroot
+            if code == 11 and rb.res.nroot > cap:
+                cap = rb.res.nroot
                 continue
             _check(code)
             break
-        n = res.nroot
-        sol = Solution(omega=bufs[0][:n].copy(), fL=bufs[1][:n].copy(), fV=bufs[2][:n].copy(),
-                       RL=bufs[3][:n].copy(), RV=bufs[4][:n].copy(),
-                       alpha0=np.array(res.alpha0[:]), no=res.no, nv=res.nv, nex=res.nex,
-                       nexpt=res.nexpt, new=res.new_pt, nci=res.nci, csf_hash=res.csf_hash,
-                       ms=res.ms_total, velo=(not kw.rpa) and kw.velcorr,
-                       extras=dict(resid=bufs[5][:n].copy()))
+        sol = rb.solution((not kw.rpa) and kw.velcorr)
         a = alpha[:nom * 9].reshape(nom, 3, 3) if nom else None
         return sol, a, (ares[:nom] if nom else None), dict(
             queued_ms=timing[0], run_ms=timing[1], latency_ms=timing[2])

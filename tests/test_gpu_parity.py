@@ -311,3 +311,40 @@ def test_indefinite_overlap_is_refused(water):
         eng.solve(Keywords(ax=1.0, e_thr_ev=20.0))
     assert e.value.name == "ES_NOT_PD"
     eng.close()
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+@pytest.mark.parametrize("rpa", [False, True])
+def test_dominant_csfs_and_error_estimates(water, precision, rpa):
+    """The state table's three dominant CSFs per root (stda.f:1222-1358)
+    against the oracle's restatement of the reference's selection, and the
+    per-root error estimate: |w - w_FP64 exact| stays below err_est for every
+    root that has one (Davidson and dense TDA)."""
+    from oracle.stda_fp64 import dominant_csfs
+    from stda_b200 import synth
+    mol, ints = synth.random_molecule(28, seed=9, with_ints=True)
+    kw = dict(ax=0.5, e_thr_ev=8.0, rpa=rpa)
+    ref = _oracle(mol, ints, **kw)
+    val, oi, oa = dominant_csfs(ref)
+    for nroots, solver in ((0, 1), (8, 2)):
+        eng, sol, iconf, ed = _run(mol, ints, precision, nroots=nroots, solver=solver,
+                                   conv_tol=1e-8, **kw)
+        eng.close()
+        n = len(sol.omega)
+        dom = sol.extras["dominant"]
+        # the leading CSF of every root is the oracle's; the three weights agree
+        # (the order of nearly equal second / third weights may differ)
+        assert np.array_equal(dom["i"][:, 0], oi[:n, 0])
+        assert np.array_equal(dom["a"][:, 0], oa[:n, 0])
+        if rpa:
+            assert np.allclose(dom["value"], val[:n], atol=1e-6)
+        else:
+            assert np.allclose(np.abs(dom["value"]), np.abs(val[:n]), atol=1e-6)
+        err = sol.extras["err_est"]
+        resid = sol.extras["resid"]
+        if rpa and solver == 1:
+            assert np.all(err == -1.0) and np.all(resid == -1.0)
+        else:
+            assert np.all(err >= 0.0) and np.all(resid >= 0.0)
+            assert np.all(np.abs(sol.omega - ref.omega[:n]) <= err + 1e-12), (
+                np.abs(sol.omega - ref.omega[:n]), err)
