@@ -2,12 +2,13 @@
 // column-major, op = N or T, optionally batched with fixed strides.
 //
 // B200 has no FP64 kind of tcgen05; its FP64 tensor path is the warp-level
-// DMMA (mma.sync m8n8k4 .f64).  Each CTA (4 warps) computes a 64 x 64 tile of C
-// over a K range in steps of 16: the A (64 x 16) and B (16 x 64) tiles arrive
-// by 8-byte cp.async in a 4-stage shared-memory ring (three tiles in flight
-// while one is multiplied), kept in the global layout's fast order and
+// DMMA (mma.sync m8n8k4 .f64).  Each CTA (4 warps) computes a 64 x 128 tile
+// of C over a K range in steps of 16: the A (64 x 16) and B (16 x 128) tiles
+// arrive by 8-byte cp.async in a 4-stage shared-memory ring (three tiles in
+// flight while one is multiplied), kept in the global layout's fast order and
 // XOR-swizzled so that the fragment reads are conflict-free, and each warp
-// owns a 32 x 32 sub-tile = 4 x 4 DMMA tiles (32 accumulators per thread).
+// owns a 32 x 64 sub-tile = 4 x 8 DMMA tiles (64 accumulators per thread, so
+// that an accumulator is reused only every 32 DMMAs).
 //
 // Tall-skinny products (the Davidson projections V^T W: 300 x 75 outputs over
 // 5e4-long sums) split K across CTAs.  The partial tiles go to a workspace and
@@ -22,14 +23,17 @@
 namespace std2g {
 
 namespace dg {
-constexpr int BM = 64, BN = 64, BK = 16, THREADS = 128, STAGES = 4;
-constexpr int TILE = 64 * BK;                      // doubles per operand tile (no padding)
-constexpr int SMEM_BYTES = STAGES * 2 * TILE * 8;  // 64 KB: three CTAs per SM
+constexpr int BM = 64, BK = 16, THREADS = 128, STAGES = 4;
+constexpr int TILE_A = BM * BK;                              // doubles per A tile
+template <int BN> __host__ __device__ constexpr int stage_doubles() { return TILE_A + BN * BK; }
+// 64 x 32 tiles: 48 KB (four CTAs per SM); 64 x 64: 64 KB (three); 64 x 128: 96 KB (two)
+template <int BN> __host__ __device__ constexpr int smem_bytes() { return STAGES * stage_doubles<BN>() * 8; }
 // Shared-memory positions, XOR-swizzled so that the fragment reads of a half
 // warp (g = 0..3 along m or n, t = 0..3 along k) hit 16 distinct 8-byte banks:
-// operand stored with m (or n) fastest, [BK][64]:
-__device__ __forceinline__ int pos_mfast(int k, int m) { return k * 64 + (m ^ ((k & 3) << 2)); }
-// operand stored with k fastest, [64][BK]:
+// operand stored with m (or n) fastest, [BK][W]:
+template <int W>
+__device__ __forceinline__ int pos_mfast(int k, int m) { return k * W + (m ^ ((k & 3) << 2)); }
+// operand stored with k fastest, [rows][BK]:
 __device__ __forceinline__ int pos_kfast(int m, int k) { return m * 16 + (k ^ ((m & 3) << 2)); }
 }
 
@@ -62,58 +66,91 @@ __device__ __forceinline__ void cp_async_wait() {
 // A tiles are kept in the global layout's fast order: m fastest for op(A) = A
 // ([k][m]), k fastest for op(A) = A^T ([m][k]); B tiles k fastest for
 // op(B) = B ([n][k]), n fastest for op(B) = B^T ([k][n]); swizzled (pos_*).
-template <bool TA, bool TB>
-__global__ void __launch_bounds__(dg::THREADS, 3)
+// CTA tile 64 x BN (BN = 32, 64, 128); warp w owns rows 32 (w & 1) .. +32 and
+// columns (BN / 2)(w >> 1) .. +BN / 2: 4 x BN / 16 DMMA tiles.
+template <bool TA, bool TB, int BN>
+__global__ void __launch_bounds__(dg::THREADS, BN == 32 ? 4 : (BN == 64 ? 3 : 2))
     k_dgemm(int M, int N, int K, double alpha, const double *__restrict__ A, int64_t lda,
             int64_t sA, const double *__restrict__ B, int64_t ldb, int64_t sB, double beta,
             double *__restrict__ C, int64_t ldc, int64_t sC, int ksplit, int kchunk,
-            double *__restrict__ work) {
+            double *__restrict__ work, int tri) {
   using namespace dg;
   extern __shared__ __align__(16) double smem_d[];
   const int tiles_m = (M + BM - 1) / BM;
   const int m0 = (blockIdx.x % tiles_m) * BM, n0 = (blockIdx.x / tiles_m) * BN;
+  // tri > 0: column n is the pair (i, j) = (n / tri, n % tri) of a symmetric
+  // pair array and only j <= i is wanted: a tile whose columns all lie above
+  // the diagonal is skipped (the caller mirrors those columns)
+  if (tri > 0) {
+    const int i0 = n0 / tri, i1 = min(N - 1, n0 + BN - 1) / tri;
+    if (i0 == i1 && n0 - i0 * tri > i0) return;
+  }
   const int batch = blockIdx.y / ksplit, split = blockIdx.y % ksplit;
   const int kb = split * kchunk, ke = min(K, kb + kchunk);
   A += batch * sA;
   B += batch * sB;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int g = lane >> 2, t = lane & 3;
-  const int wm = (warp & 1) * 32, wn = (warp >> 1) * 32;
-  auto As = [&](int st) { return smem_d + (size_t)st * 2 * TILE; };
-  auto Bs = [&](int st) { return smem_d + (size_t)st * 2 * TILE + TILE; };
+  constexpr int NJ = BN / 16, STAGE = stage_doubles<BN>(), TILE_B = BN * BK;
+  const int wm = (warp & 1) * 32, wn = (warp >> 1) * (BN / 2);
+  auto As = [&](int st) { return smem_d + (size_t)st * STAGE; };
+  auto Bs = [&](int st) { return smem_d + (size_t)st * STAGE + TILE_A; };
 
-  // issue the copies of the K tile starting at k0 into stage st
+  // issue the copies of the K tile starting at k0 into stage st; element q of
+  // this thread is idx = tid + 128 q, so along the tile's slow dimension it
+  // moves by a fixed stride and one source pointer per operand serves all q
   auto issue = [&](int st, int k0) {
     double *a = As(st), *b = Bs(st);
+    if (!TA) {   // m fastest: m = tid % 64, k = tid / 64 + 2 q
+      const int m = tid & 63, kq = tid >> 6;
+      const bool okm = m0 + m < M;
+      const double *src = A + (m0 + m) + (int64_t)(k0 + kq) * lda;
 #pragma unroll
-    for (int q = 0; q < 8; ++q) {
-      const int idx = tid + THREADS * q;
-      if (!TA) {
-        const int m = idx & 63, k = idx >> 6, gm = m0 + m, gk = k0 + k;
-        const bool ok = gm < M && gk < ke;
-        cp_async8(a + pos_mfast(k, m), ok ? A + gm + (int64_t)gk * lda : A, ok);
-      } else {
-        const int k = idx & 15, m = idx >> 4, gm = m0 + m, gk = k0 + k;
-        const bool ok = gm < M && gk < ke;
-        cp_async8(a + pos_kfast(m, k), ok ? A + gk + (int64_t)gm * lda : A, ok);
+      for (int q = 0; q < TILE_A / THREADS; ++q) {
+        const int k = kq + 2 * q;
+        const bool ok = okm && k0 + k < ke;
+        cp_async8(a + pos_mfast<BM>(k, m), ok ? src + (int64_t)(2 * q) * lda : A, ok);
       }
-      if (!TB) {
-        const int k = idx & 15, n = idx >> 4, gn = n0 + n, gk = k0 + k;
-        const bool ok = gn < N && gk < ke;
-        cp_async8(b + pos_kfast(n, k), ok ? B + gk + (int64_t)gn * ldb : B, ok);
-      } else {
-        const int n = idx & 63, k = idx >> 6, gn = n0 + n, gk = k0 + k;
-        const bool ok = gn < N && gk < ke;
-        cp_async8(b + pos_mfast(k, n), ok ? B + gn + (int64_t)gk * ldb : B, ok);
+    } else {     // k fastest: k = tid % 16, m = tid / 16 + 8 q
+      const int k = tid & 15, mq = tid >> 4;
+      const bool okk = k0 + k < ke;
+      const double *src = A + (k0 + k) + (int64_t)(m0 + mq) * lda;
+#pragma unroll
+      for (int q = 0; q < TILE_A / THREADS; ++q) {
+        const int m = mq + 8 * q;
+        const bool ok = okk && m0 + m < M;
+        cp_async8(a + pos_kfast(m, k), ok ? src + (int64_t)(8 * q) * lda : A, ok);
+      }
+    }
+    if (!TB) {   // k fastest: k = tid % 16, n = tid / 16 + 8 q
+      const int k = tid & 15, nq = tid >> 4;
+      const bool okk = k0 + k < ke;
+      const double *src = B + (k0 + k) + (int64_t)(n0 + nq) * ldb;
+#pragma unroll
+      for (int q = 0; q < TILE_B / THREADS; ++q) {
+        const int n = nq + 8 * q;
+        const bool ok = okk && n0 + n < N;
+        cp_async8(b + pos_kfast(n, k), ok ? src + (int64_t)(8 * q) * ldb : B, ok);
+      }
+    } else {     // n fastest: n = tid % BN, k = tid / BN + (128 / BN) q
+      constexpr int KS = THREADS / BN;
+      const int n = tid & (BN - 1), kq = tid / BN;
+      const bool okn = n0 + n < N;
+      const double *src = B + (n0 + n) + (int64_t)(k0 + kq) * ldb;
+#pragma unroll
+      for (int q = 0; q < TILE_B / THREADS; ++q) {
+        const int k = kq + KS * q;
+        const bool ok = okn && k0 + k < ke;
+        cp_async8(b + pos_mfast<BN>(k, n), ok ? src + (int64_t)(KS * q) * ldb : B, ok);
       }
     }
   };
 
-  double acc[4][4][2];
+  double acc[4][NJ][2];
 #pragma unroll
   for (int i = 0; i < 4; ++i)
 #pragma unroll
-    for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+    for (int j = 0; j < NJ; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
 
   const int nt = ke > kb ? (ke - kb + BK - 1) / BK : 0;
 #pragma unroll
@@ -132,21 +169,21 @@ __global__ void __launch_bounds__(dg::THREADS, 3)
     const double *a = As(it % STAGES), *b = Bs(it % STAGES);
 #pragma unroll
     for (int ks = 0; ks < BK; ks += 4) {
-      double fa[4], fb[4];
+      double fa[4], fb[NJ];
 #pragma unroll
       for (int i = 0; i < 4; ++i) {
         const int m = wm + 8 * i + g, k = ks + t;
-        fa[i] = TA ? a[pos_kfast(m, k)] : a[pos_mfast(k, m)];
+        fa[i] = TA ? a[pos_kfast(m, k)] : a[pos_mfast<BM>(k, m)];
       }
 #pragma unroll
-      for (int j = 0; j < 4; ++j) {
+      for (int j = 0; j < NJ; ++j) {
         const int n = wn + 8 * j + g, k = ks + t;
-        fb[j] = TB ? b[pos_mfast(k, n)] : b[pos_kfast(n, k)];
+        fb[j] = TB ? b[pos_mfast<BN>(k, n)] : b[pos_kfast(n, k)];
       }
 #pragma unroll
       for (int i = 0; i < 4; ++i)
 #pragma unroll
-        for (int j = 0; j < 4; ++j) dmma_8x8x4(acc[i][j][0], acc[i][j][1], fa[i], fb[j]);
+        for (int j = 0; j < NJ; ++j) dmma_8x8x4(acc[i][j][0], acc[i][j][1], fa[i], fb[j]);
     }
   }
   cp_async_wait<0>();
@@ -159,7 +196,7 @@ __global__ void __launch_bounds__(dg::THREADS, 3)
       const int row = m0 + wm + 8 * i + g;
       if (row >= M) continue;
 #pragma unroll
-      for (int j = 0; j < 4; ++j)
+      for (int j = 0; j < NJ; ++j)
 #pragma unroll
         for (int e = 0; e < 2; ++e) {
           const int col = n0 + wn + 8 * j + 2 * t + e;
@@ -176,7 +213,7 @@ __global__ void __launch_bounds__(dg::THREADS, 3)
       const int row = m0 + wm + 8 * i + g;
       if (row >= M) continue;
 #pragma unroll
-      for (int j = 0; j < 4; ++j)
+      for (int j = 0; j < NJ; ++j)
 #pragma unroll
         for (int e = 0; e < 2; ++e) {
           const int col = n0 + wn + 8 * j + 2 * t + e;
@@ -223,10 +260,10 @@ struct Dgemm {
   // op(A) is m x k, op(B) is k x n; strides between batch members (0 for one).
   void run(cudaStream_t s, bool ta, bool tb, int m, int n, int k, double alpha, const double *A,
            int64_t lda, int64_t sA, const double *B, int64_t ldb, int64_t sB, double beta,
-           double *C, int64_t ldc, int64_t sC, int batch = 1) {
+           double *C, int64_t ldc, int64_t sC, int batch = 1, int tri = 0) {
     if (m <= 0 || n <= 0 || batch <= 0) return;
     if (k < 0) throw Error{STD2G_EINVAL, "dgemm: negative k"};
-    if (lib) {
+    if (lib && tri == 0) {
       const cublasOperation_t oa = ta ? CUBLAS_OP_T : CUBLAS_OP_N, ob = tb ? CUBLAS_OP_T : CUBLAS_OP_N;
       S2G_CUBLAS(cublasSetStream(lib, s));
       if (batch == 1)
@@ -237,39 +274,60 @@ struct Dgemm {
                                              (int)ldb, sB, &beta, C, (int)ldc, sC, batch));
       return;
     }
-    const int tiles = (int)(div_up(m, dg::BM) * div_up(n, dg::BN));
-    // split K to fill the device: CTAs run in waves of 3 per SM; pick the
-    // split count with the fewest K steps on the busiest SM (each split at
-    // least 256 long; a split adds its workspace pass, weighted 3 %)
-    const int64_t ctas = (int64_t)tiles * batch, slots = 3 * (int64_t)nsm;
-    const int kmax = (int)std::max<int64_t>(1, std::min<int64_t>(64, k / 256));
-    int ksplit = 1;
+    // tile width and split-K: CTAs run in waves (four 64 x 32, three 64 x 64
+    // or two 64 x 128 CTAs per SM); for each width pick the split count with
+    // the fewest K steps on the busiest SM (each split at least 256 long; a
+    // split adds its workspace pass, weighted 3 %), then the width with the
+    // lower cost (the time of one K step of a full wave, measured on B200: a
+    // 64 x 32 / 64 x 128 wave step takes 0.74 / 1.31 of a 64 x 64 one)
+    int bn = 64, ksplit = 1;
     double best = 0.0;
-    for (int ks = 1; ks <= kmax; ++ks) {
-      const int64_t steps = div_up(ctas * ks, slots) * div_up(div_up(std::max(k, 1), ks), dg::BK);
-      const double cost = (double)steps * (ks > 1 ? 1.03 : 1.0);
-      if (ks == 1 || cost < best) {
-        best = cost;
-        ksplit = ks;
+    const int kmax = (int)std::max<int64_t>(1, std::min<int64_t>(64, k / 256));
+    for (int w : {32, 64, 128}) {
+      const int64_t ctas = div_up(m, dg::BM) * div_up(n, w) * (int64_t)batch;
+      const int64_t slots = (w == 32 ? 4 : (w == 64 ? 3 : 2)) * (int64_t)nsm;
+      const double per_step = w == 32 ? 0.74 : (w == 64 ? 1.0 : 1.31);
+      for (int ks = 1; ks <= kmax; ++ks) {
+        const int64_t steps = div_up(ctas * ks, slots) * div_up(div_up(std::max(k, 1), ks), dg::BK);
+        const double cost = (double)steps * per_step * (ks > 1 ? 1.03 : 1.0);
+        if (best == 0.0 || cost < best) {
+          best = cost;
+          bn = w;
+          ksplit = ks;
+        }
       }
     }
+    const int tiles = (int)(div_up(m, dg::BM) * div_up(n, bn));
     int kchunk = (int)div_up(div_up(std::max(k, 1), ksplit), dg::BK) * dg::BK;
     ksplit = (int)div_up(std::max(k, 1), kchunk);
     if (batch * ksplit > 65535) throw Error{STD2G_EINVAL, "dgemm: batch too large"};
     double *wk = nullptr;
     if (ksplit > 1) wk = work.ensure((size_t)ksplit * batch * m * n);
     const dim3 grid(tiles, batch * ksplit);
-#define S2G_DGEMM(TA_, TB_)                                                                   \
+#define S2G_DGEMM(TA_, TB_, BN_)                                                              \
   do {                                                                                        \
-    S2G_CUDA(cudaFuncSetAttribute(k_dgemm<TA_, TB_>,                                          \
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize, dg::SMEM_BYTES)); \
-    S2G_LAUNCH((k_dgemm<TA_, TB_>), grid, dg::THREADS, dg::SMEM_BYTES, s, m, n, k, alpha, A,   \
-               lda, sA, B, ldb, sB, beta, C, ldc, sC, ksplit, kchunk, wk);                    \
+    S2G_CUDA(cudaFuncSetAttribute(k_dgemm<TA_, TB_, BN_>,                                     \
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize,                \
+                                  dg::smem_bytes<BN_>()));                                    \
+    S2G_LAUNCH((k_dgemm<TA_, TB_, BN_>), grid, dg::THREADS, dg::smem_bytes<BN_>(), s, m, n, k, \
+               alpha, A, lda, sA, B, ldb, sB, beta, C, ldc, sC, ksplit, kchunk, wk, tri);     \
   } while (0)
-    if (!ta && !tb) S2G_DGEMM(false, false);
-    else if (!ta && tb) S2G_DGEMM(false, true);
-    else if (ta && !tb) S2G_DGEMM(true, false);
-    else S2G_DGEMM(true, true);
+    if (bn == 32) {
+      if (!ta && !tb) S2G_DGEMM(false, false, 32);
+      else if (!ta && tb) S2G_DGEMM(false, true, 32);
+      else if (ta && !tb) S2G_DGEMM(true, false, 32);
+      else S2G_DGEMM(true, true, 32);
+    } else if (bn == 64) {
+      if (!ta && !tb) S2G_DGEMM(false, false, 64);
+      else if (!ta && tb) S2G_DGEMM(false, true, 64);
+      else if (ta && !tb) S2G_DGEMM(true, false, 64);
+      else S2G_DGEMM(true, true, 64);
+    } else {
+      if (!ta && !tb) S2G_DGEMM(false, false, 128);
+      else if (!ta && tb) S2G_DGEMM(false, true, 128);
+      else if (ta && !tb) S2G_DGEMM(true, false, 128);
+      else S2G_DGEMM(true, true, 128);
+    }
 #undef S2G_DGEMM
     ++launches;
     if (ksplit > 1) {

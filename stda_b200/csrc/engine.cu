@@ -931,22 +931,25 @@ static void solve(Ctx &c, const std2g_params &p_in, std2g_result *res, const Res
     // always the same (maximum) value, never a size of this molecule
     S2G_CUDA(cudaFuncSetAttribute(k_charges_tiled, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   227 * 1024));
-    auto tiled = [&](double *out, int p0, int np, int q0, int nq) {
+    auto tiled = [&](double *out, int p0, int np, int q0, int nq, int tri) {
       const dim3 g((unsigned)div_up(nq, kChTQ), (unsigned)div_up(np, kChTP),
                    (unsigned)div_up(N, kChAtoms));
       S2G_LAUNCH(k_charges_tiled, g, 256, shb, s, out, Clow, nao, N, aop, aol, p0, np, q0, nq,
-                 c.chunk_rows);
+                 c.chunk_rows, tri);
     };
-    tiled(Qia, 0, no, no, nv);
-    tiled(Qoo, 0, no, 0, no);
-    tiled(Qvv, no, nv, no, nv);
+    tiled(Qia, 0, no, no, nv, 0);
+    tiled(Qoo, 0, no, 0, no, 1);   // only q_ij, j <= i: it feeds P_oo alone
+    tiled(Qvv, no, nv, no, nv, 0);
   }
   // p = gamma q (ssymm, stda.f:558-590, 742-743)
   double *Pii = c.w_Pii.ensure((size_t)N * no), *uci = c.w_uci.ensure((size_t)nv * no);
   gemm(c, CUBLAS_OP_N, CUBLAS_OP_N, N, no, N, 1.0, gj, N, Qii, N, 0.0, Pii, N);
   gemm(c, CUBLAS_OP_T, CUBLAS_OP_N, nv, no, N, 1.0, Qaa, N, Pii, N, 0.0, uci, nv);
   gemm(c, CUBLAS_OP_N, CUBLAS_OP_N, N, (int)nov, N, 1.0, gk, N, Qia, N, 0.0, Pia, N);
-  gemm(c, CUBLAS_OP_N, CUBLAS_OP_N, N, no * no, N, 1.0, gj, N, Qoo, N, 0.0, Poo, N);
+  // P_oo is symmetric in (i, j): the product over the pairs j <= i, then the
+  // upper pairs mirrored
+  c.dg.run(s, false, false, N, no * no, N, 1.0, gj, N, 0, Qoo, N, 0, 0.0, Poo, N, 0, 1, no);
+  S2G_LAUNCH(k_mirror_pairs, grid_for((int64_t)no * no * N), 256, 0, s, Poo, N, no);
 
   // ---- diagonal + energy screen (stda.f:593-668) ----
   record(c, PH_SCREEN);

@@ -292,12 +292,14 @@ constexpr int kChTP = 8, kChTQ = 32, kChAtoms = 16;
 __global__ void __launch_bounds__(256)
 k_charges_tiled(double *__restrict__ out, const double *__restrict__ C, int nao, int N,
                 const int *__restrict__ ao_ptr, const int *__restrict__ ao_list, int p0, int np,
-                int q0, int nq, int max_rows) {
+                int q0, int nq, int max_rows, int tri) {
   extern __shared__ double sh[];
   double *cp = sh;                                 // [max_rows][kChTP]
   double *cq = cp + (size_t)max_rows * kChTP;      // [max_rows][kChTQ]
   double *st = cq + (size_t)max_rows * kChTQ;      // [256][kChAtoms + 1]
   const int pt = blockIdx.y * kChTP, qt = blockIdx.x * kChTQ;
+  // tri: a symmetric block (p, q over the same MOs) wanted for q <= p only
+  if (tri && qt > pt + kChTP - 1) return;
   const int pi = threadIdx.x / kChTQ, qi = threadIdx.x % kChTQ;
   constexpr int kCols = kChTP + kChTQ, kSt = kChAtoms + 1;
   {
@@ -331,6 +333,18 @@ k_charges_tiled(double *__restrict__ out, const double *__restrict__ C, int nao,
       const int p = pt + pl / kChTQ, q = qt + pl % kChTQ;
       if (p < np && q < nq) out[((int64_t)p * nq + q) * N + A0 + a] = st[pl * kSt + a];
     }
+  }
+}
+
+// P[:, (i, j)] = P[:, (j, i)] for j > i: the upper pairs of a symmetric pair
+// array [pair][atom] (pair (i, j) at column i n + j) from the lower ones
+__global__ void k_mirror_pairs(double *__restrict__ P, int N, int n) {
+  const int64_t total = (int64_t)n * n * N;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t col = t / N, A = t - col * N;
+    const int i = (int)(col / n), j = (int)(col - (int64_t)i * n);
+    if (j > i) P[t] = P[((int64_t)j * n + i) * N + A];
   }
 }
 
