@@ -98,6 +98,9 @@ typedef struct {
                         the mixed form from 4096 CSFs; the mixed form's inner
                         products use the tensor cores from 1.5e6 atoms x CSFs) */
   double conv_tol;   /* Davidson residual norm tolerance (0: 1e-6) */
+  double shftmax_somo; /* unrestricted K-shift path: extra shift of SOMO
+                          excitations, eV (somo_shift, sutda.f:2402-2422; the
+                          -xtb default 1.0, main.f:208) */
 } std2g_params;
 
 /* ---- results of one solve ---------------------------------------------- */
@@ -152,6 +155,18 @@ int std2g_load(void *ctx, int ncent, int nmo, int nao,
                const double *xyz, const double *C, const double *eps,
                const double *occ, const int *iaoat, const double *S,
                const double *mu_L, const double *mu_V, const double *mu_M);
+
+/* Mark the loaded wavefunction as unrestricted (UKS): csp[k] = 1 (alpha) or
+   2 (beta) for each of the nmo MOs, occupations 1 / 0 per spin MO, as the
+   reference passes csp to sutda (main.f:933, sutda.f:54).  std2g_solve then
+   runs UKS sTDA / sTD-DFT: per-spin windows, (ia|jb) between all CSFs and
+   (ij|ab) within a spin (ak = 1), ptselect_uks, the SOMO shift with the
+   K-shift, no spin factor in the properties.  The CSF list is the alpha block
+   then the beta block; std2g_get_csf indexes the window's occupied MOs as
+   [alpha, beta] and its virtual MOs likewise.  Response, beta and 2PA stay
+   restricted-only (STD2G_EINVAL).  A new std2g_load / std2g_load_prims
+   returns the context to restricted input. */
+int std2g_set_spins(void *ctx, const int *csp);
 
 /* AO one-electron integrals on the device from the primitive list the
    reference's readers fill (readbasmold.f:330-517, readxtb.f:150-160) and its

@@ -93,6 +93,7 @@ class Params:
     shftmax: float = 0.5
     shftwidth: float = 0.1
     shftsteep: float = 4.0
+    shftmax_somo: float = 1.0 # UKS: extra shift of SOMO excitations (main.f:208)
 
 
 @dataclass
@@ -971,3 +972,228 @@ def dominant_csfs(res: Result):
             oi[r, q] = res.iconf[j, 0] + 1
             oa[r, q] = res.iconf[j, 1] + res.no + 1
     return val, oi, oa
+
+
+def stda_uks(xyz4, C, eps, occ, csp, iaoat, S, Lao, Vao, Mao, p: Params, want_A=True):
+    """UKS sTDA / sTD-DFT in FP64, restating ``sutda`` (sutda.f:54-1788).
+
+    ``csp`` (nmo) is the spin of each MO (1 alpha, 2 beta).  Per spin: the
+    active window (sutda.f:178-360; occupied occ > 0.99 above
+    vmin - deps, virtual occ < 0.01 below omax + deps, both limits over all
+    MOs), Loewdin MOs, charges, the diagonal A(ia,ia) = de - (ii|aa) + (ia|ia)
+    (ak = 1, UCIS) with the K-shift and the SOMO shift (``somo_shift``,
+    sutda.f:2402-2422), primaries sorted by energy within their spin.
+    ``ptselect_uks`` (sutda.f:1822-2030): every candidate couples to the
+    primaries of its own spin by (ia|jb) - (ij|ab) and to those of the other
+    spin by (ia|jb) alone; selected alpha / beta candidates are appended to
+    their spin's list.  CSF order: alpha block, then beta block.  A
+    (``utdamat`` :2311-2399), A+B / A-B (``urpamat`` :2036-2305: cross-spin
+    blocks 2(ia|jb) and 0), properties without a spin factor, the velocity
+    correction (``utdacorr`` apbtrafo.f:645-750, ``apbtrafo_uks`` :318-574).
+
+    Result: ``iconf`` rows (i, a) index the spin's active occupied / virtual
+    MOs (0-based); ``extras['spin']`` (nci) gives 1 / 2 per CSF;
+    ``extras['no'], ['nv']`` the per-spin counts ((noa, nob), (nva, nvb)).
+    Active MOs of each spin are sorted occupied and virtual separately (as the
+    restricted oracle does, stda.f:333 note).
+    """
+    res = Result()
+    res.extras["uks"] = True
+    ncent = xyz4.shape[1]
+    thr = p.e_thr_ev / EH2EV_IN
+    fthr = p.fthr_ev / EH2EV_IN if p.fthr_ev < 1.79e308 else np.inf
+    Z = np.rint(xyz4[3]).astype(int)
+    res.xmolw = float(np.sum(AMS[Z - 1]))
+    csp = np.asarray(csp)
+    deps = 2.0 * (1.0 + 0.8 * p.ax) * thr
+    occm, virm = occ > 0.99, occ < 0.01
+    omax = eps[occm].max() if occm.any() else -1e42
+    vmin = eps[virm].min() if virm.any() else 1e42
+    othr, vthr = vmin - deps, deps + omax
+    nuhf = int(np.sum(occm & (csp == 1))) - int(np.sum(occm & (csp == 2)))
+    ak = 1.0
+    alpha_k, beta_j = default_alpha_beta(p)
+    gj, gk = gamma_matrices(xyz4, p.ax, alpha_k, beta_j)
+
+    spins = []
+    for s in (1, 2):
+        oidx = np.nonzero(occm & (csp == s) & (eps > othr))[0]
+        vidx = np.nonzero(virm & (csp == s) & (eps < vthr))[0]
+        oo = oidx[np.argsort(eps[oidx], kind="stable")]
+        vv = vidx[np.argsort(eps[vidx], kind="stable")]
+        no, nv = len(oo), len(vv)
+        Cact = C[:, np.concatenate([oo, vv])]
+        epsi = np.concatenate([eps[oo], eps[vv]])
+        Co, Cv = Cact[:, :no], Cact[:, no:]
+        mu = {name: np.stack([mo_ov(mat[d], Co, Cv) for d in range(3)])
+              for name, mat in (("L", Lao), ("V", Vao), ("M", Mao))}
+        Clow = lowdin_orthogonal_mos(S, Cact)
+        io_all, ia_all = np.meshgrid(np.arange(no), np.arange(nv), indexing="ij")
+        io_all, ia_all = io_all.ravel(), ia_all.ravel()
+        qii = charges(Clow, iaoat, ncent, np.arange(no), np.arange(no))
+        qaa = charges(Clow, iaoat, ncent, no + np.arange(nv), no + np.arange(nv))
+        uci = qaa.T @ (gj @ qii)
+        qia = charges_block(Clow, iaoat, ncent, np.arange(no), no + np.arange(nv))
+        pia = gk @ qia
+        ek = np.einsum("Ak,Ak->k", pia, qia)
+        de = (epsi[no + ia_all] - epsi[io_all]) - uci[ia_all, io_all] + ak * ek
+        if p.kshift:
+            sau = p.shftmax * 0.036749320
+            wau = p.shftwidth * 0.036749320
+            de = de + sau / (1.0 + (ek / wau) ** p.shftsteep)     # kshift_to_ediag
+            nsomo = no - nuhf if s == 1 else no + nuhf            # sutda.f:700, 785
+            io1, iv1 = io_all + 1, no + ia_all + 1                # 1-based within the spin
+            somo = (io1 > nsomo) | (iv1 <= nsomo)
+            sau2 = p.shftmax_somo * 0.036749320
+            wau2 = p.shftwidth * 0.036749320 * 5.0
+            de = np.where(somo, de + sau2 / (1.0 + (ek / wau2) ** p.shftsteep), de)
+        pk = np.nonzero(de <= thr)[0]
+        ck = np.nonzero((de > thr) & (de < fthr))[0]
+        pk = pk[np.argsort(de[pk], kind="stable")]
+        qoo = charges_block(Clow, iaoat, ncent, np.arange(no), np.arange(no)).reshape(ncent, no, no)
+        qvv = charges_block(Clow, iaoat, ncent, no + np.arange(nv),
+                            no + np.arange(nv)).reshape(ncent, nv, nv)
+        poo = (gj @ qoo.reshape(ncent, -1)).reshape(qoo.shape)
+        spins.append(dict(no=no, nv=nv, oo=oo, vv=vv, epsi=epsi, mu=mu, io=io_all, ia=ia_all,
+                          qia=qia, pia=pia, ek=ek, de=de, pk=pk, ck=ck, ed=de[pk].copy(),
+                          poo=poo, qvv=qvv))
+    A_, B_ = spins
+    if (A_["no"] == 0 or A_["nv"] == 0) and (B_["no"] == 0 or B_["nv"] == 0):
+        raise OracleError("no CSF, increase energy threshold (-e option)")
+    if len(A_["pk"]) + len(B_["pk"]) < 1:
+        raise OracleError("No CSF, increase energy threshold (-e option)")
+
+    def coupling(sr, kr, sc, kc):
+        """(ia|jb) - delta_{spin} (ij|ab) between CSFs kr of spin sr and kc of sc."""
+        R, Cc = spins[sr], spins[sc]
+        K = R["pia"][:, kr].T @ Cc["qia"][:, kc]
+        if sr != sc:
+            return ak * K
+        i1, a1, i2, a2 = R["io"][kr], R["ia"][kr], R["io"][kc], R["ia"][kc]
+        J = np.einsum("Auv,Auv->uv", R["poo"][:, i1[:, None], i2[None, :]],
+                      R["qvv"][:, a1[:, None], a2[None, :]])
+        return ak * K - J
+
+    # ptselect_uks: alpha candidates, then beta candidates
+    pt2 = [np.zeros(len(A_["pk"])), np.zeros(len(B_["pk"]))]
+    new = []
+    for s in (0, 1):
+        S_ = spins[s]
+        ck = S_["ck"]
+        incl = np.zeros(len(ck), dtype=bool)
+        for q, k in enumerate(ck):
+            pts = []
+            for t in (0, 1):
+                T_ = spins[t]
+                if len(T_["pk"]) == 0:
+                    pts.append(np.zeros(0))
+                    continue
+                amat = coupling(s, np.array([k]), t, T_["pk"])[0]
+                pts.append(amat ** 2 / (S_["de"][k] - T_["ed"] + 1e-10))
+            pert = pts[0].sum() + pts[1].sum()
+            if pert > p.thrp:
+                incl[q] = True
+            else:
+                pt2[0] += pts[0]
+                pt2[1] += pts[1]
+        new.append(ck[incl])
+    res.extras["nuhf"] = nuhf
+    blocks = []
+    for s in (0, 1):
+        S_ = spins[s]
+        ks = np.concatenate([S_["pk"], new[s]])
+        eds = np.concatenate([S_["ed"] - pt2[s], S_["de"][new[s]]])
+        blocks.append((ks, eds))
+    res.nex = len(A_["pk"]) + len(B_["pk"])
+    res.nexpt = len(A_["ck"]) + len(B_["ck"])
+    res.new = len(new[0]) + len(new[1])
+    (ka, eda), (kb, edb) = blocks
+    nexa, nexb = len(ka), len(kb)
+    nci = nexa + nexb
+    res.iconf = np.concatenate([np.stack([A_["io"][ka], A_["ia"][ka]], axis=1),
+                                np.stack([B_["io"][kb], B_["ia"][kb]], axis=1)]).astype(int)
+    res.ed = np.concatenate([eda, edb])
+    res.pt2 = np.concatenate([pt2[0], pt2[1]])
+    spin = np.concatenate([np.ones(nexa, dtype=int), np.full(nexb, 2)])
+    res.extras.update(spin=spin, no=(A_["no"], B_["no"]), nv=(A_["nv"], B_["nv"]),
+                      nexa=nexa, nexb=nexb)
+    res.no, res.nv = A_["no"] + B_["no"], A_["nv"] + B_["nv"]
+    if not want_A:
+        return res
+
+    # A (utdamat), blocks [alpha, beta]
+    sl = [slice(0, nexa), slice(nexa, nci)]
+    kk = [ka, kb]
+    A = np.zeros((nci, nci))
+    Kov = np.zeros((nci, nci))
+    Kx = np.zeros((nci, nci))
+    for s in (0, 1):
+        for t in (0, 1):
+            if len(kk[s]) == 0 or len(kk[t]) == 0:
+                continue
+            A[sl[s], sl[t]] = coupling(s, kk[s], t, kk[t])
+            Kov[sl[s], sl[t]] = spins[s]["pia"][:, kk[s]].T @ spins[t]["qia"][:, kk[t]]
+        S_ = spins[s]
+        if len(kk[s]):
+            # (ib|ja) within the spin (exchange type, rrpamat / utdacorr)
+            i1, a1 = S_["io"][kk[s]], S_["ia"][kk[s]]
+            nv_s = S_["nv"]
+            kib = i1[:, None] * nv_s + a1[None, :]
+            kja = i1[None, :] * nv_s + a1[:, None]
+            Kx[sl[s], sl[s]] = np.einsum("Auv,Auv->uv", S_["pia"][:, kib], S_["qia"][:, kja])
+    np.fill_diagonal(A, res.ed)
+    Kd = np.concatenate([A_["ek"][ka], B_["ek"][kb]])
+    mL = np.concatenate([A_["mu"]["L"][:, A_["io"][ka], A_["ia"][ka]],
+                         B_["mu"]["L"][:, B_["io"][kb], B_["ia"][kb]]], axis=1)
+    mV = np.concatenate([A_["mu"]["V"][:, A_["io"][ka], A_["ia"][ka]],
+                         B_["mu"]["V"][:, B_["io"][kb], B_["ia"][kb]]], axis=1)
+    mM = np.concatenate([A_["mu"]["M"][:, A_["io"][ka], A_["ia"][ka]],
+                         B_["mu"]["M"][:, B_["io"][kb], B_["ia"][kb]]], axis=1)
+    if p.rpa:
+        Apb = 2.0 * Kov - p.ax * Kx - (Kov - A)
+        Amb = p.ax * Kx - (Kov - A)
+        np.fill_diagonal(Apb, res.ed - p.ax * Kd + Kd)
+        np.fill_diagonal(Amb, res.ed - Kd + p.ax * Kd)
+        if abs(p.ax) < 1e-6:
+            Amb = np.diag(res.ed - Kd)
+        res.Apb, res.Amb = Apb, Amb
+        e, U = np.linalg.eigh(Amb)
+        if e[0] < 0:
+            raise OracleError("matrix power impossible")
+        Ambh = (U * np.sqrt(e)) @ U.T
+        w, Zv = sla.eigh(Ambh @ Apb @ Ambh, subset_by_value=(0.0, thr * thr))
+        if len(w) < 1:
+            raise OracleError("internal error in diag")
+        om = np.sqrt(w)
+        XpY = (Ambh @ Zv) / np.sqrt(om)
+        XmY = (Apb @ XpY) / om
+        X = 0.5 * (XpY + XmY)
+        res.omega, res.X, res.Y = om, X, XpY - X
+        uu, pp = XpY, XmY
+    else:
+        res.A = A
+        w, Xv = sla.eigh(A, subset_by_value=(0.0, thr))
+        if len(w) < 1:
+            raise OracleError("internal error in diag")
+        res.omega, res.X = w, Xv
+        uu = pp = Xv
+    om = res.omega
+    ef = 1.0 / (om + 1e-8)
+    tl, tv, tm = mL @ uu, mV @ pp, mM @ pp
+    res.fL = om * (2.0 / 3.0) * np.sum(tl * tl, axis=0)
+    res.fV = ef * (2.0 / 3.0) * np.sum(tv * tv, axis=0)
+    res.RL = ROT_FAC * np.sum(tl * tm, axis=0)
+    res.RV = ROT_FAC * np.sum(tv * tm, axis=0) * ef
+    res.alpha0 = 2.0 * np.array([np.sum(tl[0] * tl[0] * ef), np.sum(tl[0] * tl[1] * ef),
+                                 np.sum(tl[1] * tl[1] * ef), np.sum(tl[0] * tl[2] * ef),
+                                 np.sum(tl[1] * tl[2] * ef), np.sum(tl[2] * tl[2] * ef)])
+    if (not p.rpa) and p.velcorr:
+        Bh = 0.5 * Kov - 0.5 * p.ax * Kx
+        np.fill_diagonal(Bh, 0.5 * (Kd - p.ax * Kd))
+        Xn = (Bh @ res.X) * ef[None, :]
+        xl, xv, xm = mL @ res.X, mV @ res.X, mM @ res.X
+        xv2, xm2 = mV @ Xn, mM @ Xn
+        hilf = 1.0 - np.exp(-150.0 * om * om)
+        efmod = 1.0 / (om ** hilf + 1e-8)
+        res.RV = ROT_FAC * np.sum(xv * xm + xv2 * xm + xv * xm2, axis=0) * efmod
+    return res

@@ -63,6 +63,9 @@ struct Ctx {
   int maxa = 1;
   int chunk_rows = 1;   // largest AO count of kChAtoms consecutive atoms
   bool sqrtS_ready = false;
+  // unrestricted wavefunction (std2g_set_spins): spin of each MO, 1 alpha / 2 beta
+  bool uks = false;
+  std::vector<int> h_csp;
   int ns_iters = 0;            // Newton-Schulz steps of the last S^1/2
   DBuf<double> w_ns;           // its scale / error words
   // work buffers
@@ -326,6 +329,8 @@ static void load(Ctx &c, int ncent, int nmo, int nao, const double *xyz, const d
     S2G_LAUNCH(k_unpack, g, 256, 0, s, ao9 + nn * q, pk + npk * (1 + q), nao, q < 3 ? 0 : 1);
   S2G_CUDA(cudaStreamSynchronize(s));
   c.sqrtS_ready = false;
+  c.uks = false;
+  c.h_csp.clear();
   c.loaded = true;
 }
 
@@ -836,26 +841,68 @@ static void solve(Ctx &c, const std2g_params &p_in, std2g_result *res, const Res
   record(c, PH_SETUP);
   const double thr = p.e_thr_ev / kEh2eV_in;
   const double fthr = p.fthr_ev < 1.79e308 ? p.fthr_ev / kEh2eV_in : INFINITY;
-  const double ak = p.triplet ? 0.0 : 2.0;
+  if (c.uks) {
+    if (p.triplet) throw Error{STD2G_EINVAL, "unrestricted input: no triplet keyword (sutda)"};
+    if (resp || tpa)
+      throw Error{STD2G_EINVAL, "unrestricted input: response and 2PA are restricted-only"};
+  }
+  // UCIS scaling of (ia|jb): 1 unrestricted (sutda.f:625), 2 singlet, 0 triplet
+  const double ak = c.uks ? 1.0 : (p.triplet ? 0.0 : 2.0);
   const double beta_j = p.beta_j >= -99.0 ? p.beta_j : 0.20 + 1.830 * p.ax;
   const double alpha_k = p.alpha_k >= -99.0 ? p.alpha_k : 1.420 + 0.480 * p.ax;
   const bool want_quad = (resp && resp->quad) || (tpa && tpa->ntpa > 0);
 
   // ---- orbital window and energy sort (stda.f:145-192, 261-308, 333) ----
   const double deps = 2.0 * (1.0 + 0.8 * p.ax) * thr;
+  // occupation limits: closed shell 2 / 0; unrestricted 1 / 0 per spin MO
+  // (sutda.f:169-174: occ > 0.99, occ < 0.01)
+  const double occ_hi = c.uks ? 0.99 : 1.990;
   double omax = -1e42, vmin = 1e42;
   for (int i = 0; i < c.nmo; ++i) {
-    if (c.h_occ[i] > 1.990 && c.h_eps[i] > omax) omax = c.h_eps[i];
+    if (c.h_occ[i] > occ_hi && c.h_eps[i] > omax) omax = c.h_eps[i];
     if (c.h_occ[i] < 0.010 && c.h_eps[i] < vmin) vmin = c.h_eps[i];
   }
-  std::vector<int> oidx, vidx;
-  for (int i = 0; i < c.nmo; ++i) {
-    if (c.h_occ[i] > 1.990 && c.h_eps[i] > vmin - deps) oidx.push_back(i);
-    if (c.h_occ[i] < 0.010 && c.h_eps[i] < omax + deps) vidx.push_back(i);
-  }
   auto by_eps = [&](int a, int b) { return c.h_eps[a] < c.h_eps[b]; };
-  std::stable_sort(oidx.begin(), oidx.end(), by_eps);
-  std::stable_sort(vidx.begin(), vidx.end(), by_eps);
+  std::vector<int> oidx, vidx;
+  UksScreen us;
+  if (!c.uks) {
+    for (int i = 0; i < c.nmo; ++i) {
+      if (c.h_occ[i] > 1.990 && c.h_eps[i] > vmin - deps) oidx.push_back(i);
+      if (c.h_occ[i] < 0.010 && c.h_eps[i] < omax + deps) vidx.push_back(i);
+    }
+    std::stable_sort(oidx.begin(), oidx.end(), by_eps);
+    std::stable_sort(vidx.begin(), vidx.end(), by_eps);
+  } else {
+    // sutda.f:178-360: per spin, occupied then virtual, each sorted by energy;
+    // the window's occupied MOs are alpha then beta, its virtual ones alike
+    int nocc_a = 0, nocc_b = 0;
+    std::vector<int> o[2], v[2];
+    for (int i = 0; i < c.nmo; ++i) {
+      const int sp = c.h_csp[i] - 1;
+      if (c.h_occ[i] > 0.99) (sp == 0 ? nocc_a : nocc_b)++;
+      if (c.h_occ[i] > 0.99 && c.h_eps[i] > vmin - deps) o[sp].push_back(i);
+      if (c.h_occ[i] < 0.010 && c.h_eps[i] < omax + deps) v[sp].push_back(i);
+    }
+    for (int sp = 0; sp < 2; ++sp) {
+      std::stable_sort(o[sp].begin(), o[sp].end(), by_eps);
+      std::stable_sort(v[sp].begin(), v[sp].end(), by_eps);
+    }
+    oidx = o[0];
+    oidx.insert(oidx.end(), o[1].begin(), o[1].end());
+    vidx = v[0];
+    vidx.insert(vidx.end(), v[1].begin(), v[1].end());
+    const int nuhf = nocc_a - nocc_b;
+    us.uks = 1;
+    us.noa = (int)o[0].size();
+    us.nob = (int)o[1].size();
+    us.nva = (int)v[0].size();
+    us.nsomo_a = us.noa - nuhf;
+    us.nsomo_b = us.nob + nuhf;
+    us.sau2 = p.shftmax_somo * 0.036749320;
+    us.wau2 = p.shftwidth * 0.036749320 * 5.0;
+    if ((o[0].empty() || v[0].empty()) && (o[1].empty() || v[1].empty()))
+      throw Error{STD2G_ENOCSF, "no CSF, increase energy threshold"};
+  }
   const int no = (int)oidx.size(), nv = (int)vidx.size(), moci = no + nv;
   if (no == 0 || nv == 0) throw Error{STD2G_ENOCSF, "no CSF, increase energy threshold"};
   std::vector<int> act(oidx);
@@ -940,6 +987,14 @@ static void solve(Ctx &c, const std2g_params &p_in, std2g_result *res, const Res
     tiled(Qia, 0, no, no, nv, 0);
     tiled(Qoo, 0, no, 0, no, 1);   // only q_ij, j <= i: it feeds P_oo alone
     tiled(Qvv, no, nv, no, nv, 0);
+    if (c.uks) {
+      S2G_LAUNCH(k_zero_cross_spin, grid_for((int64_t)N * no * nv), 256, 0, s, Qia, N, no, nv,
+                 us.noa, us.nva);
+      S2G_LAUNCH(k_zero_cross_spin, grid_for((int64_t)N * no * no), 256, 0, s, Qoo, N, no, no,
+                 us.noa, us.noa);
+      S2G_LAUNCH(k_zero_cross_spin, grid_for((int64_t)N * nv * nv), 256, 0, s, Qvv, N, nv, nv,
+                 us.nva, us.nva);
+    }
   }
   // p = gamma q (ssymm, stda.f:558-590, 742-743)
   double *Pii = c.w_Pii.ensure((size_t)N * no), *uci = c.w_uci.ensure((size_t)nv * no);
@@ -957,7 +1012,7 @@ static void solve(Ctx &c, const std2g_params &p_in, std2g_result *res, const Res
   int *flag = c.w_flag.ensure(nov);
   S2G_LAUNCH(k_diag_screen, grid_for(nov * 32), 256, 0, s, Pia, Qia, N, no, nv,
              c.d_eps_act.get(), uci, ak, p.kshift, p.shftmax * 0.036749320,
-             p.shftwidth * 0.036749320, p.shftsteep, thr, fthr, de, ek, flag);
+             p.shftwidth * 0.036749320, p.shftsteep, thr, fthr, de, ek, flag, us);
   std::vector<int> h_flag(nov);
   int h_status[4];
   S2G_CUDA(cudaMemcpyAsync(h_flag.data(), flag, sizeof(int) * nov, cudaMemcpyDeviceToHost, s));
@@ -1128,11 +1183,6 @@ static void solve(Ctx &c, const std2g_params &p_in, std2g_result *res, const Res
   const int nci = nex + nnew;
   std::vector<int> allk(pk);
   allk.insert(allk.end(), newk.begin(), newk.end());
-  std::vector<int> ci(nci), ca(nci);
-  for (int u = 0; u < nci; ++u) {
-    ci[u] = allk[u] / nv;
-    ca[u] = allk[u] % nv;
-  }
   std::vector<double> ed_all(ed_lowered);
   if (nnew > 0) {
     int *d_new = c.w_tmpi.ensure(std::max<size_t>(2 * (size_t)nex, nnew));
@@ -1144,6 +1194,28 @@ static void solve(Ctx &c, const std2g_params &p_in, std2g_result *res, const Res
     S2G_CUDA(cudaMemcpyAsync(h_de.data(), d_denew, sizeof(double) * nnew, cudaMemcpyDeviceToHost, s));
     S2G_CUDA(cudaStreamSynchronize(s));
     ed_all.insert(ed_all.end(), h_de.begin(), h_de.end());
+  }
+  if (c.uks) {
+    // sutda's CSF order: alpha primaries (energy order), alpha PT-selected
+    // (candidate order), then the same for beta (ptselect_uks, sutda.f:1929-2007)
+    std::vector<int> order;
+    for (int sp = 0; sp < 2; ++sp)
+      for (int part = 0; part < 2; ++part)
+        for (int u = part ? nex : 0; u < (part ? nci : nex); ++u)
+          if ((allk[u] / nv < us.noa) == (sp == 0)) order.push_back(u);
+    std::vector<int> k2(nci);
+    std::vector<double> e2(nci);
+    for (int u = 0; u < nci; ++u) {
+      k2[u] = allk[order[u]];
+      e2[u] = ed_all[order[u]];
+    }
+    allk.swap(k2);
+    ed_all.swap(e2);
+  }
+  std::vector<int> ci(nci), ca(nci);
+  for (int u = 0; u < nci; ++u) {
+    ci[u] = allk[u] / nv;
+    ca[u] = allk[u] % nv;
   }
 
   // ---- A / A+-B build (rtdamat stda.f:2010-2056, rrpamat stda.f:1870-2004) ----
@@ -1555,7 +1627,7 @@ static void solve(Ctx &c, const std2g_params &p_in, std2g_result *res, const Res
   double *dom_c = c.w_domc.ensure((size_t)3 * nroot);
   int *dom_ia = c.w_domi.ensure((size_t)6 * nroot);
   S2G_LAUNCH(k_dominant_csfs, nroot, 256, 0, s, X, p.rpa ? Yv : (const double *)nullptr, nci,
-             d_ci, d_ca, no, dom_c, dom_ia, dom_ia + 3 * nroot);
+             d_ci, d_ca, no, dom_c, dom_ia, dom_ia + 3 * nroot, c.uks ? 0 : 1);
   record(c, PH_RESPONSE);
   record(c, PH_COUNT);
 
@@ -1747,6 +1819,17 @@ int std2g_load_prims(void *ctx, int ncent, int nmo, int nao, const double *xyz, 
     std2g::load(*c, ncent, nmo, nao, xyz, C, eps, occ, iaoat.data(), nullptr, nullptr, nullptr,
                 nullptr, pk);
   });
+}
+
+int std2g_set_spins(void *ctx, const int *csp) {
+  if (!ctx || !csp) return STD2G_EINVAL;
+  auto *c = (Ctx *)ctx;
+  if (!c->loaded) return STD2G_ESTATE;
+  for (int i = 0; i < c->nmo; ++i)
+    if (csp[i] != 1 && csp[i] != 2) return STD2G_EINVAL;
+  c->h_csp.assign(csp, csp + c->nmo);
+  c->uks = true;
+  return STD2G_OK;
 }
 
 int std2g_solve(void *ctx, const std2g_params *par, std2g_result *res) {

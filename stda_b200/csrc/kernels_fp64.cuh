@@ -117,15 +117,17 @@ __global__ void k_abs_max(const double *__restrict__ x, int64_t n,
 // ones already taken; the reported value is the coefficient c_j.  One block
 // per root, three block-wide arg-max passes.
 // sTD-DFT (Y given): u = X + Y, p = X - Y and the first pick follows the
-// reference's running comparison |u p| > umax with umax = u p (signed), the
-// second and third u p > umax; reported value X^2 - Y^2.  That comparison is
+// reference's running comparison |u p| > umax with umax = u p (signed; the
+// unrestricted table, sutda.f:1315-1335, compares u p without the absolute
+// value: first_abs = 0), the second and third u p > umax; reported value
+// X^2 - Y^2.  That comparison is
 // order dependent, so one thread of the block scans the CSFs in order.
 // out_i / out_a: occupied and virtual MO of the CSF (1-based, virtual
 // numbered after the no occupied MOs).
 __global__ void k_dominant_csfs(const double *__restrict__ X, const double *__restrict__ Y,
                                 int nci, const int *__restrict__ ci, const int *__restrict__ ca,
                                 int no, double *__restrict__ out_c, int *__restrict__ out_i,
-                                int *__restrict__ out_a) {
+                                int *__restrict__ out_a, int first_abs) {
   const int r = blockIdx.x;
   const double *x = X + (int64_t)r * nci;
   const double *y = Y ? Y + (int64_t)r * nci : nullptr;
@@ -138,7 +140,7 @@ __global__ void k_dominant_csfs(const double *__restrict__ X, const double *__re
       double um = -1.0;
       for (int j = 0; j < nci; ++j) {
         const double v = (x[j] + y[j]) * (x[j] - y[j]);
-        if (fabs(v) > um) { um = v; k0 = j; }
+        if ((first_abs ? fabs(v) : v) > um) { um = v; k0 = j; }
       }
       um = -1.0;
       for (int j = 0; j < nci; ++j) {
@@ -336,6 +338,21 @@ k_charges_tiled(double *__restrict__ out, const double *__restrict__ C, int nao,
   }
 }
 
+// Unrestricted: zero the charges of pairs (p, q) of mixed spin in a pair array
+// [pair][atom] (pair p nq + q; p < psplit and q < qsplit are alpha), so that
+// the Coulomb (ij|ab) and exchange (ib|ja) terms vanish between spins
+// (utdamat / urpamat, sutda.f:2036-2399)
+__global__ void k_zero_cross_spin(double *__restrict__ Q, int N, int np, int nq, int psplit,
+                                  int qsplit) {
+  const int64_t total = (int64_t)np * nq * N;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t col = t / N;
+    const int pp = (int)(col / nq), qq = (int)(col - (int64_t)pp * nq);
+    if ((pp < psplit) != (qq < qsplit)) Q[t] = 0.0;
+  }
+}
+
 // P[:, (i, j)] = P[:, (j, i)] for j > i: the upper pairs of a symmetric pair
 // array [pair][atom] (pair (i, j) at column i n + j) from the lower ones
 __global__ void k_mirror_pairs(double *__restrict__ P, int N, int n) {
@@ -356,12 +373,24 @@ inline size_t charges_tiled_smem(int max_rows) {
 //   ek = p_ia . q_ia,  de = (e_a - e_i) - (ii|aa) + ak*ek [+ kshift]
 //   flag = 1 primary (de <= thr), 2 PT candidate (thr < de < fthr), 0 neither
 // One warp per ia pair, fixed-order lane reduction (deterministic).
+// Unrestricted (sutda) layout of the active window: occupied = alpha (noa)
+// then beta, virtual = alpha (nva) then beta; pairs of mixed spin are no CSFs.
+// SOMO shift (somo_shift, sutda.f:2402-2422) of the K-shift path: for a pair
+// with 1-based in-spin indices io, iv (iv numbered after the spin's occupied
+// MOs), de += sau2 / (1 + (ek / wau2)^steep) when io > nsomo or iv <= nsomo,
+// nsomo = noa - nuhf (alpha) or nob + nuhf (beta).
+struct UksScreen {
+  int uks = 0;                 // 0: restricted
+  int noa = 0, nob = 0, nva = 0, nsomo_a = 0, nsomo_b = 0;
+  double sau2 = 0.0, wau2 = 1.0;
+};
+
 __global__ void k_diag_screen(const double *__restrict__ P, const double *__restrict__ Q, int N,
                               int no, int nv, const double *__restrict__ eps_act,
                               const double *__restrict__ uci, double ak, int kshift,
                               double sau, double wau, double steep, double thr, double fthr,
                               double *__restrict__ de_out, double *__restrict__ ek_out,
-                              int *__restrict__ flag) {
+                              int *__restrict__ flag, UksScreen us) {
   int64_t npair = (int64_t)no * nv;
   int lane = threadIdx.x & 31;
   int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
@@ -375,9 +404,20 @@ __global__ void k_diag_screen(const double *__restrict__ P, const double *__rest
       int i = (int)(k / nv), a = (int)(k - (int64_t)i * nv);
       double de = (eps_act[no + a] - eps_act[i]) - uci[a + (int64_t)nv * i] + ak * s;
       if (kshift) de += sau / (1.0 + pow(s / wau, steep));
+      bool csf = true;
+      if (us.uks) {
+        const bool ai = i < us.noa, aa = a < us.nva;
+        csf = ai == aa;
+        if (csf && kshift) {
+          const int io = ai ? i + 1 : i - us.noa + 1;
+          const int iv = ai ? us.noa + a + 1 : us.nob + (a - us.nva) + 1;
+          const int nsomo = ai ? us.nsomo_a : us.nsomo_b;
+          if (io > nsomo || iv <= nsomo) de += us.sau2 / (1.0 + pow(s / us.wau2, steep));
+        }
+      }
       de_out[k] = de;
       ek_out[k] = s;
-      flag[k] = (de <= thr) ? 1 : ((de > thr && de < fthr) ? 2 : 0);
+      flag[k] = !csf ? 0 : ((de <= thr) ? 1 : ((de > thr && de < fthr) ? 2 : 0));
     }
   }
 }

@@ -33,7 +33,7 @@ EXPORTS = [
     "std2g_destroy", "std2g_screen_noalloc", "std2g_server_create", "std2g_server_submit",
     "std2g_server_poll", "std2g_server_wait", "std2g_server_stats", "std2g_server_destroy",
     "std2g_symeig_check", "std2g_set_sm_limit", "std2g_hyperpolarizability", "std2g_two_photon",
-    "std2g_ao_integrals", "std2g_load_prims", "std2g_dgemm_check",
+    "std2g_ao_integrals", "std2g_load_prims", "std2g_dgemm_check", "std2g_set_spins",
 ]
 
 
@@ -58,7 +58,8 @@ class Params(C.Structure):
                 ("alpha_k", C.c_double), ("beta_j", C.c_double), ("fthr_ev", C.c_double),
                 ("triplet", C.c_int), ("rpa", C.c_int), ("velcorr", C.c_int), ("kshift", C.c_int),
                 ("shftmax", C.c_double), ("shftwidth", C.c_double), ("shftsteep", C.c_double),
-                ("nroots", C.c_int), ("solver", C.c_int), ("conv_tol", C.c_double)]
+                ("nroots", C.c_int), ("solver", C.c_int), ("conv_tol", C.c_double),
+                ("shftmax_somo", C.c_double)]
 
 
 class ServerOpts(C.Structure):
@@ -139,6 +140,7 @@ def library():
                                            dp, dp, dp, dp, dp, dp]
         lib.std2g_load_prims.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, dp, dp, dp, dp,
                                          C.c_int, ip, ip, ip, dp, dp]
+        lib.std2g_set_spins.argtypes = [C.c_void_p, C.POINTER(C.c_int)]
         lib.std2g_solve.argtypes = [C.c_void_p, C.POINTER(Params), C.POINTER(Result)]
         lib.std2g_polarizability.argtypes = [C.c_void_p, C.POINTER(Params), dp, C.c_int, dp, dp]
         lib.std2g_hyperpolarizability.argtypes = [C.c_void_p, C.POINTER(Params), dp, C.c_int, dp,
@@ -207,12 +209,13 @@ class Keywords:
     nroots: int = 0
     solver: int = 0
     conv_tol: float = 0.0
+    shftmax_somo: float = 1.0
 
     def to_c(self) -> Params:
         return Params(self.ax, self.e_thr_ev, self.thrp, self.alpha_k, self.beta_j, self.fthr_ev,
                       int(self.triplet), int(self.rpa), int(self.velcorr), int(self.kshift),
                       self.shftmax, self.shftwidth, self.shftsteep, int(self.nroots),
-                      int(self.solver), float(self.conv_tol))
+                      int(self.solver), float(self.conv_tol), float(self.shftmax_somo))
 
 
 @dataclass
@@ -401,6 +404,12 @@ class Engine:
                                          _dp(xyz4), _dp(Cf), _dp(eps), _dp(occ), pr.nprims,
                                          ip(pr.ipty), ip(pr.ipao), ip(pr.ipat), _dp(pr.exip),
                                          _dp(pr.cxip)))
+
+    def set_spins(self, csp):
+        """Mark the loaded wavefunction unrestricted: csp[k] = 1 (alpha) or 2
+        (beta) per MO (std2g_set_spins)."""
+        csp = np.ascontiguousarray(csp, dtype=np.int32)
+        _check(self.lib.std2g_set_spins(self.ctx, csp.ctypes.data_as(C.POINTER(C.c_int))))
 
     def solve(self, kw: Keywords, cap: int = 4096) -> Solution:
         """One solve; ``cap`` is the initial room for roots.  When the window

@@ -21,8 +21,10 @@ boundary takes exactly those arrays, so the reader fixes the same conventions:
 * MO coefficients omitted in the file (TeraChem prints non-zero ones only) are
   zero (``readbasmold.f:606-628``).
 
-Only the Cartesian closed-shell (RKS) case that the sTDA path consumes is
-supported; spherical and open-shell inputs raise ``ValueError``.
+Cartesian closed-shell (RKS) and open-shell (UKS) files are read: a file
+with ``Spin= Beta`` MOs sets ``Molecule.csp`` (1 alpha / 2 beta per MO), which
+the engine takes through ``std2g_set_spins`` (the reference dispatches such
+files to ``sutda``, ``main.f:933``).  Spherical inputs raise ``ValueError``.
 """
 from __future__ import annotations
 
@@ -93,6 +95,7 @@ class Molecule:
     eps: np.ndarray | None = None
     occ: np.ndarray | None = None
     title: str = ""
+    csp: np.ndarray | None = None  # spin of each MO (1 alpha, 2 beta); None: restricted
 
     @property
     def ncent(self) -> int:
@@ -204,7 +207,7 @@ def read_molden(path: str) -> Molecule:
 
     # [MO]
     im = find("[mo]")
-    eps, occ, cols = [], [], []
+    eps, occ, cols, spin = [], [], [], []
     cur = None
     i = im + 1
     while i < len(lines):
@@ -221,8 +224,8 @@ def read_molden(path: str) -> Molecule:
                 eps.append(_ffloat(val))
             elif k == "occup":
                 occ.append(_ffloat(val))
-            elif k == "spin" and val.lower().startswith("beta"):
-                raise ValueError("open-shell molden files are not supported")
+            elif k == "spin":
+                spin.append(2 if val.lower().startswith("beta") else 1)
         else:
             tok = s.split()
             if len(tok) == 2 and re.fullmatch(r"\d+", tok[0]):
@@ -237,6 +240,10 @@ def read_molden(path: str) -> Molecule:
     mol.occ = np.asarray(occ, dtype=np.float64)
     if mol.C.shape[1] != len(mol.eps) or len(mol.occ) != len(mol.eps):
         raise ValueError("inconsistent [MO] section")
+    if 2 in spin:
+        if len(spin) != len(mol.eps):
+            raise ValueError("inconsistent Spin= lines in the [MO] section")
+        mol.csp = np.asarray(spin, dtype=np.int32)
     return mol
 
 
@@ -266,7 +273,8 @@ def write_molden(mol: Molecule, path: str, title: str = "") -> None:
     for m in range(mol.C.shape[1]):
         out.append(" Sym=  1")
         out.append(f" Ene= {mol.eps[m]:.15e}")
-        out.append(" Spin= Alpha")
+        beta = mol.csp is not None and int(mol.csp[m]) == 2
+        out.append(" Spin= Beta" if beta else " Spin= Alpha")
         out.append(f" Occup= {mol.occ[m]:.6f}")
         col = mol.C[:, m]
         for k in range(mol.nao):

@@ -221,3 +221,24 @@ def random_molecule(natoms: int, seed: int, with_ints=False):
     ints = ao_integrals(mol)
     attach_mos(mol, nelec // 2, seed + 7, ints)
     return (mol, ints) if with_ints else mol
+
+
+def open_shell(mol: Molecule, n_alpha: int, n_beta: int, seed: int, ints=None):
+    """An unrestricted wavefunction on the molecule's basis: independent
+    S-orthonormal alpha and beta MO sets (C = S^-1/2 Q, Q Haar-random), sorted
+    uniform orbital energies, occupations 1 / 0 per spin MO.  Returns
+    (C [nao, 2 nao], eps, occ, csp) with the alpha MOs first (csp 1, 2)."""
+    rng = np.random.default_rng(seed)
+    S = (ints if ints is not None else ao_integrals(mol))[0]
+    e, U = np.linalg.eigh(S)
+    Sm12 = (U / np.sqrt(e)) @ U.T
+    n = mol.nao
+    Cs, epss, occs = [], [], []
+    for ne in (n_alpha, n_beta):
+        Cs.append(Sm12 @ haar_orthogonal(n, rng))
+        eo = np.sort(rng.uniform(-0.8, -0.2, ne))
+        ev = np.sort(rng.uniform(0.0, 0.6, n - ne))
+        epss.append(np.concatenate([eo, ev]))
+        occs.append(np.concatenate([np.ones(ne), np.zeros(n - ne)]))
+    csp = np.concatenate([np.ones(n, dtype=np.int32), np.full(n, 2, dtype=np.int32)])
+    return np.hstack(Cs), np.concatenate(epss), np.concatenate(occs), csp

@@ -17,7 +17,8 @@ that xtb4stda writes and std2 reads in ``readxtb0`` / ``readxtb``
 
 The primitive arrays are exactly what the engine's device integrals take
 (``std2g_load_prims``); the coefficients already carry every normalisation
-(``fnorm`` = 1 for xTB input, ``main.f:832-838``).
+(``fnorm`` = 1 for xTB input, ``main.f:832-838``).  Unrestricted files load as
+UKS (``std2g_set_spins``).
 
 ``-xtb`` sets ax = 0.5, alpha = 2.0, beta = 4.0 and switches the K-shift of
 the diagonal on with shftmax = 0.5 eV, shftwidth = 0.1 eV, shftsteep = 4.0
@@ -180,8 +181,16 @@ def from_molecule(mol) -> XtbWavefunction:
 
 
 def load_xtb(engine, wf: XtbWavefunction) -> None:
-    """Load a restricted xTB wavefunction; the AO integrals are formed on the
-    device from its primitive list (std2g_load_prims)."""
-    if wf.imethod != 1:
-        raise ValueError("wfn.xtb: unrestricted (UKS) input is not supported by this engine")
-    engine.load_prims(wf.xyz4(), wf.C, wf.eps, wf.occ, wf.prims)
+    """Load an xTB wavefunction; the AO integrals are formed on the device from
+    its primitive list (std2g_load_prims).  Unrestricted input (imethod 2) is
+    loaded as the alpha MOs followed by the beta MOs and marked with their
+    spins (std2g_set_spins), as ``main.f:729-738`` sets ``ccspin``."""
+    if wf.imethod == 1:
+        engine.load_prims(wf.xyz4(), wf.C, wf.eps, wf.occ, wf.prims)
+        return
+    nmo = wf.C.shape[-1]
+    C2 = np.hstack([wf.C[0], wf.C[1]])
+    engine.load_prims(wf.xyz4(), C2, np.concatenate([wf.eps[0], wf.eps[1]]),
+                      np.concatenate([wf.occ[0], wf.occ[1]]), wf.prims)
+    engine.set_spins(np.concatenate([np.ones(nmo, dtype=np.int32),
+                                     np.full(nmo, 2, dtype=np.int32)]))

@@ -74,7 +74,7 @@ def test_angstrom_sp_shells_and_sparse_coefficients(tmp_path):
     assert np.array_equal(a.eps, [-0.5, 0.3]) and np.array_equal(a.occ, [2.0, 0.0])
 
 
-def test_refuses_spherical_and_open_shell(tmp_path):
+def test_refuses_spherical_reads_open_shell(tmp_path):
     sph = tmp_path / "s.molden"
     sph.write_text(MINI.format(unit="AU", x=1.0, y=1.0).replace("[GTO]", "[5D]\n[GTO]"))
     with pytest.raises(ValueError, match="spherical"):
@@ -82,5 +82,23 @@ def test_refuses_spherical_and_open_shell(tmp_path):
     uhf = tmp_path / "u.molden"
     uhf.write_text(MINI.format(unit="AU", x=1.0, y=1.0).replace(
         " Ene= 0.3\n Spin= Alpha", " Ene= 0.3\n Spin= Beta"))
-    with pytest.raises(ValueError, match="open-shell"):
-        read_molden(str(uhf))
+    mol = read_molden(str(uhf))
+    assert mol.csp is not None and list(mol.csp).count(2) == 1
+
+
+def test_open_shell_molden_round_trip(tmp_path):
+    """Spin= Beta MOs give Molecule.csp (the reference sends such files to
+    sutda, main.f:933); a written open-shell file reads back unchanged."""
+    import copy
+    from stda_b200 import synth
+    from stda_b200.molden import read_molden, write_molden
+    mol = synth.random_molecule(8, seed=2)
+    C2, eps2, occ2, csp = synth.open_shell(mol, 9, 8, seed=3)
+    m = copy.deepcopy(mol)
+    m.C, m.eps, m.occ, m.csp = C2, eps2, occ2, csp
+    path = str(tmp_path / "uks.molden")
+    write_molden(m, path)
+    back = read_molden(path)
+    assert back.csp is not None and np.array_equal(back.csp, csp)
+    assert np.allclose(back.C, C2, atol=1e-13) and np.allclose(back.eps, eps2)
+    assert np.array_equal(back.occ, occ2)

@@ -92,3 +92,32 @@ def test_xtb_path_matches_oracle(tmp_path, precision):
     assert np.abs(sol.omega - ref.omega[:n]).max() < (1e-8 if precision == 0 else 4e-6)
     big = ref.fL[:n] > 1e-3
     assert np.allclose(sol.fL[big], ref.fL[:n][big], rtol=1e-4)
+
+
+@pytest.mark.gpu
+def test_xtb_unrestricted_path_matches_uks_oracle(tmp_path):
+    """An unrestricted wfn.xtb (imethod 2) goes through the device integrals
+    and the UKS path: the sutda restatement's CSFs and roots under -xtb."""
+    from oracle.stda_fp64 import Params, stda_uks
+    from stda_b200 import synth
+    from stda_b200.engine import Engine
+    from stda_b200.xtb import XtbWavefunction, load_xtb
+    mol, ints = synth.random_molecule(20, seed=14, with_ints=True)
+    nel = int(np.rint(np.sum(mol.occ)))
+    C2, eps2, occ2, csp = synth.open_shell(mol, nel // 2 + 1, nel // 2 - 1 + nel % 2, seed=15,
+                                           ints=ints)
+    n = mol.nao
+    base = from_molecule(mol)
+    wf = XtbWavefunction(2, base.atnam, base.xyz, base.Z, n, base.prims,
+                         np.stack([C2[:, :n], C2[:, n:]]), np.stack([eps2[:n], eps2[n:]]),
+                         np.stack([occ2[:n], occ2[n:]]))
+    p = str(tmp_path / "wfn.xtb")
+    write_wfn_xtb(p, wf)
+    kw = xtb_keywords(e_thr_ev=7.0, nroots=8, conv_tol=1e-9)
+    eng = Engine(0, 0)
+    load_xtb(eng, read_wfn_xtb(p))
+    sol = eng.solve(kw)
+    eng.close()
+    ref = stda_uks(mol.xyz4(), C2, eps2, occ2, csp, mol.iaoat(), *ints,
+                   Params(ax=0.5, e_thr_ev=7.0, alpha_k=2.0, beta_j=4.0, kshift=True))
+    assert np.abs(sol.omega - ref.omega[:len(sol.omega)]).max() < 1e-8
