@@ -13,12 +13,25 @@ steps of ``value`` reuse it and the ``e2e`` steps, which reload, include it.
   CUDA events on the engine's stream (max over ranks).
 * ``e2e``: the same through the C ABI with host buffers: every step copies the
   wavefunction and AO integrals host->device (std2g_load) and reads the
-  results back.
-* ``fp64_form``: the plain FP64 GPU form of the same solve (the denominator
-  of the mixed-vs-FP64 comparison) and the mixed form's deviation from it.
+  results back; ``e2e.device_integrals`` instead copies only the MOs and the
+  primitive list and forms S and the dipole integrals on the device
+  (std2g_load_prims).
+* ``fp64_form``: the plain FP64 GPU form of the same solve with its FP64
+  products on cuBLAS (the library baseline, the denominator of the
+  mixed-vs-FP64 comparison), the same form on the engine's own DMMA products,
+  and the mixed form's deviation from it (roots; f_L per degenerate level).
 * ``roofline``: the tensor-core contractions of the PT selection, algorithmic
   FLOPs (2 M N K with K = atoms) over their device time, against the measured
   dense 16-bit tensor peak.
+* ``roofline_fp64``: the engine's FP64 products in the FP64 form (every
+  product event-timed in one extra solve), against a cuBLAS DGEMM of an
+  8192^3 square measured in the same run; the same products on cuBLAS beside
+  it.
+* ``response``: alpha(w) of a 200-atom chain at 5 frequencies in the FP64
+  form (the reference's algorithm) and the mixed form with FP64 refinement.
+* ``served`` / ``batched``: the request server under Poisson arrivals (with
+  the saturation throughput at a p99 objective) and with a batch submitted at
+  once, both forms, with their deviation from each other.
 * ``cpu_baseline``: the CPU restatement of the reference algorithm (the
   reference's pair loops in C with real*4 dots, numpy for the rest, all host
   threads) on a bounded sample of the same solve, and the same estimator
@@ -248,6 +261,30 @@ def plain_fp64(pool, reqs, device):
     eng.close()
     return {"solves_per_s": len(reqs) / dt, "requests": len(reqs),
             "note": "sequential load + solve on one context, same molecules"}
+
+
+def cublas_dgemm_rate(device, n=8192, reps=5):
+    """cuBLAS FP64 GEMM throughput (TFLOP/s) on an n^3 square product, timed
+    with CUDA events after warm-up: the denominator of the FP64 roofline."""
+    import torch
+    dev = torch.device(f"cuda:{device}")
+    g = torch.Generator(device=dev).manual_seed(1)
+    a = torch.randn(n, n, dtype=torch.float64, device=dev, generator=g)
+    c = torch.randn(n, n, dtype=torch.float64, device=dev, generator=g)
+    for _ in range(2):
+        torch.matmul(a, c)
+    st = torch.cuda.current_stream(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize(dev)
+    e0.record(st)
+    for _ in range(reps):
+        torch.matmul(a, c)
+    e1.record(st)
+    e1.synchronize()
+    rate = 2.0 * n ** 3 * reps / (e0.elapsed_time(e1) / 1e3) / 1e12
+    del a, c
+    torch.cuda.empty_cache()
+    return rate
 
 
 def level_fL(omega, fL, gap=1e-5):
@@ -562,6 +599,13 @@ def main():
         own.load(b)
         own.solve(kw)
         l64_own = [own.solve(kw).ms for _ in range(2)]
+        # the FP64 products of one more solve of each, product by product
+        gst = {}
+        for name, e in (("own", own), ("cublas", e64)):
+            e.set_gemm_timing(True)
+            e.solve(kw)
+            gst[name] = e.gemm_stats()
+            e.set_gemm_timing(False)
         own.close()
         iconf_m, _ = eng.csf()
         iconf_d, _ = e64.csf()
@@ -582,6 +626,20 @@ def main():
             "fp64_products": "cuBLAS DGEMM (library baseline)",
             "own_dmma_products_ms": statistics.median(l64_own)}
         e64.close()
+        dpk = cublas_dgemm_rate(local)
+        ach64 = gst["own"]["flop"] / (gst["own"]["ms"] / 1e3) / 1e12
+        out["roofline_fp64"] = {
+            "bound": "tensor", "achieved": ach64, "peak": dpk, "unit": "TFLOP/s",
+            "frac": ach64 / dpk, "traffic": None,
+            "kernel": "k_dgemm (DMMA m8n8k4 FP64: Davidson / RR / response products, P_oo, "
+                      "Newton-Schulz) in the FP64 form",
+            "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (FP64 tensor cores)",
+            "calls_per_solve": gst["own"]["calls"], "flop_per_solve": gst["own"]["flop"],
+            "ms_per_solve": gst["own"]["ms"],
+            "same_products_cublas_tflops": gst["cublas"]["flop"] / (gst["cublas"]["ms"] / 1e3) / 1e12,
+            "same_products_cublas_ms": gst["cublas"]["ms"],
+            "note": "each product bracketed by an event pair (std2g_set_gemm_timing); "
+                    "FLOP = 2 m n k per product"}
 
     if rank == 0 and world == 1 and not args.no_serve:
         out.update(response_cfg2(local))

@@ -251,6 +251,15 @@ int64_t std2g_kernel_launches(void *ctx);
    (ms), number of launches and algorithmic FLOPs (used for the roofline). */
 int std2g_kernel_stats(void *ctx, double *ms, int64_t *launches, double *flop);
 
+/* FP64 matrix-product statistics of the last solve.  With timing on, every
+   product is bracketed by an event pair on its stream (off by default: the
+   events add a host call per product); std2g_gemm_stats returns the summed
+   device time of the timed products (0 with timing off), their number and
+   their algorithmic FLOPs 2 m n k.  The products of the load (the overlap's
+   square root) are not counted. */
+int std2g_set_gemm_timing(void *ctx, int on);
+int std2g_gemm_stats(void *ctx, double *ms, int64_t *calls, double *flop);
+
 /* Statistics of the last solve: Davidson iterations, sigma vectors formed
    with tensor-core (mixed) products and with FP64 products, and the number of
    PT candidates whose selection was re-decided in FP64 (mixed form). */

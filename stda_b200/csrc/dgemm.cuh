@@ -18,6 +18,8 @@
 
 #include <cublas_v2.h>
 
+#include <vector>
+
 #include "common.cuh"
 
 namespace std2g {
@@ -248,6 +250,39 @@ struct Dgemm {
   // set: the products go to cuBLAS on this handle instead (the library
   // baseline of the plain FP64 form, STD2G_FLAG_LIBRARY_FP64)
   cublasHandle_t lib = nullptr;
+  // per-product device time (an event pair around each product) and the
+  // algorithmic FLOPs 2 m n k of the products since the last reset()
+  bool timed = false;
+  std::vector<cudaEvent_t> ev;
+  size_t nev = 0;
+  double flop = 0;
+  int64_t calls = 0;
+  ~Dgemm() {
+    for (cudaEvent_t e : ev) cudaEventDestroy(e);
+  }
+  void reset() {
+    nev = 0;
+    flop = 0;
+    calls = 0;
+  }
+  // device time of the timed products since reset(); the stream must have
+  // passed them (the caller synchronises first)
+  double elapsed_ms() const {
+    double ms = 0;
+    for (size_t q = 0; q + 1 < nev; q += 2) {
+      float t = 0;
+      if (cudaEventElapsedTime(&t, ev[q], ev[q + 1]) == cudaSuccess) ms += t;
+    }
+    return ms;
+  }
+  void mark(cudaStream_t s) {
+    if (nev == ev.size()) {
+      cudaEvent_t e;
+      S2G_CUDA(cudaEventCreate(&e));
+      ev.push_back(e);
+    }
+    S2G_CUDA(cudaEventRecord(ev[nev++], s));
+  }
 
   // the argument order of cublasDgemm (alpha / beta by pointer, host values)
   void gemm(cudaStream_t s, cublasOperation_t ta, cublasOperation_t tb, int m, int n, int k,
@@ -263,6 +298,16 @@ struct Dgemm {
            double *C, int64_t ldc, int64_t sC, int batch = 1, int tri = 0) {
     if (m <= 0 || n <= 0 || batch <= 0) return;
     if (k < 0) throw Error{STD2G_EINVAL, "dgemm: negative k"};
+    flop += 2.0 * m * n * (double)k * batch;
+    ++calls;
+    if (timed) mark(s);
+    struct EndMark {
+      Dgemm &g;
+      cudaStream_t s;
+      ~EndMark() {
+        if (g.timed) g.mark(s);
+      }
+    } end_mark{*this, s};
     if (lib && tri == 0) {
       const cublasOperation_t oa = ta ? CUBLAS_OP_T : CUBLAS_OP_N, ob = tb ? CUBLAS_OP_T : CUBLAS_OP_N;
       S2G_CUBLAS(cublasSetStream(lib, s));

@@ -833,6 +833,8 @@ static void solve(Ctx &c, const std2g_params &p_in, std2g_result *res, const Res
   c.tc_ms = 0;
   c.tc_flop = 0;
   c.tc_launches = 0;
+  c.dg.reset();
+  c.mftc.side.dg.reset();
   c.mixed.rechecked = 0;
   c.mixed.ed_bound_max = 0.0;   // the FP64 PT path lowers the diagonal in FP64
   c.dav_iters = 0;
@@ -1962,6 +1964,26 @@ int std2g_kernel_stats(void *ctx, double *ms, int64_t *launches, double *flop) {
   if (launches) *launches = c->tc_launches;
   if (flop) *flop = c->tc_flop;
   return STD2G_OK;
+}
+
+int std2g_set_gemm_timing(void *ctx, int on) {
+  if (!ctx) return STD2G_EINVAL;
+  auto *c = (Ctx *)ctx;
+  c->dg.timed = on != 0;
+  c->mftc.side.dg.timed = on != 0;
+  return STD2G_OK;
+}
+
+int std2g_gemm_stats(void *ctx, double *ms, int64_t *calls, double *flop) {
+  if (!ctx) return STD2G_EINVAL;
+  auto *c = (Ctx *)ctx;
+  return guard([&] {
+    S2G_CUDA(cudaSetDevice(c->opts.device));
+    S2G_CUDA(cudaDeviceSynchronize());
+    if (ms) *ms = c->dg.elapsed_ms() + c->mftc.side.dg.elapsed_ms();
+    if (calls) *calls = c->dg.calls + c->mftc.side.dg.calls;
+    if (flop) *flop = c->dg.flop + c->mftc.side.dg.flop;
+  });
 }
 
 int std2g_solver_stats(void *ctx, int *iters, int64_t *matvecs, int64_t *matvecs_fp64,

@@ -34,6 +34,7 @@ EXPORTS = [
     "std2g_server_poll", "std2g_server_wait", "std2g_server_stats", "std2g_server_destroy",
     "std2g_symeig_check", "std2g_set_sm_limit", "std2g_hyperpolarizability", "std2g_two_photon",
     "std2g_ao_integrals", "std2g_load_prims", "std2g_dgemm_check", "std2g_set_spins",
+    "std2g_set_gemm_timing", "std2g_gemm_stats",
 ]
 
 
@@ -154,6 +155,8 @@ def library():
         lib.std2g_kernel_launches.argtypes = [C.c_void_p]
         lib.std2g_kernel_launches.restype = C.c_int64
         lib.std2g_kernel_stats.argtypes = [C.c_void_p, dp, C.POINTER(C.c_int64), dp]
+        lib.std2g_set_gemm_timing.argtypes = [C.c_void_p, C.c_int]
+        lib.std2g_gemm_stats.argtypes = [C.c_void_p, dp, C.POINTER(C.c_int64), dp]
         lib.std2g_solver_stats.argtypes = [C.c_void_p, ip, C.POINTER(C.c_int64),
                                             C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
         lib.std2g_server_create.argtypes = [C.POINTER(C.c_void_p), C.POINTER(ServerOpts)]
@@ -486,6 +489,17 @@ class Engine:
         n = C.c_int64()
         _check(self.lib.std2g_kernel_stats(self.ctx, C.byref(ms), C.byref(n), C.byref(fl)))
         return {"tc_ms": ms.value, "tc_launches": n.value, "tc_flop": fl.value}
+
+    def set_gemm_timing(self, on: bool) -> None:
+        """Bracket every FP64 product of later solves with an event pair."""
+        _check(self.lib.std2g_set_gemm_timing(self.ctx, int(bool(on))))
+
+    def gemm_stats(self):
+        """FP64 products of the last solve: device time (timing on), count, FLOPs."""
+        ms, fl = C.c_double(), C.c_double()
+        n = C.c_int64()
+        _check(self.lib.std2g_gemm_stats(self.ctx, C.byref(ms), C.byref(n), C.byref(fl)))
+        return {"ms": ms.value, "calls": n.value, "flop": fl.value}
 
     def solver_stats(self):
         it = C.c_int()

@@ -65,3 +65,33 @@ def test_dgemm_k0_beta0_batch_and_determinism():
     g2, _ = dgemm_check(A, B, Cm, ta=True)
     assert np.array_equal(g1, g2)
     assert np.abs(g1 - A.T @ B).max() < 1e-11
+
+
+def test_gemm_stats_own_and_library_count_the_same_products():
+    """std2g_gemm_stats: the FP64 products of a solve, counted with their
+    algorithmic FLOPs; event timing only when switched on; the library
+    baseline (cuBLAS) is counted the same way."""
+    from stda_b200 import synth
+    from stda_b200.engine import FLAG_LIBRARY_FP64, Engine, Keywords, boundary_inputs
+    mol, ints = synth.benzene(with_ints=True)
+    b = boundary_inputs(mol, ints)
+    kw = Keywords(ax=0.5, e_thr_ev=10.0, nroots=4)
+    st = {}
+    for name, flags in (("own", 0), ("lib", FLAG_LIBRARY_FP64)):
+        eng = Engine(0, 0, flags=flags)
+        eng.load(b)
+        eng.solve(kw)
+        off = eng.gemm_stats()
+        assert off["calls"] > 0 and off["flop"] > 0 and off["ms"] == 0.0
+        eng.set_gemm_timing(True)
+        eng.solve(kw)
+        st[name] = eng.gemm_stats()
+        assert st[name]["ms"] > 0.0
+        assert st[name]["calls"] == off["calls"] and st[name]["flop"] == off["flop"]
+        eng.set_gemm_timing(False)
+        eng.solve(kw)
+        assert eng.gemm_stats()["ms"] == 0.0
+        eng.close()
+    # the two forms may take a different number of Davidson iterations (their
+    # rounding differs), so only the setup products are compared loosely
+    assert abs(st["own"]["flop"] - st["lib"]["flop"]) <= 0.5 * st["own"]["flop"]
