@@ -255,8 +255,8 @@ int std2g_kernel_stats(void *ctx, double *ms, int64_t *launches, double *flop);
    product is bracketed by an event pair on its stream (off by default: the
    events add a host call per product); std2g_gemm_stats returns the summed
    device time of the timed products (0 with timing off), their number and
-   their algorithmic FLOPs 2 m n k.  The products of the load (the overlap's
-   square root) are not counted. */
+   their algorithmic FLOPs 2 m n k.  The first solve after a load also
+   counts the products of the overlap's square root (formed once per load). */
 int std2g_set_gemm_timing(void *ctx, int on);
 int std2g_gemm_stats(void *ctx, double *ms, int64_t *calls, double *flop);
 
@@ -354,9 +354,9 @@ int std2g_server_stats(void *srv, int64_t *stats);
 void std2g_server_destroy(void *srv);
 
 /* Cap the persistent tensor-core kernels of this context at max_sms CTAs (one
-   per SM; 0 = all SMs), so that several contexts sharing a device (the
-   request server's slots) leave SMs to each other's kernels.  No reference
-   counterpart. */
+   per SM; 0 = all SMs), and size the split-K of its FP64 products for that
+   many SMs, so that several contexts sharing a device (the request server's
+   slots) leave SMs to each other's kernels.  No reference counterpart. */
 int std2g_set_sm_limit(void *ctx, int max_sms);
 
 /* Diagnostic: the engine's FP64 matrix product (DMMA kernel with split-K,

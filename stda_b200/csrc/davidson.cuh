@@ -256,9 +256,9 @@ struct SectionClock {
 using MatVec = std::function<void(const double *V, int nb, double *W)>;
 
 // Rayleigh-Ritz problems up to this size go to the engine's own eigensolver
-// (symeig_small.cuh: 0.43 / 1.09 ms at m = 64 / 128 against 0.88 / 2.1 ms for
-// syevd); larger ones to cuSOLVER syevd.
-constexpr int kRRSmallMax = 128;
+// (symeig_small.cuh: 0.31 / 0.58 / 1.96 ms of kernel time at m = 64 / 120 /
+// 300 against 1.1 / 2.3 / 3.2 ms for syevd); larger ones to cuSOLVER syevd.
+constexpr int kRRSmallMax = kSymEigMaxN;
 
 // Orthonormalises the nc columns of T (n x nc) against the m orthonormal
 // columns of V and among themselves, and appends the result to V after column

@@ -57,6 +57,7 @@ struct Ctx {
   DBuf<double> w_Ares, w_Rres, w_part, w_rn, w_domc;   // dense residuals, dominant CSFs
   DBuf<int> w_domi;
   Dgemm dg;         // the engine's FP64 matrix products (dgemm.cuh)
+  int dev_sms = 148;   // SMs of the context's device
   // device inputs
   DBuf<double> d_xyz, d_C, d_eps_act, d_eta, d_Sfull, d_sqrtS, d_ao9;
   DBuf<int> d_ao_ptr, d_ao_list, d_iaoat, d_slot_ao;
@@ -1747,6 +1748,7 @@ int std2g_create(void **ctx, const std2g_opts *opts) {
     S2G_CUDA(cudaSetDevice(o.device));
     auto *c = new Ctx();
     c->opts = o;
+    c->dev_sms = prop.multiProcessorCount;
     c->dg.nsm = prop.multiProcessorCount;
     c->dav.dg = &c->dg;
     c->mf.dg = &c->dg;
@@ -1954,6 +1956,9 @@ int std2g_set_sm_limit(void *ctx, int max_sms) {
   auto *c = (std2g::Ctx *)ctx;
   c->mixed.tc.max_ctas = max_sms;
   c->mftc.tc.max_ctas = max_sms;
+  // the FP64 products size their split-K for the same share of the SMs
+  c->dg.nsm = max_sms > 0 ? std::min(max_sms, c->dev_sms) : c->dev_sms;
+  c->mftc.side.dg.nsm = c->dg.nsm;
   return STD2G_OK;
 }
 

@@ -1,15 +1,10 @@
 // Lowest k eigenpairs of a small dense symmetric matrix (n <= kSymEigMaxN),
-// for the Rayleigh-Ritz step of the Davidson solver, in three kernels with no
+// for the Rayleigh-Ritz step of the Davidson solver, in four kernels with no
 // host synchronisation:
 //   1. k_symeig_tridiag: Householder reduction to tridiagonal form
-//      T = Q^T A Q (LAPACK dsytd2, lower, restated) by a cluster of
-//      kClusterCtas CTAs.  CTA r holds the full columns j = r (mod
-//      kClusterCtas) in its shared memory; per reflector the owner of the
-//      column broadcasts v through distributed shared memory, every CTA forms
-//      its partial A v over its columns, the partials are summed in a fixed
-//      order by every CTA (so all hold the same p, w), and each CTA applies the
-//      rank-2 update to its own columns.  d, e, tau and the reflectors go to a
-//      global workspace;
+//      T = Q^T A Q (LAPACK dsytd2, lower, restated) by a cluster of 4 or 8
+//      CTAs with one cluster barrier per reflector (the scheme is described
+//      at the kernel); d, e, tau and the reflectors go to a global workspace;
 //   2. k_symeig_values (one warp per eigenvalue, any number of CTAs): bisection
 //      on Sturm counts (LAPACK dstebz's principle), each lane evaluating the
 //      count at one of 32 points of the current interval per round;
@@ -19,8 +14,10 @@
 //      modified Gram-Schmidt against the earlier members of the cluster, three
 //      iterations from a fixed start vector; the cluster threshold is
 //      1e-5 ||T||, tighter than dstein's 1e-3, so that the dense Rayleigh-Ritz
-//      spectra do not collapse into one serial cluster), then the
-//      back-transformation z = Q y by the stored reflectors.
+//      spectra do not collapse into one serial cluster), vectors in T's basis;
+//   4. k_symeig_backtransform (one warp per eigenvector, held in registers):
+//      z = Q y with the reflectors staged through shared memory in blocks
+//      that all warps of the CTA apply.
 // cuSOLVER's syevd takes 1-3 ms at n = 75-300, most of it launch and host
 // synchronisation latency.
 // Eigenvalues ascending in w[0..k), eigenvectors in the columns of Z (ld ldz).
@@ -34,16 +31,8 @@
 
 namespace std2g {
 
-constexpr int kClusterCtas = 4;        // CTAs of the tridiagonal reduction
 constexpr int kTridiagThreads = 512;
-constexpr int kSymEigMaxN = 320;       // full columns of n/4 per CTA within 227 KB
-
-// shared memory of one CTA of k_symeig_tridiag: its columns, v, partial p,
-// p / w, reduction scratch
-__host__ __device__ inline size_t symeig_smem_bytes(int n) {
-  const size_t ncol = (size_t)(n + kClusterCtas - 1) / kClusterCtas;
-  return sizeof(double) * (ncol * n + 3 * (size_t)n + 64);
-}
+constexpr int kSymEigMaxN = 320;       // full columns of n/8 per CTA, 119 KB
 
 // global workspace (doubles): packed reflectors, d, e, tau, 8 spare, and per
 // eigenvector its final y in T's basis (n)
@@ -114,111 +103,149 @@ struct SymEigWork {
 };
 
 // ---- 1. tridiagonal reduction (Q^T A Q = T, Q = H_0 ... H_{n-3}) ----------
-// A: lower triangle read (lda).  Every CTA of the cluster takes the same
-// number of cluster barriers (the decisions depend on data all CTAs share).
-__global__ void __cluster_dims__(kClusterCtas, 1, 1) __launch_bounds__(kTridiagThreads, 1)
+// A cluster of C CTAs; CTA r holds the full columns j = r (mod C) in shared
+// memory, and every CTA also keeps the current column c (cur) and forms the
+// reflector of step c from it itself, with the same arithmetic in every CTA,
+// so that a step takes one cluster barrier:
+//   phase 1: each CTA forms p_j = tau (A v)_j for its own columns j > c as the
+//            dot product of column j with v (A is symmetric), and the owner of
+//            column c+1 publishes that column;
+//   barrier;
+//   phase 2: each CTA gathers p and column c+1 from the owners (distributed
+//            shared memory), forms w = p - (tau p^T v / 2) v, applies the
+//            rank-2 update A -= v w^T + w v^T to its own columns and to its copy
+//            of column c+1, and forms the next reflector from that copy.
+// The published p pieces and columns alternate between two buffers: a CTA
+// that writes buffer (c+1) % 2 has passed the barrier of step c, so every CTA
+// has finished reading that buffer at step c-1.  Every CTA takes the same
+// barriers (all decisions depend on data the CTAs hold identically).
+__host__ __device__ inline int symeig_cluster_ctas(int n) { return n <= 96 ? 4 : 8; }
+
+__host__ __device__ inline size_t symeig_smem_bytes(int n, int C) {
+  const size_t ncol = (size_t)(n + C - 1) / C;
+  // own columns, v, p, w, cur, published p pieces [2][ncol], published column
+  // [2][n], reduction scratch
+  return sizeof(double) * (ncol * n + 4 * (size_t)n + 2 * ncol + 2 * (size_t)n + 64);
+}
+
+// reflector H_c = I - tau v v^T of the current column c (cur, rows c+1..n-1;
+// LAPACK dlarfg's convention: v[c+1] = 1, beta = -sign(alpha) ||x||);
+// the writer CTA stores v, tau, beta = e[c] and d[c] = cur[c]
+__device__ double symeig_reflector(const double *cur, int c, int n, double *v, double *red,
+                                   const SymEigWork &g, bool writer) {
+  const int r0 = c + 1, tid = threadIdx.x, nt = blockDim.x;
+  const double alpha = cur[r0];
+  double s = 0.0;
+  for (int i = r0 + 1 + tid; i < n; i += nt) s += cur[i] * cur[i];
+  const double xn2 = symeig_block_sum(s, red);
+  double tc = 0.0, beta = alpha, scal = 0.0;
+  if (xn2 != 0.0) {
+    beta = -copysign(sqrt(alpha * alpha + xn2), alpha);
+    tc = (beta - alpha) / beta;
+    scal = 1.0 / (alpha - beta);
+  }
+  for (int i = r0 + tid; i < n; i += nt) {
+    const double vi = i == r0 ? 1.0 : cur[i] * scal;
+    v[i] = vi;
+    if (writer && i > r0) g.ap[pk_idx(i, c, n)] = vi;   // kept for the back-transformation
+  }
+  if (writer && tid == 0) {
+    g.tau[c] = tc;
+    g.e[c] = beta;
+    g.d[c] = cur[c];
+  }
+  __syncthreads();
+  return tc;
+}
+
+template <int C>
+__global__ void __cluster_dims__(C, 1, 1) __launch_bounds__(kTridiagThreads, 1)
 k_symeig_tridiag(const double *__restrict__ A, int lda, int n, double *__restrict__ work) {
   namespace cg = cooperative_groups;
   cg::cluster_group cl = cg::this_cluster();
   const int rank = (int)cl.block_rank();
   extern __shared__ double sm[];
-  const int ncol = (n + kClusterCtas - 1) / kClusterCtas;   // local columns j = rank + CL*lj
-  double *Aloc = sm;                                        // [lj * n + i]
-  double *v = Aloc + (size_t)ncol * n;                      // reflector, rows r0..n-1
-  double *pp = v + n;                                       // this CTA's partial A v
-  double *pw = pp + n;                                      // p, then w
-  double *red = pw + n;                                     // [0..31] sums, [32..] scalars
-  const int tid = threadIdx.x, nt = blockDim.x;
+  const int ncol = (n + C - 1) / C;   // local columns j = rank + C * lj
+  double *Aloc = sm;                  // [lj * n + i]
+  double *v = Aloc + (size_t)ncol * n, *p = v + n, *w = p + n, *cur = w + n;
+  double *pubp = cur + n;             // [2][ncol]
+  double *pubc = pubp + 2 * ncol;     // [2][n]
+  double *red = pubc + 2 * n;         // [64]
+  const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5;
+  const int nw = nt >> 5;
+  const bool writer = rank == 0;
   SymEigWork g(work, n);
   for (int lj = 0; lj < ncol; ++lj) {
-    const int j = rank + kClusterCtas * lj;
+    const int j = rank + C * lj;
     if (j >= n) break;
     for (int i = tid; i < n; i += nt)
       Aloc[(size_t)lj * n + i] = i >= j ? A[i + (size_t)lda * j] : A[j + (size_t)lda * i];
   }
+  for (int i = tid; i < n; i += nt) cur[i] = A[i];   // column 0
   __syncthreads();
+  double tc = n >= 3 ? symeig_reflector(cur, 0, n, v, red, g, writer) : 0.0;
   for (int c = 0; c + 2 < n; ++c) {
-    const int r0 = c + 1, owner = c % kClusterCtas;
-    if (rank == owner) {
-      const double *col = Aloc + (size_t)(c / kClusterCtas) * n;
-      const double alpha = col[r0];
-      double s = 0.0;
-      for (int i = r0 + 1 + tid; i < n; i += nt) s += col[i] * col[i];
-      const double xn2 = symeig_block_sum(s, red);
-      double tc = 0.0, beta = alpha, scal = 0.0;
-      if (xn2 != 0.0) {
-        beta = -copysign(sqrt(alpha * alpha + xn2), alpha);
-        tc = (beta - alpha) / beta;
-        scal = 1.0 / (alpha - beta);
-      }
-      for (int i = r0 + tid; i < n; i += nt) {
-        const double vi = i == r0 ? 1.0 : col[i] * scal;
-        v[i] = vi;
-        if (i > r0) g.ap[pk_idx(i, c, n)] = vi;   // kept for the back-transformation
-      }
-      if (tid == 0) {
-        red[32] = tc;
-        g.tau[c] = tc;
-        g.e[c] = beta;
-        g.d[c] = col[c];
-      }
-    }
-    cl.sync();   // the owner's v and tau are ready
-    if (rank != owner) {
-      const double *rv = cl.map_shared_rank(v, owner);
-      const double *rr = cl.map_shared_rank(red, owner);
-      for (int i = r0 + tid; i < n; i += nt) v[i] = rv[i];
-      if (tid == 0) red[32] = rr[32];
-    }
-    __syncthreads();
-    const double tc = red[32];
+    const int r0 = c + 1, nxt = c + 1, own_nxt = nxt % C, buf = c & 1;
+    // first local column with j >= r0
+    const int lj0 = r0 > rank ? (r0 - rank + C - 1) / C : 0;
+    // ---- phase 1
     if (tc != 0.0) {
-      // partial p over this CTA's columns j >= r0, rows i >= r0
-      for (int i = r0 + tid; i < n; i += nt) {
-        double acc = 0.0;
-        for (int lj = 0; lj < ncol; ++lj) {
-          const int j = rank + kClusterCtas * lj;
-          if (j >= r0 && j < n) acc += Aloc[(size_t)lj * n + i] * v[j];
-        }
-        pp[i] = acc;
+      for (int lj = lj0 + warp; lj < ncol; lj += nw) {
+        const int j = rank + C * lj;
+        if (j >= n) break;
+        const double *col = Aloc + (size_t)lj * n;
+        double sdot = 0.0;
+        for (int i = r0 + lane; i < n; i += 32) sdot += col[i] * v[i];
+        for (int o = 16; o > 0; o >>= 1) sdot += __shfl_xor_sync(0xffffffffu, sdot, o);
+        if (lane == 0) pubp[buf * ncol + lj] = tc * sdot;
       }
     }
-    cl.sync();   // every partial is ready
-    if (tc != 0.0) {
-      const double *rp[kClusterCtas];
-#pragma unroll
-      for (int r = 0; r < kClusterCtas; ++r) rp[r] = cl.map_shared_rank(pp, r);
-      double pv = 0.0;
-      for (int i = r0 + tid; i < n; i += nt) {
-        double s = 0.0;
-#pragma unroll
-        for (int r = 0; r < kClusterCtas; ++r) s += rp[r][i];   // fixed order in every CTA
-        const double p = tc * s;
-        pw[i] = p;
-        pv += p * v[i];
+    if (rank == own_nxt) {
+      const double *col = Aloc + (size_t)(nxt / C) * n;
+      for (int i = r0 + tid; i < n; i += nt) pubc[buf * n + i] = col[i];
+    }
+    cl.sync();
+    // ---- phase 2
+    const double *rc = cl.map_shared_rank(pubc + buf * n, own_nxt);
+    double pv = 0.0;
+    for (int i = r0 + tid; i < n; i += nt) {
+      cur[i] = rc[i];
+      if (tc != 0.0) {
+        const double *rp = cl.map_shared_rank(pubp + buf * ncol, i % C);
+        const double pi = rp[i / C];
+        p[i] = pi;
+        pv += pi * v[i];
       }
-      const double K = 0.5 * tc * symeig_block_sum(pv, red);
-      for (int i = r0 + tid; i < n; i += nt) pw[i] -= K * v[i];   // w
+    }
+    if (tc != 0.0) {
+      const double K = 0.5 * tc * symeig_block_sum(pv, red);   // same value in every CTA
+      for (int i = r0 + tid; i < n; i += nt) w[i] = p[i] - K * v[i];
       __syncthreads();
-      // A22 -= v w^T + w v^T on this CTA's columns (full columns, rows >= r0)
-      for (int lj = 0; lj < ncol; ++lj) {
-        const int j = rank + kClusterCtas * lj;
-        if (j < r0 || j >= n) continue;
-        const double vj = v[j], wj = pw[j];
+      const double vn = v[nxt], wn = w[nxt];
+      for (int i = r0 + tid; i < n; i += nt) cur[i] -= v[i] * wn + w[i] * vn;
+      for (int lj = lj0 + warp; lj < ncol; lj += nw) {
+        const int j = rank + C * lj;
+        if (j >= n) break;
+        const double vj = v[j], wj = w[j];
         double *col = Aloc + (size_t)lj * n;
-        for (int i = r0 + tid; i < n; i += nt) col[i] -= v[i] * wj + pw[i] * vj;
+        for (int i = r0 + lane; i < n; i += 32) col[i] -= v[i] * wj + w[i] * vj;
       }
     }
     __syncthreads();
+    if (c + 3 < n) tc = symeig_reflector(cur, nxt, n, v, red, g, writer);
   }
-  // last two diagonal elements and the last off-diagonal one
-  for (int c = (n >= 2 ? n - 2 : 0); c < n; ++c) {
-    if (c % kClusterCtas != rank || tid != 0) continue;
-    const double *col = Aloc + (size_t)(c / kClusterCtas) * n;
-    g.d[c] = col[c];
-    g.tau[c] = 0.0;
-    if (c + 1 < n) g.e[c] = col[c + 1];
-    else g.e[c] = 0.0;
+  // the trailing 2 x 2 block: cur holds column n-2, column n-1 is on its owner
+  if (writer && tid == 0) {
+    if (n >= 2) {
+      g.d[n - 2] = cur[n - 2];
+      g.e[n - 2] = cur[n - 1];
+      g.tau[n - 2] = 0.0;
+    }
+  }
+  if (rank == (n - 1) % C && tid == 0) {
+    g.d[n - 1] = Aloc[(size_t)((n - 1) / C) * n + (n - 1)];
+    g.e[n - 1] = 0.0;
+    g.tau[n - 1] = 0.0;
   }
   cl.sync();   // no CTA leaves while others may still read its shared memory
 }
@@ -257,7 +284,7 @@ k_symeig_values(int n, int k, const double *__restrict__ work, double *__restric
   if (lane == 0) w[j] = 0.5 * (a + b);
 }
 
-// ---- 3. eigenvectors of T and back-transformation, one warp per cluster ----
+// ---- 3. eigenvectors of T, one warp per cluster of close eigenvalues --------
 // Cluster threshold: eigenvalues closer than 1e-5 ||T|| are orthogonalised
 // against each other; further apart, inverse iteration alone gives vectors
 // orthogonal to ~eps ||T|| / gap <= 2e-11.  Shared memory: d, e, then per
@@ -267,8 +294,7 @@ __host__ __device__ inline size_t symeig_vec_smem_bytes(int n) {
 }
 
 __global__ void __launch_bounds__(kSymEigWarps * 32)
-k_symeig_vectors(int n, int k, double *__restrict__ work, const double *__restrict__ w,
-                 double *__restrict__ Z, int ldz, int *info) {
+k_symeig_vectors(int n, int k, double *__restrict__ work, const double *__restrict__ w) {
   extern __shared__ double sm[];
   double *d = sm, *e = sm + n;
   const SymEigWork g(work, n);
@@ -365,32 +391,75 @@ k_symeig_vectors(int n, int k, double *__restrict__ work, const double *__restri
     for (int i = lane; i < n; i += 32) g.vec[(size_t)m * n + i] = y[i];
     __syncwarp();
   }
-  // back-transformation z = H_0 ... H_{n-3} y of every member, written to Z
-  for (int m = j0; m < j1; ++m) {
-    double *z = y;
-    for (int i = lane; i < n; i += 32) z[i] = g.vec[(size_t)m * n + i];
-    __syncwarp();
-    for (int c = n - 3; c >= 0; --c) {
-      const double tc = g.tau[c];
+}
+
+// ---- 4. back-transformation z = H_0 ... H_{n-3} y ----------------------------
+constexpr int kBtBlock = 16;                        // reflectors staged per round
+constexpr int kBtPerLane = (kSymEigMaxN + 31) / 32;  // vector elements per lane
+
+__host__ __device__ inline size_t symeig_bt_smem_bytes(int n) {
+  return sizeof(double) * ((size_t)kBtBlock * n + kBtBlock);
+}
+
+__global__ void __launch_bounds__(kSymEigWarps * 32)
+k_symeig_backtransform(int n, int k, const double *__restrict__ work,
+                       const double *__restrict__ w, double *__restrict__ Z, int ldz,
+                       int *info) {
+  extern __shared__ double sm[];
+  double *R = sm;                      // [kBtBlock][n]: v of H_c, zero above row c+1
+  double *tt = sm + (size_t)kBtBlock * n;
+  const SymEigWork g(const_cast<double *>(work), n);
+  const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
+  const int m = blockIdx.x * kSymEigWarps + wl;
+  const bool live = m < k;
+  double y[kBtPerLane];
+#pragma unroll
+  for (int t = 0; t < kBtPerLane; ++t) {
+    const int i = lane + 32 * t;
+    y[t] = live && i < n ? g.vec[(size_t)m * n + i] : 0.0;
+  }
+  // H_{n-3} first, H_0 last
+  for (int c1 = n - 3; c1 >= 0; c1 -= kBtBlock) {
+    const int nr = min(kBtBlock, c1 + 1);   // reflectors c1, c1-1, ..., c1-nr+1
+    __syncthreads();
+    for (int e = threadIdx.x; e < nr * n; e += blockDim.x) {
+      const int r = e / n, i = e - r * n, c = c1 - r;
+      R[e] = i <= c ? 0.0 : (i == c + 1 ? 1.0 : g.ap[pk_idx(i, c, n)]);
+    }
+    for (int r = threadIdx.x; r < nr; r += blockDim.x) tt[r] = g.tau[c1 - r];
+    __syncthreads();
+    if (!live) continue;
+    for (int r = 0; r < nr; ++r) {
+      const double tc = tt[r];
       if (tc == 0.0) continue;
-      const double *vc = g.ap + pk_idx(c + 1, c, n);   // v[c+1..n-1], v[c+1] = 1 implied
+      const double *vr = R + (size_t)r * n;
       double dot = 0.0;
-      for (int i = c + 1 + lane; i < n; i += 32) dot += (i == c + 1 ? 1.0 : vc[i - c - 1]) * z[i];
+#pragma unroll
+      for (int t = 0; t < kBtPerLane; ++t) {
+        const int i = lane + 32 * t;
+        if (i < n) dot += vr[i] * y[t];
+      }
       for (int o = 16; o > 0; o >>= 1) dot += __shfl_xor_sync(0xffffffffu, dot, o);
       const double f = tc * dot;
-      for (int i = c + 1 + lane; i < n; i += 32) z[i] -= f * (i == c + 1 ? 1.0 : vc[i - c - 1]);
-      __syncwarp();
+#pragma unroll
+      for (int t = 0; t < kBtPerLane; ++t) {
+        const int i = lane + 32 * t;
+        if (i < n) y[t] -= f * vr[i];
+      }
     }
-    bool bad = false;
-    for (int i = lane; i < n; i += 32) {
-      const double zi = z[i];
-      bad |= !isfinite(zi);
-      Z[i + (size_t)ldz * m] = zi;
-    }
-    if (lane == 0) bad |= !isfinite(w[m]);
-    if (__any_sync(0xffffffffu, bad) && lane == 0) atomicExch(info, 1);
-    __syncwarp();
   }
+  if (!live) return;
+  bool bad = false;
+#pragma unroll
+  for (int t = 0; t < kBtPerLane; ++t) {
+    const int i = lane + 32 * t;
+    if (i < n) {
+      bad |= !isfinite(y[t]);
+      Z[i + (size_t)ldz * m] = y[t];
+    }
+  }
+  if (lane == 0) bad |= !isfinite(w[m]);
+  if (__any_sync(0xffffffffu, bad) && lane == 0) atomicExch(info, 1);
 }
 
 // host launcher: n <= kSymEigMaxN, k <= n; work: symeig_work_doubles(n, k)
@@ -398,16 +467,24 @@ inline void symeig_small(cudaStream_t s, const double *A, int lda, int n, int k,
                          double *Z, int ldz, double *work, int *info) {
   if (n < 1 || n > kSymEigMaxN || k < 1 || k > n)
     throw Error{STD2G_EINVAL, "symeig_small: size out of range"};
-  S2G_CUDA(cudaFuncSetAttribute(k_symeig_tridiag, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)symeig_smem_bytes(kSymEigMaxN)));
+  const int C = symeig_cluster_ctas(n);
+  const int tsm = (int)symeig_smem_bytes(n, C);
+  if (C == 4) {
+    S2G_CUDA(cudaFuncSetAttribute(k_symeig_tridiag<4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  tsm));
+    S2G_LAUNCH(k_symeig_tridiag<4>, 4, kTridiagThreads, tsm, s, A, lda, n, work);
+  } else {
+    S2G_CUDA(cudaFuncSetAttribute(k_symeig_tridiag<8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  tsm));
+    S2G_LAUNCH(k_symeig_tridiag<8>, 8, kTridiagThreads, tsm, s, A, lda, n, work);
+  }
   S2G_CUDA(cudaFuncSetAttribute(k_symeig_vectors, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)symeig_vec_smem_bytes(kSymEigMaxN)));
-  S2G_LAUNCH(k_symeig_tridiag, kClusterCtas, kTridiagThreads, symeig_smem_bytes(n), s, A, lda, n,
-             work);
   const int nb = (k + kSymEigWarps - 1) / kSymEigWarps;
   S2G_LAUNCH(k_symeig_values, nb, kSymEigWarps * 32, 3 * n * sizeof(double), s, n, k, work, w);
-  S2G_LAUNCH(k_symeig_vectors, nb, kSymEigWarps * 32, symeig_vec_smem_bytes(n), s, n, k, work, w,
-             Z, ldz, info);
+  S2G_LAUNCH(k_symeig_vectors, nb, kSymEigWarps * 32, symeig_vec_smem_bytes(n), s, n, k, work, w);
+  S2G_LAUNCH(k_symeig_backtransform, nb, kSymEigWarps * 32, symeig_bt_smem_bytes(n), s, n, k,
+             work, w, Z, ldz, info);
 }
 
 }  // namespace std2g

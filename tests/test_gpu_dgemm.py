@@ -81,7 +81,10 @@ def test_gemm_stats_own_and_library_count_the_same_products():
         eng = Engine(0, 0, flags=flags)
         eng.load(b)
         eng.solve(kw)
+        first = eng.gemm_stats()   # includes the S^1/2 products (once per load)
+        eng.solve(kw)
         off = eng.gemm_stats()
+        assert first["calls"] > off["calls"]
         assert off["calls"] > 0 and off["flop"] > 0 and off["ms"] == 0.0
         eng.set_gemm_timing(True)
         eng.solve(kw)
