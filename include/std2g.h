@@ -354,9 +354,9 @@ int std2g_server_stats(void *srv, int64_t *stats);
 void std2g_server_destroy(void *srv);
 
 /* Cap the persistent tensor-core kernels of this context at max_sms CTAs (one
-   per SM; 0 = all SMs), and size the split-K of its FP64 products for that
-   many SMs, so that several contexts sharing a device (the request server's
-   slots) leave SMs to each other's kernels.  No reference counterpart. */
+   per SM; 0 = all SMs), so that several contexts sharing a device (the
+   request server's slots) leave SMs to each other's kernels.  No reference
+   counterpart. */
 int std2g_set_sm_limit(void *ctx, int max_sms);
 
 /* Diagnostic: the engine's FP64 matrix product (DMMA kernel with split-K,

@@ -1956,9 +1956,9 @@ int std2g_set_sm_limit(void *ctx, int max_sms) {
   auto *c = (std2g::Ctx *)ctx;
   c->mixed.tc.max_ctas = max_sms;
   c->mftc.tc.max_ctas = max_sms;
-  // the FP64 products size their split-K for the same share of the SMs
-  c->dg.nsm = max_sms > 0 ? std::min(max_sms, c->dev_sms) : c->dev_sms;
-  c->mftc.side.dg.nsm = c->dg.nsm;
+  // (the FP64 products keep sizing their split-K for all SMs: they are short
+  // and latency-bound, and a share of the SMs made the server's batches
+  // slower, 61 against 83 solves/s)
   return STD2G_OK;
 }
 
