@@ -370,8 +370,13 @@ inline int davidson(DavidsonWork &dw, cublasHandle_t blas, cusolverDnHandle_t so
                     bool warm = false, bool buffer_roots = true) {
   if (k > n) k = n;
   const int kwant = k;
-  if (buffer_roots) k = std::min(n, k + std::max(4, k / 2));
-  const int mmax = std::min(n, std::max(4 * k, k + 32));
+  // buffer roots (a quarter of the wanted ones, at least 4) and a subspace of
+  // up to six blocks, kept within the engine's own Rayleigh-Ritz solver when the
+  // block allows: measured against k/2 buffer roots and four blocks, 124 vs
+  // 135 ms for the 50 roots of the C384H48 flake, 666 vs 841 ms for 48
+  // molecules of 20-150 atoms with 20 roots each
+  if (buffer_roots) k = std::min(n, k + std::max(4, k / 4));
+  const int mmax = std::min(n, std::max(k + 32, std::min(kSymEigMaxN, 6 * k)));
   const int grid = 148 * 4;
   if (warm && dw.X.n < (size_t)n * k) warm = false;
   double *V = dw.V.ensure((size_t)n * mmax), *W = dw.W.ensure((size_t)n * mmax);
