@@ -255,6 +255,30 @@ constexpr int kRowThreads = 128;
 constexpr int kRowStage = 256;   // primaries staged in shared memory at a time
 constexpr int kRowBatch = 8;     // primaries whose loads are issued together
 
+// One PT term t = a^2 / (E_r - E_q) in FP32 and the bound on its error:
+//   a = ak K - J from the FP32 couplings kv, jv; the coupling error is
+//   dn (the Cauchy-Schwarz term e_c (ak |p_r| |q_q| + |p_ij| |q_ab|), formed by
+//   the caller) plus the FP32 rounding of a (2 u (ak |kv| + |jv|));
+//   den = (rh - eh) + (rl - el) from hi / lo energy pairs, rden its correctly
+//   rounded reciprocal; the relative error of rden is ed = 4 u + 3e-14 rden;
+//   bound (2 |a| da + da^2) rden + t (2 ed + cr), cr the rounding allowance of
+//   the term's products (6 u) and of the caller's FP32 partial sums.
+// The bound is used only while den > 0 and ed < 0.25, i.e. 0 < rden < 8.33e12
+// (tested as 0 < rden < 8e12; NaN fails the test): otherwise it is infinite.
+__device__ __forceinline__ float2 pt_term(float akf, float kv, float jv, float rh, float rl,
+                                          float eh, float el, float dn, float cr) {
+  const float am = fmaf(akf, kv, -jv);
+  const float den = (rh - eh) + (rl - el);
+  const float rden = __frcp_rn(den);
+  const float tt = am * am * rden;
+  const float da = fmaf(2.f * kU32, fmaf(akf, fabsf(kv), fabsf(jv)), dn);
+  const float bt = rden > 0.f && rden < 8.0e12f
+                       ? fmaf(da * fmaf(2.f, fabsf(am), da), rden,
+                              tt * fmaf(6e-14f, rden, cr + 8.f * kU32))
+                       : INFINITY;
+  return make_float2(tt, bt);
+}
+
 // Partial PT sums of the candidate rows (ii, a) over primaries
 // [z * qlen, (z + 1) * qlen): part_t[z][ii * nv + a] = sum of the terms,
 // part_b[z][...] = bound on the error of that sum.  Terms are formed in FP32
@@ -277,7 +301,7 @@ k_ptq_rows(const float *__restrict__ K, const float *__restrict__ J, int ni, int
   const double d = de_all[k] + 1e-10;
   const float rh = (float)d, rl = (float)(d - (double)rh);
   if (z == 0 && live) rhl[ii * nv + a] = make_float2(rh, rl);
-  const float pr = pn[k];
+  const float apr = ecoup * akf * pn[k];   // e_c ak |p_r|
   double acc_t = 0.0, acc_b = 0.0;
   const float *Kp = K + ((int64_t)ii * nex + q0) * nva + al;
   const float *Jp = J + ((int64_t)ii * nex + q0) * nva + al;
@@ -289,40 +313,47 @@ k_ptq_rows(const float *__restrict__ K, const float *__restrict__ J, int ni, int
       s_eh[t] = cols.eh[q];
       s_el[t] = cols.el[q];
       s_qn[t] = cols.qn[q];
-      s_wn[t] = wn[(int64_t)(i0 + ii) * no + cols.jq[q]];
+      s_wn[t] = ecoup * wn[(int64_t)(i0 + ii) * no + cols.jq[q]];
       s_g[t] = cols.gq[q];
     }
     __syncthreads();
     for (int t0 = 0; t0 < ns; t0 += kRowBatch) {
-      const int nb = min(kRowBatch, ns - t0);
       float kv[kRowBatch], jv[kRowBatch], vv[kRowBatch];
-#pragma unroll
-      for (int u = 0; u < kRowBatch; ++u) {   // all loads of the batch first
-        const int t = t0 + (u < nb ? u : 0);
-        kv[u] = Kp[(int64_t)t * nva];
-        jv[u] = Jp[(int64_t)t * nva];
-        vv[u] = vn[(int64_t)s_g[t] * nv + al];
-      }
       float gt = 0.f, gb = 0.f;
+      if (t0 + kRowBatch <= ns) {   // a full batch: no guards
 #pragma unroll
-      for (int u = 0; u < kRowBatch; ++u) {
-        const int t = t0 + u;
-        const float am = akf * kv[u] - jv[u];
-        const float den = (rh - s_eh[t < ns ? t : t0]) + (rl - s_el[t < ns ? t : t0]);
-        const float rden = __frcp_rn(den);   // correctly rounded
-        const float tt = am * am * rden;
-        // coupling error (Cauchy-Schwarz) plus the FP32 rounding of am
-        const float da = ecoup * (akf * pr * s_qn[t < ns ? t : t0] + s_wn[t < ns ? t : t0] * vv[u]) +
-                         2.f * kU32 * (akf * fabsf(kv[u]) + fabsf(jv[u]));
-        // denominator: FP32 rounding and the hi/lo representation of both
-        // energies; term: reciprocal and two products (4 roundings)
-        const float ed = 4.f * kU32 + 3e-14f * rden;
-        const float bt = den > 0.f && ed < 0.25f
-                             ? (2.f * fabsf(am) * da + da * da) * rden + tt * (2.f * ed + 6.f * kU32)
-                             : INFINITY;
-        if (u < nb) {
-          gt += tt;
-          gb += bt;
+        for (int u = 0; u < kRowBatch; ++u) {   // all loads of the batch first
+          const int t = t0 + u;
+          kv[u] = Kp[(int64_t)t * nva];
+          jv[u] = Jp[(int64_t)t * nva];
+          vv[u] = vn[(int64_t)s_g[t] * nv + al];
+        }
+#pragma unroll
+        for (int u = 0; u < kRowBatch; ++u) {
+          const int t = t0 + u;
+          const float2 r = pt_term(akf, kv[u], jv[u], rh, rl, s_eh[t], s_el[t],
+                                   fmaf(apr, s_qn[t], s_wn[t] * vv[u]), 6.f * kU32);
+          gt += r.x;
+          gb += r.y;
+        }
+      } else {
+        const int nb = ns - t0;
+#pragma unroll
+        for (int u = 0; u < kRowBatch; ++u) {
+          const int t = t0 + (u < nb ? u : 0);
+          kv[u] = Kp[(int64_t)t * nva];
+          jv[u] = Jp[(int64_t)t * nva];
+          vv[u] = vn[(int64_t)s_g[t] * nv + al];
+        }
+#pragma unroll
+        for (int u = 0; u < kRowBatch; ++u) {
+          const int t = t0 + (u < nb ? u : 0);
+          const float2 r = pt_term(akf, kv[u], jv[u], rh, rl, s_eh[t], s_el[t],
+                                   fmaf(apr, s_qn[t], s_wn[t] * vv[u]), 6.f * kU32);
+          if (u < nb) {
+            gt += r.x;
+            gb += r.y;
+          }
         }
       }
       acc_t += (double)gt;
@@ -404,7 +435,7 @@ k_ptq_cols(const float *__restrict__ K, const float *__restrict__ J, int ni, int
   }
   const int64_t nrow = (int64_t)ni * nv;
   for (int64_t e0 = threadIdx.x; e0 < nrow; e0 += (int64_t)blockDim.x * kColRows) {
-    float kv[kColRows][kColQ], jv[kColRows][kColQ], w[kColRows], pr[kColRows], wr[kColRows];
+    float kv[kColRows][kColQ], jv[kColRows][kColQ], w[kColRows], apr[kColRows], wr[kColRows];
     float2 r[kColRows];
 #pragma unroll
     for (int v = 0; v < kColRows; ++v) {   // rows e0, e0 + blockDim, ...: coalesced
@@ -413,8 +444,8 @@ k_ptq_cols(const float *__restrict__ K, const float *__restrict__ J, int ni, int
       const int ii = (int)(e / nv), a = (int)(e - (int64_t)ii * nv);
       w[v] = (ev < nrow && use[e]) ? 1.f : 0.f;
       r[v] = rhl[e];
-      pr[v] = cb.pn[(int64_t)(cb.i0 + ii) * nv + a];
-      wr[v] = cb.wrow[cb.i0 + ii];
+      apr[v] = cb.ecoup * akf * cb.pn[(int64_t)(cb.i0 + ii) * nv + a];
+      wr[v] = cb.ecoup * cb.wrow[cb.i0 + ii];
       const int64_t o = ((int64_t)ii * nex + q0) * nva + a;
 #pragma unroll
       for (int u = 0; u < kColQ; ++u) {
@@ -428,21 +459,12 @@ k_ptq_cols(const float *__restrict__ K, const float *__restrict__ J, int ni, int
       float t = 0.f, b = 0.f;
 #pragma unroll
       for (int v = 0; v < kColRows; ++v) {
-        const float am = akf * kv[v][u] - jv[v][u];
-        const float den = (r[v].x - ehq[u]) + (r[v].y - elq[u]);
-        const float rden = __frcp_rn(den);
-        const float tt = am * am * rden;
-        t += w[v] * tt;
         // the row pass's term bound with the coupling's J norms bounded by
         // their row / slab maxima, plus the FP32 partial sum of kColRows terms
-        const float da = cb.ecoup * (akf * pr[v] * qnq[u] + wr[v] * vmq[u]) +
-                         2.f * kU32 * (akf * fabsf(kv[v][u]) + fabsf(jv[v][u]));
-        const float ed = 4.f * kU32 + 3e-14f * rden;
-        const float bt = den > 0.f && ed < 0.25f
-                             ? (2.f * fabsf(am) * da + da * da) * rden +
-                                   fabsf(tt) * (2.f * ed + (6.f + kColRows) * kU32)
-                             : INFINITY;
-        b += w[v] * bt;
+        const float2 tb = pt_term(akf, kv[v][u], jv[v][u], r[v].x, r[v].y, ehq[u], elq[u],
+                                  fmaf(apr[v], qnq[u], wr[v] * vmq[u]), (6.f + kColRows) * kU32);
+        t = fmaf(w[v], tb.x, t);
+        b = fmaf(w[v], tb.y, b);
       }
       acc[u] += (double)t;
       accb[u] += (double)b * (1.0 + 8.0 * kU32);
@@ -492,6 +514,7 @@ __global__ void k_pt2_bound_finish(const double *__restrict__ colbnd, int nchunk
   double s = 0.0;
   if (c < nex)
     for (int q = 0; q < nchunk; ++q) s += colbnd[(int64_t)q * nex + c];
+  s *= 1.001;                   // the terms' bounds were formed in FP32
   if (!(s >= 0.0)) s = 1e300;   // INF / NaN: no usable bound
   for (int o = 16; o > 0; o >>= 1) s = fmax(s, __shfl_xor_sync(0xffffffffu, s, o));
   if ((threadIdx.x & 31) == 0) atomicMax(maxb, (unsigned long long)__double_as_longlong(s));
