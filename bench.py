@@ -61,8 +61,9 @@ KW = dict(ax=0.5, e_thr_ev=7.0, thrp=1e-4, nroots=50)
 # the engine's own DMMA products are reported beside it
 LIB64 = 2
 # DRAM bytes (read + write) per FP32 coupling of the PT contractions, from one
-# ncu capture of both coupling launches on the C216H36 flake: (ia|jb) 1.60 GB
-# for 354 M couplings, (ij|ab) 2.72 GB for 360 M couplings
+# ncu capture (one-pass DRAM byte counters) of both coupling launches of the
+# first occupied chunk of this workload: (ia|jb) 2.32 GB and (ij|ab) 4.13 GB for
+# 2 x 0.53 G couplings (6.04 B; the C216H36 flake gives 6.17 B)
 TC_BYTES_PER_COUPLING = 6.05
 WORKLOAD = ("graphene flake C384H48, valence minimal basis (1584 AOs), ax=0.5, E_thr=7 eV, "
             "thrp=1e-4, lowest 50 roots")
@@ -583,15 +584,15 @@ def main():
         pk, src = peaks()
         ach = tc_flop / (tc_ms / 1e3) / 1e12
         # DRAM bytes per FP32 coupling written, measured by ncu on the two
-        # coupling launches of the C216H36 flake (the same kernel and tile
-        # schedule on a workload small enough to capture), times the couplings
-        # of an average launch here (algorithmic FLOP / (2 N_atoms))
+        # coupling launches of one occupied chunk of this workload, times the
+        # couplings of an average launch here (algorithmic FLOP / (2 N_atoms))
         traffic = TC_BYTES_PER_COUPLING * (tc_flop / tc_launch) / (2.0 * b.ncent)
         out["roofline"] = {"bound": "tensor", "achieved": ach, "peak": pk["bf16_tflops"],
                            "unit": "TFLOP/s", "frac": ach / pk["bf16_tflops"],
                            "traffic": traffic,
                            "traffic_source": f"ncu dram bytes per coupling ({TC_BYTES_PER_COUPLING} B, "
-                                             "C216H36 flake capture) x couplings per launch",
+                                             "one-pass capture of this workload's first "
+                                             "chunk) x couplings per launch",
                            "kernel": "k_tc_gemm_bf16x3<PairTiles> (PT-selection couplings "
                                      "(ia|jb) and (ij|ab))",
                            "flop_count": "algorithmic 2*M*N*N_atoms; the split-FP16 operands "
