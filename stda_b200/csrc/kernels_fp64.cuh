@@ -308,17 +308,18 @@ k_charges_tiled(double *__restrict__ out, const double *__restrict__ C, int nao,
     const int A0 = blockIdx.z * kChAtoms;
     const int A1 = min(N, A0 + kChAtoms);
     const int r0 = ao_ptr[A0], nr = ao_ptr[A1] - r0;
-    // stage C[rows of the chunk, tile columns]; consecutive threads take
-    // consecutive rows of one column
-    for (int t = threadIdx.x; t < nr * kCols; t += blockDim.x) {
-      const int c = t / nr, r = t - c * nr;
-      const int k = ao_list[r0 + r];
-      if (c < kChTP) {
-        const int p = pt + c;
-        cp[r * kChTP + c] = p < np ? C[k + (int64_t)nao * (p0 + p)] : 0.0;
-      } else {
-        const int q = qt + (c - kChTP);
-        cq[r * kChTQ + (c - kChTP)] = q < nq ? C[k + (int64_t)nao * (q0 + q)] : 0.0;
+    // stage C[rows of the chunk, tile columns]: warp w takes columns w, w + 8,
+    // ..., its lanes consecutive rows of one column
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int c = warp; c < kCols; c += 8) {
+      const bool isp = c < kChTP;
+      const int col = isp ? pt + c : qt + (c - kChTP);
+      const bool ok = col < (isp ? np : nq);
+      const double *src = C + (int64_t)nao * ((isp ? p0 : q0) + (ok ? col : 0));
+      for (int r = lane; r < nr; r += 32) {
+        const double v = ok ? src[ao_list[r0 + r]] : 0.0;
+        if (isp) cp[r * kChTP + c] = v;
+        else cq[r * kChTQ + (c - kChTP)] = v;
       }
     }
     __syncthreads();
@@ -330,10 +331,18 @@ k_charges_tiled(double *__restrict__ out, const double *__restrict__ C, int nao,
     }
     __syncthreads();
     const int na = A1 - A0;
-    for (int t = threadIdx.x; t < kChTP * kChTQ * na; t += blockDim.x) {
-      const int pl = t / na, a = t - pl * na;
-      const int p = pt + pl / kChTQ, q = qt + pl % kChTQ;
-      if (p < np && q < nq) out[((int64_t)p * nq + q) * N + A0 + a] = st[pl * kSt + a];
+    if (na == kChAtoms) {   // a full chunk: 16 threads write one pair's 128 bytes
+      for (int t = threadIdx.x; t < kChTP * kChTQ * kChAtoms; t += blockDim.x) {
+        const int pl = t / kChAtoms, a = t % kChAtoms;
+        const int p = pt + pl / kChTQ, q = qt + pl % kChTQ;
+        if (p < np && q < nq) out[((int64_t)p * nq + q) * N + A0 + a] = st[pl * kSt + a];
+      }
+    } else {
+      for (int t = threadIdx.x; t < kChTP * kChTQ * na; t += blockDim.x) {
+        const int pl = t / na, a = t - pl * na;
+        const int p = pt + pl / kChTQ, q = qt + pl % kChTQ;
+        if (p < np && q < nq) out[((int64_t)p * nq + q) * N + A0 + a] = st[pl * kSt + a];
+      }
     }
   }
 }

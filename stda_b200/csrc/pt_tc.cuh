@@ -290,8 +290,10 @@ k_ptq_rows(const float *__restrict__ K, const float *__restrict__ J, int ni, int
            const int *__restrict__ cand_pos, PtCols cols, const float *__restrict__ pn,
            const float *__restrict__ wn, const float *__restrict__ vn, float akf, float ecoup,
            double *__restrict__ part_t, double *__restrict__ part_b, float2 *__restrict__ rhl) {
-  __shared__ float s_eh[kRowStage], s_el[kRowStage], s_qn[kRowStage], s_wn[kRowStage];
-  __shared__ int s_g[kRowStage];
+  // per staged primary: energy hi / lo, |q_q| and e_c |p_{i j_q}| in one vector
+  // load, and the offset of its slab's row of vn
+  __shared__ float4 s_c[kRowStage];
+  __shared__ int s_go[kRowStage];
   const int a = blockIdx.x * kRowThreads + threadIdx.x;
   const int ii = blockIdx.y, z = blockIdx.z;
   const int q0 = z * qlen, q1 = min(nex, q0 + qlen);
@@ -310,11 +312,9 @@ k_ptq_rows(const float *__restrict__ K, const float *__restrict__ J, int ni, int
     __syncthreads();
     for (int t = threadIdx.x; t < ns; t += kRowThreads) {
       const int q = s0 + t;
-      s_eh[t] = cols.eh[q];
-      s_el[t] = cols.el[q];
-      s_qn[t] = cols.qn[q];
-      s_wn[t] = ecoup * wn[(int64_t)(i0 + ii) * no + cols.jq[q]];
-      s_g[t] = cols.gq[q];
+      s_c[t] = make_float4(cols.eh[q], cols.el[q], cols.qn[q],
+                           ecoup * wn[(int64_t)(i0 + ii) * no + cols.jq[q]]);
+      s_go[t] = cols.gq[q] * nv;
     }
     __syncthreads();
     for (int t0 = 0; t0 < ns; t0 += kRowBatch) {
@@ -326,13 +326,14 @@ k_ptq_rows(const float *__restrict__ K, const float *__restrict__ J, int ni, int
           const int t = t0 + u;
           kv[u] = Kp[(int64_t)t * nva];
           jv[u] = Jp[(int64_t)t * nva];
-          vv[u] = vn[(int64_t)s_g[t] * nv + al];
+          vv[u] = vn[s_go[t] + al];
         }
 #pragma unroll
         for (int u = 0; u < kRowBatch; ++u) {
           const int t = t0 + u;
-          const float2 r = pt_term(akf, kv[u], jv[u], rh, rl, s_eh[t], s_el[t],
-                                   fmaf(apr, s_qn[t], s_wn[t] * vv[u]), 6.f * kU32);
+          const float4 c = s_c[t];
+          const float2 r = pt_term(akf, kv[u], jv[u], rh, rl, c.x, c.y,
+                                   fmaf(apr, c.z, c.w * vv[u]), 6.f * kU32);
           gt += r.x;
           gb += r.y;
         }
@@ -343,13 +344,14 @@ k_ptq_rows(const float *__restrict__ K, const float *__restrict__ J, int ni, int
           const int t = t0 + (u < nb ? u : 0);
           kv[u] = Kp[(int64_t)t * nva];
           jv[u] = Jp[(int64_t)t * nva];
-          vv[u] = vn[(int64_t)s_g[t] * nv + al];
+          vv[u] = vn[s_go[t] + al];
         }
 #pragma unroll
         for (int u = 0; u < kRowBatch; ++u) {
           const int t = t0 + (u < nb ? u : 0);
-          const float2 r = pt_term(akf, kv[u], jv[u], rh, rl, s_eh[t], s_el[t],
-                                   fmaf(apr, s_qn[t], s_wn[t] * vv[u]), 6.f * kU32);
+          const float4 c = s_c[t];
+          const float2 r = pt_term(akf, kv[u], jv[u], rh, rl, c.x, c.y,
+                                   fmaf(apr, c.z, c.w * vv[u]), 6.f * kU32);
           if (u < nb) {
             gt += r.x;
             gb += r.y;

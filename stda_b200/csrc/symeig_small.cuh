@@ -468,14 +468,16 @@ inline void symeig_small(cudaStream_t s, const double *A, int lda, int n, int k,
   if (n < 1 || n > kSymEigMaxN || k < 1 || k > n)
     throw Error{STD2G_EINVAL, "symeig_small: size out of range"};
   const int C = symeig_cluster_ctas(n);
+  // the attribute is the same for every call (contexts on other host threads
+  // launch the same kernel concurrently), the launch takes what n needs
   const int tsm = (int)symeig_smem_bytes(n, C);
   if (C == 4) {
     S2G_CUDA(cudaFuncSetAttribute(k_symeig_tridiag<4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  tsm));
+                                  (int)symeig_smem_bytes(kSymEigMaxN, 4)));
     S2G_LAUNCH(k_symeig_tridiag<4>, 4, kTridiagThreads, tsm, s, A, lda, n, work);
   } else {
     S2G_CUDA(cudaFuncSetAttribute(k_symeig_tridiag<8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  tsm));
+                                  (int)symeig_smem_bytes(kSymEigMaxN, 8)));
     S2G_LAUNCH(k_symeig_tridiag<8>, 8, kTridiagThreads, tsm, s, A, lda, n, work);
   }
   S2G_CUDA(cudaFuncSetAttribute(k_symeig_vectors, cudaFuncAttributeMaxDynamicSharedMemorySize,
