@@ -1240,11 +1240,13 @@ static void solve(Ctx &c, const std2g_params &p_in, std2g_result *res, const Res
   double *ekd = c.w_tmp.ensure(std::max<size_t>(nci, (size_t)2 * nao * nao));
   S2G_LAUNCH(k_gather_cols, grid_for(nci), 256, 0, s, ekd, ek, (int64_t)1, d_allk, (int64_t)nci,
              (int64_t)1);
-  // Large TDA problems with a root count use the matrix-free operators and the
-  // blocked Davidson solver; everything else builds the matrices explicitly.
+  // TDA problems with a root count above 320 CSFs use the matrix-free operators
+  // and the blocked Davidson solver (a dense eigen-decomposition of 320-1024
+  // CSFs took longer: 48 molecules of 20-150 atoms, 20 roots, 723 against
+  // 735 ms); everything else builds the matrices explicitly.
   // (sTD-DFT roots: the matrix-free A+B, A-B products and the Davidson of
   // davidson_rpa.cuh, FP64 products in both forms)
-  const bool use_mf = !resp && p.nroots > 0 && (p.solver == 2 || (p.solver == 0 && nci > 1024));
+  const bool use_mf = !resp && p.nroots > 0 && (p.solver == 2 || (p.solver == 0 && nci > 320));
   // Mixed form: the tensor-core first Davidson stage pays off once the
   // products dominate; below kTcDavidsonMin CSFs (solver auto) the solve is
   // latency-bound and runs the single FP64 stage.  The tensor-core stage

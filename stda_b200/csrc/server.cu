@@ -90,7 +90,7 @@ struct Server {
 // work arrays, the PT coupling buffers up to their chunk budget, and either
 // the dense CSF matrices or the matrix-free solvers' subspaces, chosen by the
 // engine's own rules (std2g_solve: dense eigensolve for all roots, solver 1 or
-// up to 1024 CSFs; std2g_polarizability: matrix-free for solver 2, when the
+// up to 320 CSFs; std2g_polarizability: matrix-free for solver 2, when the
 // dense form needs more than 24 GB, and in the mixed form (precision 1) with
 // solver 0 above 4096 CSFs).
 int64_t footprint_estimate(const Job &j, int precision) {
@@ -103,7 +103,7 @@ int64_t footprint_estimate(const Job &j, int precision) {
   b += 8 * (16 * nao * nao + 12 * (int64_t)j.nmo * nao);
   b += std::min<int64_t>(6000000000LL, 8 * pairs * std::min<int64_t>(pairs, 4096));
   const int64_t nci = std::min<int64_t>(pairs, 30000);
-  bool dense = j.par.nroots <= 0 || j.par.solver == 1 || nci <= 1024;
+  bool dense = j.par.nroots <= 0 || j.par.solver == 1 || nci <= 320;
   if (!j.omega.empty()) {
     const bool resp_mf = j.par.solver == 2 || (double)nci * nci * 8.0 * 10.0 > 24e9 ||
                          (precision == 1 && j.par.solver == 0 && nci > 4096);
