@@ -409,7 +409,7 @@ __global__ void k_ptq_use(int ni, int nv, int i0, const int *__restrict__ cand_p
 
 // ---------------------------------------------------------------- column pass
 constexpr int kColQ = 4;     // primaries per block
-constexpr int kColRows = 4;  // candidate rows per thread and step (loads issued together)
+constexpr int kColRows = 2;  // candidate rows per thread and step (loads issued together)
 
 // colpart[q] = sum over the non-selected candidates (ii, a) of the chunk of
 // the terms t_(ii,a),q, for kColQ primaries per block: the block's threads
@@ -417,7 +417,7 @@ constexpr int kColRows = 4;  // candidate rows per thread and step (loads issued
 // loads issued first, terms of rows that are not summed multiplied by zero;
 // per-thread FP64 sums, then a fixed-order warp and block reduction
 // (deterministic).
-__global__ void __launch_bounds__(256, 2)
+__global__ void __launch_bounds__(256, 3)
 k_ptq_cols(const float *__restrict__ K, const float *__restrict__ J, int ni, int nv, int nva,
            int nex, const unsigned char *__restrict__ use, const float2 *__restrict__ rhl,
            const float *__restrict__ eh, const float *__restrict__ el, float akf,

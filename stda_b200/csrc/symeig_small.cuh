@@ -11,8 +11,10 @@
 //   3. k_symeig_vectors (one warp per cluster of close eigenvalues, its work
 //      arrays in shared memory): inverse iteration with a pivoted tridiagonal
 //      LU (LAPACK dstein's scheme: shifts of equal eigenvalues nudged apart,
-//      modified Gram-Schmidt against the earlier members of the cluster, three
-//      iterations from a fixed start vector; the cluster threshold is
+//      modified Gram-Schmidt against the earlier members of the cluster, two
+//      iterations from a fixed start vector (bisection leaves the eigenvalue
+//      within a few ulps of ||T||, so the first solve already grows the wanted
+//      component by ~1/eps); the cluster threshold is
 //      1e-5 ||T||, tighter than dstein's 1e-3, so that the dense Rayleigh-Ritz
 //      spectra do not collapse into one serial cluster), vectors in T's basis;
 //   4. k_symeig_backtransform (one warp per eigenvector, held in registers):
@@ -353,7 +355,7 @@ k_symeig_vectors(int n, int k, double *__restrict__ work, const double *__restri
     }
     for (int i = lane; i < n; i += 32) y[i] = 1.0 + 0.5 * sin(0.7 * (i + 1) + 0.3 * (m + 1));
     __syncwarp();
-    for (int it = 0; it < 3; ++it) {
+    for (int it = 0; it < 2; ++it) {
       if (lane == 0) {
         for (int i = 0; i + 1 < n; ++i) {   // y <- L^-1 P y
           if (fl[i] != 0.0) {

@@ -12,14 +12,14 @@ LOG = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))),
 
 # kernel -> most registers per thread.  The HBM-bound passes need enough loads
 # in flight: half of the SM's 2048 threads resident (65536 / 1024 = 64
-# registers), or, for the PT column pass, which issues 4 rows x 4 primaries of
+# registers), or, for the PT column pass, which issues 2 rows x 4 primaries of
 # loads per thread before using them and carries a second (error-bound)
-# accumulator per primary, two 256-thread CTAs (128 registers); the
+# accumulator per primary, three 256-thread CTAs (85 registers); the
 # tensor-core kernel runs one 256-thread CTA per SM.
 HOT = {
     "k_tc_gemm_bf16x3": 255,
     "k_ptq_rows": 80,
-    "k_ptq_cols": 128,
+    "k_ptq_cols": 85,
     "k_charges_tiled": 64,
     "k_diag_screen": 64,
 }
