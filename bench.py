@@ -409,13 +409,24 @@ def served_and_batched(device, args):
     atoms, pool = molecule_pool("batch", args.batch_pool, seed=3)
     kw = Keywords(ax=0.5, e_thr_ev=6.5, nroots=20, conv_tol=1e-7)
     reqs = [(k % len(pool), kw, None) for k in range(args.batch_requests)]
+    # each form twice, interleaved, the faster run of each kept: the batch runs
+    # for seconds on a shared GPU and single runs vary by ~10 %
     rm, bm = run_server(1, pool, reqs, None, args.slots, device)
     rd, bd = run_server(0, pool, reqs, None, args.slots, device)
     _, bo = run_server(0, pool, reqs, None, args.slots, device, library=False)
+    for prec, lib, key in ((1, True, "m"), (0, True, "d"), (0, False, "o")):
+        _, again = run_server(prec, pool, reqs, None, args.slots, device, library=lib)
+        if key == "m" and again["solves_per_s"] > bm["solves_per_s"]:
+            bm = again
+        elif key == "d" and again["solves_per_s"] > bd["solves_per_s"]:
+            bd = again
+        elif key == "o" and again["solves_per_s"] > bo["solves_per_s"]:
+            bo = again
     plain = plain_fp64(pool, reqs[:len(pool)], device)
     out["batched"] = {"workload": f"{len(reqs)} molecules ({len(pool)} distinct, "
                                   f"{int(atoms.min())}-{int(atoms.max())} atoms log-uniform), "
-                                  "E_thr 6.5 eV, 20 roots (residual 1e-7), submitted at once",
+                                  "E_thr 6.5 eV, 20 roots (residual 1e-7), submitted at once; "
+                                  "best of 2 interleaved runs per form",
                       "mixed": bm, "fp64": bd, "fp64_own_products": bo,
                       "fp64_plain": plain,
                       "speedup_mixed_vs_fp64_same_slots": bm["solves_per_s"] / bd["solves_per_s"],
