@@ -490,7 +490,7 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--no-serve", action="store_true",
                     help="skip the served-stream and batch measurements")
-    ap.add_argument("--slots", type=int, default=4, help="request-server contexts")
+    ap.add_argument("--slots", type=int, default=8, help="request-server contexts")
     ap.add_argument("--serve-rate", type=float, default=8.0, help="Poisson arrivals per second")
     ap.add_argument("--serve-requests", type=int, default=120)
     ap.add_argument("--serve-pool", type=int, default=24)
