@@ -673,6 +673,9 @@ def main():
                     "FLOP = 2 m n k per product"}
 
     if rank == 0 and world == 1 and not args.no_serve:
+        # the benchmark solve's context holds tens of GB that the servers'
+        # admission budget (a share of the free memory) would otherwise miss
+        eng.close()
         out.update(response_cfg2(local))
         out.update(served_and_batched(local, args))
 
