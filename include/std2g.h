@@ -64,6 +64,9 @@ enum {
 /* FP64 matrix products through cuBLAS instead of the engine's own DMMA kernel
    (the library baseline that the plain FP64 form is compared with). */
 #define STD2G_FLAG_LIBRARY_FP64 2
+/* Request server only (std2g_server_opts.flags): the slots' contexts share one
+   batched eigensolver (std2g_batch_create / std2g_attach_batch). */
+#define STD2G_FLAG_BATCH_EIGEN 4
 
 typedef struct {
   int device;            /* CUDA device ordinal */
@@ -349,6 +352,10 @@ int std2g_server_wait(void *srv, int64_t ticket, std2g_result *res, double *alph
 /* stats[7]: submitted, completed, in flight, peak in flight, bytes in flight
    (estimated), peak bytes in flight, budget. */
 int std2g_server_stats(void *srv, int64_t *stats);
+/* With STD2G_FLAG_BATCH_EIGEN: std2g_batch_stats of the server's batch (zeros
+   without it). */
+int std2g_server_batch_stats(void *srv, int64_t *problems, int64_t *iterations,
+                             int64_t *members, double *ms);
 /* Stop the workers after their current requests (queued ones are dropped) and
    free the contexts; call after the last wait. */
 void std2g_server_destroy(void *srv);
@@ -358,6 +365,32 @@ void std2g_server_destroy(void *srv);
    request server's slots) leave SMs to each other's kernels.  No reference
    counterpart. */
 int std2g_set_sm_limit(void *ctx, int max_sms);
+
+/* ---- batched eigensolves across contexts ---------------------------------
+   Many molecules' excitation solves share one lockstep Davidson: contexts
+   attached to a batch, each solving on its own host thread, hand the TDA
+   eigenproblem of a std2g_solve (321 to 6144 CSFs, a root request of
+   p.nroots > 0 with solver 0, roots + buffer roots <= 112) to the batch, whose
+   coordinator thread runs one Davidson iteration of every waiting problem per
+   round of launches (grouped FP64 products, batched Rayleigh-Ritz, batched
+   residual and Cholesky-QR kernels; three host synchronisations per round for
+   the whole batch).  Problems join at the next iteration and leave when their
+   roots converge (continuous batching).  Results are those of the unbatched
+   Davidson (same algorithm, FP64 throughout; dense A instead of matrix-free
+   products) to the convergence tolerance.  No reference counterpart: the
+   reference solves one molecule per process with ssyevr (stda.f:1133-1150).
+   std2g_batch_destroy: after every attached context has finished its solves. */
+int std2g_batch_create(int device, void **batch);
+/* Attach (batch) or detach (NULL) a context; same device as the batch. */
+int std2g_attach_batch(void *ctx, void *batch);
+/* Problems solved, batched iterations run, members summed over iterations;
+   ms (NULL or [2]): wall time of the iterations, total and up to their first
+   host synchronisation (products, Rayleigh-Ritz, residuals). */
+int std2g_batch_stats(void *batch, int64_t *problems, int64_t *iterations, int64_t *members,
+                      double *ms);
+void std2g_batch_destroy(void *batch);
+/* 1 when the last std2g_solve of ctx took its eigensolve from a batch. */
+int std2g_last_batched(void *ctx);
 
 /* Diagnostic: the engine's FP64 matrix product (DMMA kernel with split-K,
    used for ONETRI, the Loewdin transform, gamma.q and the property

@@ -6,7 +6,9 @@
 #include <cublas_v2.h>
 #include <cusolverDn.h>
 
+#include <algorithm>
 #include <cstdint>
+#include <cstring>
 #include <atomic>
 #include <cstdio>
 #include <string>
@@ -92,5 +94,47 @@ struct DBuf {
 };
 
 inline int64_t div_up(int64_t a, int64_t b) { return (a + b - 1) / b; }
+
+// Page-locked host staging memory for small host -> device uploads (launch
+// descriptors): a copy from pageable memory may wait for the stream, one from
+// here is asynchronous.  Regions are handed out in order and must stay
+// untouched until the stream has passed their copies: the owner calls reset()
+// only after synchronising the stream.  Grows (freeing the old block after a
+// device synchronisation) when a request does not fit.
+struct PinnedArena {
+  char *base = nullptr;
+  size_t cap = 0, off = 0;
+  PinnedArena() = default;
+  PinnedArena(const PinnedArena &) = delete;
+  PinnedArena &operator=(const PinnedArena &) = delete;
+  ~PinnedArena() {
+    if (base) cudaFreeHost(base);
+  }
+  void reset() { off = 0; }
+  // n bytes of the arena (16-byte aligned), uninitialised
+  void *take(size_t n) { return put(nullptr, n); }
+  // copy of n bytes at p in the arena (16-byte aligned; p = NULL: no copy)
+  void *put(const void *p, size_t n) {
+    const size_t at = (off + 15) & ~(size_t)15;
+    if (!base || at + n > cap) {
+      // a larger block; copies still pending read the old one, so the device
+      // is synchronised before it is freed
+      const size_t ncap = std::max<size_t>(2 * cap, std::max<size_t>(at + n, 1 << 16));
+      char *nb = nullptr;
+      S2G_CUDA(cudaMallocHost(&nb, ncap));
+      if (base) {
+        S2G_CUDA(cudaDeviceSynchronize());
+        cudaFreeHost(base);
+      }
+      base = nb;
+      cap = ncap;
+      off = 0;
+      return put(p, n);
+    }
+    if (p) std::memcpy(base + at, p, n);
+    off = at + n;
+    return base + at;
+  }
+};
 
 }  // namespace std2g

@@ -142,9 +142,9 @@ __global__ void k_diag_matrix(double *__restrict__ H, int ld, int k, const doubl
 // factorisation, then one forward substitution per column of L^-1 (thread j
 // solves L x = e_j); deterministic.
 constexpr int kCholMax = 112;   // 2 nc^2 doubles of shared memory
-__global__ void __launch_bounds__(256)
-k_chol_inv(const double *__restrict__ G, int nc, double tol, double *__restrict__ out,
-           double *__restrict__ stat) {
+__device__ __forceinline__ void chol_inv_body(const double *__restrict__ G, int nc, double tol,
+                                              double *__restrict__ out,
+                                              double *__restrict__ stat) {
   extern __shared__ double sm[];
   double *L = sm;               // column-major nc x nc
   double *X = sm + nc * nc;     // X[j*nc + i] = (L^-1)[i][j]
@@ -213,6 +213,13 @@ k_chol_inv(const double *__restrict__ G, int nc, double tol, double *__restrict_
     stat[1] = dmin;
   }
 }
+
+__global__ void __launch_bounds__(256)
+k_chol_inv(const double *__restrict__ G, int nc, double tol, double *__restrict__ out,
+           double *__restrict__ stat) {
+  chol_inv_body(G, nc, tol, out, stat);
+}
+
 
 struct DavidsonWork {
   DBuf<double> V, W, H, Hs, theta, X, R, T, tmp, rn, proj, G, Gc, Gz, lam, work2, part, eigwork,

@@ -62,35 +62,20 @@ __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
-// blockIdx.x: tile of C (m fastest); blockIdx.y: batch * ksplit + split.
-// Each split covers K range [split * kchunk, min(K, (split + 1) * kchunk)).
-// ksplit == 1: C = alpha acc + beta C;  else work[(b * ksplit + split)][m + n M] = acc.
+// Main loop of one CTA tile: acc = op(A) op(B) over the K range [kb, ke) for
+// the 64 x BN tile of C at (m0, n0), shared by the strided-batch kernel
+// k_dgemm and the grouped kernel k_dgemm_grouped.
 // A tiles are kept in the global layout's fast order: m fastest for op(A) = A
 // ([k][m]), k fastest for op(A) = A^T ([m][k]); B tiles k fastest for
 // op(B) = B ([n][k]), n fastest for op(B) = B^T ([k][n]); swizzled (pos_*).
 // CTA tile 64 x BN (BN = 32, 64, 128); warp w owns rows 32 (w & 1) .. +32 and
 // columns (BN / 2)(w >> 1) .. +BN / 2: 4 x BN / 16 DMMA tiles.
 template <bool TA, bool TB, int BN>
-__global__ void __launch_bounds__(dg::THREADS, BN == 32 ? 4 : (BN == 64 ? 3 : 2))
-    k_dgemm(int M, int N, int K, double alpha, const double *__restrict__ A, int64_t lda,
-            int64_t sA, const double *__restrict__ B, int64_t ldb, int64_t sB, double beta,
-            double *__restrict__ C, int64_t ldc, int64_t sC, int ksplit, int kchunk,
-            double *__restrict__ work, int tri) {
+__device__ __forceinline__ void dgemm_mainloop(int M, int N, const double *__restrict__ A,
+                                               int64_t lda, const double *__restrict__ B,
+                                               int64_t ldb, int m0, int n0, int kb, int ke,
+                                               double *smem_d, double (&acc)[4][BN / 16][2]) {
   using namespace dg;
-  extern __shared__ __align__(16) double smem_d[];
-  const int tiles_m = (M + BM - 1) / BM;
-  const int m0 = (blockIdx.x % tiles_m) * BM, n0 = (blockIdx.x / tiles_m) * BN;
-  // tri > 0: column n is the pair (i, j) = (n / tri, n % tri) of a symmetric
-  // pair array and only j <= i is wanted: a tile whose columns all lie above
-  // the diagonal is skipped (the caller mirrors those columns)
-  if (tri > 0) {
-    const int i0 = n0 / tri, i1 = min(N - 1, n0 + BN - 1) / tri;
-    if (i0 == i1 && n0 - i0 * tri > i0) return;
-  }
-  const int batch = blockIdx.y / ksplit, split = blockIdx.y % ksplit;
-  const int kb = split * kchunk, ke = min(K, kb + kchunk);
-  A += batch * sA;
-  B += batch * sB;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int g = lane >> 2, t = lane & 3;
   constexpr int NJ = BN / 16, STAGE = stage_doubles<BN>(), TILE_B = BN * BK;
@@ -148,7 +133,6 @@ __global__ void __launch_bounds__(dg::THREADS, BN == 32 ? 4 : (BN == 64 ? 3 : 2)
     }
   };
 
-  double acc[4][NJ][2];
 #pragma unroll
   for (int i = 0; i < 4; ++i)
 #pragma unroll
@@ -189,6 +173,38 @@ __global__ void __launch_bounds__(dg::THREADS, BN == 32 ? 4 : (BN == 64 ? 3 : 2)
     }
   }
   cp_async_wait<0>();
+}
+
+// blockIdx.x: tile of C (m fastest); blockIdx.y: batch * ksplit + split.
+// Each split covers K range [split * kchunk, min(K, (split + 1) * kchunk)).
+// ksplit == 1: C = alpha acc + beta C;  else work[(b * ksplit + split)][m + n M] = acc.
+template <bool TA, bool TB, int BN>
+__global__ void __launch_bounds__(dg::THREADS, BN == 32 ? 4 : (BN == 64 ? 3 : 2))
+    k_dgemm(int M, int N, int K, double alpha, const double *__restrict__ A, int64_t lda,
+            int64_t sA, const double *__restrict__ B, int64_t ldb, int64_t sB, double beta,
+            double *__restrict__ C, int64_t ldc, int64_t sC, int ksplit, int kchunk,
+            double *__restrict__ work, int tri) {
+  using namespace dg;
+  extern __shared__ __align__(16) double smem_d[];
+  const int tiles_m = (M + BM - 1) / BM;
+  const int m0 = (blockIdx.x % tiles_m) * BM, n0 = (blockIdx.x / tiles_m) * BN;
+  // tri > 0: column n is the pair (i, j) = (n / tri, n % tri) of a symmetric
+  // pair array and only j <= i is wanted: a tile whose columns all lie above
+  // the diagonal is skipped (the caller mirrors those columns)
+  if (tri > 0) {
+    const int i0 = n0 / tri, i1 = min(N - 1, n0 + BN - 1) / tri;
+    if (i0 == i1 && n0 - i0 * tri > i0) return;
+  }
+  const int batch = blockIdx.y / ksplit, split = blockIdx.y % ksplit;
+  const int kb = split * kchunk, ke = min(K, kb + kchunk);
+  A += batch * sA;
+  B += batch * sB;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  constexpr int NJ = BN / 16;
+  const int wm = (warp & 1) * 32, wn = (warp >> 1) * (BN / 2);
+  double acc[4][NJ][2];
+  dgemm_mainloop<TA, TB, BN>(M, N, A, lda, B, ldb, m0, n0, kb, ke, smem_d, acc);
 
   // epilogue: element (i, j, e) of this thread is C[m0 + wm + 8 i + g][n0 + wn + 8 j + 2 t + e]
   if (ksplit == 1) {
@@ -242,6 +258,90 @@ __global__ void k_dgemm_reduce(int M, int N, int batch, int ksplit, double alpha
   }
 }
 
+// One member of a grouped launch: C = alpha op(A) op(B) + beta C with op(A)
+// M x K and op(B) K x N (column-major; beta = 0: C is not read).
+struct DgProblem {
+  int M, N, K;
+  double alpha, beta;
+  const double *A, *B;
+  double *C;
+  int64_t lda, ldb, ldc;
+  int ks = 1;          // K splits (set by Dgemm::grouped)
+  int64_t woff = 0;    // the member's partial tiles in the workspace (ks > 1)
+};
+
+// Products of different shapes and operands in one launch (one op(A), op(B)
+// and tile width for all): blockIdx.x runs over the tiles of every member,
+// member p owning tiles [tile0[p], tile0[p + 1]) (m fastest, then the K
+// split); a binary search maps the CTA to its member.  A member with ks > 1
+// splits K into ks ranges whose partial tiles go to work + woff and are added
+// in split order by k_dgemm_grouped_reduce (deterministic, no atomics).
+template <bool TA, bool TB, int BN>
+__global__ void __launch_bounds__(dg::THREADS, BN == 32 ? 4 : (BN == 64 ? 3 : 2))
+    k_dgemm_grouped(const DgProblem *__restrict__ probs, const int *__restrict__ tile0,
+                    int nprob, double *__restrict__ work) {
+  using namespace dg;
+  extern __shared__ __align__(16) double smem_d[];
+  const int tb = blockIdx.x;
+  int lo = 0, hi = nprob;   // tile0[lo] <= tb < tile0[hi]
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (tile0[mid] <= tb) lo = mid;
+    else hi = mid;
+  }
+  const DgProblem pr = probs[lo];
+  const int tiles_m = (pr.M + BM - 1) / BM, tiles_mn = tiles_m * ((pr.N + BN - 1) / BN);
+  const int local = (tb - tile0[lo]) % tiles_mn, split = (tb - tile0[lo]) / tiles_mn;
+  const int m0 = (local % tiles_m) * BM, n0 = (local / tiles_m) * BN;
+  const int kchunk = (((pr.K + pr.ks - 1) / pr.ks + BK - 1) / BK) * BK;
+  const int kb = split * kchunk, ke = min(pr.K, kb + kchunk);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  constexpr int NJ = BN / 16;
+  const int wm = (warp & 1) * 32, wn = (warp >> 1) * (BN / 2);
+  double acc[4][NJ][2];
+  dgemm_mainloop<TA, TB, BN>(pr.M, pr.N, pr.A, pr.lda, pr.B, pr.ldb, m0, n0, kb, ke, smem_d,
+                             acc);
+  double *wp = work + pr.woff + (int64_t)split * pr.M * pr.N;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int row = m0 + wm + 8 * i + g;
+    if (row >= pr.M) continue;
+#pragma unroll
+    for (int j = 0; j < NJ; ++j)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int col = n0 + wn + 8 * j + 2 * t + e;
+        if (col >= pr.N) continue;
+        if (pr.ks > 1) {
+          wp[row + (int64_t)col * pr.M] = acc[i][j][e];
+        } else {
+          double *p = pr.C + row + (int64_t)col * pr.ldc;
+          const double v = pr.alpha * acc[i][j][e];
+          *p = pr.beta == 0.0 ? v : v + pr.beta * *p;
+        }
+      }
+  }
+}
+
+// C = alpha sum_s work[woff + s M N] + beta C for the members with ks > 1
+// (blockIdx.y = member), splits added in order 0, 1, ...
+__global__ void k_dgemm_grouped_reduce(const DgProblem *__restrict__ probs,
+                                       const double *__restrict__ work) {
+  const DgProblem pr = probs[blockIdx.y];
+  if (pr.ks <= 1) return;
+  const int64_t mn = (int64_t)pr.M * pr.N;
+  for (int64_t x = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; x < mn;
+       x += (int64_t)gridDim.x * blockDim.x) {
+    const double *w = work + pr.woff + x;
+    double s = 0.0;
+    for (int q = 0; q < pr.ks; ++q) s += w[q * mn];
+    const int64_t col = x / pr.M, row = x - col * pr.M;
+    double *p = pr.C + row + col * pr.ldc;
+    *p = pr.beta == 0.0 ? pr.alpha * s : pr.alpha * s + pr.beta * *p;
+  }
+}
+
 // Launch wrapper with the split-K workspace.
 struct Dgemm {
   DBuf<double> work;
@@ -282,6 +382,66 @@ struct Dgemm {
       ev.push_back(e);
     }
     S2G_CUDA(cudaEventRecord(ev[nev++], s));
+  }
+
+  // grouped launch (k_dgemm_grouped, 64 x 32 tiles) of the members with a
+  // non-empty output; the descriptors go to `gdesc` / `gtile0` (same stream:
+  // a later launch's upload waits for this launch), from `stage` when given
+  DBuf<DgProblem> gdesc;
+  DBuf<int> gtile0;
+  DBuf<double> gwork;   // partial tiles of the split members
+  void grouped(cudaStream_t s, bool ta, bool tb, const std::vector<DgProblem> &in,
+               PinnedArena *stage = nullptr) {
+    std::vector<DgProblem> pr;
+    std::vector<int> t0(1, 0);
+    int64_t wtot = 0;
+    int64_t mnmax = 0;
+    for (DgProblem q : in) {
+      if (q.M <= 0 || q.N <= 0) continue;
+      // long sums over few output tiles (the Davidson's projections, A V of
+      // a small block) split K: at least 256 per split, about 128 CTAs
+      const int64_t tmn = div_up(q.M, dg::BM) * div_up(q.N, 32);
+      q.ks = (int)std::max<int64_t>(
+          1, std::min<int64_t>({32, q.K / 256, std::max<int64_t>(1, 128 / tmn)}));
+      q.woff = wtot;
+      if (q.ks > 1) wtot += (int64_t)q.ks * q.M * q.N;
+      mnmax = std::max<int64_t>(mnmax, (int64_t)q.M * q.N);
+      pr.push_back(q);
+      t0.push_back(t0.back() + (int)(tmn * q.ks));
+      flop += 2.0 * q.M * q.N * (double)q.K;
+    }
+    if (pr.empty()) return;
+    ++calls;
+    const int np = (int)pr.size();
+    double *wk = wtot > 0 ? gwork.ensure((size_t)wtot) : nullptr;
+    DgProblem *d = gdesc.ensure(pr.size());
+    int *dt = gtile0.ensure(t0.size());
+    const void *hp = pr.data(), *ht = t0.data();
+    if (stage) {
+      hp = stage->put(pr.data(), sizeof(DgProblem) * pr.size());
+      ht = stage->put(t0.data(), sizeof(int) * t0.size());
+    }
+    S2G_CUDA(cudaMemcpyAsync(d, hp, sizeof(DgProblem) * pr.size(), cudaMemcpyHostToDevice, s));
+    S2G_CUDA(cudaMemcpyAsync(dt, ht, sizeof(int) * t0.size(), cudaMemcpyHostToDevice, s));
+#define S2G_DGEMM_G(TA_, TB_)                                                                   \
+  do {                                                                                          \
+    S2G_CUDA(cudaFuncSetAttribute(k_dgemm_grouped<TA_, TB_, 32>,                                \
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize,                  \
+                                  dg::smem_bytes<32>()));                                       \
+    S2G_LAUNCH((k_dgemm_grouped<TA_, TB_, 32>), t0.back(), dg::THREADS, dg::smem_bytes<32>(), s, \
+               d, dt, np, wk);                                                                  \
+  } while (0)
+    if (!ta && !tb) S2G_DGEMM_G(false, false);
+    else if (ta && !tb) S2G_DGEMM_G(true, false);
+    else if (!ta && tb) S2G_DGEMM_G(false, true);
+    else S2G_DGEMM_G(true, true);
+#undef S2G_DGEMM_G
+    ++launches;
+    if (wtot > 0) {
+      const int g = (int)std::max<int64_t>(1, std::min<int64_t>(div_up(mnmax, 256), 64));
+      S2G_LAUNCH(k_dgemm_grouped_reduce, dim3(g, np), 256, 0, s, d, wk);
+      ++launches;
+    }
   }
 
   // the argument order of cublasDgemm (alpha / beta by pointer, host values)

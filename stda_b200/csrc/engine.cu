@@ -29,6 +29,7 @@
 #include "pt_tc.cuh"
 #include "response_mixed.cuh"
 #include "symeig_small.cuh"
+#include "batch_davidson.cuh"
 
 namespace std2g {
 
@@ -108,6 +109,11 @@ struct Ctx {
   bool last_rpa = false;
   double ph_ms[PH_COUNT] = {0};
   cudaEvent_t ev[PH_COUNT + 1];
+  // shared batched eigensolver (std2g_attach_batch) and the events that order
+  // this context's stream with the batch's
+  BatchDavidson *batch = nullptr;
+  cudaEvent_t ev_bready = nullptr, ev_bdone = nullptr;
+  bool last_batched = false;
 };
 
 // --------------------------------------------------------------------------
@@ -1246,7 +1252,18 @@ static void solve(Ctx &c, const std2g_params &p_in, std2g_result *res, const Res
   // 735 ms); everything else builds the matrices explicitly.
   // (sTD-DFT roots: the matrix-free A+B, A-B products and the Davidson of
   // davidson_rpa.cuh, FP64 products in both forms)
-  const bool use_mf = !resp && p.nroots > 0 && (p.solver == 2 || (p.solver == 0 && nci > 320));
+  // A context attached to a shared batched eigensolver (std2g_attach_batch):
+  // TDA root requests of 321 to kBatchMaxCsf CSFs build the dense A and join
+  // the batch's lockstep Davidson (batch_davidson.cuh) instead of running
+  // their own; the batch is FP64 in both forms.
+  constexpr int kBatchMaxCsf = 6144;
+  const bool batch_eig = c.batch != nullptr && !resp && !p.rpa && p.nroots > 0 &&
+                         p.solver == 0 && nci > 320 && nci <= kBatchMaxCsf &&
+                         bd_fits(nci, std::min(p.nroots, nci)) &&
+                         !(c.opts.flags & STD2G_FLAG_TENSOR_ALWAYS);
+  c.last_batched = batch_eig;
+  const bool use_mf = !batch_eig && !resp && p.nroots > 0 &&
+                      (p.solver == 2 || (p.solver == 0 && nci > 320));
   // Mixed form: the tensor-core first Davidson stage pays off once the
   // products dominate; below kTcDavidsonMin CSFs (solver auto) the solve is
   // latency-bound and runs the single FP64 stage.  The tensor-core stage
@@ -1435,26 +1452,70 @@ static void solve(Ctx &c, const std2g_params &p_in, std2g_result *res, const Res
     }
     record(c, PH_EIGEN);
     om = c.w_eval.ensure(std::max(nci, nao));
-    nroot = dense_eig(c, A, nci, 0.0, thr, p.nroots, om);
-    X = A;
-    c.mixed.lastX = X;
-    if (nroot < 1) throw Error{STD2G_ENOROOT, "no root below the energy threshold"};
-    // FP64 residuals ||A x - w x|| of the returned eigenvectors: A rebuilt
-    // from K, J and the diagonal (its storage now holds the eigenvectors)
-    {
-      double *Ar = c.w_Ares.ensure(n2), *Rr = c.w_Rres.ensure((size_t)nci * nroot);
-      S2G_LAUNCH(k_combine_tda, grid_for(n2), 256, 0, s, Ar, K, J, (int64_t)nci, ak, d_edall);
-      gemm(c, CUBLAS_OP_N, CUBLAS_OP_N, nci, nroot, nci, 1.0, Ar, nci, X, nci, 0.0, Rr, nci);
-      double *part = c.w_part.ensure((size_t)nroot * kColSplit), *rn = c.w_rn.ensure(nroot);
-      S2G_LAUNCH(k_dav_resid, dim3(kColSplit, (unsigned)nroot), 256, 0, s, Rr, X, om, nci, part);
-      S2G_LAUNCH(k_colnorm_finish, (int)div_up(nroot, 128), 128, 0, s, part, kColSplit, nroot,
-                 rn);
-      root_resid.assign(nroot, 0.0);
-      root_ritz.assign(nroot, 0.0);
-      S2G_CUDA(cudaMemcpyAsync(root_resid.data(), rn, sizeof(double) * nroot,
-                               cudaMemcpyDeviceToHost, s));
-      S2G_CUDA(cudaMemcpyAsync(root_ritz.data(), om, sizeof(double) * nroot,
-                               cudaMemcpyDeviceToHost, s));
+    if (batch_eig) {
+      // the lowest p.nroots roots, as the matrix-free Davidson of an unbatched
+      // solve gives them, from the shared batch
+      BatchProblem bp;
+      bp.dw = &c.dav;
+      bp.blas = c.blas;
+      bp.sol = c.solver;
+      bp.A = A;
+      bp.diag = d_edall;
+      bp.n = nci;
+      bp.kwant = std::min(p.nroots, nci);
+      bp.tol = p.conv_tol > 0 ? p.conv_tol : 1e-6;
+      bp.max_iter = 300;
+      bd_prepare(bp);
+      nroot = bp.kwant;
+      bp.omega_out = om;
+      bp.X_out = c.w_X.ensure((size_t)nci * nroot);
+      std::vector<int> order(nci);
+      std::iota(order.begin(), order.end(), 0);
+      std::stable_sort(order.begin(), order.end(),
+                       [&](int x, int y) { return ed_all[x] < ed_all[y]; });
+      bp.init_idx.assign(order.begin(), order.begin() + bp.k);
+      if (!c.ev_bready) {
+        S2G_CUDA(cudaEventCreateWithFlags(&c.ev_bready, cudaEventDisableTiming));
+        S2G_CUDA(cudaEventCreateWithFlags(&c.ev_bdone, cudaEventDisableTiming));
+      }
+      bp.ready = c.ev_bready;
+      bp.done = c.ev_bdone;
+      S2G_CUDA(cudaEventRecord(c.ev_bready, s));
+      c.batch->solve(bp);
+      S2G_CUDA(cudaStreamWaitEvent(s, c.ev_bdone, 0));
+      if (bp.status != STD2G_OK) throw Error{bp.status, bp.msg};
+      c.dav_iters = bp.iters;
+      c.dav_matvecs = 0;
+      c.dav_fp64_matvecs = bp.matvecs;
+      if (bp.nconv < nroot)
+        throw Error{STD2G_ENOCONV, "Davidson (batched): " + std::to_string(bp.nconv) + " of " +
+                                       std::to_string(nroot) + " roots converged"};
+      X = bp.X_out;
+      c.mixed.lastX = X;
+      root_resid = bp.final_resid;
+      root_ritz = bp.final_theta;
+    } else {
+      nroot = dense_eig(c, A, nci, 0.0, thr, p.nroots, om);
+      X = A;
+      c.mixed.lastX = X;
+      if (nroot < 1) throw Error{STD2G_ENOROOT, "no root below the energy threshold"};
+      // FP64 residuals ||A x - w x|| of the returned eigenvectors: A rebuilt
+      // from K, J and the diagonal (its storage now holds the eigenvectors)
+      {
+        double *Ar = c.w_Ares.ensure(n2), *Rr = c.w_Rres.ensure((size_t)nci * nroot);
+        S2G_LAUNCH(k_combine_tda, grid_for(n2), 256, 0, s, Ar, K, J, (int64_t)nci, ak, d_edall);
+        gemm(c, CUBLAS_OP_N, CUBLAS_OP_N, nci, nroot, nci, 1.0, Ar, nci, X, nci, 0.0, Rr, nci);
+        double *part = c.w_part.ensure((size_t)nroot * kColSplit), *rn = c.w_rn.ensure(nroot);
+        S2G_LAUNCH(k_dav_resid, dim3(kColSplit, (unsigned)nroot), 256, 0, s, Rr, X, om, nci, part);
+        S2G_LAUNCH(k_colnorm_finish, (int)div_up(nroot, 128), 128, 0, s, part, kColSplit, nroot,
+                   rn);
+        root_resid.assign(nroot, 0.0);
+        root_ritz.assign(nroot, 0.0);
+        S2G_CUDA(cudaMemcpyAsync(root_resid.data(), rn, sizeof(double) * nroot,
+                                 cudaMemcpyDeviceToHost, s));
+        S2G_CUDA(cudaMemcpyAsync(root_ritz.data(), om, sizeof(double) * nroot,
+                                 cudaMemcpyDeviceToHost, s));
+      }
     }
   } else {
     double *Apb = nullptr, *Amb = nullptr;
@@ -1714,6 +1775,7 @@ static void solve(Ctx &c, const std2g_params &p_in, std2g_result *res, const Res
 // ============================ C boundary =================================
 using std2g::Ctx;
 using std2g::Error;
+using std2g::BatchDavidson;
 
 static thread_local std::string g_last_error;
 
@@ -1964,6 +2026,35 @@ int std2g_set_sm_limit(void *ctx, int max_sms) {
   return STD2G_OK;
 }
 
+int std2g_batch_create(int device, void **batch) {
+  if (!batch) return STD2G_EINVAL;
+  *batch = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev)
+    return STD2G_ENODEV;
+  return guard([&] { *batch = new BatchDavidson(device); });
+}
+
+int std2g_attach_batch(void *ctx, void *batch) {
+  if (!ctx) return STD2G_EINVAL;
+  auto *c = (Ctx *)ctx;
+  auto *b = (BatchDavidson *)batch;
+  if (b && b->device() != c->opts.device) return STD2G_EINVAL;
+  c->batch = b;
+  return STD2G_OK;
+}
+
+int std2g_batch_stats(void *batch, int64_t *problems, int64_t *iterations, int64_t *members,
+                      double *ms) {
+  if (!batch || !problems || !iterations || !members) return STD2G_EINVAL;
+  ((BatchDavidson *)batch)->stats(problems, iterations, members, ms);
+  return STD2G_OK;
+}
+
+void std2g_batch_destroy(void *batch) { delete (BatchDavidson *)batch; }
+
+int std2g_last_batched(void *ctx) { return ctx ? (int)((Ctx *)ctx)->last_batched : 0; }
+
 int std2g_kernel_stats(void *ctx, double *ms, int64_t *launches, double *flop) {
   if (!ctx) return STD2G_EINVAL;
   auto *c = (Ctx *)ctx;
@@ -2117,6 +2208,8 @@ void std2g_destroy(void *ctx) {
   cudaSetDevice(c->opts.device);
   cudaStreamSynchronize(c->stream);
   for (auto &e : c->ev) cudaEventDestroy(e);
+  if (c->ev_bready) cudaEventDestroy(c->ev_bready);
+  if (c->ev_bdone) cudaEventDestroy(c->ev_bdone);
   if (c->solver_params) cusolverDnDestroyParams(c->solver_params);
   if (c->solver) cusolverDnDestroy(c->solver);
   if (c->blas) cublasDestroy(c->blas);

@@ -82,6 +82,7 @@ struct Server {
   int64_t submitted = 0, completed = 0, peak_bytes = 0;
   int peak_inflight = 0;
   int dev_sms = 148;
+  void *batch = nullptr;   // shared batched eigensolver (STD2G_FLAG_BATCH_EIGEN)
 };
 
 // Estimated device bytes of one request from the input sizes alone (the CSF
@@ -93,7 +94,7 @@ struct Server {
 // up to 320 CSFs; std2g_polarizability: matrix-free for solver 2, when the
 // dense form needs more than 24 GB, and in the mixed form (precision 1) with
 // solver 0 above 4096 CSFs).
-int64_t footprint_estimate(const Job &j, int precision) {
+int64_t footprint_estimate(const Job &j, int precision, bool batched) {
   int64_t nocc = 0;
   for (double o : j.occ)
     if (o > 1e-8) ++nocc;
@@ -109,10 +110,14 @@ int64_t footprint_estimate(const Job &j, int precision) {
                          (precision == 1 && j.par.solver == 0 && nci > 4096);
     dense |= !resp_mf;
   }
-  if (dense)
+  if (dense) {
     b += 12 * 8 * nci * nci;   // dense K, J, Kx, A+B, A-B and their work copies
-  else
+  } else {
     b += 4 * 8 * nci * 512;    // Davidson subspace and products, CG vectors
+    // a batched eigensolve (up to 6144 CSFs) builds the dense K, J, Kx, A and B
+    if (batched && j.omega.empty() && j.par.rpa == 0)
+      b += 5 * 8 * std::min<int64_t>(nci, 6144) * std::min<int64_t>(nci, 6144);
+  }
   return b;
 }
 
@@ -225,6 +230,7 @@ int renew_context(Server *s, int slot) {
   const int st = std2g_create(&ctx, &eo);
   if (st != STD2G_OK) return st;
   s->ctxs[slot] = ctx;
+  if (s->batch) std2g_attach_batch(ctx, s->batch);
   return STD2G_OK;
 }
 
@@ -323,6 +329,16 @@ int std2g_server_create(void **srv, const std2g_server_opts *o) {
     }
     s->ctxs.push_back(ctx);
   }
+  if (o->flags & STD2G_FLAG_BATCH_EIGEN) {
+    int st = std2g_batch_create(o->device, &s->batch);
+    for (void *c : s->ctxs)
+      if (st == STD2G_OK) st = std2g_attach_batch(c, s->batch);
+    if (st != STD2G_OK) {
+      for (void *c : s->ctxs) std2g_destroy(c);
+      std2g_batch_destroy(s->batch);
+      return st;
+    }
+  }
   s->alive_workers = o->slots;
   for (int k = 0; k < o->slots; ++k) s->workers.emplace_back(worker, s.get(), k);
   *srv = s.release();
@@ -364,7 +380,8 @@ int std2g_server_submit(void *srv, const std2g_request *rq, int64_t *ticket) {
   }
   if (rq->nomega > 0) j->omega = copy_of(rq->omega, (size_t)rq->nomega);
   j->par = rq->params;
-  j->footprint = footprint_estimate(*j, s->opts.precision);
+  j->footprint = footprint_estimate(*j, s->opts.precision,
+                                    (s->opts.flags & STD2G_FLAG_BATCH_EIGEN) != 0);
   j->t_submit = Clock::now();
   {
     std::lock_guard<std::mutex> lk(s->mu);
@@ -472,7 +489,20 @@ void std2g_server_destroy(void *srv) {
   for (auto &t : s->workers) t.join();
   for (void *c : s->ctxs)
     if (c) std2g_destroy(c);
+  std2g_batch_destroy(s->batch);
   delete s;
+}
+
+int std2g_server_batch_stats(void *srv, int64_t *problems, int64_t *iterations,
+                             int64_t *members, double *ms) {
+  if (!srv || !problems || !iterations || !members) return STD2G_EINVAL;
+  auto *s = (Server *)srv;
+  if (!s->batch) {
+    *problems = *iterations = *members = 0;
+    if (ms) ms[0] = ms[1] = 0.0;
+    return STD2G_OK;
+  }
+  return std2g_batch_stats(s->batch, problems, iterations, members, ms);
 }
 
 }  // extern "C"

@@ -27,7 +27,9 @@
 
 #include <cooperative_groups.h>
 
+#include <algorithm>
 #include <cmath>
+#include <vector>
 
 #include "common.cuh"
 
@@ -104,6 +106,18 @@ struct SymEigWork {
   }
 };
 
+// One problem of a batched launch (k_symeig_*_b: blockIdx.y selects the
+// problem; every kernel of the batch covers the largest member, the blocks
+// past a member's own size return early or stay idle as in a single launch).
+struct SymEigJob {
+  const double *A;
+  int lda, n, k;
+  double *w, *Z;
+  int ldz;
+  double *work;
+  int *info;
+};
+
 // ---- 1. tridiagonal reduction (Q^T A Q = T, Q = H_0 ... H_{n-3}) ----------
 // A cluster of C CTAs; CTA r holds the full columns j = r (mod C) in shared
 // memory, and every CTA also keeps the current column c (cur) and forms the
@@ -161,8 +175,8 @@ __device__ double symeig_reflector(const double *cur, int c, int n, double *v, d
 }
 
 template <int C>
-__global__ void __cluster_dims__(C, 1, 1) __launch_bounds__(kTridiagThreads, 1)
-k_symeig_tridiag(const double *__restrict__ A, int lda, int n, double *__restrict__ work) {
+__device__ __forceinline__ void
+symeig_tridiag_body(const double *__restrict__ A, int lda, int n, double *__restrict__ work) {
   namespace cg = cooperative_groups;
   cg::cluster_group cl = cg::this_cluster();
   const int rank = (int)cl.block_rank();
@@ -252,10 +266,24 @@ k_symeig_tridiag(const double *__restrict__ A, int lda, int n, double *__restric
   cl.sync();   // no CTA leaves while others may still read its shared memory
 }
 
+template <int C>
+__global__ void __cluster_dims__(C, 1, 1) __launch_bounds__(kTridiagThreads, 1)
+k_symeig_tridiag(const double *__restrict__ A, int lda, int n, double *__restrict__ work) {
+  symeig_tridiag_body<C>(A, lda, n, work);
+}
+
+// batched form: cluster blockIdx.y solves jobs[blockIdx.y]
+template <int C>
+__global__ void __cluster_dims__(C, 1, 1) __launch_bounds__(kTridiagThreads, 1)
+k_symeig_tridiag_b(const SymEigJob *__restrict__ jobs) {
+  const SymEigJob j = jobs[blockIdx.y];
+  symeig_tridiag_body<C>(j.A, j.lda, j.n, j.work);
+}
+
 // ---- 2. eigenvalues: multisection on Sturm counts, one warp per eigenvalue --
 constexpr int kSymEigWarps = 8;   // warps per CTA of phases 2 and 3
-__global__ void __launch_bounds__(kSymEigWarps * 32)
-k_symeig_values(int n, int k, const double *__restrict__ work, double *__restrict__ w) {
+__device__ __forceinline__ void
+symeig_values_body(int n, int k, const double *__restrict__ work, double *__restrict__ w) {
   extern __shared__ double sm[];
   double *d = sm, *e = sm + n, *e2 = sm + 2 * n;
   const SymEigWork g(const_cast<double *>(work), n);
@@ -286,6 +314,17 @@ k_symeig_values(int n, int k, const double *__restrict__ work, double *__restric
   if (lane == 0) w[j] = 0.5 * (a + b);
 }
 
+__global__ void __launch_bounds__(kSymEigWarps * 32)
+k_symeig_values(int n, int k, const double *__restrict__ work, double *__restrict__ w) {
+  symeig_values_body(n, k, work, w);
+}
+
+__global__ void __launch_bounds__(kSymEigWarps * 32)
+k_symeig_values_b(const SymEigJob *__restrict__ jobs) {
+  const SymEigJob j = jobs[blockIdx.y];
+  symeig_values_body(j.n, j.k, j.work, j.w);
+}
+
 // ---- 3. eigenvectors of T, one warp per cluster of close eigenvalues --------
 // Cluster threshold: eigenvalues closer than 1e-5 ||T|| are orthogonalised
 // against each other; further apart, inverse iteration alone gives vectors
@@ -295,8 +334,8 @@ __host__ __device__ inline size_t symeig_vec_smem_bytes(int n) {
   return sizeof(double) * (2 * (size_t)n + (size_t)kSymEigWarps * 6 * n);
 }
 
-__global__ void __launch_bounds__(kSymEigWarps * 32)
-k_symeig_vectors(int n, int k, double *__restrict__ work, const double *__restrict__ w) {
+__device__ __forceinline__ void
+symeig_vectors_body(int n, int k, double *__restrict__ work, const double *__restrict__ w) {
   extern __shared__ double sm[];
   double *d = sm, *e = sm + n;
   const SymEigWork g(work, n);
@@ -395,6 +434,17 @@ k_symeig_vectors(int n, int k, double *__restrict__ work, const double *__restri
   }
 }
 
+__global__ void __launch_bounds__(kSymEigWarps * 32)
+k_symeig_vectors(int n, int k, double *__restrict__ work, const double *__restrict__ w) {
+  symeig_vectors_body(n, k, work, w);
+}
+
+__global__ void __launch_bounds__(kSymEigWarps * 32)
+k_symeig_vectors_b(const SymEigJob *__restrict__ jobs) {
+  const SymEigJob j = jobs[blockIdx.y];
+  symeig_vectors_body(j.n, j.k, j.work, j.w);
+}
+
 // ---- 4. back-transformation z = H_0 ... H_{n-3} y ----------------------------
 constexpr int kBtBlock = 16;                        // reflectors staged per round
 constexpr int kBtPerLane = (kSymEigMaxN + 31) / 32;  // vector elements per lane
@@ -403,8 +453,8 @@ __host__ __device__ inline size_t symeig_bt_smem_bytes(int n) {
   return sizeof(double) * ((size_t)kBtBlock * n + kBtBlock);
 }
 
-__global__ void __launch_bounds__(kSymEigWarps * 32)
-k_symeig_backtransform(int n, int k, const double *__restrict__ work,
+__device__ __forceinline__ void
+symeig_backtransform_body(int n, int k, const double *__restrict__ work,
                        const double *__restrict__ w, double *__restrict__ Z, int ldz,
                        int *info) {
   extern __shared__ double sm[];
@@ -464,6 +514,19 @@ k_symeig_backtransform(int n, int k, const double *__restrict__ work,
   if (__any_sync(0xffffffffu, bad) && lane == 0) atomicExch(info, 1);
 }
 
+__global__ void __launch_bounds__(kSymEigWarps * 32)
+k_symeig_backtransform(int n, int k, const double *__restrict__ work,
+                       const double *__restrict__ w, double *__restrict__ Z, int ldz,
+                       int *info) {
+  symeig_backtransform_body(n, k, work, w, Z, ldz, info);
+}
+
+__global__ void __launch_bounds__(kSymEigWarps * 32)
+k_symeig_backtransform_b(const SymEigJob *__restrict__ jobs) {
+  const SymEigJob j = jobs[blockIdx.y];
+  symeig_backtransform_body(j.n, j.k, j.work, j.w, j.Z, j.ldz, j.info);
+}
+
 // host launcher: n <= kSymEigMaxN, k <= n; work: symeig_work_doubles(n, k)
 inline void symeig_small(cudaStream_t s, const double *A, int lda, int n, int k, double *w,
                          double *Z, int ldz, double *work, int *info) {
@@ -489,6 +552,56 @@ inline void symeig_small(cudaStream_t s, const double *A, int lda, int n, int k,
   S2G_LAUNCH(k_symeig_vectors, nb, kSymEigWarps * 32, symeig_vec_smem_bytes(n), s, n, k, work, w);
   S2G_LAUNCH(k_symeig_backtransform, nb, kSymEigWarps * 32, symeig_bt_smem_bytes(n), s, n, k,
              work, w, Z, ldz, info);
+}
+
+// Batched launcher: the problems of `jobs` (each n <= kSymEigMaxN, 1 <= k <= n)
+// in four launches for all of them, plus one tridiagonalisation launch per
+// cluster size.  The job table goes to `dj` (same stream: a later upload
+// waits for these kernels), from `stage` when given.
+inline void symeig_small_batched(cudaStream_t s, const std::vector<SymEigJob> &jobs,
+                                 DBuf<SymEigJob> &dj, PinnedArena *stage = nullptr) {
+  if (jobs.empty()) return;
+  std::vector<SymEigJob> ord;
+  int n4 = 0, nmax = 0, kmax = 0;
+  size_t sm4 = 0, sm8 = 0;
+  for (int pass = 0; pass < 2; ++pass)
+    for (const SymEigJob &j : jobs) {
+      if (j.n < 1 || j.n > kSymEigMaxN || j.k < 1 || j.k > j.n)
+        throw Error{STD2G_EINVAL, "symeig_small_batched: size out of range"};
+      const int C = symeig_cluster_ctas(j.n);
+      if ((pass == 0) != (C == 4)) continue;
+      ord.push_back(j);
+      if (C == 4) {
+        ++n4;
+        sm4 = std::max(sm4, symeig_smem_bytes(j.n, 4));
+      } else {
+        sm8 = std::max(sm8, symeig_smem_bytes(j.n, 8));
+      }
+      nmax = std::max(nmax, j.n);
+      kmax = std::max(kmax, j.k);
+    }
+  const int nj = (int)ord.size();
+  SymEigJob *d = dj.ensure(ord.size());
+  const void *h = stage ? stage->put(ord.data(), sizeof(SymEigJob) * ord.size()) : ord.data();
+  S2G_CUDA(cudaMemcpyAsync(d, h, sizeof(SymEigJob) * ord.size(), cudaMemcpyHostToDevice, s));
+  if (n4 > 0) {
+    S2G_CUDA(cudaFuncSetAttribute(k_symeig_tridiag_b<4>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)symeig_smem_bytes(kSymEigMaxN, 4)));
+    S2G_LAUNCH(k_symeig_tridiag_b<4>, dim3(4, n4), kTridiagThreads, sm4, s, d);
+  }
+  if (nj > n4) {
+    S2G_CUDA(cudaFuncSetAttribute(k_symeig_tridiag_b<8>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)symeig_smem_bytes(kSymEigMaxN, 8)));
+    S2G_LAUNCH(k_symeig_tridiag_b<8>, dim3(8, nj - n4), kTridiagThreads, sm8, s, d + n4);
+  }
+  S2G_CUDA(cudaFuncSetAttribute(k_symeig_vectors_b, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)symeig_vec_smem_bytes(kSymEigMaxN)));
+  const dim3 g((kmax + kSymEigWarps - 1) / kSymEigWarps, nj);
+  S2G_LAUNCH(k_symeig_values_b, g, kSymEigWarps * 32, 3 * nmax * sizeof(double), s, d);
+  S2G_LAUNCH(k_symeig_vectors_b, g, kSymEigWarps * 32, symeig_vec_smem_bytes(nmax), s, d);
+  S2G_LAUNCH(k_symeig_backtransform_b, g, kSymEigWarps * 32, symeig_bt_smem_bytes(nmax), s, d);
 }
 
 }  // namespace std2g

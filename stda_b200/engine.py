@@ -34,7 +34,8 @@ EXPORTS = [
     "std2g_server_poll", "std2g_server_wait", "std2g_server_stats", "std2g_server_destroy",
     "std2g_symeig_check", "std2g_set_sm_limit", "std2g_hyperpolarizability", "std2g_two_photon",
     "std2g_ao_integrals", "std2g_load_prims", "std2g_dgemm_check", "std2g_set_spins",
-    "std2g_set_gemm_timing", "std2g_gemm_stats",
+    "std2g_set_gemm_timing", "std2g_gemm_stats", "std2g_batch_create", "std2g_attach_batch",
+    "std2g_batch_stats", "std2g_batch_destroy", "std2g_last_batched", "std2g_server_batch_stats",
 ]
 
 
@@ -52,6 +53,7 @@ class Opts(C.Structure):
 
 FLAG_TENSOR_ALWAYS = 1
 FLAG_LIBRARY_FP64 = 2   # FP64 products through cuBLAS (library baseline)
+FLAG_BATCH_EIGEN = 4    # request server: the slots share one batched eigensolver
 
 
 class Params(C.Structure):
@@ -172,6 +174,14 @@ def library():
         lib.std2g_symeig_check.argtypes = [C.c_int, C.c_int, C.c_int, dp, dp, dp, dp]
         lib.std2g_server_destroy.argtypes = [C.c_void_p]
         lib.std2g_server_destroy.restype = None
+        i64p = C.POINTER(C.c_int64)
+        lib.std2g_server_batch_stats.argtypes = [C.c_void_p, i64p, i64p, i64p, dp]
+        lib.std2g_batch_create.argtypes = [C.c_int, C.POINTER(C.c_void_p)]
+        lib.std2g_attach_batch.argtypes = [C.c_void_p, C.c_void_p]
+        lib.std2g_batch_stats.argtypes = [C.c_void_p, i64p, i64p, i64p, dp]
+        lib.std2g_batch_destroy.argtypes = [C.c_void_p]
+        lib.std2g_batch_destroy.restype = None
+        lib.std2g_last_batched.argtypes = [C.c_void_p]
         lib.std2g_screen_noalloc.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                                               C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                               C.POINTER(Params), C.c_void_p, C.c_void_p,
@@ -594,6 +604,19 @@ class Server:
         a = alpha[:nom * 9].reshape(nom, 3, 3) if nom else None
         return sol, a, (ares[:nom] if nom else None), dict(
             queued_ms=timing[0], run_ms=timing[1], latency_ms=timing[2])
+
+    def batch_stats(self) -> dict:
+        """The shared batched eigensolver's counters (server flag
+        STD2G_FLAG_BATCH_EIGEN): problems solved, batched iterations, and the
+        mean number of problems per iteration."""
+        pr, it, mem = C.c_int64(), C.c_int64(), C.c_int64()
+        ms = np.zeros(2)
+        _check(self.lib.std2g_server_batch_stats(self.srv, C.byref(pr), C.byref(it),
+                                                 C.byref(mem), _dp(ms)))
+        n = max(1, it.value)
+        return {"problems": pr.value, "iterations": it.value,
+                "mean_batch": mem.value / n, "iteration_ms": ms[0] / n,
+                "to_first_sync_ms": ms[1] / n}
 
     def stats(self) -> dict:
         st = (C.c_int64 * 7)()
