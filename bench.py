@@ -194,15 +194,17 @@ def warm_server(srv, pool, reqs, slots):
         srv.wait(t)
 
 
-def run_server(precision, pool, reqs, arrivals, slots, device, library=True):
+def run_server(precision, pool, reqs, arrivals, slots, device, library=True, batch=False):
     """Submit reqs [(pool index, Keywords, omegas)] at the given arrival times
     (s, None = all at once) to a request server; return per-request results
     and the throughput / latency summary.  The FP64 form runs its products on
-    cuBLAS unless library is False."""
-    from stda_b200.engine import Server
-    srv = Server(device, precision, slots=slots,
-                 flags=LIB64 if precision == 0 and library else 0)
+    cuBLAS unless library is False; with batch the slots share the batched
+    eigensolver (STD2G_FLAG_BATCH_EIGEN)."""
+    from stda_b200.engine import FLAG_BATCH_EIGEN, Server
+    flags = (LIB64 if precision == 0 and library else 0) | (FLAG_BATCH_EIGEN if batch else 0)
+    srv = Server(device, precision, slots=slots, flags=flags)
     warm_server(srv, pool, reqs, slots)
+    b0 = srv.batch_stats()
     t0 = time.perf_counter()
     tickets = []
     for k, (i, kw, om) in enumerate(reqs):
@@ -214,12 +216,23 @@ def run_server(precision, pool, reqs, arrivals, slots, device, library=True):
     res = [srv.wait(t) for t in tickets]
     makespan = time.perf_counter() - t0
     st = srv.stats()
+    b1 = srv.batch_stats()
     srv.close()
     lat = [r[3]["latency_ms"] for r in res]
-    return res, {"solves_per_s": len(reqs) / makespan, "makespan_s": makespan,
-                 "latency_ms": {"p50": float(np.percentile(lat, 50)),
-                                "p99": float(np.percentile(lat, 99))},
-                 "peak_in_flight": st["peak_in_flight"], "slots": slots}
+    out = {"solves_per_s": len(reqs) / makespan, "makespan_s": makespan,
+           "latency_ms": {"p50": float(np.percentile(lat, 50)),
+                          "p99": float(np.percentile(lat, 99))},
+           "peak_in_flight": st["peak_in_flight"], "slots": slots}
+    if batch:
+        it = b1["iterations"] - b0["iterations"]
+        out["batched_eigensolve"] = {
+            "problems": b1["problems"] - b0["problems"], "iterations": it,
+            "mean_problems_per_iteration":
+                (b1["mean_batch"] * b1["iterations"] - b0["mean_batch"] * b0["iterations"])
+                / max(it, 1),
+            "iteration_ms": (b1["iteration_ms"] * b1["iterations"]
+                             - b0["iteration_ms"] * b0["iterations"]) / max(it, 1)}
+    return res, out
 
 
 def served_saturation(precision, pool, reqs, slots, device, rates=(8, 16, 32, 64, 128),
@@ -403,13 +416,15 @@ def served_and_batched(device, args):
     arrivals = np.cumsum(rng.exponential(1.0 / args.serve_rate, len(reqs)))
     rm, sm = run_server(1, pool, reqs, arrivals, args.slots, device)
     rd, sd = run_server(0, pool, reqs, arrivals, args.slots, device)
+    rbs, sbs = run_server(1, pool, reqs, arrivals, args.slots, device, batch=True)
     sat_m = served_saturation(1, pool, reqs, args.slots, device)
     sat_d = served_saturation(0, pool, reqs, args.slots, device)
     out["served"] = {"workload": f"{len(reqs)} requests, Poisson {args.serve_rate}/s, "
                                  f"{len(pool)} molecules of {int(atoms.min())}-{int(atoms.max())} "
                                  "atoms (lognormal, median 60), E_thr 6.5 eV, 32 roots (residual 1e-7), "
                                  "20 % with alpha(w) at 3 w",
-                     "mixed": sm, "fp64": sd,
+                     "mixed": sm, "fp64": sd, "mixed_batched_eigensolve": sbs,
+                     "accuracy_batched_eigensolve_vs_fp64": compare_forms(rbs, rd),
                      "p99_ratio_fp64_over_mixed": sd["latency_ms"]["p99"] / sm["latency_ms"]["p99"],
                      "saturation": {"mixed": sat_m, "fp64": sat_d,
                                     "ratio_mixed_over_fp64":
@@ -425,14 +440,18 @@ def served_and_batched(device, args):
     rm, bm = run_server(1, pool, reqs, None, args.slots, device)
     rd, bd = run_server(0, pool, reqs, None, args.slots, device)
     _, bo = run_server(0, pool, reqs, None, args.slots, device, library=False)
-    for prec, lib, key in ((1, True, "m"), (0, True, "d"), (0, False, "o")):
-        _, again = run_server(prec, pool, reqs, None, args.slots, device, library=lib)
+    rb, bb = run_server(1, pool, reqs, None, args.slots, device, batch=True)
+    for prec, lib, key in ((1, True, "m"), (0, True, "d"), (0, False, "o"), (1, True, "b")):
+        _, again = run_server(prec, pool, reqs, None, args.slots, device, library=lib,
+                              batch=key == "b")
         if key == "m" and again["solves_per_s"] > bm["solves_per_s"]:
             bm = again
         elif key == "d" and again["solves_per_s"] > bd["solves_per_s"]:
             bd = again
         elif key == "o" and again["solves_per_s"] > bo["solves_per_s"]:
             bo = again
+        elif key == "b" and again["solves_per_s"] > bb["solves_per_s"]:
+            bb = again
     plain = plain_fp64(pool, reqs[:len(pool)], device)
     out["batched"] = {"workload": f"{len(reqs)} molecules ({len(pool)} distinct, "
                                   f"{int(atoms.min())}-{int(atoms.max())} atoms log-uniform), "
@@ -448,7 +467,13 @@ def served_and_batched(device, args):
                               "'fp64' runs it on cuBLAS",
                       "speedup_mixed_served_vs_fp64_plain":
                           bm["solves_per_s"] / plain["solves_per_s"],
+                      "mixed_batched_eigensolve": bb,
+                      "speedup_batched_eigensolve_vs_fp64_same_slots":
+                          bb["solves_per_s"] / bd["solves_per_s"],
+                      "speedup_batched_eigensolve_vs_fp64_plain":
+                          bb["solves_per_s"] / plain["solves_per_s"],
                       "accuracy": compare_forms(rm, rd),
+                      "accuracy_batched_eigensolve_vs_fp64": compare_forms(rb, rd),
                       "nci_range": [int(min(r[0].nci for r in rm)), int(max(r[0].nci for r in rm))]}
     return out
 
