@@ -205,28 +205,40 @@ static void sqrt_overlap(Ctx &c, const double *S, int n, double *out) {
   cudaStream_t s = c.stream;
   const size_t nn = (size_t)n * n;
   double *A = c.w_tmp.ensure(nn * 4), *Z = A + nn, *P = A + 2 * nn, *T = A + 3 * nn;
-  auto *flags = (unsigned long long *)c.w_ns.ensure(2);
-  S2G_CUDA(cudaMemsetAsync(flags, 0, 2 * sizeof(unsigned long long), s));
+  // steps run in groups of kGroup between host reads of their errors (one
+  // synchronisation per group); steps past convergence stay at the fixed
+  // point Z A Z = I to rounding and are harmless
+  constexpr int kGroup = 3;
+  auto *flags = (unsigned long long *)c.w_ns.ensure(1 + kGroup);
+  S2G_CUDA(cudaMemsetAsync(flags, 0, (1 + kGroup) * sizeof(unsigned long long), s));
   S2G_LAUNCH(k_row_abs_max, (int)div_up(n, 256), 256, 0, s, S, n, flags);
   S2G_LAUNCH(k_ns_init, grid_for((int64_t)nn), 256, 0, s, A, Z, S, n, flags);
-  unsigned long long h[2] = {0, 0};
+  unsigned long long h[1 + kGroup] = {0};
   double err = 1.0, prev = 2.0;
   int it = 0;
   // quadratic convergence ends at the rounding level of the products: stop at
   // 1e-14, or once below 1e-10 a step no longer halves the error
-  for (; it < 100 && err >= 1e-14 && !(err < 1e-10 && err > 0.5 * prev); ++it) {
-    prev = err;
-    gemm(c, CUBLAS_OP_N, CUBLAS_OP_N, n, n, n, 1.0, A, n, Z, n, 0.0, P, n);   // P = A Z
-    gemm(c, CUBLAS_OP_N, CUBLAS_OP_N, n, n, n, 1.0, Z, n, P, n, 0.0, T, n);   // T = Z A Z
-    S2G_CUDA(cudaMemsetAsync(flags + 1, 0, sizeof(unsigned long long), s));
-    S2G_LAUNCH(k_ns_step, grid_for((int64_t)nn), 256, 0, s, T, n, flags + 1);
-    gemm(c, CUBLAS_OP_N, CUBLAS_OP_N, n, n, n, 1.0, T, n, Z, n, 0.0, P, n);   // Z <- T Z
-    std::swap(Z, P);
+  bool done = false;
+  while (!done && it < 99) {
+    S2G_CUDA(cudaMemsetAsync(flags + 1, 0, kGroup * sizeof(unsigned long long), s));
+    for (int q = 0; q < kGroup; ++q) {
+      gemm(c, CUBLAS_OP_N, CUBLAS_OP_N, n, n, n, 1.0, A, n, Z, n, 0.0, P, n);   // P = A Z
+      gemm(c, CUBLAS_OP_N, CUBLAS_OP_N, n, n, n, 1.0, Z, n, P, n, 0.0, T, n);   // T = Z A Z
+      S2G_LAUNCH(k_ns_step, grid_for((int64_t)nn), 256, 0, s, T, n, flags + 1 + q);
+      gemm(c, CUBLAS_OP_N, CUBLAS_OP_N, n, n, n, 1.0, T, n, Z, n, 0.0, P, n);   // Z <- T Z
+      std::swap(Z, P);
+    }
     S2G_CUDA(cudaMemcpyAsync(h, flags, sizeof(h), cudaMemcpyDeviceToHost, s));
     S2G_CUDA(cudaStreamSynchronize(s));
-    std::memcpy(&err, &h[1], sizeof(double));
-    if (!std::isfinite(err) || err > 1e6) break;
+    for (int q = 0; q < kGroup && !done; ++q) {
+      prev = err;
+      std::memcpy(&err, &h[1 + q], sizeof(double));
+      ++it;
+      if (!std::isfinite(err) || err > 1e6 || err < 1e-14 || (err < 1e-10 && err > 0.5 * prev))
+        done = true;
+    }
   }
+  it = (it + kGroup - 1) / kGroup * kGroup;   // steps executed
   c.ns_iters = it;
   double cmax;
   std::memcpy(&cmax, &h[0], sizeof(double));

@@ -526,59 +526,74 @@ __global__ void k_pt2_bound_finish(const double *__restrict__ colbnd, int nchunk
 // FP64 PT sum for candidate rows near the threshold (ptselect stda.f:1805-1834),
 // couplings as gathered FP64 dot products over atoms.  Grid (nrc, nsplit):
 // block (q, y) sums the primaries c = y*8 + warp, + nsplit*8, ...
-__global__ void k_pt_recheck(const int *__restrict__ rows, int nrc, const int *__restrict__ cand_k,
+// rows r in [r0, r1) whose sum lies within its bound of thrp (|pert - thrp| <=
+// bnd, NaN included) are appended to list (count *cnt; the order of the
+// entries varies, each row's result does not depend on it)
+__global__ void k_pt_recheck_rows(const double *__restrict__ pert, const double *__restrict__ bnd,
+                                  int r0, int r1, double thrp, int *__restrict__ list,
+                                  int *__restrict__ cnt) {
+  for (int r = r0 + blockIdx.x * blockDim.x + threadIdx.x; r < r1; r += gridDim.x * blockDim.x)
+    if (!(fabs(pert[r] - thrp) > bnd[r])) list[atomicAdd(cnt, 1)] = r;
+}
+
+// FP64 PT sums of the listed rows (*nrc of them; blocks x walk the list)
+__global__ void k_pt_recheck(const int *__restrict__ rows, const int *__restrict__ nrc,
+                             const int *__restrict__ cand_k,
                              const int *__restrict__ pk, int nex, const double *__restrict__ Pia,
                              const double *__restrict__ Qia, const double *__restrict__ Poo,
                              const double *__restrict__ Qvv, int N, int no, int nv,
                              const double *__restrict__ de_all, const double *__restrict__ ed,
                              double ak, double *__restrict__ part) {
-  int q = blockIdx.x;
-  if (q >= nrc) return;
-  int r = rows[q];
-  int k = cand_k[r];
-  int i = k / nv, a = k - i * nv;
-  double de_r = de_all[k];
-  const double *pr = Pia + (int64_t)N * k;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarp = blockDim.x >> 5;
-  double s = 0.0;   // meaningful in lane 0 of each warp
-  for (int c = blockIdx.y * nwarp + warp; c < nex; c += gridDim.y * nwarp) {
-    int kc = pk[c];
-    int j = kc / nv, b = kc - j * nv;
-    const double *qc = Qia + (int64_t)N * kc;
-    const double *pij = Poo + (int64_t)N * ((int64_t)i * no + j);
-    const double *qab = Qvv + (int64_t)N * ((int64_t)a * nv + b);
-    double kv = 0.0, jv = 0.0;
-    for (int A = lane; A < N; A += 32) {
-      kv += pr[A] * qc[A];
-      jv += pij[A] * qab[A];
+  const int n_rows = *nrc;
+  for (int q = blockIdx.x; q < n_rows; q += gridDim.x) {
+    int r = rows[q];
+    int k = cand_k[r];
+    int i = k / nv, a = k - i * nv;
+    double de_r = de_all[k];
+    const double *pr = Pia + (int64_t)N * k;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarp = blockDim.x >> 5;
+    double s = 0.0;   // meaningful in lane 0 of each warp
+    for (int c = blockIdx.y * nwarp + warp; c < nex; c += gridDim.y * nwarp) {
+      int kc = pk[c];
+      int j = kc / nv, b = kc - j * nv;
+      const double *qc = Qia + (int64_t)N * kc;
+      const double *pij = Poo + (int64_t)N * ((int64_t)i * no + j);
+      const double *qab = Qvv + (int64_t)N * ((int64_t)a * nv + b);
+      double kv = 0.0, jv = 0.0;
+      for (int A = lane; A < N; A += 32) {
+        kv += pr[A] * qc[A];
+        jv += pij[A] * qab[A];
+      }
+      for (int o = 16; o > 0; o >>= 1) {
+        kv += __shfl_xor_sync(0xffffffffu, kv, o);
+        jv += __shfl_xor_sync(0xffffffffu, jv, o);
+      }
+      double amat = ak * kv - jv;
+      s += amat * amat / (de_r - ed[c] + 1e-10);
     }
-    for (int o = 16; o > 0; o >>= 1) {
-      kv += __shfl_xor_sync(0xffffffffu, kv, o);
-      jv += __shfl_xor_sync(0xffffffffu, jv, o);
+    __shared__ double red[32];
+    if (lane == 0) red[warp] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t = 0.0;
+      for (int w = 0; w < nwarp; ++w) t += red[w];
+      part[(int64_t)q * gridDim.y + blockIdx.y] = t;
     }
-    double amat = ak * kv - jv;
-    s += amat * amat / (de_r - ed[c] + 1e-10);
-  }
-  __shared__ double red[32];
-  if (lane == 0) red[warp] = s;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double t = 0.0;
-    for (int w = 0; w < nwarp; ++w) t += red[w];
-    part[(int64_t)q * gridDim.y + blockIdx.y] = t;
+    __syncthreads();
   }
 }
 
 // pert[rows[q]] = sum_y part[q][y] (fixed order); selection pert > thrp
-__global__ void k_pt_recheck_finish(const int *__restrict__ rows, int nrc, int nsplit,
-                                    const double *__restrict__ part, double thrp,
+__global__ void k_pt_recheck_finish(const int *__restrict__ rows, const int *__restrict__ nrc,
+                                    int nsplit, const double *__restrict__ part, double thrp,
                                     double *__restrict__ pert_out, unsigned char *__restrict__ sel) {
-  int q = blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= nrc) return;
-  double t = 0.0;
-  for (int y = 0; y < nsplit; ++y) t += part[(int64_t)q * nsplit + y];
-  pert_out[rows[q]] = t;
-  sel[rows[q]] = t > thrp ? 1 : 0;
+  const int n_rows = *nrc;
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n_rows; q += gridDim.x * blockDim.x) {
+    double t = 0.0;
+    for (int y = 0; y < nsplit; ++y) t += part[(int64_t)q * nsplit + y];
+    pert_out[rows[q]] = t;
+    sel[rows[q]] = t > thrp ? 1 : 0;
+  }
 }
 
 // ---------------------------------------------------------------- driver
@@ -597,14 +612,16 @@ struct MixedWork {
   int64_t rechecked = 0;
   double ms = 0, flop = 0;
   int64_t launches = 0;
-  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  // per chunk: events around its two contractions (read after the final
+  // synchronisation) and its count of FP64-rechecked rows
+  std::vector<cudaEvent_t> tev;
+  DBuf<int> recheck_cnt;
   // optional per-step timing (synchronises): operands, (ia|jb), (ij|ab), row
   // pass, FP64 recheck, column pass
   bool profile = false;
   double sec_ms[6] = {0, 0, 0, 0, 0, 0};
   ~MixedWork() {
-    if (e0) cudaEventDestroy(e0);
-    if (e1) cudaEventDestroy(e1);
+    for (cudaEvent_t e : tev) cudaEventDestroy(e);
   }
 };
 
@@ -635,10 +652,6 @@ inline void mixed_pt_select(MixedWork &mw, cudaStream_t s, const PtProblem &pb,
   mw.rechecked = 0;
   mw.ms = mw.flop = 0;
   mw.launches = 0;
-  if (!mw.e0) {
-    S2G_CUDA(cudaEventCreate(&mw.e0));
-    S2G_CUDA(cudaEventCreate(&mw.e1));
-  }
   for (double &v : mw.sec_ms) v = 0;
   auto t_last = std::chrono::steady_clock::now();
   auto tick = [&](int slot) {
@@ -724,8 +737,17 @@ inline void mixed_pt_select(MixedWork &mw, cudaStream_t s, const PtProblem &pb,
   double *colpart = mw.colpart.ensure((size_t)nchunk * nex);
   double *colbnd = mw.colbnd.ensure((size_t)nchunk * nex);
   double *bnd = mw.bnd.ensure(std::max(nexpt, 1));
-  std::vector<double> h_pert, h_bnd;
-  std::vector<int> rows;
+  // rows to recheck, listed on the device per chunk (no host round trip
+  // between the chunks)
+  int *d_rlist = mw.recheck.ensure(std::max(nexpt, 1));
+  int *d_rcnt = mw.recheck_cnt.ensure(nchunk);
+  S2G_CUDA(cudaMemsetAsync(d_rcnt, 0, sizeof(int) * nchunk, s));
+  const int nsplit_rc = (int)std::max<int64_t>(1, std::min<int64_t>(div_up(nex, 64), 128));
+  while (mw.tev.size() < 2 * (size_t)nchunk) {
+    cudaEvent_t e;
+    S2G_CUDA(cudaEventCreate(&e));
+    mw.tev.push_back(e);
+  }
   int r_begin = 0;
   for (int ch = 0; ch < nchunk; ++ch) {
     const int i0 = ch * occ_chunk, ni = std::min(occ_chunk, no - i0);
@@ -750,7 +772,7 @@ inline void mixed_pt_select(MixedWork &mw, cudaStream_t s, const PtProblem &pb,
     const size_t nbuf = (size_t)nex * ni * nva;
     float *K = mw.K.ensure(nbuf), *J = mw.J.ensure(nbuf);
     const double fl = 2.0 * ni * (double)nv * nex * N;
-    S2G_CUDA(cudaEventRecord(mw.e0, s));
+    S2G_CUDA(cudaEventRecord(mw.tev[2 * ch], s));
     PairTiles tk{0,       ni,      nv,      nva,   nex,          nab, nqb, 0,
                  (int64_t)ni * nab * nqb, nullptr, nullptr, nullptr, a_inv, mw.qinv.get()};
     mw.tc.run_direct<PairTiles, true>(s, mw.a_hi.get(), mw.a_lo.get(), (int64_t)ni * nv,
@@ -762,7 +784,7 @@ inline void mixed_pt_select(MixedWork &mw, cudaStream_t s, const PtProblem &pb,
     mw.tc.run_direct<PairTiles, true>(s, mw.v_hi.get(), mw.v_lo.get(), (int64_t)ng * nv,
                                       mw.w_hi.get(), mw.w_lo.get(), rows_w, Kpad, tj, tj.ntiles,
                                       J, fl);
-    S2G_CUDA(cudaEventRecord(mw.e1, s));
+    S2G_CUDA(cudaEventRecord(mw.tev[2 * ch + 1], s));
     tick(2);
     mw.flop += 2 * fl;
     mw.launches += 2;
@@ -779,37 +801,18 @@ inline void mixed_pt_select(MixedWork &mw, cudaStream_t s, const PtProblem &pb,
                bnd, sel);
     // candidates whose sum lies within its bound of thrp: FP64
     const int nr = r_end - r_begin;
-    h_pert.resize(nr);
-    h_bnd.resize(nr);
-    if (nr > 0) {
-      S2G_CUDA(cudaMemcpyAsync(h_pert.data(), pert + r_begin, sizeof(double) * nr,
-                               cudaMemcpyDeviceToHost, s));
-      S2G_CUDA(cudaMemcpyAsync(h_bnd.data(), bnd + r_begin, sizeof(double) * nr,
-                               cudaMemcpyDeviceToHost, s));
-    }
-    S2G_CUDA(cudaStreamSynchronize(s));
     tick(3);
-    {
-      float tms = 0;
-      S2G_CUDA(cudaEventElapsedTime(&tms, mw.e0, mw.e1));
-      mw.ms += tms;
-    }
     if (nr > 0) {
-      rows.clear();
-      for (int r = 0; r < nr; ++r)
-        if (!(std::fabs(h_pert[r] - pb.thrp) > h_bnd[r])) rows.push_back(r_begin + r);
-      if (!rows.empty()) {
-        const int nrc = (int)rows.size();
-        int *d_rows = up(mw.recheck, rows);
-        const int nsplit = (int)std::max<int64_t>(1, std::min<int64_t>(div_up(nex, 64), 128));
-        double *part = mw.recheck_part.ensure((size_t)nrc * nsplit);
-        S2G_LAUNCH(k_pt_recheck, dim3((unsigned)nrc, (unsigned)nsplit), 256, 0, s, d_rows, nrc,
-                   d_ck, d_pk, nex, pb.Pia, pb.Qia, pb.Poo, pb.Qvv, N, no, nv, pb.de_all, d_ed,
-                   pb.ak, part);
-        S2G_LAUNCH(k_pt_recheck_finish, (int)div_up(nrc, 128), 128, 0, s, d_rows, nrc, nsplit,
-                   part, pb.thrp, pert, sel);
-        mw.rechecked += nrc;
-      }
+      int *rl = d_rlist + r_begin;
+      S2G_LAUNCH(k_pt_recheck_rows, (int)std::min<int64_t>(div_up(nr, 256), 148 * 8), 256, 0, s,
+                 pert, bnd, r_begin, r_end, pb.thrp, rl, d_rcnt + ch);
+      double *part = mw.recheck_part.ensure((size_t)nr * nsplit_rc);
+      const int gq = std::min(nr, 1024);
+      S2G_LAUNCH(k_pt_recheck, dim3((unsigned)gq, (unsigned)nsplit_rc), 256, 0, s, rl,
+                 d_rcnt + ch, d_ck, d_pk, nex, pb.Pia, pb.Qia, pb.Poo, pb.Qvv, N, no, nv,
+                 pb.de_all, d_ed, pb.ak, part);
+      S2G_LAUNCH(k_pt_recheck_finish, (int)div_up(std::min(nr, 1024 * 128), 128), 128, 0, s, rl,
+                 d_rcnt + ch, nsplit_rc, part, pb.thrp, pert, sel);
     }
     tick(4);
     // column sums over the candidates that stay out
@@ -827,9 +830,17 @@ inline void mixed_pt_select(MixedWork &mw, cudaStream_t s, const PtProblem &pb,
   S2G_CUDA(cudaMemsetAsync(mb, 0, sizeof(unsigned long long), s));
   S2G_LAUNCH(k_pt2_bound_finish, (int)div_up(nex, 128), 128, 0, s, colbnd, nchunk, nex, mb);
   double h_mb = 0.0;
+  std::vector<int> h_cnt(nchunk);
   S2G_CUDA(cudaMemcpyAsync(&h_mb, mb, sizeof(double), cudaMemcpyDeviceToHost, s));
+  S2G_CUDA(cudaMemcpyAsync(h_cnt.data(), d_rcnt, sizeof(int) * nchunk, cudaMemcpyDeviceToHost, s));
   S2G_CUDA(cudaStreamSynchronize(s));
   mw.ed_bound_max = h_mb;
+  for (int ch = 0; ch < nchunk; ++ch) {
+    float tms = 0;
+    S2G_CUDA(cudaEventElapsedTime(&tms, mw.tev[2 * ch], mw.tev[2 * ch + 1]));
+    mw.ms += tms;
+    mw.rechecked += h_cnt[ch];
+  }
 }
 
 }  // namespace std2g
