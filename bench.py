@@ -416,7 +416,7 @@ def served_and_batched(device, args):
     arrivals = np.cumsum(rng.exponential(1.0 / args.serve_rate, len(reqs)))
     rm, sm = run_server(1, pool, reqs, arrivals, args.slots, device)
     rd, sd = run_server(0, pool, reqs, arrivals, args.slots, device)
-    rbs, sbs = run_server(1, pool, reqs, arrivals, args.slots, device, batch=True)
+    rbs, sbs = run_server(1, pool, reqs, arrivals, args.batch_slots, device, batch=True)
     sat_m = served_saturation(1, pool, reqs, args.slots, device)
     sat_d = served_saturation(0, pool, reqs, args.slots, device)
     out["served"] = {"workload": f"{len(reqs)} requests, Poisson {args.serve_rate}/s, "
@@ -440,10 +440,11 @@ def served_and_batched(device, args):
     rm, bm = run_server(1, pool, reqs, None, args.slots, device)
     rd, bd = run_server(0, pool, reqs, None, args.slots, device)
     _, bo = run_server(0, pool, reqs, None, args.slots, device, library=False)
-    rb, bb = run_server(1, pool, reqs, None, args.slots, device, batch=True)
+    rb, bb = run_server(1, pool, reqs, None, args.batch_slots, device, batch=True)
     for prec, lib, key in ((1, True, "m"), (0, True, "d"), (0, False, "o"), (1, True, "b")):
-        _, again = run_server(prec, pool, reqs, None, args.slots, device, library=lib,
-                              batch=key == "b")
+        _, again = run_server(prec, pool, reqs, None,
+                              args.batch_slots if key == "b" else args.slots, device,
+                              library=lib, batch=key == "b")
         if key == "m" and again["solves_per_s"] > bm["solves_per_s"]:
             bm = again
         elif key == "d" and again["solves_per_s"] > bd["solves_per_s"]:
@@ -516,6 +517,8 @@ def main():
     ap.add_argument("--no-serve", action="store_true",
                     help="skip the served-stream and batch measurements")
     ap.add_argument("--slots", type=int, default=8, help="request-server contexts")
+    ap.add_argument("--batch-slots", type=int, default=16,
+                    help="request-server contexts of the batched-eigensolve runs")
     ap.add_argument("--serve-rate", type=float, default=8.0, help="Poisson arrivals per second")
     ap.add_argument("--serve-requests", type=int, default=120)
     ap.add_argument("--serve-pool", type=int, default=24)

@@ -84,6 +84,7 @@ struct Ctx {
   // response vectors, and the work arrays of the M Y products
   DBuf<double> w_To, w_moo, w_mvv, w_Uall, w_Vall, w_qx, w_qy, w_qbox, w_qmy, w_qsel, w_qg,
       w_tpx, w_tpy;
+  DBuf<double> w_jbox;   // (ij|ab) / (ib|ja) box of the dense build
   DBuf<int> w_info;
   DBuf<char> w_cub;
   MixedWork mixed;
@@ -1308,12 +1309,36 @@ static void solve(Ctx &c, const std2g_params &p_in, std2g_result *res, const Res
     K = c.w_K.ensure(n2);
     J = c.w_J.ensure(n2);
     gemm(c, CUBLAS_OP_T, CUBLAS_OP_N, nci, nci, N, 1.0, Ps, N, Qs, N, 0.0, K, nci);
-    S2G_LAUNCH(k_pairdot, grid_for(n2 * 32), 256, 0, s, J, (int64_t)nci, d_ci, d_ca, nci, Poo,
-               Qvv, N, no, nv, 0);
+    // J (and the exchange couplings Kx) gathered from the box of all
+    // (ij|ab) ((ib|ja)) formed by one FP64 GEMM (an (i j) x (a b) product of
+    // N-long dots) while the box stays within kBoxMax doubles and within 16x
+    // the nci^2 elements wanted; otherwise one gathered dot (2N loads) per
+    // element
+    constexpr double kBoxMax = 1.5e8;
+    const int64_t noo = (int64_t)no * no, nvv = (int64_t)nv * nv;
+    auto box_pays = [&](double cells) { return cells <= kBoxMax && cells <= 16.0 * (double)n2; };
+    if (box_pays((double)noo * (double)nvv)) {
+      double *box = c.w_jbox.ensure((size_t)(noo * nvv));
+      gemm(c, CUBLAS_OP_T, CUBLAS_OP_N, (int)noo, (int)nvv, N, 1.0, Poo, N, Qvv, N, 0.0, box,
+           (int)noo);
+      S2G_LAUNCH(k_box_gather, grid_for(n2), 256, 0, s, J, (int64_t)nci, box, d_ci, d_ca, nci,
+                 no, nv, 0);
+    } else {
+      S2G_LAUNCH(k_pairdot, grid_for(n2 * 32), 256, 0, s, J, (int64_t)nci, d_ci, d_ca, nci, Poo,
+                 Qvv, N, no, nv, 0);
+    }
     if (p.rpa || p.velcorr) {
       Kx = c.w_Kx.ensure(n2);
-      S2G_LAUNCH(k_pairdot, grid_for(n2 * 32), 256, 0, s, Kx, (int64_t)nci, d_ci, d_ca, nci, Pia,
-                 Qia, N, no, nv, 1);
+      if (box_pays((double)nov * (double)nov)) {
+        double *box = c.w_jbox.ensure((size_t)(nov * nov));
+        gemm(c, CUBLAS_OP_T, CUBLAS_OP_N, (int)nov, (int)nov, N, 1.0, Pia, N, Qia, N, 0.0, box,
+             (int)nov);
+        S2G_LAUNCH(k_box_gather, grid_for(n2), 256, 0, s, Kx, (int64_t)nci, box, d_ci, d_ca,
+                   nci, no, nv, 1);
+      } else {
+        S2G_LAUNCH(k_pairdot, grid_for(n2 * 32), 256, 0, s, Kx, (int64_t)nci, d_ci, d_ca, nci,
+                   Pia, Qia, N, no, nv, 1);
+      }
     }
   } else {
     // matrix-free operators (matfree.cuh): padded Loewdin MOs, atom-major P

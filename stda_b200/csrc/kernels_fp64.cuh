@@ -577,6 +577,27 @@ __global__ void k_pairdot(double *__restrict__ out, int64_t ld, const int *__res
   }
 }
 
+// The same couplings gathered from a box of all of them, formed by one GEMM
+// (J: box[(i j) + no^2 (a b)] = p_ij . q_ab, the (ij) x (ab) product of the
+// gamma^J-contracted occupied pairs with the virtual pairs; mode 1, exchange:
+// box[(i b) + nov (j a)] = p_ib . q_ja):
+//   mode 0: out[u + ld v] = (i_u j_v | a_u b_v)
+//   mode 1: out[u + ld v] = (i_u b_v | j_v a_u)
+__global__ void k_box_gather(double *__restrict__ out, int64_t ld, const double *__restrict__ box,
+                             const int *__restrict__ ci, const int *__restrict__ ca, int nci,
+                             int no, int nv, int mode) {
+  const int64_t total = (int64_t)nci * nci;
+  const int64_t noo = (int64_t)no * no, nov = (int64_t)no * nv;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int v = (int)(t / nci), u = (int)(t - (int64_t)v * nci);
+    const int64_t o = mode == 0
+                          ? ((int64_t)ci[u] * no + ci[v]) + noo * ((int64_t)ca[u] * nv + ca[v])
+                          : ((int64_t)ci[u] * nv + ca[v]) + nov * ((int64_t)ci[v] * nv + ca[u]);
+    out[u + ld * v] = box[o];
+  }
+}
+
 // A = ak*K - J off the diagonal, A_uu = ed_u (rtdamat stda.f:2044-2051)
 __global__ void k_combine_tda(double *__restrict__ A, const double *__restrict__ K,
                               const double *__restrict__ J, int64_t n, double ak,

@@ -110,13 +110,15 @@ int64_t footprint_estimate(const Job &j, int precision, bool batched) {
                          (precision == 1 && j.par.solver == 0 && nci > 4096);
     dense |= !resp_mf;
   }
+  // the (ij|ab) / (ib|ja) box of a dense build (at most 1.5e8 doubles)
+  const int64_t box = 8 * std::min<int64_t>(150000000LL, pairs * pairs);
   if (dense) {
-    b += 12 * 8 * nci * nci;   // dense K, J, Kx, A+B, A-B and their work copies
+    b += 12 * 8 * nci * nci + box;   // dense K, J, Kx, A+B, A-B, work copies, box
   } else {
     b += 4 * 8 * nci * 512;    // Davidson subspace and products, CG vectors
     // a batched eigensolve (up to 6144 CSFs) builds the dense K, J, Kx, A and B
     if (batched && j.omega.empty() && j.par.rpa == 0)
-      b += 5 * 8 * std::min<int64_t>(nci, 6144) * std::min<int64_t>(nci, 6144);
+      b += 5 * 8 * std::min<int64_t>(nci, 6144) * std::min<int64_t>(nci, 6144) + box;
   }
   return b;
 }
