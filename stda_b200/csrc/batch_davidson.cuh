@@ -465,6 +465,8 @@ inline void BatchDavidson::loop() {
         act.push_back(p);
       } catch (const Error &e) {
         fail(p, e);
+      } catch (const std::exception &e) {
+        fail(p, Error{STD2G_ECUDA, e.what()});
       }
     }
     if (act.empty()) continue;

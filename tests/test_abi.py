@@ -74,6 +74,24 @@ def test_server_arguments_checked_before_any_device_call():
     lib.std2g_server_destroy(None)       # a null server is ignored
 
 
+def test_batch_arguments_checked_before_any_device_call():
+    """The batched-eigensolve entry points reject null arguments and bad
+    devices without touching a device (and so without a GPU)."""
+    from stda_b200 import engine
+    lib = engine.library()
+    one = ctypes.c_int64()
+    assert lib.std2g_batch_create(0, None) == 1
+    b = ctypes.c_void_p()
+    assert lib.std2g_batch_create(-1, ctypes.byref(b)) == 12 and not b.value
+    assert lib.std2g_attach_batch(None, None) == 1
+    assert lib.std2g_batch_stats(None, ctypes.byref(one), ctypes.byref(one),
+                                 ctypes.byref(one), None) == 1
+    assert lib.std2g_server_batch_stats(None, ctypes.byref(one), ctypes.byref(one),
+                                        ctypes.byref(one), None) == 1
+    assert lib.std2g_last_batched(None) == 0
+    lib.std2g_batch_destroy(None)         # a null batch is ignored
+
+
 C_HOST = r"""
 #include <stdio.h>
 #include <string.h>
