@@ -479,6 +479,28 @@ def served_and_batched(device, args):
     return out
 
 
+def batched_sharded(dist, local, world, rank, args):
+    """The batch configuration on `world` GPUs: the requests split by
+    shard_by_cost (cost ~ nao^2 of the molecule) over the ranks, each rank
+    solving its share through its own request server (mixed form, batched
+    eigensolve); whole-job solves/s = all requests / the slowest rank's time."""
+    from stda_b200 import replicas
+    from stda_b200.engine import Keywords
+    dev = f"cuda:{local}"
+    atoms, pool = molecule_pool("batch", args.batch_pool, seed=3)
+    kw = Keywords(ax=0.5, e_thr_ev=6.5, nroots=20, conv_tol=1e-7)
+    reqs = [(k % len(pool), kw, None) for k in range(args.batch_requests)]
+    mine = replicas.shard_by_cost([float(pool[i].nao) ** 2 for i, _, _ in reqs], world)[rank]
+    replicas.barrier(dist, dev)
+    _, st = run_server(1, pool, [reqs[q] for q in mine], None, args.batch_slots, local,
+                       batch=True)
+    span = replicas.max_over_ranks(dist, st["makespan_s"], dev)
+    return {"workload": f"{len(reqs)} molecules of the batch configuration split over "
+                        f"{world} GPUs by nao^2 (longest-processing-time bin-pack)",
+            "solves_per_s": len(reqs) / span, "slowest_rank_s": span,
+            "requests_this_rank": len(mine)}
+
+
 def run_reference(args):
     if int(os.environ.get("RANK", "0")) != 0:
         return
@@ -706,6 +728,12 @@ def main():
         eng.close()
         out.update(response_cfg2(local))
         out.update(served_and_batched(local, args))
+
+    if world > 1 and not args.no_serve:
+        # the batch of independent molecules split over the ranks (no data-path
+        # collective): every rank solves its share through its own server
+        eng.close()
+        out["batched_sharded"] = batched_sharded(dist, local, world, rank, args)
 
     if rank == 0 and world == 1 and not args.no_cpu:
         info = cpu_sample(mol, ints, budget_s=args.cpu_budget)

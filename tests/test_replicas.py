@@ -1,7 +1,10 @@
 """Replica path of bench.py --gpus N on CPU: two gloo ranks on 127.0.0.1.
 
 Each rank reports a different timed region; both must see the maximum, and the
-whole-job rate must count the units of every rank against that maximum.
+whole-job rate must count the units of every rank against that maximum.  The
+split of independent molecules over ranks (shard_by_cost) covers every
+molecule exactly once, is the same on every rank, and keeps the loads within
+one molecule's cost of each other.
 """
 import os
 import socket
@@ -55,3 +58,60 @@ def test_single_process_without_a_group():
     assert replicas.max_over_ranks(None, 3.5) == 3.5
     replicas.barrier(None)
     assert replicas.whole_job_rate(5, 1, 0.5) == pytest.approx(10.0)
+
+
+def test_shard_by_cost_covers_all_and_balances():
+    import numpy as np
+    from stda_b200 import replicas
+    rng = np.random.default_rng(5)
+    costs = rng.integers(1, 1000, size=97).tolist()
+    for world in (1, 2, 3, 8):
+        parts = replicas.shard_by_cost(costs, world)
+        assert len(parts) == world
+        flat = sorted(i for p in parts for i in p)
+        assert flat == list(range(len(costs)))
+        loads = [sum(costs[i] for i in p) for p in parts]
+        assert max(loads) - min(loads) <= max(costs)
+        assert replicas.shard_by_cost(costs, world) == parts       # deterministic
+    assert replicas.shard_by_cost([], 4) == [[], [], [], []]
+    with pytest.raises(ValueError):
+        replicas.shard_by_cost([1.0], 0)
+
+
+def _shard_rank(rank, world, port, out):
+    import datetime
+    import torch
+    import torch.distributed as dist
+    from stda_b200 import replicas
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=60))
+    costs = [(7 * k) % 23 + 1 for k in range(40)]
+    mine = replicas.shard_by_cost(costs, world)[rank]
+    # every rank's share, gathered only to check the split here
+    got = [None] * world
+    dist.all_gather_object(got, mine)
+    done = torch.tensor([float(len(mine))])
+    dist.all_reduce(done)
+    dist.destroy_process_group()
+    out.put((rank, got, int(done.item())))
+
+
+def test_two_gloo_ranks_split_molecules():
+    import multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_shard_rank, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = sorted(q.get(timeout=120) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    shares = res[0][1]
+    assert res[1][1] == shares                       # the same split on both ranks
+    assert sorted(shares[0] + shares[1]) == list(range(40))
+    assert not set(shares[0]) & set(shares[1])
+    assert res[0][2] == res[1][2] == 40
