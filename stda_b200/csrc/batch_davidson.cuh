@@ -319,10 +319,10 @@ class BatchDavidson {
     cv_done_.wait(lk, [&] { return p.finished; });
   }
 
-  // problems solved, batched iterations run, and the sum over iterations of
-  // the members in flight (mean batch = members / iterations)
-  // and the wall time of the iterations (ms), total and up to their first
-  // host synchronisation (products, Rayleigh-Ritz, residuals)
+  // problems solved, batched iterations run, the sum over iterations of the
+  // members in flight (mean batch = members / iterations), and in ms[0..1]
+  // the wall time of the iterations, total and up to their first host
+  // synchronisation (products, Rayleigh-Ritz, residuals)
   void stats(int64_t *problems, int64_t *iterations, int64_t *members, double *ms) {
     std::lock_guard<std::mutex> lk(mu_);
     *problems = n_problems_;
@@ -418,15 +418,28 @@ inline void BatchDavidson::admit(BatchProblem &p) {
 
 // results of a problem that leaves the batch (final_resid / final_theta set
 // from its last residual step): the wanted Ritz pairs to the caller's arrays
-// (on the batch's stream, then `done`)
+// (on the batch's stream, then `done`).  Never throws: a failed copy becomes
+// the problem's status.  The caller has already taken p out of the active set
+// (once finished, its owner may return and p no longer exists).
 inline void BatchDavidson::finish(BatchProblem &p) {
   DavidsonWork &dw = *p.dw;
-  p.max_resid = *std::max_element(p.final_resid.begin(), p.final_resid.begin() + p.kwant);
-  S2G_CUDA(cudaMemcpyAsync(p.omega_out, dw.theta.get(), sizeof(double) * p.kwant,
-                           cudaMemcpyDeviceToDevice, cs_));
-  S2G_CUDA(cudaMemcpyAsync(p.X_out, dw.X.get(), sizeof(double) * p.n * p.kwant,
-                           cudaMemcpyDeviceToDevice, cs_));
-  S2G_CUDA(cudaEventRecord(p.done, cs_));
+  if (!p.final_resid.empty())
+    p.max_resid = *std::max_element(p.final_resid.begin(),
+                                    p.final_resid.begin() + std::min<size_t>(p.kwant,
+                                                                             p.final_resid.size()));
+  try {
+    S2G_CUDA(cudaMemcpyAsync(p.omega_out, dw.theta.get(), sizeof(double) * p.kwant,
+                             cudaMemcpyDeviceToDevice, cs_));
+    S2G_CUDA(cudaMemcpyAsync(p.X_out, dw.X.get(), sizeof(double) * p.n * p.kwant,
+                             cudaMemcpyDeviceToDevice, cs_));
+    S2G_CUDA(cudaEventRecord(p.done, cs_));
+  } catch (const Error &e) {
+    if (p.status == STD2G_OK) {
+      p.status = e.code;
+      p.msg = e.msg;
+    }
+    cudaEventRecord(p.done, cs_);
+  }
   {
     std::lock_guard<std::mutex> lk(mu_);
     p.finished = true;
@@ -576,8 +589,7 @@ inline void BatchDavidson::iterate(std::vector<BatchProblem *> &act) {
   }
   // ---- convergence (davidson()'s test); members that stay get their
   // unconverged columns
-  std::vector<BatchProblem *> stay;
-  std::vector<int> offs;
+  std::vector<BatchProblem *> stay, leaving;
   {
     int off = 0;
     for (int b = 0; b < P; ++b) {
@@ -589,7 +601,7 @@ inline void BatchDavidson::iterate(std::vector<BatchProblem *> &act) {
       if (h_info[b] != 0) {
         p->status = STD2G_ENOCONV;
         p->msg = "Davidson: Rayleigh-Ritz eigensolve failed (" + std::to_string(h_info[b]) + ")";
-        finish(*p);
+        leaving.push_back(p);
         continue;
       }
       p->unc.clear();
@@ -601,7 +613,7 @@ inline void BatchDavidson::iterate(std::vector<BatchProblem *> &act) {
         }
       p->nconv = p->kwant - nunc_wanted;
       if (nunc_wanted == 0 || p->iters >= p->max_iter) {
-        finish(*p);
+        leaving.push_back(p);
         continue;
       }
       p->nc = (int)p->unc.size();
@@ -610,6 +622,7 @@ inline void BatchDavidson::iterate(std::vector<BatchProblem *> &act) {
     }
   }
   act.swap(stay);
+  for (BatchProblem *p : leaving) finish(*p);
   if (act.empty()) return;
   const int Q = (int)act.size();
   // ---- preconditioned corrections T; restarts to the Ritz vectors
@@ -744,16 +757,13 @@ inline void BatchDavidson::iterate(std::vector<BatchProblem *> &act) {
     }
   }
   // ---- next block sizes; members without new directions leave
-  std::vector<BatchProblem *> next;
+  std::vector<BatchProblem *> next, done;
   for (BatchProblem *p : act) {
     p->nb = p->ncur;
-    if (p->nb == 0) {
-      finish(*p);
-      continue;
-    }
-    next.push_back(p);
+    (p->nb == 0 ? done : next).push_back(p);
   }
   act.swap(next);
+  for (BatchProblem *p : done) finish(*p);
 }
 
 }  // namespace std2g
