@@ -479,21 +479,25 @@ def served_and_batched(device, args):
     return out
 
 
-def batched_sharded(dist, local, world, rank, args):
+def batched_sharded(dist, local, world, rank, args, dev="cuda", runner=None):
     """The batch configuration on `world` GPUs: the requests split by
     shard_by_cost (cost ~ nao^2 of the molecule) over the ranks, each rank
     solving its share through its own request server (mixed form, batched
-    eigensolve); whole-job solves/s = all requests / the slowest rank's time."""
+    eigensolve); whole-job solves/s = all requests / the slowest rank's time.
+    `dev` is the device of the collectives' tensors ("cuda": this rank's GPU,
+    None: the host, as the gloo tests run it); `runner` stands in for
+    run_server."""
     from stda_b200 import replicas
     from stda_b200.engine import Keywords
-    dev = f"cuda:{local}"
+    if dev == "cuda":
+        dev = f"cuda:{local}"
+    runner = runner or run_server
     atoms, pool = molecule_pool("batch", args.batch_pool, seed=3)
     kw = Keywords(ax=0.5, e_thr_ev=6.5, nroots=20, conv_tol=1e-7)
     reqs = [(k % len(pool), kw, None) for k in range(args.batch_requests)]
     mine = replicas.shard_by_cost([float(pool[i].nao) ** 2 for i, _, _ in reqs], world)[rank]
     replicas.barrier(dist, dev)
-    _, st = run_server(1, pool, [reqs[q] for q in mine], None, args.batch_slots, local,
-                       batch=True)
+    _, st = runner(1, pool, [reqs[q] for q in mine], None, args.batch_slots, local, batch=True)
     span = replicas.max_over_ranks(dist, st["makespan_s"], dev)
     return {"workload": f"{len(reqs)} molecules of the batch configuration split over "
                         f"{world} GPUs by nao^2 (longest-processing-time bin-pack)",

@@ -115,3 +115,47 @@ def test_two_gloo_ranks_split_molecules():
     assert sorted(shares[0] + shares[1]) == list(range(40))
     assert not set(shares[0]) & set(shares[1])
     assert res[0][2] == res[1][2] == 40
+
+
+def _bench_rank(rank, world, port, out):
+    import datetime
+    import types
+    import torch.distributed as dist
+    import bench
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=120))
+    seen = []
+
+    def fake_server(precision, pool, reqs, arrivals, slots, device, batch=False):
+        # stands in for the request server: rank r "takes" 1 + r seconds
+        seen.extend(i for i, _, _ in reqs)
+        return [], {"makespan_s": 1.0 + rank}
+
+    args = types.SimpleNamespace(batch_pool=3, batch_requests=9, batch_slots=2)
+    res = bench.batched_sharded(dist, 0, world, rank, args, dev=None, runner=fake_server)
+    dist.destroy_process_group()
+    out.put((rank, res, seen))
+
+
+def test_bench_batched_sharded_on_two_gloo_ranks():
+    """bench.py's --gpus N batch path with the server replaced by a fake:
+    each rank takes its own share, and the whole-job rate counts every
+    request against the slowest rank's time."""
+    import multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_bench_rank, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = sorted(q.get(timeout=300) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    (r0, out0, seen0), (r1, out1, seen1) = res
+    assert out0["requests_this_rank"] + out1["requests_this_rank"] == 9
+    assert out0["slowest_rank_s"] == out1["slowest_rank_s"] == 2.0
+    assert out0["solves_per_s"] == pytest.approx(9 / 2.0)
+    assert sorted(seen0 + seen1) == sorted(k % 3 for k in range(9))
