@@ -23,6 +23,8 @@
 // cuSOLVER's syevd takes 1-3 ms at n = 75-300, most of it launch and host
 // synchronisation latency.
 // Eigenvalues ascending in w[0..k), eigenvectors in the columns of Z (ld ldz).
+// The *_b kernels run the same four phases for many problems per launch
+// (blockIdx.y selects the problem; symeig_small_batched).
 #pragma once
 
 #include <cooperative_groups.h>
